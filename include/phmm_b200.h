@@ -1,0 +1,182 @@
+/*
+ * phmm_b200 — B200-native PairHMM likelihood engine, C ABI.
+ *
+ * This is the drop-in boundary for the reference's PairHMM entry point
+ *   DoubleVector2D (*rovaca::call_pairhmm)(const HaplotypeVector& hs, ReadVector& rs,
+ *       int32_t min_quality_threshold, PcrIndelModel pcr_option, pMemoryPool pool)
+ *   (src/haplotypecaller/pairhmm/pairhmm_engine.h:14, bound in pairhmm_engine.cpp:19-37,
+ *    implemented by call_roDV_pairhmm_scheduled in pairhmm_internal.cpp:576-623)
+ * and for the vector API the reference's tests drive
+ *   bool pairhmm::schedule::schedule_pairhmm(haplotypes, reads, result, quality, ins, del, gcp, ...)
+ *   (src/haplotypecaller/pairhmm/roDV_schedule.h:16-27, roDV_schedule.cpp:154-361).
+ *
+ * Plain C types only: host pointers and sizes in, host pointers out.  Every call returns a
+ * phmm_status; none throws, none aborts the process.  All sequence data is 1 byte per base
+ * (ASCII A/C/G/T/N) and all qualities are raw Phred values (not +33), exactly as the reference's
+ * TestCase carries them (roDV_common/common.h:27-36).
+ *
+ * Likelihood layout: for every region, a block of n_haps * n_reads doubles in [hap][read] order,
+ * the layout call_pairhmm returns (pairhmm_internal.cpp:499-508,613); blocks follow region order.
+ */
+#ifndef PHMM_B200_H
+#define PHMM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define PHMM_API __attribute__((visibility("default")))
+#else
+#define PHMM_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum phmm_status {
+    PHMM_OK = 0,
+    PHMM_ERR_INVALID_ARGUMENT = 1, /* null pointer, inconsistent sizes, bad enum */
+    PHMM_ERR_LIMIT_EXCEEDED = 2,   /* region beyond the reference's limits (roDV_schedule.cpp:70-73):
+                                      more than 4096 haplotypes, a read longer than 768 or a
+                                      haplotype longer than 1536 */
+    PHMM_ERR_OUT_OF_MEMORY = 3,    /* device or pinned-host allocation failed */
+    PHMM_ERR_CUDA = 4,             /* a CUDA runtime call failed; see phmm_last_error() */
+    PHMM_ERR_NOT_INITIALIZED = 5,  /* engine handle is null or was destroyed */
+    PHMM_ERR_TIMEOUT = 6,          /* phmm_wait deadline passed (the request keeps running) */
+    PHMM_ERR_CANCELLED = 7,        /* request was cancelled before it was admitted */
+    PHMM_ERR_QUEUE_FULL = 8,       /* serving queue at capacity */
+    PHMM_ERR_DEVICE_STATUS = 9,    /* a kernel reported an error status word */
+    PHMM_ERR_NO_DEVICE = 10,       /* no CUDA device, or the requested ordinal does not exist */
+    PHMM_ERR_INTERNAL = 11
+} phmm_status;
+
+/* PCR indel error model, same enumerators and meaning as the reference's PcrIndelModel
+ * (src/haplotypecaller/common/enum.h:8) and its caps (pairhmm/adapter.h:13-15). */
+typedef enum phmm_pcr_model {
+    PHMM_PCR_NONE = 0,
+    PHMM_PCR_HOSTILE = 1,
+    PHMM_PCR_AGGRESSIVE = 2,
+    PHMM_PCR_CONSERVATIVE = 3
+} phmm_pcr_model;
+
+typedef struct phmm_engine phmm_engine;
+
+typedef struct phmm_config {
+    int32_t device;            /* CUDA device ordinal */
+    int32_t use_cuda_graph;    /* 1: replay the device-side batch pipeline from a captured CUDA graph */
+    int32_t autotune;          /* 1: pick launch shapes by timing candidates on first use */
+    int32_t reserved0;
+    uint64_t hbm_budget_bytes; /* serving-loop admission budget for resident region data; 0 = 40 GiB */
+    uint64_t reserved1;
+} phmm_config;
+
+/* A batch of independent active regions in flat, concatenated arrays (host memory). */
+typedef struct phmm_batch {
+    uint32_t n_regions;
+    const uint32_t* n_haps;    /* [n_regions] haplotypes per region */
+    const uint32_t* n_reads;   /* [n_regions] reads per region */
+    const uint8_t* hap_bases;  /* all haplotypes, region-major */
+    const uint64_t* hap_off;   /* [sum(n_haps) + 1] offsets into hap_bases */
+    const uint8_t* read_bases; /* all reads, region-major */
+    const uint8_t* read_qual;  /* base quality per read base */
+    const uint8_t* read_ins;   /* insertion gap-open quality per read base */
+    const uint8_t* read_del;   /* deletion gap-open quality per read base */
+    const uint8_t* read_gcp;   /* gap-continuation quality per read base */
+    const uint64_t* read_off;  /* [sum(n_reads) + 1] offsets into the five read arrays */
+} phmm_batch;
+
+typedef struct phmm_stats {
+    uint64_t regions;
+    uint64_t pairs;         /* read x haplotype pairs computed */
+    uint64_t cells;         /* sum over pairs of read_len * hap_len */
+    uint64_t pairs_f64;     /* pairs recomputed in FP64 because the FP32 sum fell below 1e-28 */
+    uint64_t work_items;    /* wavefront work items of the FP32 pass */
+    uint64_t h2d_bytes;
+    uint64_t d2h_bytes;
+    double device_ms;       /* CUDA-event time of the device pipeline (prep + FP32 + FP64) */
+    double fp32_ms;         /* CUDA-event time of the FP32 wavefront kernel alone */
+    double fp64_ms;         /* CUDA-event time of the FP64 recompute kernel alone */
+    double host_ms;         /* wall time of the whole call */
+} phmm_stats;
+
+/* ---- engine lifetime ------------------------------------------------------------------- */
+
+/* cfg may be NULL (device 0, graphs on, autotune on, 40 GiB budget). */
+PHMM_API phmm_status phmm_engine_create(const phmm_config* cfg, phmm_engine** out_engine);
+PHMM_API phmm_status phmm_engine_destroy(phmm_engine* engine);
+PHMM_API const char* phmm_status_string(phmm_status status);
+/* Detail of the last error raised on the calling thread ("" if none). */
+PHMM_API const char* phmm_last_error(void);
+/* Library build string (kernel variants, target architecture). */
+PHMM_API const char* phmm_version(void);
+
+/* ---- synchronous batch ------------------------------------------------------------------ */
+
+/* Computes every read x haplotype log10 likelihood of every region in the batch.
+ *   out        : sum(n_haps[r] * n_reads[r]) doubles; region blocks in order, [hap][read] inside.
+ *   pair_flags : optional (may be NULL), same shape; bit 0 set when the pair was recomputed in
+ *                FP64 (FP32 sum below 1e-28, roDV_schedule.cpp:35,704).
+ *   stats      : optional.
+ * Reads are used exactly as given (no quality capping): the semantics of schedule_pairhmm.
+ * A pair with an empty read or haplotype gets NaN, as the region API leaves such pairs. */
+PHMM_API phmm_status phmm_compute_regions(phmm_engine* engine, const phmm_batch* batch, double* out, uint8_t* pair_flags,
+                                 phmm_stats* stats);
+
+/* One region through the full call_pairhmm path (call_roDV_pairhmm_scheduled,
+ * pairhmm_internal.cpp:576-623 and the region-API read preparation of roDV_schedule.cpp:522-649):
+ *   1. base quality q -> min(q, mapq); below min_quality_threshold -> 6;
+ *   2. insertion/deletion gap-open 45 and gap continuation 10 for every base;
+ *   3. with a PCR model other than NONE, gap-open capped by tandem-repeat length (deletion uses
+ *      the same capped values as insertion);
+ *   4. likelihoods, each read's row capped at best - 4.5;
+ *   5. reads whose best likelihood is below -4 * min(2, ceil(0.02 * len)) are dropped.
+ * out    : [n_haps][n_reads] doubles; column k holds the k-th kept read, trailing columns NaN.
+ * keep   : [n_reads] bytes, 1 where the read was kept (the caller erases the others, in order).
+ * n_kept : number of kept reads. */
+PHMM_API phmm_status phmm_call_region(phmm_engine* engine, uint32_t n_haps, const uint8_t* hap_bases, const uint64_t* hap_off,
+                             uint32_t n_reads, const uint8_t* read_bases, const uint8_t* read_qual,
+                             const uint64_t* read_off, const uint8_t* mapq, int32_t min_quality_threshold,
+                             int32_t pcr_model, double* out, uint8_t* keep, uint32_t* n_kept);
+
+/* ---- host-only pieces of the region path (no GPU involved) ----------------------------- */
+
+/* Base qualities as the region API prepares them: min(q, mapq), below the threshold -> 6
+ * (roDV_schedule.cpp:540-565). */
+PHMM_API void phmm_host_prepare_quals(const uint8_t* q, uint32_t n, uint8_t mapq, int32_t min_quality_threshold, uint8_t* out);
+/* PCR indel model: caps gap_open[i] (i < n-1) by the tandem-repeat length at i
+ * (apply_pcr_error_model_rolling, pairhmm_internal.cpp:431-476). */
+PHMM_API void phmm_host_pcr_model(const uint8_t* bases, uint32_t n, uint8_t* gap_open, int32_t pcr_model);
+/* Tandem-repeat length at offset (find_tandem_repeat_units_rolling, pairhmm_internal.cpp:317-389). */
+PHMM_API int32_t phmm_host_tandem_repeat_length(const uint8_t* bases, uint32_t n, uint32_t offset);
+/* Post-processing of call_pairhmm on a [hap][read] likelihood matrix: cap each read at best - 4.5,
+ * drop poorly modelled reads, compact kept reads into the first columns (NaN after them). */
+PHMM_API void phmm_host_normalize_filter(const double* lk_hap_read, uint32_t n_haps, uint32_t n_reads, const uint64_t* read_len,
+                                double* out, uint8_t* keep, uint32_t* n_kept);
+
+/* ---- serving loop ----------------------------------------------------------------------- */
+
+typedef uint64_t phmm_ticket;
+
+/* Submits one region (a phmm_batch with n_regions == 1).  Inputs are copied before the call
+ * returns; out / pair_flags (same shape as for phmm_compute_regions) must stay valid until the
+ * request completes.  Requests are admitted as device slots and the HBM budget free up, and
+ * batched with whatever else is in flight.  Thread-safe. */
+PHMM_API phmm_status phmm_submit(phmm_engine* engine, const phmm_batch* region, double* out, uint8_t* pair_flags,
+                        phmm_ticket* ticket);
+/* *done = 1 once the request's results are in out (or it failed / was cancelled). */
+PHMM_API phmm_status phmm_poll(phmm_engine* engine, phmm_ticket ticket, int32_t* done);
+/* Blocks up to timeout_us (negative = forever).  Once the request is done it returns the request's
+ * own status, reports its timing (optional, may be NULL: time queued before admission and time from
+ * submit to completion, in microseconds) and releases the ticket.  On PHMM_ERR_TIMEOUT the ticket
+ * stays valid. */
+PHMM_API phmm_status phmm_wait(phmm_engine* engine, phmm_ticket ticket, int64_t timeout_us, double* queued_us,
+                      double* total_us);
+/* Cancels a request that has not been admitted to the device yet. */
+PHMM_API phmm_status phmm_cancel(phmm_engine* engine, phmm_ticket ticket);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PHMM_B200_H */

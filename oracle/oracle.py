@@ -1,0 +1,224 @@
+"""Python access to the PairHMM oracle (test infrastructure only).
+
+* ``Oracle`` -- the C restatement in oracle/phmm_oracle.c (built into oracle/_build/).
+* ``Ref``    -- the reference's own kernels and vector-API scheduler, compiled from the reference
+  sources by oracle/build_ref.sh into oracle/_ref/ (present wherever that recipe has run).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this module, as the checker;
+the engine in rovaca_b200/ never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ORACLE_SRC = HERE / "phmm_oracle.c"
+ORACLE_SCHED_SRC = HERE / "phmm_oracle_sched.cpp"
+ORACLE_LIB = HERE / "_build" / "libphmm_oracle.so"
+REF_LIB = HERE / "_ref" / "libphmm_ref.so"
+
+INTER, INTRA = 0, 1
+UNFUSED, FUSED = 0, 1
+
+
+def build_oracle(force: bool = False) -> Path:
+    """Compiles oracle/_build/libphmm_oracle.so (no FMA contraction beyond the explicit fma calls)."""
+    ORACLE_LIB.parent.mkdir(exist_ok=True)
+    srcs = (ORACLE_SRC, ORACLE_SCHED_SRC)
+    if force or not ORACLE_LIB.exists() or any(ORACLE_LIB.stat().st_mtime < s.stat().st_mtime for s in srcs):
+        flags = ["-O2", "-ffp-contract=off", "-fno-fast-math", "-fPIC", "-Wall"]
+        tmp = ORACLE_LIB.parent
+        subprocess.run(["gcc", *flags, "-c", str(ORACLE_SRC), "-o", str(tmp / "phmm_oracle.o")], check=True)
+        subprocess.run(["g++", *flags, "-std=c++17", "-c", str(ORACLE_SCHED_SRC), "-o", str(tmp / "phmm_oracle_sched.o")],
+                       check=True)
+        subprocess.run(["g++", "-shared", "-o", str(ORACLE_LIB), str(tmp / "phmm_oracle.o"),
+                        str(tmp / "phmm_oracle_sched.o"), "-lm"], check=True)
+    return ORACLE_LIB
+
+
+def build_ref(reference_root: str = "/root/reference") -> Path | None:
+    """Builds oracle/_ref from the reference sources when they are present; returns the library."""
+    if not Path(reference_root, "src/haplotypecaller/pairhmm").is_dir():
+        return REF_LIB if REF_LIB.exists() else None
+    srcs = [HERE / "ref_shim.cpp", HERE / "ref_kernels.cpp", HERE / "ref_unreached.cpp", HERE / "build_ref.sh"]
+    if REF_LIB.exists() and all(REF_LIB.stat().st_mtime >= s.stat().st_mtime for s in srcs):
+        return REF_LIB
+    subprocess.run(["bash", str(HERE / "build_ref.sh"), reference_root], check=True)
+    return REF_LIB
+
+
+def _b(x) -> bytes:
+    if isinstance(x, (bytes, bytearray)):
+        return bytes(x)
+    if isinstance(x, str):
+        return x.encode()
+    return np.ascontiguousarray(np.asarray(x, np.uint8)).tobytes()
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class Oracle:
+    def __init__(self):
+        lib = C.CDLL(str(build_oracle()))
+        cp, u32, i32, D, F = C.c_char_p, C.c_uint32, C.c_int, C.c_double, C.c_float
+        pair = [cp, u32, cp, u32, cp, cp, cp, cp]
+        for name, res, extra in [("oracle_raw_f32", F, [i32, i32]), ("oracle_raw_f64", D, [i32, i32]),
+                                 ("oracle_log10_f64", D, []),
+                                 ("oracle_log10_switch", D, [i32, i32, C.POINTER(C.c_int)])]:
+            f = getattr(lib, name)
+            f.restype = res
+            f.argtypes = pair + extra
+        lib.oracle_log10_from_f32.restype = D
+        lib.oracle_log10_from_f32.argtypes = [F]
+        for name, res in [("oracle_ph2pr_f32", F), ("oracle_ph2pr_f64", D)]:
+            getattr(lib, name).restype = res
+            getattr(lib, name).argtypes = [i32]
+        for name, res in [("oracle_mm_f32", F), ("oracle_mm_f64", D)]:
+            getattr(lib, name).restype = res
+            getattr(lib, name).argtypes = [i32, i32]
+        P = C.c_void_p
+        lib.oracle_batch.restype = C.c_uint64
+        lib.oracle_batch.argtypes = [u32, P, P, P, P, P, P, P, P, P, P, i32, i32, P, P]
+        lib.oracle_schedule.restype = i32
+        lib.oracle_schedule.argtypes = [u32, P, P, u32, P, P, P, P, P, P, D, D, u32, u32, P, P]
+        self.lib = lib
+
+    @staticmethod
+    def _args(hap, read, q, i, d, c):
+        hap, read = _b(hap), _b(read)
+        return [hap, len(hap), read, len(read), _b(q), _b(i), _b(d), _b(c)]
+
+    def raw_f32(self, hap, read, q, i, d, c, kernel=INTER, fused=FUSED) -> float:
+        return self.lib.oracle_raw_f32(*self._args(hap, read, q, i, d, c), kernel, fused)
+
+    def raw_f64(self, hap, read, q, i, d, c, kernel=INTER, fused=FUSED) -> float:
+        return self.lib.oracle_raw_f64(*self._args(hap, read, q, i, d, c), kernel, fused)
+
+    def log10_f64(self, hap, read, q, i, d, c) -> float:
+        """All-FP64 oracle (plain multiply/add, inter prior)."""
+        return self.lib.oracle_log10_f64(*self._args(hap, read, q, i, d, c))
+
+    def pair(self, hap, read, q, i, d, c, kernel=None, fused=FUSED) -> tuple[float, bool]:
+        """Reference semantics for one pair: FP32, FP64 below 1e-28; N pairs on the intra variant."""
+        if kernel is None:
+            kernel = INTRA if (b"N" in _b(hap) or b"N" in _b(read)) else INTER
+        u = C.c_int()
+        v = self.lib.oracle_log10_switch(*self._args(hap, read, q, i, d, c), kernel, fused, C.byref(u))
+        return v, bool(u.value)
+
+    def batch(self, pb, fused=FUSED, fp64_only=False):
+        """A PackedBatch with reference semantics: (likelihoods, used_f64) in the engine's layout."""
+        n = pb.out_size
+        out = np.empty(n, np.float64)
+        used = np.empty(n, np.uint8)
+        self.lib.oracle_batch(pb.n_regions, _p(pb.n_haps), _p(pb.n_reads), _p(pb.hap_bases), _p(pb.hap_off),
+                              _p(pb.read_bases), _p(pb.read_qual), _p(pb.read_ins), _p(pb.read_del), _p(pb.read_gcp),
+                              _p(pb.read_off), fused, int(fp64_only), _p(out), _p(used))
+        return out, used.astype(bool)
+
+
+    # routes of oracle_schedule: which reference kernel and precision produced a pair
+    ROUTE_F64 = (1, 3, 4)
+
+    def schedule_region(self, pb, g: int, idle_f: float = 0.02, idle_d: float = 0.02, width_f: int = 16,
+                        width_d: int = 8):
+        """Region g through the restated vector-API scheduler (AVX-512 widths by default).
+
+        Returns (log10 [hap][read], route [hap][read]); route codes are listed in
+        oracle/phmm_oracle_sched.cpp, and route in ROUTE_F64 means the pair ended in FP64."""
+        h0, r0 = int(pb.n_haps[:g].sum()), int(pb.n_reads[:g].sum())
+        m, n = int(pb.n_haps[g]), int(pb.n_reads[g])
+        hoff = np.ascontiguousarray(pb.hap_off[h0:h0 + m + 1])
+        roff = np.ascontiguousarray(pb.read_off[r0:r0 + n + 1])
+        out = np.empty(m * n, np.float64)
+        route = np.empty(m * n, np.uint8)
+        rc = self.lib.oracle_schedule(m, _p(pb.hap_bases), _p(hoff), n, _p(pb.read_bases), _p(pb.read_qual),
+                                      _p(pb.read_ins), _p(pb.read_del), _p(pb.read_gcp), _p(roff), idle_f, idle_d,
+                                      width_f, width_d, _p(out), _p(route))
+        if rc != 0:
+            raise ValueError("oracle_schedule: empty region")
+        return out.reshape(m, n), route.reshape(m, n)
+
+
+class Ref:
+    """The reference's own PairHMM (oracle/_ref/libphmm_ref.so)."""
+
+    def __init__(self, path: Path | str | None = None):
+        p = Path(path) if path else REF_LIB
+        if not p.exists():
+            raise FileNotFoundError(f"{p} not built (oracle/build_ref.sh needs the reference sources)")
+        lib = C.CDLL(str(p))
+        cp, u32, i32, D, F, P = C.c_char_p, C.c_uint32, C.c_int, C.c_double, C.c_float, C.c_void_p
+        pair = [cp, u32, cp, u32, cp, cp, cp, cp]
+        lib.ref_init.restype = None
+        lib.ref_isa_bits.restype = i32
+        lib.ref_inter_width_f32.restype = i32
+        lib.ref_inter_width_f64.restype = i32
+        lib.ref_intra_raw_f32.restype = F
+        lib.ref_intra_raw_f32.argtypes = pair
+        lib.ref_intra_raw_f64.restype = D
+        lib.ref_intra_raw_f64.argtypes = pair
+        lib.ref_intra_log10.restype = D
+        lib.ref_intra_log10.argtypes = pair + [i32]
+        lib.ref_inter.restype = i32
+        lib.ref_inter.argtypes = [i32, u32, P, P, P, P, P, P, P, P, i32, P]
+        lib.ref_schedule.restype = i32
+        lib.ref_schedule.argtypes = [u32, P, P, u32, P, P, P, P, P, P, D, D, P]
+        lib.ref_init()
+        self.lib = lib
+        self.isa = lib.ref_isa_bits()
+        self.width_f32 = lib.ref_inter_width_f32()
+        self.width_f64 = lib.ref_inter_width_f64()
+
+    def init_thread(self) -> None:
+        """Flush-to-zero on the calling thread, as the reference sets it (pairhmm_engine.cpp:36)."""
+        self.lib.ref_init()
+
+    def intra_raw_f32(self, hap, read, q, i, d, c) -> float:
+        return self.lib.ref_intra_raw_f32(*Oracle._args(hap, read, q, i, d, c))
+
+    def intra_raw_f64(self, hap, read, q, i, d, c) -> float:
+        return self.lib.ref_intra_raw_f64(*Oracle._args(hap, read, q, i, d, c))
+
+    def intra_log10(self, hap, read, q, i, d, c, use_double=False) -> float:
+        return self.lib.ref_intra_log10(*Oracle._args(hap, read, q, i, d, c), int(use_double))
+
+    def inter(self, pairs, dbl=False, raw=True) -> np.ndarray:
+        """pairs: exactly width_f32 (or width_f64) tuples (hap, read, q, i, d, c)."""
+        n = len(pairs)
+        cols = [[_b(p[k]) for p in pairs] for k in range(6)]
+        arrs = [(C.c_char_p * n)(*col) for col in cols]
+        hl = (C.c_uint32 * n)(*[len(x) for x in cols[0]])
+        rl = (C.c_uint32 * n)(*[len(x) for x in cols[1]])
+        out = (C.c_double * n)()
+        rc = self.lib.ref_inter(int(dbl), n, arrs[0], hl, arrs[1], rl, arrs[2], arrs[3], arrs[4], arrs[5], int(raw), out)
+        if rc != 0:
+            raise ValueError(f"ref_inter returned {rc} (needs exactly the SIMD width of pairs)")
+        return np.array(out[:], np.float64)
+
+    def schedule_region(self, pb, g: int, idle_f: float = 0.02, idle_d: float = 0.02) -> np.ndarray:
+        """Region g of a PackedBatch through schedule_pairhmm; returns [hap][read] (engine layout)."""
+        h0, r0 = int(pb.n_haps[:g].sum()), int(pb.n_reads[:g].sum())
+        m, n = int(pb.n_haps[g]), int(pb.n_reads[g])
+        hoff = np.ascontiguousarray(pb.hap_off[h0:h0 + m + 1])
+        roff = np.ascontiguousarray(pb.read_off[r0:r0 + n + 1])
+        out = np.empty(n * m, np.float64)
+        rc = self.lib.ref_schedule(m, _p(pb.hap_bases), _p(hoff), n, _p(pb.read_bases), _p(pb.read_qual),
+                                   _p(pb.read_ins), _p(pb.read_del), _p(pb.read_gcp), _p(roff), idle_f, idle_d, _p(out))
+        if rc != 0:
+            raise RuntimeError(f"ref_schedule failed ({rc})")
+        return out.reshape(n, m).T.copy()
+
+
+def ref_available() -> bool:
+    return REF_LIB.exists()
+
+
+__all__ = ["Oracle", "Ref", "build_oracle", "build_ref", "ref_available", "INTER", "INTRA", "FUSED", "UNFUSED"]

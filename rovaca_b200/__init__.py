@@ -1,0 +1,8 @@
+"""B200-native PairHMM likelihood engine (drop-in for the HaplotypeCaller PairHMM path).
+
+The engine is libphmm_b200.so (C ABI in include/phmm_b200.h); this package is its Python host
+interface, the seeded workload generators and the in-tree build.
+"""
+from .pairhmm import Engine, PackedBatch, PhmmError, Region, call_pairhmm, default_engine, schedule_pairhmm
+
+__all__ = ["Engine", "PackedBatch", "PhmmError", "Region", "call_pairhmm", "default_engine", "schedule_pairhmm"]

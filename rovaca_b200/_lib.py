@@ -1,0 +1,100 @@
+"""ctypes binding of include/phmm_b200.h (the engine's C ABI).
+
+The library is built in-tree (``python -m rovaca_b200.build``).  There is no fallback: if the
+library or a CUDA device is missing, calls raise instead of computing anything on the CPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import re
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "libphmm_b200.so"
+HEADER_PATH = Path(__file__).resolve().parent.parent / "include" / "phmm_b200.h"
+
+PHMM_OK = 0
+STATUS_NAMES = {
+    0: "PHMM_OK", 1: "PHMM_ERR_INVALID_ARGUMENT", 2: "PHMM_ERR_LIMIT_EXCEEDED", 3: "PHMM_ERR_OUT_OF_MEMORY",
+    4: "PHMM_ERR_CUDA", 5: "PHMM_ERR_NOT_INITIALIZED", 6: "PHMM_ERR_TIMEOUT", 7: "PHMM_ERR_CANCELLED",
+    8: "PHMM_ERR_QUEUE_FULL", 9: "PHMM_ERR_DEVICE_STATUS", 10: "PHMM_ERR_NO_DEVICE", 11: "PHMM_ERR_INTERNAL",
+}
+PCR_MODELS = {"NONE": 0, "HOSTILE": 1, "AGGRESSIVE": 2, "CONSERVATIVE": 3}
+
+
+class PhmmError(RuntimeError):
+    """A non-OK phmm_status, with the library's detail message."""
+
+    def __init__(self, status: int, detail: str):
+        self.status = status
+        self.name = STATUS_NAMES.get(status, f"status {status}")
+        super().__init__(f"{self.name}: {detail}" if detail else self.name)
+
+
+class Config(C.Structure):
+    _fields_ = [("device", C.c_int32), ("use_cuda_graph", C.c_int32), ("autotune", C.c_int32),
+                ("reserved0", C.c_int32), ("hbm_budget_bytes", C.c_uint64), ("reserved1", C.c_uint64)]
+
+
+class Batch(C.Structure):
+    _fields_ = [("n_regions", C.c_uint32), ("n_haps", C.c_void_p), ("n_reads", C.c_void_p),
+                ("hap_bases", C.c_void_p), ("hap_off", C.c_void_p), ("read_bases", C.c_void_p),
+                ("read_qual", C.c_void_p), ("read_ins", C.c_void_p), ("read_del", C.c_void_p),
+                ("read_gcp", C.c_void_p), ("read_off", C.c_void_p)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("regions", C.c_uint64), ("pairs", C.c_uint64), ("cells", C.c_uint64), ("pairs_f64", C.c_uint64),
+                ("work_items", C.c_uint64), ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64),
+                ("device_ms", C.c_double), ("fp32_ms", C.c_double), ("fp64_ms", C.c_double), ("host_ms", C.c_double)]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    """Loads libphmm_b200.so (once) and declares every entry point's signature."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python -m rovaca_b200.build`")
+    lib = C.CDLL(str(LIB_PATH))
+    P, U32, U64, I32, I64, D = C.c_void_p, C.c_uint32, C.c_uint64, C.c_int32, C.c_int64, C.c_double
+    sig = {
+        "phmm_engine_create": (I32, [C.POINTER(Config), C.POINTER(P)]),
+        "phmm_engine_destroy": (I32, [P]),
+        "phmm_status_string": (C.c_char_p, [I32]),
+        "phmm_last_error": (C.c_char_p, []),
+        "phmm_version": (C.c_char_p, []),
+        "phmm_compute_regions": (I32, [P, C.POINTER(Batch), P, P, C.POINTER(Stats)]),
+        "phmm_call_region": (I32, [P, U32, P, P, U32, P, P, P, P, I32, I32, P, P, C.POINTER(U32)]),
+        "phmm_host_prepare_quals": (None, [P, U32, C.c_uint8, I32, P]),
+        "phmm_host_pcr_model": (None, [P, U32, P, I32]),
+        "phmm_host_tandem_repeat_length": (I32, [P, U32, U32]),
+        "phmm_host_normalize_filter": (None, [P, U32, U32, P, P, P, C.POINTER(U32)]),
+        "phmm_submit": (I32, [P, C.POINTER(Batch), P, P, C.POINTER(U64)]),
+        "phmm_poll": (I32, [P, U64, C.POINTER(I32)]),
+        "phmm_wait": (I32, [P, U64, I64, C.POINTER(D), C.POINTER(D)]),
+        "phmm_cancel": (I32, [P, U64]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(status: int) -> None:
+    if status != PHMM_OK:
+        detail = load().phmm_last_error().decode(errors="replace")
+        raise PhmmError(status, detail)
+
+
+def declared_symbols() -> list[str]:
+    """Every function include/phmm_b200.h declares."""
+    text = HEADER_PATH.read_text()
+    return sorted(set(re.findall(r"^PHMM_API\s+[\w\s\*]+?\b(phmm_\w+)\s*\(", text, flags=re.M)))

@@ -1,0 +1,276 @@
+// Device-side PairHMM forward wavefront for sm_100a.
+//
+// Reference arithmetic reproduced here (paths inside the reference project):
+//   per-row tables    src/haplotypecaller/pairhmm/roDV_inter/pairhmm_inter.cpp:59-101
+//                     src/haplotypecaller/pairhmm/roDV_intra/pairhmm_impl.cpp:88-112,149-156
+//   cell update       src/haplotypecaller/pairhmm/roDV_inter/pairhmm_inter.cpp:165-195 (inter)
+//                     src/haplotypecaller/pairhmm/roDV_intra/pairhmm_impl.cpp:235-280 (intra)
+//   boundary, sum     src/haplotypecaller/pairhmm/roDV_inter/pairhmm_inter.cpp:230-273
+//   N as wildcard     src/haplotypecaller/pairhmm/roDV_intra/pairhmm_impl.cpp:13-44
+//   FP32 -> FP64      src/haplotypecaller/pairhmm/roDV_schedule.cpp:35,269-279
+//
+// The reference's AVX-512 objects are built by GCC with FMA available, and GCC contracts the
+// cell update into this order (checked bit for bit against the reference build):
+//   inter  s = fma(Ddiag, gapm, fma(Mdiag, mm, Idiag*gapm))
+//   intra  s = fma(Ddiag, gapm, fma(Idiag, gapm, Mdiag*mm))
+//   both   M = s * prior,  I = fma(Iup, xx, Mup*mx),  D = fma(Dleft, yy, Mleft*my)
+// The kernels below issue exactly these operations with explicit round-to-nearest intrinsics
+// (never re-contracted), with flush-to-zero like the reference's MXCSR setting, so each pair's
+// raw FP32 (and FP64) sum is bit-identical to the reference kernel of the same variant.
+//
+// Mapping.  One warp owns one read (one "stripe" of 32*K padded rows: lane l holds rows
+// l*K .. l*K+K-1) and streams a run of the region's haplotypes through it as one concatenated
+// column stream.  At step t lane l works on stream column p = t - l; the three values of its
+// bottom row go to lane l+1 by warp shuffle, and lane 31's bottom row is the read's last row,
+// whose M and I are summed per haplotype.  Rows are padded at the top, and a pad row carries
+// coefficients (prior 0, mx = my = 0, xx = 1) that make it reproduce the boundary row exactly
+// (M = I = 0, D = C/H), so the read's last row is always lane 31's last slot.  Crossing from one
+// haplotype to the next only resets a lane's left-hand state, so the fill/drain of the wavefront
+// is paid once per work item instead of once per pair.  Reads longer than 32*8 rows run as
+// several stripes, the bottom row of one stripe feeding the next through a per-warp scratch row.
+#pragma once
+
+#include <cstdint>
+
+#include "phmm_types.h"
+
+namespace phmm {
+
+// Explicitly rounded arithmetic: these are never contracted or reassociated by the compiler.
+__device__ __forceinline__ float rmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float rfma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ float radd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double rmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double rfma(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ double radd(double a, double b) { return __dadd_rn(a, b); }
+
+// FP64 has no hardware flush-to-zero; the reference's MXCSR.FTZ flushes tiny double results, so
+// the FP64 path flushes explicitly.  Results below 2^-1022 only arise far below any likelihood
+// that survives the FP32 -> FP64 switch, so this only keeps the two paths identical.
+__device__ __forceinline__ float ftz(float x) { return x; }  // FP32: hardware FTZ (-ftz=true)
+__device__ __forceinline__ double ftz(double x) { return fabs(x) < 2.2250738585072014e-308 ? 0.0 * x : x; }
+
+template <typename T>
+struct Scale;
+template <>
+struct Scale<float> {
+    // 2^120, log10(2^120) as the float constant of adapter.h:25, threshold of roDV_schedule.cpp:35
+    __device__ static float initial() { return 1.329227995784916e36f; }
+    __device__ static double log10_initial() { return (double)36.1236000061f; }
+};
+template <>
+struct Scale<double> {
+    __device__ static double initial() { return 1.1235582092889474e307; }  // 2^1020
+    __device__ static double log10_initial() { return 307.050595577260822; }
+};
+
+template <typename T>
+__device__ __forceinline__ T shfl_up1(T v)
+{
+    return __shfl_up_sync(0xffffffffu, v, 1);
+}
+
+// One lane's rows of the current stripe.
+template <typename T, int K>
+struct LaneRows {
+    T Mp[K], Ip[K], Dp[K];        // values at the previous column
+    T pa[K], pb[K], mm[K], gm[K], mx[K], xx[K], my[K];
+    uint32_t rc[K];
+    uint32_t padmask;             // bit k: slot k is a pad row
+};
+
+template <typename T, int K, int V>
+__device__ __forceinline__ void load_rows(LaneRows<T, K>& L, const BatchView& b, const ProbTables<T>& tb,
+                                          uint64_t roff, int R, int first_padded_row, int pad, int lane)
+{
+    L.padmask = 0;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        const int i = first_padded_row + lane * K + k - pad;  // 0-based read position
+        if (i >= 0 && i < R) {
+            const uint64_t o = roff + (uint64_t)i;
+            const int q = b.read_q[o] & 127, iq = b.read_i[o] & 127, dq = b.read_d[o] & 127, c = b.read_c[o] & 127;
+            L.pa[k] = tb.pmat[q];
+            L.pb[k] = (V == kInter) ? tb.pmis_inter[q] : tb.pmis_intra[q];
+            L.mm[k] = tb.mm[iq * 128 + dq];
+            L.gm[k] = tb.gapm[c];
+            L.mx[k] = tb.ph2pr[iq];
+            L.xx[k] = tb.ph2pr[c];
+            L.my[k] = tb.ph2pr[dq];
+            L.rc[k] = match_code(b.read_bases[o], V);
+        } else {
+            L.pa[k] = T(0);
+            L.pb[k] = T(0);
+            L.mm[k] = T(0);
+            L.gm[k] = T(0);
+            L.mx[k] = T(0);
+            L.xx[k] = T(1);
+            L.my[k] = T(0);
+            L.rc[k] = 0u;
+            L.padmask |= 1u << k;
+        }
+    }
+}
+
+// Compute column p for all K rows of this lane.  (sM, sI, sD): the row above this lane's first
+// row at column p; (dM, dI, dD): the same row at column p-1.
+template <typename T, int K, int V>
+__device__ __forceinline__ void cells(LaneRows<T, K>& L, uint32_t hc, T sM, T sI, T dM, T dI, T dD)
+{
+    T diM = dM, diI = dI, diD = dD, upM = sM, upI = sI;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        const T oM = L.Mp[k], oI = L.Ip[k], oD = L.Dp[k];
+        const T prior = (hc & L.rc[k]) ? L.pa[k] : L.pb[k];
+        T s;
+        if (V == kInter)
+            s = ftz(rfma(diD, L.gm[k], ftz(rfma(diM, L.mm[k], ftz(rmul(diI, L.gm[k]))))));
+        else
+            s = ftz(rfma(diD, L.gm[k], ftz(rfma(diI, L.gm[k], ftz(rmul(diM, L.mm[k]))))));
+        const T nM = ftz(rmul(s, prior));
+        const T nI = ftz(rfma(upI, L.xx[k], ftz(rmul(upM, L.mx[k]))));
+        const T nD = ftz(rfma(oD, L.xx[k], ftz(rmul(oM, L.my[k]))));
+        L.Mp[k] = nM;
+        L.Ip[k] = nI;
+        L.Dp[k] = nD;
+        diM = oM;
+        diI = oI;
+        diD = oD;
+        upM = nM;
+        upI = nI;
+    }
+}
+
+struct SweepOut {
+    double* out;
+    uint8_t* pair_flags;
+    uint64_t out_base;            // output index of the stream's first haplotype
+    uint32_t out_stride;          // output index step between consecutive haplotypes
+    uint32_t read;                // global read index (for the rerun list)
+    bool fp32_pass;               // append underflowed pairs to the rerun list
+};
+
+// Sweep one stripe over the column stream of haplotypes [g_lo, g_hi) (global indices).
+//   FROM_SCR: the row above the stripe comes from scratch (stripe > 0), else the boundary row.
+//   TO_SCR:   the stripe's bottom row goes to scratch (not the last stripe), else it is summed.
+//   above_row0: the row above this lane's first slot is the boundary row 0 or a pad row.
+template <typename T, int K, int V, bool FROM_SCR, bool TO_SCR>
+__device__ void sweep(LaneRows<T, K>& L, const BatchView& b, const PassControl& pc, const SweepOut& so, uint32_t g_lo,
+                      uint32_t g_hi, T* scr, int lane, bool above_row0)
+{
+    const uint64_t s0 = b.hap_off[g_lo];
+    const int Tcols = (int)(b.hap_off[g_hi] - s0);
+    const uint32_t* codes = (V == kInter ? b.codes_inter : b.codes_intra) + kCodePad + s0;
+    const T C = Scale<T>::initial();
+
+    // Per-lane stream cursor: cur = haplotype being processed, nb = stream column of the next
+    // boundary (first column of the next haplotype, or the end of the stream).
+    uint32_t cur = g_lo;
+    int nb = 0;
+    bool started = false;
+    T D0 = T(0);
+    T sumM = T(0), sumI = T(0);
+    T dM = T(0), dI = T(0), dD = T(0);
+
+    const int steps = Tcols + kWarp;  // lane 31 reaches column Tcols (the end) at step Tcols + 31
+
+    // Run by a lane whose column p has reached nb, after the step's shuffles.
+    auto boundary = [&]() {
+        if (started) {
+            if (!TO_SCR && lane == kWarp - 1) {
+                const T tot = ftz(radd(sumM, sumI));
+                const uint64_t oi = so.out_base + (uint64_t)(cur - g_lo) * so.out_stride;
+                so.out[oi] = log10((double)tot) - Scale<T>::log10_initial();
+                if (so.fp32_pass) {
+                    const bool under = (double)tot < (double)1e-28f;
+                    if (under) {
+                        const unsigned int slot = atomicAdd(&pc.cd->rerun_count, 1u);
+                        if (slot < pc.cd->rerun_cap) {
+                            RerunEntry e;
+                            e.out_idx = oi;
+                            e.read = so.read;
+                            e.hap = cur;
+                            pc.rerun[pc.cd->rerun_off + slot] = e;
+                        } else {
+                            atomicOr(pc.status, kStatusRerunOverflow);
+                        }
+                    }
+                    if (so.pair_flags) so.pair_flags[oi] = under ? 1 : 0;
+                }
+            }
+            ++cur;
+        }
+        started = true;
+        if (cur < g_hi) {
+            const int H = (int)(b.hap_off[cur + 1] - b.hap_off[cur]);
+            nb += H;
+            D0 = C / (T)H;
+            // Left edge of the new haplotype: column 0 is zero in every real row; pad rows stand
+            // for the boundary row 0, whose D is C/H in every column.
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                L.Mp[k] = T(0);
+                L.Ip[k] = T(0);
+                L.Dp[k] = ((L.padmask >> k) & 1u) ? D0 : T(0);
+            }
+            dM = T(0);
+            dI = T(0);
+            dD = above_row0 ? D0 : T(0);
+            sumM = T(0);
+            sumI = T(0);
+        } else {
+            nb = 0x7fffffff;
+        }
+    };
+
+    auto step = [&](int t, bool check) {
+        const int p = t - lane;
+        T sM = shfl_up1(L.Mp[K - 1]);
+        T sI = shfl_up1(L.Ip[K - 1]);
+        T sD = shfl_up1(L.Dp[K - 1]);
+        if (check && p == nb) boundary();
+        if (lane == 0) {
+            if (FROM_SCR) {
+                const bool ok = p >= 0 && p < Tcols;
+                sM = ok ? scr[3 * p + 0] : T(0);
+                sI = ok ? scr[3 * p + 1] : T(0);
+                sD = ok ? scr[3 * p + 2] : T(0);
+            } else {
+                sM = T(0);
+                sI = T(0);
+                sD = D0;
+            }
+        }
+        const uint32_t hc = codes[p];
+        cells<T, K, V>(L, hc, sM, sI, dM, dI, dD);
+        dM = sM;
+        dI = sI;
+        dD = sD;
+        if (TO_SCR) {
+            if (lane == kWarp - 1 && p >= 0 && p < Tcols) {
+                scr[3 * p + 0] = L.Mp[K - 1];
+                scr[3 * p + 1] = L.Ip[K - 1];
+                scr[3 * p + 2] = L.Dp[K - 1];
+            }
+        } else {
+            sumM = ftz(radd(sumM, L.Mp[K - 1]));
+            sumI = ftz(radd(sumI, L.Ip[K - 1]));
+        }
+    };
+
+    for (int t0 = 0; t0 < steps; t0 += kChunk) {
+        // Lanes cover stream columns [t0-31, t0+kChunk-1] in this chunk.  Lane 31 trails, so its
+        // next boundary is the first boundary at or after t0-31: past the chunk means no lane
+        // meets a boundary and the chunk needs no per-step check.
+        const int nb31 = __shfl_sync(0xffffffffu, nb, kWarp - 1);
+        if (nb31 >= t0 + kChunk && t0 + kChunk <= steps) {
+#pragma unroll
+            for (int u = 0; u < kChunk; ++u) step(t0 + u, false);
+        } else {
+            for (int u = 0; u < kChunk; ++u)
+                if (t0 + u < steps) step(t0 + u, true);
+        }
+    }
+}
+
+}  // namespace phmm

@@ -1,0 +1,545 @@
+// PairHMM engine runtime (see phmm_engine.h).
+//
+// Device arena layout (one cudaMalloc per slot, 256-byte aligned sections):
+//   descriptor block  BatchDesc | ClassDesc x 18 | status words     (one H2D copy per batch)
+//   plan arrays       regions, read_off, hap_off, read/hap N flags, work items
+//   read data         bases, q, ins, del, gcp (1 byte per base each)
+//   haplotypes        bases, then two u32 match-code streams with guard codes on both ends
+//   results           likelihoods (f64), pair flags (u8), FP64 rerun slots (16 B per pair)
+//   scratch           per-warp stripe row for reads longer than 256 (3 values per column)
+// The arena only grows; all kernel arguments are arena pointers, so a graph captured for an arena
+// replays for every batch that fits it.
+#include "phmm_engine.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+
+#include "phmm_tables.h"
+
+namespace phmm {
+
+#define PHMM_CK(call)                                                                    \
+    do {                                                                                 \
+        cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess) {                                                         \
+            err = std::string(#call) + " failed: " + cudaGetErrorString(e_);             \
+            return PHMM_ERR_CUDA;                                                        \
+        }                                                                                \
+    } while (0)
+
+namespace {
+
+size_t align_up(size_t x, size_t a = 256) { return (x + a - 1) / a * a; }
+
+constexpr size_t kDescBytes = sizeof(BatchDesc) + sizeof(ClassDesc) * kNumClasses + 4 * sizeof(unsigned int);
+
+// Carves the arena for capacity c starting at base (nullptr: only measure).  Returns the size.
+size_t carve(const Capacity& c, char* base, Slot* s)
+{
+    size_t o = 0;
+    auto take = [&](size_t bytes) -> char* {
+        const size_t at = o;
+        o = align_up(o + std::max<size_t>(bytes, 1));
+        return base ? base + at : nullptr;
+    };
+    char* desc = take(kDescBytes);
+    char* regions = take(c.regions * sizeof(RegionDesc));
+    char* read_off = take((c.reads + 1) * sizeof(uint64_t));
+    char* hap_off = take((c.haps + 1) * sizeof(uint64_t));
+    char* read_flags = take(c.reads);
+    char* hap_flags = take(c.haps);
+    char* items = take(c.items * sizeof(WorkItem));
+    char* rb = take(c.read_bases);
+    char* rq = take(c.read_bases);
+    char* ri = take(c.read_bases);
+    char* rd = take(c.read_bases);
+    char* rc = take(c.read_bases);
+    char* hb = take(c.hap_bases);
+    char* ci = take((c.hap_bases + 2 * kCodePad) * sizeof(uint32_t));
+    char* ca = take((c.hap_bases + 2 * kCodePad) * sizeof(uint32_t));
+    char* out = take(c.out * sizeof(double));
+    char* pf = take(c.out);
+    char* rerun = take(c.rerun * sizeof(RerunEntry));
+    char* scratch = take(c.scratch_cols * 3 * sizeof(double));  // c.scratch_cols counts all warps' columns
+    if (s) {
+        s->d_desc = (BatchDesc*)desc;
+        s->d_classes = (ClassDesc*)(desc + sizeof(BatchDesc));
+        s->d_status = (unsigned int*)(desc + sizeof(BatchDesc) + sizeof(ClassDesc) * kNumClasses);
+        s->d_regions = (RegionDesc*)regions;
+        s->d_read_off = (uint64_t*)read_off;
+        s->d_hap_off = (uint64_t*)hap_off;
+        s->d_read_flags = (uint8_t*)read_flags;
+        s->d_hap_flags = (uint8_t*)hap_flags;
+        s->d_items = (WorkItem*)items;
+        s->d_rb = (uint8_t*)rb;
+        s->d_rq = (uint8_t*)rq;
+        s->d_ri = (uint8_t*)ri;
+        s->d_rd = (uint8_t*)rd;
+        s->d_rc = (uint8_t*)rc;
+        s->d_hb = (uint8_t*)hb;
+        s->d_codes_inter = (uint32_t*)ci;
+        s->d_codes_intra = (uint32_t*)ca;
+        s->d_out = (double*)out;
+        s->d_pair_flags = (uint8_t*)pf;
+        s->d_rerun = (RerunEntry*)rerun;
+        s->d_scratch = scratch;
+    }
+    return o;
+}
+
+// Pinned staging: descriptor block followed by the plan arrays.
+size_t pinned_bytes_for(const Capacity& c)
+{
+    return align_up(kDescBytes) + align_up(c.regions * sizeof(RegionDesc)) + align_up((c.reads + 1) * 8) +
+           align_up((c.haps + 1) * 8) + align_up(c.reads) + align_up(c.haps) + align_up(c.items * sizeof(WorkItem));
+}
+
+Capacity need_of(const Plan& p, uint64_t scratch_warps)
+{
+    Capacity c;
+    c.regions = p.n_regions;
+    c.reads = p.n_reads;
+    c.haps = p.n_haps;
+    c.read_bases = p.read_bases;
+    c.hap_bases = p.hap_bases;
+    c.items = p.items.size();
+    c.rerun = p.rerun_slots;
+    c.out = p.out_total;
+    c.scratch_cols = p.max_multi_stream ? scratch_warps * (uint64_t)PlanLimits().max_stream_multi : 0;
+    return c;
+}
+
+}  // namespace
+
+bool Capacity::covers(const Capacity& o) const
+{
+    return regions >= o.regions && reads >= o.reads && haps >= o.haps && read_bases >= o.read_bases &&
+           hap_bases >= o.hap_bases && items >= o.items && rerun >= o.rerun && out >= o.out &&
+           scratch_cols >= o.scratch_cols;
+}
+
+Capacity Capacity::grown_to(const Capacity& need) const
+{
+    auto g = [](uint64_t cur, uint64_t want) { return want <= cur ? cur : std::max(want, cur + cur / 2); };
+    Capacity c;
+    c.regions = g(regions, need.regions);
+    c.reads = g(reads, need.reads);
+    c.haps = g(haps, need.haps);
+    c.read_bases = g(read_bases, need.read_bases);
+    c.hap_bases = g(hap_bases, need.hap_bases);
+    c.items = g(items, need.items);
+    c.rerun = g(rerun, need.rerun);
+    c.out = g(out, need.out);
+    c.scratch_cols = std::max(scratch_cols, need.scratch_cols);
+    return c;
+}
+
+phmm_status Engine::create(const phmm_config* cfg, Engine** out, std::string& err)
+{
+    *out = nullptr;
+    Engine* e = new Engine();
+    if (cfg) {
+        e->cfg_ = *cfg;
+    } else {
+        e->cfg_.device = 0;
+        e->cfg_.use_cuda_graph = 1;
+        e->cfg_.autotune = 1;
+    }
+    if (e->cfg_.hbm_budget_bytes == 0) e->cfg_.hbm_budget_bytes = 40ull << 30;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        err = "no CUDA device available";
+        delete e;
+        return PHMM_ERR_NO_DEVICE;
+    }
+    if (e->cfg_.device < 0 || e->cfg_.device >= ndev) {
+        err = "device ordinal " + std::to_string(e->cfg_.device) + " out of range";
+        delete e;
+        return PHMM_ERR_NO_DEVICE;
+    }
+    e->dev_ = e->cfg_.device;
+    auto fail = [&](phmm_status st) {
+        delete e;
+        return st;
+    };
+#define PHMM_CKE(call)                                                               \
+    do {                                                                             \
+        cudaError_t e_ = (call);                                                     \
+        if (e_ != cudaSuccess) {                                                     \
+            err = std::string(#call) + " failed: " + cudaGetErrorString(e_);         \
+            return fail(PHMM_ERR_CUDA);                                              \
+        }                                                                            \
+    } while (0)
+    PHMM_CKE(cudaSetDevice(e->dev_));
+    cudaDeviceProp prop;
+    PHMM_CKE(cudaGetDeviceProperties(&prop, e->dev_));
+    if (prop.major < 10) {
+        err = std::string("device ") + prop.name + " is not sm_100 class; this build targets sm_100a only";
+        return fail(PHMM_ERR_NO_DEVICE);
+    }
+    e->sms_ = prop.multiProcessorCount;
+    for (int p = 0; p < 2; ++p)
+        for (int c = 0; c < kNumClasses; ++c) {
+            int b = 0;
+            PHMM_CKE(occupancy(p == 0 ? 32 : 64, c, &b));
+            e->occ_[p][c] = std::max(b, 1);
+        }
+
+    // probability tables
+    const HostTables<float>& hf = host_tables_f32();
+    const HostTables<double>& hd = host_tables_f64();
+    const size_t nf = 5 * 128 + 128 * 128;
+    const size_t bytes = nf * sizeof(float) + nf * sizeof(double);
+    PHMM_CKE(cudaMalloc(&e->d_tables_, bytes));
+    std::vector<char> host(bytes);
+    float* f = (float*)host.data();
+    double* d = (double*)(host.data() + nf * sizeof(float));
+    auto put = [](auto* dst, const auto& v) {
+        std::copy(v.begin(), v.end(), dst);
+        return dst + v.size();
+    };
+    float* fp = f;
+    fp = put(fp, hf.ph2pr);
+    fp = put(fp, hf.pmat);
+    fp = put(fp, hf.pmis_inter);
+    fp = put(fp, hf.pmis_intra);
+    fp = put(fp, hf.gapm);
+    put(fp, hf.mm);
+    double* dp = d;
+    dp = put(dp, hd.ph2pr);
+    dp = put(dp, hd.pmat);
+    dp = put(dp, hd.pmis_inter);
+    dp = put(dp, hd.pmis_intra);
+    dp = put(dp, hd.gapm);
+    put(dp, hd.mm);
+    PHMM_CKE(cudaMemcpy(e->d_tables_, host.data(), bytes, cudaMemcpyHostToDevice));
+    const float* df = (const float*)e->d_tables_;
+    const double* dd = (const double*)((const char*)e->d_tables_ + nf * sizeof(float));
+    e->tf_ = ProbTables<float>{df, df + 128, df + 256, df + 384, df + 512, df + 640};
+    e->td_ = ProbTables<double>{dd, dd + 128, dd + 256, dd + 384, dd + 512, dd + 640};
+#undef PHMM_CKE
+    phmm_status st = e->make_slot(0, &e->default_slot_, err);
+    if (st != PHMM_OK) return fail(st);
+    *out = e;
+    return PHMM_OK;
+}
+
+Engine::~Engine()
+{
+    cudaSetDevice(dev_);
+    if (default_slot_) free_slot(default_slot_);
+    if (d_tables_) cudaFree(d_tables_);
+}
+
+phmm_status Engine::make_slot(int id, Slot** out, std::string& err)
+{
+    *out = nullptr;
+    PHMM_CK(cudaSetDevice(dev_));
+    Slot* s = new Slot();
+    s->id = id;
+    auto cleanup = [&]() { free_slot(s); };
+    cudaError_t e = cudaStreamCreateWithFlags(&s->main, cudaStreamNonBlocking);
+    for (int c = 0; c < kNumClasses && e == cudaSuccess; ++c) e = cudaStreamCreateWithFlags(&s->side[c], cudaStreamNonBlocking);
+    for (int c = 0; c < kNumClasses && e == cudaSuccess; ++c) e = cudaEventCreateWithFlags(&s->ev_side[c], cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreate(&s->ev_t0);
+    if (e == cudaSuccess) e = cudaEventCreate(&s->ev_t1);
+    if (e == cudaSuccess) e = cudaEventCreate(&s->ev_t2);
+    if (e == cudaSuccess) e = cudaEventCreate(&s->ev_t3);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_done, cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+        err = std::string("stream/event creation failed: ") + cudaGetErrorString(e);
+        cleanup();
+        return PHMM_ERR_CUDA;
+    }
+    *out = s;
+    return PHMM_OK;
+}
+
+void Engine::free_slot(Slot* s)
+{
+    if (!s) return;
+    cudaSetDevice(dev_);
+    if (s->main) cudaStreamSynchronize(s->main);
+    if (s->graph) cudaGraphExecDestroy(s->graph);
+    if (s->dev) cudaFree(s->dev);
+    if (s->pinned) cudaFreeHost(s->pinned);
+    for (int c = 0; c < kNumClasses; ++c) {
+        if (s->side[c]) cudaStreamDestroy(s->side[c]);
+        if (s->ev_side[c]) cudaEventDestroy(s->ev_side[c]);
+    }
+    for (cudaEvent_t ev : {s->ev_fork, s->ev_t0, s->ev_t1, s->ev_t2, s->ev_t3, s->ev_done})
+        if (ev) cudaEventDestroy(ev);
+    if (s->main) cudaStreamDestroy(s->main);
+    delete s;
+}
+
+uint64_t Engine::arena_bytes_for(const Plan& plan) const
+{
+    const uint64_t warps = (uint64_t)sms_ * occ_[1][8] * (kFwdBlock / kWarp);
+    return carve(need_of(plan, warps), nullptr, nullptr);
+}
+
+phmm_status Engine::ensure_capacity(Slot& s, const Plan& plan, std::string& err)
+{
+    // multi-stripe scratch: one row per resident warp of the widest multi-stripe class
+    const uint64_t warps = (uint64_t)sms_ * std::max(occ_[0][8], occ_[1][8]) * (kFwdBlock / kWarp);
+    const Capacity need = need_of(plan, warps);
+    if (s.dev && s.cap.covers(need)) return PHMM_OK;
+    const Capacity nc = s.dev ? s.cap.grown_to(need) : need;
+    PHMM_CK(cudaSetDevice(dev_));
+    if (s.main) PHMM_CK(cudaStreamSynchronize(s.main));
+    if (s.graph) {
+        cudaGraphExecDestroy(s.graph);
+        s.graph = nullptr;
+    }
+    if (s.dev) {
+        cudaFree(s.dev);
+        s.dev = nullptr;
+    }
+    if (s.pinned) {
+        cudaFreeHost(s.pinned);
+        s.pinned = nullptr;
+    }
+    const size_t bytes = carve(nc, nullptr, nullptr);
+    cudaError_t e = cudaMalloc((void**)&s.dev, bytes);
+    if (e != cudaSuccess) {
+        s.dev = nullptr;
+        cudaGetLastError();
+        err = "device arena of " + std::to_string(bytes) + " bytes: " + cudaGetErrorString(e);
+        return PHMM_ERR_OUT_OF_MEMORY;
+    }
+    s.dev_bytes = bytes;
+    carve(nc, s.dev, &s);
+    const size_t pb = pinned_bytes_for(nc);
+    e = cudaMallocHost((void**)&s.pinned, pb);
+    if (e != cudaSuccess) {
+        s.pinned = nullptr;
+        cudaGetLastError();
+        err = "pinned staging of " + std::to_string(pb) + " bytes: " + cudaGetErrorString(e);
+        return PHMM_ERR_OUT_OF_MEMORY;
+    }
+    s.pinned_bytes = pb;
+    s.cap = nc;
+    return PHMM_OK;
+}
+
+int Engine::grid_for(int precision, int cls, uint32_t work) const
+{
+    const int full = occ_[precision == 32 ? 0 : 1][cls] * sms_;
+    const int warps_per_block = kFwdBlock / kWarp;
+    const int need = (int)std::min<uint64_t>(((uint64_t)work + warps_per_block - 1) / warps_per_block, (uint64_t)full);
+    return std::max(need, 1);
+}
+
+phmm_status Engine::launch_pipeline(Slot& s, bool want_flags, const Plan* plan, std::string& err)
+{
+    // plan == nullptr: graph capture (every class launched, persistent full grids).
+    BatchView v;
+    v.read_bases = s.d_rb;
+    v.read_q = s.d_rq;
+    v.read_i = s.d_ri;
+    v.read_d = s.d_rd;
+    v.read_c = s.d_rc;
+    v.read_off = s.d_read_off;
+    v.read_flags = s.d_read_flags;
+    v.hap_off = s.d_hap_off;
+    v.codes_inter = s.d_codes_inter;
+    v.codes_intra = s.d_codes_intra;
+    v.hap_flags = s.d_hap_flags;
+    v.regions = s.d_regions;
+    v.out = s.d_out;
+    v.pair_flags = want_flags ? s.d_pair_flags : nullptr;
+    const uint64_t warps = (uint64_t)sms_ * std::max(occ_[0][8], occ_[1][8]) * (kFwdBlock / kWarp);
+    const unsigned int scr_cols = s.cap.scratch_cols ? (unsigned int)(s.cap.scratch_cols / warps) : 0u;
+    const unsigned int rec = plan ? cudaEventRecordDefault : cudaEventRecordExternal;
+
+    PHMM_CK(cudaEventRecordWithFlags(s.ev_t0, s.main, rec));
+    PHMM_CK(launch_prep(s.d_desc, s.d_hb, s.d_codes_inter, s.d_codes_intra, s.d_out, v.pair_flags, sms_, s.main));
+    for (int pass = 0; pass < 2; ++pass) {
+        const int precision = pass == 0 ? 32 : 64;
+        PHMM_CK(cudaEventRecord(s.ev_fork, s.main));
+        for (int c = 0; c < kNumClasses; ++c) {
+            uint32_t work = 0;
+            if (plan) {
+                work = pass == 0 ? plan->classes[c].n_items : plan->classes[c].rerun_cap;
+                if (work == 0) continue;
+            }
+            const int grid = plan ? grid_for(precision, c, work) : occ_[pass][c] * sms_;
+            PassControl pc;
+            pc.cd = s.d_classes + c;
+            pc.items = s.d_items;
+            pc.rerun = s.d_rerun;
+            pc.status = s.d_status;
+            pc.scratch = s.d_scratch;
+            pc.scratch_cols = scr_cols;
+            PHMM_CK(cudaStreamWaitEvent(s.side[c], s.ev_fork, 0));
+            PHMM_CK(launch_fwd(precision, c, v, tf_, td_, pc, grid, s.side[c]));
+            PHMM_CK(cudaEventRecord(s.ev_side[c], s.side[c]));
+            PHMM_CK(cudaStreamWaitEvent(s.main, s.ev_side[c], 0));
+        }
+        PHMM_CK(cudaEventRecordWithFlags(pass == 0 ? s.ev_t1 : s.ev_t2, s.main, rec));
+    }
+    return PHMM_OK;
+}
+
+phmm_status Engine::capture_graph(Slot& s, bool want_flags, std::string& err)
+{
+    if (s.graph) {
+        cudaGraphExecDestroy(s.graph);
+        s.graph = nullptr;
+    }
+    cudaGraph_t g = nullptr;
+    PHMM_CK(cudaStreamBeginCapture(s.main, cudaStreamCaptureModeThreadLocal));
+    std::string lerr;
+    phmm_status st = launch_pipeline(s, want_flags, nullptr, lerr);
+    cudaError_t e = cudaStreamEndCapture(s.main, &g);
+    if (st != PHMM_OK) {
+        if (g) cudaGraphDestroy(g);
+        err = lerr;
+        return st;
+    }
+    if (e != cudaSuccess) {
+        err = std::string("graph capture failed: ") + cudaGetErrorString(e);
+        return PHMM_ERR_CUDA;
+    }
+    e = cudaGraphInstantiate(&s.graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        s.graph = nullptr;
+        err = std::string("graph instantiate failed: ") + cudaGetErrorString(e);
+        return PHMM_ERR_CUDA;
+    }
+    s.graph_flags = want_flags;
+    return PHMM_OK;
+}
+
+phmm_status Engine::enqueue(Slot& s, const Plan& plan, const phmm_batch& b, bool want_flags, std::string& err)
+{
+    phmm_status st = ensure_capacity(s, plan, err);
+    if (st != PHMM_OK) return st;
+    PHMM_CK(cudaSetDevice(dev_));
+    // stage descriptors + plan arrays in pinned memory, then copy
+    char* p = s.pinned;
+    size_t o = 0;
+    auto stage = [&](const void* src, size_t bytes) -> char* {
+        char* at = p + o;
+        if (bytes) std::memcpy(at, src, bytes);
+        o = align_up(o + std::max<size_t>(bytes, 1));
+        return at;
+    };
+    BatchDesc bd{};
+    bd.hap_bases_total = plan.hap_bases;
+    bd.out_total = plan.out_total;
+    bd.n_regions = plan.n_regions;
+    bd.n_reads = plan.n_reads;
+    bd.n_haps = plan.n_haps;
+    bd.n_items = (uint32_t)plan.items.size();
+    char* desc = p;
+    std::memcpy(desc, &bd, sizeof(bd));
+    std::memcpy(desc + sizeof(bd), plan.classes.data(), sizeof(ClassDesc) * kNumClasses);
+    std::memset(desc + sizeof(bd) + sizeof(ClassDesc) * kNumClasses, 0, 4 * sizeof(unsigned int));
+    o = align_up(kDescBytes);
+    char* h_regions = stage(plan.regions.data(), plan.regions.size() * sizeof(RegionDesc));
+    char* h_read_off = stage(plan.read_off.data(), plan.read_off.size() * 8);
+    char* h_hap_off = stage(plan.hap_off.data(), plan.hap_off.size() * 8);
+    char* h_read_flags = stage(plan.read_flags.data(), plan.read_flags.size());
+    char* h_hap_flags = stage(plan.hap_flags.data(), plan.hap_flags.size());
+    char* h_items = stage(plan.items.data(), plan.items.size() * sizeof(WorkItem));
+
+    cudaStream_t m = s.main;
+    PHMM_CK(cudaMemcpyAsync(s.d_desc, desc, kDescBytes, cudaMemcpyHostToDevice, m));
+    PHMM_CK(cudaMemcpyAsync(s.d_regions, h_regions, plan.regions.size() * sizeof(RegionDesc), cudaMemcpyHostToDevice, m));
+    PHMM_CK(cudaMemcpyAsync(s.d_read_off, h_read_off, plan.read_off.size() * 8, cudaMemcpyHostToDevice, m));
+    PHMM_CK(cudaMemcpyAsync(s.d_hap_off, h_hap_off, plan.hap_off.size() * 8, cudaMemcpyHostToDevice, m));
+    if (!plan.read_flags.empty())
+        PHMM_CK(cudaMemcpyAsync(s.d_read_flags, h_read_flags, plan.read_flags.size(), cudaMemcpyHostToDevice, m));
+    if (!plan.hap_flags.empty())
+        PHMM_CK(cudaMemcpyAsync(s.d_hap_flags, h_hap_flags, plan.hap_flags.size(), cudaMemcpyHostToDevice, m));
+    if (!plan.items.empty())
+        PHMM_CK(cudaMemcpyAsync(s.d_items, h_items, plan.items.size() * sizeof(WorkItem), cudaMemcpyHostToDevice, m));
+    const uint64_t rb = plan.read_bases;
+    if (rb) {
+        PHMM_CK(cudaMemcpyAsync(s.d_rb, b.read_bases + plan.read_base0, rb, cudaMemcpyHostToDevice, m));
+        PHMM_CK(cudaMemcpyAsync(s.d_rq, b.read_qual + plan.read_base0, rb, cudaMemcpyHostToDevice, m));
+        PHMM_CK(cudaMemcpyAsync(s.d_ri, b.read_ins + plan.read_base0, rb, cudaMemcpyHostToDevice, m));
+        PHMM_CK(cudaMemcpyAsync(s.d_rd, b.read_del + plan.read_base0, rb, cudaMemcpyHostToDevice, m));
+        PHMM_CK(cudaMemcpyAsync(s.d_rc, b.read_gcp + plan.read_base0, rb, cudaMemcpyHostToDevice, m));
+    }
+    if (plan.hap_bases)
+        PHMM_CK(cudaMemcpyAsync(s.d_hb, b.hap_bases + plan.hap_base0, plan.hap_bases, cudaMemcpyHostToDevice, m));
+
+    if (cfg_.use_cuda_graph) {
+        if (!s.graph || s.graph_flags != want_flags) {
+            st = capture_graph(s, want_flags, err);
+            if (st != PHMM_OK) return st;
+        }
+        PHMM_CK(cudaGraphLaunch(s.graph, m));
+    } else {
+        st = launch_pipeline(s, want_flags, &plan, err);
+        if (st != PHMM_OK) return st;
+    }
+    return PHMM_OK;
+}
+
+phmm_status Engine::finish(Slot& s, const Plan& plan, double* out, uint8_t* pair_flags, phmm_stats* stats,
+                           std::string& err)
+{
+    cudaStream_t m = s.main;
+    char* desc = s.pinned;  // reuse the staged descriptor block for the read-back
+    PHMM_CK(cudaMemcpyAsync(desc, s.d_desc, kDescBytes, cudaMemcpyDeviceToHost, m));
+    if (plan.out_total) {
+        PHMM_CK(cudaMemcpyAsync(out, s.d_out, plan.out_total * sizeof(double), cudaMemcpyDeviceToHost, m));
+        if (pair_flags) PHMM_CK(cudaMemcpyAsync(pair_flags, s.d_pair_flags, plan.out_total, cudaMemcpyDeviceToHost, m));
+    }
+    PHMM_CK(cudaEventRecord(s.ev_t3, m));
+    PHMM_CK(cudaEventSynchronize(s.ev_t3));
+    const ClassDesc* cls = (const ClassDesc*)(desc + sizeof(BatchDesc));
+    const unsigned int status = *(const unsigned int*)(desc + sizeof(BatchDesc) + sizeof(ClassDesc) * kNumClasses);
+    uint64_t f64 = 0;
+    for (int c = 0; c < kNumClasses; ++c) f64 += std::min(cls[c].rerun_count, cls[c].rerun_cap);
+    if (stats) {
+        stats->regions = plan.n_regions;
+        stats->pairs = plan.pairs;
+        stats->cells = plan.cells;
+        stats->pairs_f64 = f64;
+        stats->work_items = plan.items.size();
+        stats->h2d_bytes = plan.read_bases * 5 + plan.hap_bases;
+        stats->d2h_bytes = plan.out_total * (sizeof(double) + (pair_flags ? 1 : 0));
+        float a = 0, bms = 0, c2 = 0;
+        cudaEventElapsedTime(&a, s.ev_t0, s.ev_t2);
+        cudaEventElapsedTime(&bms, s.ev_t0, s.ev_t1);
+        cudaEventElapsedTime(&c2, s.ev_t1, s.ev_t2);
+        stats->device_ms = a;
+        stats->fp32_ms = bms;
+        stats->fp64_ms = c2;
+    }
+    if (status != 0) {
+        err = "kernel status word " + std::to_string(status) +
+              ((status & kStatusBadItem) ? " (work item does not fit its kernel class)" : "") +
+              ((status & kStatusRerunOverflow) ? " (FP64 rerun list overflow)" : "");
+        return PHMM_ERR_DEVICE_STATUS;
+    }
+    return PHMM_OK;
+}
+
+phmm_status Engine::compute(const phmm_batch& b, double* out, uint8_t* pair_flags, phmm_stats* stats, std::string& err)
+{
+    const auto t0 = std::chrono::steady_clock::now();
+    std::lock_guard<std::mutex> lk(mu_);
+    Plan plan;
+    phmm_status st = build_plan(b, PlanLimits(), plan, err);
+    if (st != PHMM_OK) return st;
+    if (plan.out_total && !out) {
+        err = "out is null";
+        return PHMM_ERR_INVALID_ARGUMENT;
+    }
+    st = enqueue(*default_slot_, plan, b, pair_flags != nullptr, err);
+    if (st != PHMM_OK) return st;
+    st = finish(*default_slot_, plan, out, pair_flags, stats, err);
+    if (stats) stats->host_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return st;
+}
+
+}  // namespace phmm

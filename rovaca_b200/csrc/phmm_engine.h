@@ -1,0 +1,98 @@
+// PairHMM engine: one CUDA device, a growable device arena, and the batch pipeline
+//   reset/prep -> FP32 class kernels (forked streams) -> FP64 class kernels -> results.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/phmm_b200.h"
+#include "phmm_types.h"
+#include "phmm_kernels.h"
+#include "phmm_plan.h"
+
+namespace phmm {
+
+// Sizes an arena must hold.
+struct Capacity {
+    uint64_t regions = 0, reads = 0, haps = 0, read_bases = 0, hap_bases = 0, items = 0, rerun = 0, out = 0;
+    uint64_t scratch_cols = 0;
+    bool covers(const Capacity& o) const;
+    Capacity grown_to(const Capacity& need) const;
+};
+
+// One device arena with everything a batch needs, plus its streams, events and captured graph.
+struct Slot {
+    int id = 0;
+    char* dev = nullptr;             // device arena
+    size_t dev_bytes = 0;
+    char* pinned = nullptr;          // pinned host staging for the plan arrays and descriptors
+    size_t pinned_bytes = 0;
+    Capacity cap;
+    // carved device pointers
+    BatchDesc* d_desc = nullptr;
+    ClassDesc* d_classes = nullptr;
+    unsigned int* d_status = nullptr;
+    RegionDesc* d_regions = nullptr;
+    uint64_t *d_read_off = nullptr, *d_hap_off = nullptr;
+    uint8_t *d_read_flags = nullptr, *d_hap_flags = nullptr;
+    WorkItem* d_items = nullptr;
+    RerunEntry* d_rerun = nullptr;
+    double* d_out = nullptr;
+    uint8_t* d_pair_flags = nullptr;
+    uint8_t *d_rb = nullptr, *d_rq = nullptr, *d_ri = nullptr, *d_rd = nullptr, *d_rc = nullptr;
+    uint8_t* d_hb = nullptr;
+    uint32_t *d_codes_inter = nullptr, *d_codes_intra = nullptr;
+    void* d_scratch = nullptr;
+    // execution
+    cudaStream_t main = nullptr;
+    cudaStream_t side[kNumClasses] = {};
+    cudaEvent_t ev_fork = nullptr, ev_side[kNumClasses] = {}, ev_t0 = nullptr, ev_t1 = nullptr, ev_t2 = nullptr,
+                ev_t3 = nullptr, ev_done = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    bool graph_flags = false;        // the captured graph writes pair flags
+};
+
+class Engine {
+public:
+    static phmm_status create(const phmm_config* cfg, Engine** out, std::string& err);
+    ~Engine();
+
+    // Synchronous batch (thread-safe; calls are serialised on the engine's default slot).
+    phmm_status compute(const phmm_batch& b, double* out, uint8_t* pair_flags, phmm_stats* stats, std::string& err);
+
+    // Pieces used by the serving loop (phmm_serve.cpp), each on a caller-owned slot.
+    phmm_status make_slot(int id, Slot** out, std::string& err);
+    void free_slot(Slot* s);
+    phmm_status enqueue(Slot& s, const Plan& plan, const phmm_batch& b, bool want_flags, std::string& err);
+    phmm_status finish(Slot& s, const Plan& plan, double* out, uint8_t* pair_flags, phmm_stats* stats,
+                       std::string& err);
+
+    int device() const { return dev_; }
+    int num_sms() const { return sms_; }
+    const phmm_config& config() const { return cfg_; }
+    uint64_t arena_bytes_for(const Plan& plan) const;
+
+private:
+    Engine() = default;
+    phmm_status ensure_capacity(Slot& s, const Plan& plan, std::string& err);
+    phmm_status launch_pipeline(Slot& s, bool want_flags, const Plan* plan, std::string& err);
+    phmm_status capture_graph(Slot& s, bool want_flags, std::string& err);
+    int grid_for(int precision, int cls, uint32_t work) const;
+
+    phmm_config cfg_{};
+    int dev_ = 0;
+    int sms_ = 0;
+    int occ_[2][kNumClasses] = {};
+    // device probability tables
+    void* d_tables_ = nullptr;
+    ProbTables<float> tf_{};
+    ProbTables<double> td_{};
+    Slot* default_slot_ = nullptr;
+    std::mutex mu_;
+};
+
+}  // namespace phmm

@@ -1,0 +1,190 @@
+// PairHMM kernels for sm_100a: haplotype code preparation, the persistent FP32 wavefront pass and
+// the persistent FP64 recompute pass.  Device arithmetic lives in phmm_device.cuh.
+//
+// Every (precision, rows-per-lane K, variant) combination is its own kernel, so each gets the
+// register allocation its own live state needs (FP32: about 60 registers at K = 1 up to 140 at
+// K = 8) instead of the union of all paths.  Work items are grouped by that class on the host.
+#include <cuda_runtime.h>
+
+#include "phmm_device.cuh"
+#include "phmm_kernels.h"
+
+namespace phmm {
+
+// ------------------------------------------------------------------------------------------
+// Haplotype bytes -> per-variant match codes (grid-stride).
+// ------------------------------------------------------------------------------------------
+__global__ void prep_codes_kernel(const BatchDesc* __restrict__ desc, const uint8_t* __restrict__ hap_bases,
+                                  uint32_t* __restrict__ codes_inter, uint32_t* __restrict__ codes_intra)
+{
+    const uint64_t total = desc->hap_bases_total;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
+        const uint8_t b = hap_bases[i];
+        codes_inter[kCodePad + i] = match_code(b, kInter);
+        codes_intra[kCodePad + i] = match_code(b, kIntra);
+    }
+    // guard codes on both sides of the stream: match nothing
+    if (blockIdx.x == 0 && threadIdx.x < kCodePad) {
+        codes_inter[threadIdx.x] = 0u;
+        codes_intra[threadIdx.x] = 0u;
+        codes_inter[kCodePad + total + threadIdx.x] = 0u;
+        codes_intra[kCodePad + total + threadIdx.x] = 0u;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Output reset: every likelihood NaN (pairs with an empty read or haplotype stay NaN), flags 0.
+// ------------------------------------------------------------------------------------------
+__global__ void reset_outputs_kernel(const BatchDesc* __restrict__ desc, double* __restrict__ out,
+                                     uint8_t* __restrict__ flags)
+{
+    const uint64_t total = desc->out_total;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    const double nan = __longlong_as_double(0x7ff8000000000000ll);
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
+        out[i] = nan;
+        if (flags) flags[i] = 0;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// One read against a run of haplotypes [g_lo, g_hi).
+// ------------------------------------------------------------------------------------------
+template <typename T, int K, int V, bool MULTI>
+__device__ __forceinline__ void run_read(const BatchView& b, const ProbTables<T>& tb, const PassControl& pc,
+                                         const SweepOut& so, uint32_t g_lo, uint32_t g_hi, int lane, T* scr)
+{
+    LaneRows<T, K> L;
+    const uint64_t roff = b.read_off[so.read];
+    const int R = (int)(b.read_off[so.read + 1] - roff);
+    const int Tcols = (int)(b.hap_off[g_hi] - b.hap_off[g_lo]);
+    // A read that does not fit the class's stripe, or a multi-stripe stream longer than the
+    // scratch row, means a planning bug: report it and leave the pairs as NaN.
+    if (R <= 0 || (!MULTI && R > kWarp * K) || (MULTI && (R <= kWarp * K || Tcols > (int)pc.scratch_cols))) {
+        if (lane == 0) atomicOr(pc.status, kStatusBadItem);
+        return;
+    }
+    if (!MULTI) {
+        const int pad = kWarp * K - R;
+        load_rows<T, K, V>(L, b, tb, roff, R, 0, pad, lane);
+        sweep<T, K, V, false, false>(L, b, pc, so, g_lo, g_hi, scr, lane, lane * K <= pad);
+    } else {
+        constexpr int SR = kWarp * K;  // rows per stripe
+        const int stripes = (R + SR - 1) / SR;
+        const int pad = SR * stripes - R;
+        for (int s = 0; s < stripes; ++s) {
+            load_rows<T, K, V>(L, b, tb, roff, R, s * SR, pad, lane);
+            const bool above_row0 = (s == 0) && (lane * K <= pad);
+            if (s == 0)
+                sweep<T, K, V, false, true>(L, b, pc, so, g_lo, g_hi, scr, lane, above_row0);
+            else if (s == stripes - 1)
+                sweep<T, K, V, true, false>(L, b, pc, so, g_lo, g_hi, scr, lane, above_row0);
+            else
+                sweep<T, K, V, true, true>(L, b, pc, so, g_lo, g_hi, scr, lane, above_row0);
+            __syncwarp();  // lane 31's scratch row is read by lane 0 in the next stripe
+        }
+    }
+}
+
+__device__ __forceinline__ unsigned int claim(unsigned int* counter, int lane)
+{
+    unsigned int idx = 0;
+    if (lane == 0) idx = atomicAdd(counter, 1u);
+    return __shfl_sync(0xffffffffu, idx, 0);
+}
+
+// ------------------------------------------------------------------------------------------
+// FP32 pass for one class: persistent warps claim work items (longest first).
+// ------------------------------------------------------------------------------------------
+template <int K, int V, bool MULTI>
+__global__ void __launch_bounds__(kFwdBlock, 1) fwd_f32_kernel(BatchView b, ProbTables<float> tb, PassControl pc)
+{
+    const int lane = threadIdx.x & (kWarp - 1);
+    const unsigned int warp_id = (blockIdx.x * blockDim.x + threadIdx.x) / kWarp;
+    float* scr = MULTI ? (float*)pc.scratch + (size_t)warp_id * pc.scratch_cols * 3 : nullptr;
+    const unsigned int n = pc.cd->n_items;
+    const WorkItem* items = pc.items + pc.cd->item_off;
+    for (;;) {
+        const unsigned int idx = claim(&pc.cd->claim32, lane);
+        if (idx >= n) break;
+        const WorkItem it = items[idx];
+        const RegionDesc rg = b.regions[it.region];
+        SweepOut so;
+        so.out = b.out;
+        so.pair_flags = b.pair_flags;
+        so.out_base = rg.out_off + (uint64_t)it.hap_lo * rg.n_reads + (it.read - rg.read_begin);
+        so.out_stride = rg.n_reads;
+        so.read = it.read;
+        so.fp32_pass = true;
+        run_read<float, K, V, MULTI>(b, tb, pc, so, rg.hap_begin + it.hap_lo, rg.hap_begin + it.hap_hi, lane, scr);
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// FP64 pass for one class over the pairs its FP32 pass flagged, one pair per claim.
+// ------------------------------------------------------------------------------------------
+template <int K, int V, bool MULTI>
+__global__ void __launch_bounds__(kFwdBlock, 1) fwd_f64_kernel(BatchView b, ProbTables<double> tb, PassControl pc)
+{
+    const int lane = threadIdx.x & (kWarp - 1);
+    const unsigned int warp_id = (blockIdx.x * blockDim.x + threadIdx.x) / kWarp;
+    double* scr = MULTI ? (double*)pc.scratch + (size_t)warp_id * pc.scratch_cols * 3 : nullptr;
+    const unsigned int n = min(pc.cd->rerun_count, pc.cd->rerun_cap);
+    const RerunEntry* rerun = pc.rerun + pc.cd->rerun_off;
+    for (;;) {
+        const unsigned int idx = claim(&pc.cd->claim64, lane);
+        if (idx >= n) break;
+        const RerunEntry e = rerun[idx];
+        SweepOut so;
+        so.out = b.out;
+        so.pair_flags = nullptr;
+        so.out_base = e.out_idx;
+        so.out_stride = 0;
+        so.read = e.read;
+        so.fp32_pass = false;
+        run_read<double, K, V, MULTI>(b, tb, pc, so, e.hap, e.hap + 1, lane, scr);
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Class tables and host-side launch wrappers.
+// ------------------------------------------------------------------------------------------
+typedef void (*F32Kernel)(BatchView, ProbTables<float>, PassControl);
+typedef void (*F64Kernel)(BatchView, ProbTables<double>, PassControl);
+
+#define PHMM_CLASS_ROW(KER, V) \
+    KER<1, V, false>, KER<2, V, false>, KER<3, V, false>, KER<4, V, false>, KER<5, V, false>, KER<6, V, false>, \
+        KER<7, V, false>, KER<8, V, false>, KER<8, V, true>
+
+static const F32Kernel kF32[kNumClasses] = {PHMM_CLASS_ROW(fwd_f32_kernel, kInter), PHMM_CLASS_ROW(fwd_f32_kernel, kIntra)};
+static const F64Kernel kF64[kNumClasses] = {PHMM_CLASS_ROW(fwd_f64_kernel, kInter), PHMM_CLASS_ROW(fwd_f64_kernel, kIntra)};
+
+cudaError_t launch_prep(const BatchDesc* desc, const uint8_t* hap_bases, uint32_t* codes_inter, uint32_t* codes_intra,
+                        double* out, uint8_t* flags, int num_sms, cudaStream_t st)
+{
+    const int threads = 256;
+    reset_outputs_kernel<<<num_sms * 4, threads, 0, st>>>(desc, out, flags);
+    prep_codes_kernel<<<num_sms * 4, threads, 0, st>>>(desc, hap_bases, codes_inter, codes_intra);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fwd(int precision, int cls, const BatchView& b, const ProbTables<float>& tf,
+                       const ProbTables<double>& td, const PassControl& pc, int grid, cudaStream_t st)
+{
+    if (cls < 0 || cls >= kNumClasses || grid <= 0) return cudaErrorInvalidValue;
+    if (precision == 32)
+        kF32[cls]<<<grid, kFwdBlock, 0, st>>>(b, tf, pc);
+    else
+        kF64[cls]<<<grid, kFwdBlock, 0, st>>>(b, td, pc);
+    return cudaGetLastError();
+}
+
+cudaError_t occupancy(int precision, int cls, int* blocks_per_sm)
+{
+    if (cls < 0 || cls >= kNumClasses) return cudaErrorInvalidValue;
+    if (precision == 32) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kF32[cls], kFwdBlock, 0);
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kF64[cls], kFwdBlock, 0);
+}
+
+}  // namespace phmm

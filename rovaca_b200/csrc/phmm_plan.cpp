@@ -1,0 +1,224 @@
+// Batch planner (see phmm_plan.h).
+//
+// Reference behaviour mirrored here:
+//   limits                      src/haplotypecaller/pairhmm/roDV_schedule.cpp:70-73,374-381,445-459
+//   pairs with an N go to the   src/haplotypecaller/pairhmm/roDV_schedule.cpp:96,105,417-441
+//   intra kernel (N wildcard)   (region API tests 'N' only, :422,:435)
+//   empty read or haplotype     src/haplotypecaller/pairhmm/roDV_schedule.cpp:460 (pair skipped,
+//                               its likelihood stays NaN, pairhmm_internal.cpp:593)
+// Instead of the reference's greedy SIMD grouping (roDV_schedule.cpp:87-142), every read becomes
+// one work item per run of its region's haplotypes: a warp streams all of them through the read.
+#include "phmm_plan.h"
+
+#include <algorithm>
+#include <cstring>
+
+namespace phmm {
+
+namespace {
+
+bool has_n(const uint8_t* p, uint64_t n) { return n > 0 && std::memchr(p, 'N', (size_t)n) != nullptr; }
+
+struct Run {
+    uint16_t lo, hi;
+    uint32_t cols;
+    uint8_t variant;
+};
+
+// Splits haplotypes [0, n) of a region into runs of non-empty haplotypes whose column stream
+// stays within max_cols; with split_on_n, a run also never mixes N and non-N haplotypes.
+void make_runs(const uint64_t* hoff, const uint8_t* hflags, uint32_t n, uint32_t max_cols, bool split_on_n,
+               std::vector<Run>& runs)
+{
+    runs.clear();
+    uint32_t h = 0;
+    while (h < n) {
+        const uint64_t H = hoff[h + 1] - hoff[h];
+        if (H == 0) {
+            ++h;
+            continue;
+        }
+        Run r;
+        r.lo = (uint16_t)h;
+        r.cols = 0;
+        r.variant = split_on_n ? (hflags[h] & 1) : kIntra;
+        while (h < n) {
+            const uint64_t Hh = hoff[h + 1] - hoff[h];
+            if (Hh == 0) break;
+            if (split_on_n && (hflags[h] & 1) != r.variant) break;
+            if (r.cols > 0 && r.cols + Hh > max_cols) break;
+            r.cols += (uint32_t)Hh;
+            ++h;
+        }
+        r.hi = (uint16_t)h;
+        runs.push_back(r);
+    }
+}
+
+}  // namespace
+
+phmm_status build_plan(const phmm_batch& b, const PlanLimits& lim, Plan& plan, std::string& err)
+{
+    plan = Plan();
+    plan.classes.assign(kPlanClasses, ClassDesc{});
+    if (b.n_regions == 0) return PHMM_OK;
+    if (!b.n_haps || !b.n_reads || !b.hap_off || !b.read_off) {
+        err = "batch: n_haps, n_reads, hap_off and read_off are required";
+        return PHMM_ERR_INVALID_ARGUMENT;
+    }
+    uint64_t nh = 0, nr = 0;
+    for (uint32_t r = 0; r < b.n_regions; ++r) {
+        nh += b.n_haps[r];
+        nr += b.n_reads[r];
+        if (b.n_haps[r] > lim.max_haps_per_region) {
+            err = "region " + std::to_string(r) + ": " + std::to_string(b.n_haps[r]) + " haplotypes exceeds the limit of " +
+                  std::to_string(lim.max_haps_per_region);
+            return PHMM_ERR_LIMIT_EXCEEDED;
+        }
+    }
+    if (nh > 0xffffffffull || nr > 0xffffffffull) {
+        err = "batch: more than 2^32 haplotypes or reads";
+        return PHMM_ERR_INVALID_ARGUMENT;
+    }
+    plan.n_regions = b.n_regions;
+    plan.n_haps = (uint32_t)nh;
+    plan.n_reads = (uint32_t)nr;
+
+    // offsets: monotone, rebased to 0, lengths within the limits
+    plan.hap_base0 = b.hap_off[0];
+    plan.read_base0 = b.read_off[0];
+    plan.hap_off.resize(nh + 1);
+    plan.read_off.resize(nr + 1);
+    for (uint64_t h = 0; h <= nh; ++h) {
+        if (h > 0 && b.hap_off[h] < b.hap_off[h - 1]) {
+            err = "hap_off is not non-decreasing at " + std::to_string(h);
+            return PHMM_ERR_INVALID_ARGUMENT;
+        }
+        plan.hap_off[h] = b.hap_off[h] - plan.hap_base0;
+        if (h > 0 && plan.hap_off[h] - plan.hap_off[h - 1] > lim.max_hap_len) {
+            err = "haplotype " + std::to_string(h - 1) + " longer than " + std::to_string(lim.max_hap_len);
+            return PHMM_ERR_LIMIT_EXCEEDED;
+        }
+    }
+    for (uint64_t r = 0; r <= nr; ++r) {
+        if (r > 0 && b.read_off[r] < b.read_off[r - 1]) {
+            err = "read_off is not non-decreasing at " + std::to_string(r);
+            return PHMM_ERR_INVALID_ARGUMENT;
+        }
+        plan.read_off[r] = b.read_off[r] - plan.read_base0;
+        if (r > 0 && plan.read_off[r] - plan.read_off[r - 1] > lim.max_read_len) {
+            err = "read " + std::to_string(r - 1) + " longer than " + std::to_string(lim.max_read_len);
+            return PHMM_ERR_LIMIT_EXCEEDED;
+        }
+    }
+    plan.hap_bases = plan.hap_off[nh];
+    plan.read_bases = plan.read_off[nr];
+    if ((plan.hap_bases > 0 && !b.hap_bases) ||
+        (plan.read_bases > 0 && (!b.read_bases || !b.read_qual || !b.read_ins || !b.read_del || !b.read_gcp))) {
+        err = "batch: sequence or quality pointer is null";
+        return PHMM_ERR_INVALID_ARGUMENT;
+    }
+    const uint8_t* hb = b.hap_bases + plan.hap_base0;
+    const uint8_t* rb = b.read_bases + plan.read_base0;
+
+    plan.hap_flags.resize(nh);
+    for (uint64_t h = 0; h < nh; ++h) plan.hap_flags[h] = has_n(hb + plan.hap_off[h], plan.hap_off[h + 1] - plan.hap_off[h]);
+    plan.read_flags.resize(nr);
+    for (uint64_t r = 0; r < nr; ++r)
+        plan.read_flags[r] = has_n(rb + plan.read_off[r], plan.read_off[r + 1] - plan.read_off[r]);
+
+    // regions and work items, counted per (class, stream-length bucket) for a stable counting sort
+    constexpr int kBuckets = 64;
+    constexpr uint32_t kBucketCols = 128;
+    std::vector<uint32_t> count((size_t)kPlanClasses * kBuckets, 0);
+    plan.regions.resize(b.n_regions);
+    std::vector<Run> runs_split, runs_all, runs_split_m, runs_all_m;
+    std::vector<WorkItem> raw;
+    std::vector<uint32_t> raw_key;
+    uint64_t out_off = 0;
+    uint32_t hap_begin = 0, read_begin = 0;
+    for (uint32_t g = 0; g < b.n_regions; ++g) {
+        const uint32_t M = b.n_haps[g], N = b.n_reads[g];
+        RegionDesc& rd = plan.regions[g];
+        rd = RegionDesc{};
+        rd.out_off = out_off;
+        rd.hap_begin = hap_begin;
+        rd.n_haps = M;
+        rd.read_begin = read_begin;
+        rd.n_reads = N;
+        const uint64_t* hoff = plan.hap_off.data() + hap_begin;
+        const uint8_t* hfl = plan.hap_flags.data() + hap_begin;
+        bool runs_ready = false, runs_m_ready = false;
+        for (uint32_t r = 0; r < N; ++r) {
+            const uint32_t gr = read_begin + r;
+            const uint64_t R = plan.read_off[gr + 1] - plan.read_off[gr];
+            if (R == 0) continue;
+            const bool multi = R > (uint64_t)kWarp * kMaxK;
+            const int k = multi ? kMaxK : (int)((R + kWarp - 1) / kWarp);
+            const bool read_n = plan.read_flags[gr] & 1;
+            const std::vector<Run>* runs;
+            if (!multi) {
+                if (!runs_ready) {
+                    make_runs(hoff, hfl, M, lim.max_stream_single, true, runs_split);
+                    make_runs(hoff, hfl, M, lim.max_stream_single, false, runs_all);
+                    runs_ready = true;
+                }
+                runs = read_n ? &runs_all : &runs_split;
+            } else {
+                if (!runs_m_ready) {
+                    make_runs(hoff, hfl, M, lim.max_stream_multi, true, runs_split_m);
+                    make_runs(hoff, hfl, M, lim.max_stream_multi, false, runs_all_m);
+                    runs_m_ready = true;
+                }
+                runs = read_n ? &runs_all_m : &runs_split_m;
+            }
+            for (const Run& run : *runs) {
+                WorkItem it{};
+                it.read = gr;
+                it.region = g;
+                it.hap_lo = run.lo;
+                it.hap_hi = run.hi;
+                it.k = (uint8_t)k;
+                it.stripes = (uint8_t)(multi ? (R + kWarp * kMaxK - 1) / (kWarp * kMaxK) : 1);
+                it.variant = read_n ? (uint8_t)kIntra : run.variant;
+                const int cls = plan_class(it.variant, k, multi);
+                const uint32_t bucket = std::min<uint32_t>(run.cols / kBucketCols, kBuckets - 1);
+                const uint32_t key = (uint32_t)cls * kBuckets + (kBuckets - 1 - bucket);  // longest first
+                raw.push_back(it);
+                raw_key.push_back(key);
+                ++count[key];
+                plan.classes[cls].rerun_cap += run.hi - run.lo;
+                plan.pairs += run.hi - run.lo;
+                plan.cells += (uint64_t)run.cols * R;
+                if (multi) plan.max_multi_stream = std::max(plan.max_multi_stream, run.cols);
+            }
+        }
+        out_off += (uint64_t)M * N;
+        hap_begin += M;
+        read_begin += N;
+    }
+    plan.out_total = out_off;
+    plan.empty_pairs = out_off - plan.pairs;
+
+    // stable counting sort by key
+    std::vector<uint32_t> start(count.size() + 1, 0);
+    for (size_t i = 0; i < count.size(); ++i) start[i + 1] = start[i] + count[i];
+    plan.items.resize(raw.size());
+    {
+        std::vector<uint32_t> pos(start.begin(), start.end() - 1);
+        for (size_t i = 0; i < raw.size(); ++i) plan.items[pos[raw_key[i]]++] = raw[i];
+    }
+    uint32_t rerun_off = 0;
+    for (int c = 0; c < kPlanClasses; ++c) {
+        ClassDesc& cd = plan.classes[c];
+        cd.item_off = start[(size_t)c * kBuckets];
+        cd.n_items = start[(size_t)(c + 1) * kBuckets] - cd.item_off;
+        cd.rerun_off = rerun_off;
+        rerun_off += cd.rerun_cap;
+        cd.claim32 = cd.claim64 = cd.rerun_count = 0;
+    }
+    plan.rerun_slots = rerun_off;
+    return PHMM_OK;
+}
+
+}  // namespace phmm

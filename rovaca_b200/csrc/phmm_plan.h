@@ -1,0 +1,47 @@
+// Host-side batch planner: validates a phmm_batch, flags reads/haplotypes containing 'N', and cuts
+// the batch into wavefront work items grouped by kernel class, longest first inside a class.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/phmm_b200.h"
+#include "phmm_types.h"
+
+namespace phmm {
+
+constexpr int kPlanClasses = 18;  // same numbering as phmm_kernels.h
+
+struct PlanLimits {
+    // Reference limits, roDV_schedule.cpp:70-73 (haplotype index <= 4095, read length <= 768,
+    // haplotype length <= 1536).
+    uint32_t max_haps_per_region = 4096;
+    uint32_t max_read_len = 768;
+    uint32_t max_hap_len = 1536;
+    // Longest haplotype column stream of one work item (single-stripe reads), and of a
+    // multi-stripe item (bounded by the per-warp scratch row).
+    uint32_t max_stream_single = 8192;
+    uint32_t max_stream_multi = 4096;
+};
+
+struct Plan {
+    uint32_t n_regions = 0, n_reads = 0, n_haps = 0;
+    uint64_t read_bases = 0, hap_bases = 0, out_total = 0;
+    uint64_t read_base0 = 0, hap_base0 = 0;  // read_off[0], hap_off[0]: the copy starts there
+    uint64_t pairs = 0, cells = 0, empty_pairs = 0;
+    std::vector<RegionDesc> regions;
+    std::vector<uint64_t> read_off, hap_off;  // rebased to start at 0
+    std::vector<uint8_t> read_flags, hap_flags;
+    std::vector<WorkItem> items;
+    std::vector<ClassDesc> classes;  // kPlanClasses
+    uint64_t rerun_slots = 0;
+    uint32_t max_multi_stream = 0;   // longest stream among multi-stripe items (0 if none)
+};
+
+// Returns PHMM_OK, PHMM_ERR_INVALID_ARGUMENT or PHMM_ERR_LIMIT_EXCEEDED (err holds the detail).
+phmm_status build_plan(const phmm_batch& b, const PlanLimits& lim, Plan& plan, std::string& err);
+
+inline int plan_class(int variant, int k, bool multi) { return variant * 9 + (multi ? 8 : k - 1); }
+
+}  // namespace phmm

@@ -1,0 +1,125 @@
+// Plain data types shared by the host planner (g++) and the kernels (nvcc).
+#pragma once
+
+#include <cstdint>
+
+#ifdef __CUDACC__
+#define PHMM_HD __host__ __device__
+#else
+#define PHMM_HD
+#endif
+
+namespace phmm {
+
+constexpr int kWarp = 32;
+constexpr int kMaxK = 8;          // rows per lane in one stripe (stripe = 256 rows)
+constexpr int kCodePad = 64;      // guard codes before/after the haplotype code stream
+constexpr int kChunk = 8;         // steps per boundary-free fast chunk
+
+enum Variant : int { kInter = 0, kIntra = 1 };
+
+struct RegionDesc {               // 32 bytes
+    uint64_t out_off;             // first likelihood of this region in the output
+    uint32_t hap_begin;           // global index of the region's first haplotype
+    uint32_t n_haps;
+    uint32_t read_begin;          // global index of the region's first read
+    uint32_t n_reads;
+    uint32_t pad0, pad1;
+};
+
+struct WorkItem {                 // 16 bytes
+    uint32_t read;                // global read index
+    uint32_t region;
+    uint16_t hap_lo, hap_hi;      // haplotype range inside the region, [lo, hi)
+    uint8_t k;                    // rows per lane
+    uint8_t stripes;              // 32*k-row stripes
+    uint8_t variant;              // Variant
+    uint8_t pad;
+};
+
+struct RerunEntry {               // 16 bytes: one pair whose FP32 sum fell below 1e-28
+    uint64_t out_idx;
+    uint32_t read;                // global read index
+    uint32_t hap;                 // global haplotype index
+};
+
+template <typename T>
+struct ProbTables {               // device copies of the reference's probability tables
+    const T* ph2pr;               // [128] 10^(-q/10)
+    const T* pmat;                // [128] 1 - ph2pr[q]
+    const T* pmis_inter;          // [128] ph2pr[q] * (1/3)
+    const T* pmis_intra;          // [128] ph2pr[q] / 3
+    const T* gapm;                // [128] 1 - ph2pr[c]
+    const T* mm;                  // [128*128] match-to-match, [ins][del]
+};
+
+struct BatchView {
+    const uint8_t* read_bases;
+    const uint8_t* read_q;
+    const uint8_t* read_i;
+    const uint8_t* read_d;
+    const uint8_t* read_c;
+    const uint64_t* read_off;     // [n_reads+1]
+    const uint8_t* read_flags;    // [n_reads] bit0: contains 'N'
+    const uint64_t* hap_off;      // [n_haps+1] offsets into the code streams (without guard)
+    const uint32_t* codes_inter;  // [kCodePad + total + kCodePad]
+    const uint32_t* codes_intra;
+    const uint8_t* hap_flags;     // [n_haps] bit0: contains 'N'
+    const RegionDesc* regions;
+    double* out;
+    uint8_t* pair_flags;          // may be null
+};
+
+// Per-class launch descriptor, in device memory so that a captured launch sequence can be
+// replayed for any batch that fits the arena (the host rewrites the descriptors, not the graph).
+struct ClassDesc {                // 32 bytes
+    uint32_t item_off;            // first work item of the class
+    uint32_t n_items;
+    uint32_t rerun_off;           // first slot of the class's FP64 rerun segment
+    uint32_t rerun_cap;           // = pairs of the class, so the segment cannot overflow
+    uint32_t claim32;             // FP32 claim counter (zeroed before each batch)
+    uint32_t claim64;             // FP64 claim counter
+    uint32_t rerun_count;         // pairs appended to the rerun segment
+    uint32_t pad;
+};
+
+// Batch-wide sizes, in device memory for the same reason.
+struct BatchDesc {
+    uint64_t hap_bases_total;     // haplotype bases (length of the code streams without guards)
+    uint64_t out_total;           // likelihoods in the output
+    uint32_t n_regions, n_reads, n_haps, n_items;
+};
+
+// Status bits a kernel raises instead of touching memory it should not.
+enum StatusBits : unsigned int {
+    kStatusRerunOverflow = 1u,
+    kStatusBadItem = 2u,          // read longer than the class's stripe, or scratch too short
+};
+
+struct PassControl {
+    ClassDesc* cd;                // this class's descriptor
+    const WorkItem* items;        // all work items (class slice at cd->item_off)
+    RerunEntry* rerun;            // all rerun slots (class segment at cd->rerun_off)
+    unsigned int* status;         // StatusBits, OR-ed
+    void* scratch;                // per-warp stripe rows (multi-stripe reads)
+    unsigned int scratch_cols;    // columns per warp scratch row
+};
+
+// Per-byte match codes.  A pair matches at (i, j) when code(read[i]) & code(hap[j]) != 0.
+// Inter variant (pairs without 'N'): raw byte equality, as pairhmm_inter.cpp:166-168 compares
+// bytes; A, C, G, T get one bit each and other letters a distinct bit of their own.
+// Intra variant (pairs with an 'N'): the reference's base classes (common.h:42-55, letters other
+// than A/C/G/T/N fall in A's class) with N matching everything (pairhmm_impl.cpp:26-42).
+PHMM_HD inline uint32_t match_code(uint8_t b, int variant)
+{
+    switch (b) {
+    case 'A': return 1u;
+    case 'C': return 2u;
+    case 'G': return 4u;
+    case 'T': return 8u;
+    case 'N': return variant == kIntra ? 0xffffffffu : (1u << (4 + ('N' % 28)));
+    default: return variant == kIntra ? 1u : (1u << (4 + (b % 28)));
+    }
+}
+
+}  // namespace phmm

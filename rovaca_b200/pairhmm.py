@@ -1,0 +1,308 @@
+"""Python host interface of the B200 PairHMM engine, mirroring the reference's PairHMM entry points.
+
+Reference interfaces mirrored (paths inside the reference project):
+  * ``schedule_pairhmm`` -- the vector API the reference's tests and perf harness drive:
+    ``bool schedule_pairhmm(haplotypes, reads, result, quality, insertion_qualities,
+    deletion_qualities, gap_contiguous_qualities, ...)``, result ``[read][hap]`` log10
+    (src/haplotypecaller/pairhmm/roDV_schedule.h:16-27, roDV_schedule.cpp:154-361).
+  * ``call_pairhmm`` -- the HaplotypeCaller entry point ``DoubleVector2D call_pairhmm(hs, rs,
+    min_quality_threshold, pcr_option, pool)``, result ``[hap][read]`` with poorly modelled reads
+    removed from ``rs`` (src/haplotypecaller/pairhmm/pairhmm_engine.h:14,
+    pairhmm_internal.cpp:576-623).
+  * ``Engine.compute`` -- batched form: many regions in one persistent launch.
+  * ``Engine.submit/poll/wait/cancel`` -- the serving loop (continuous batching).
+
+All computation happens in libphmm_b200.so on the GPU; nothing here computes likelihoods.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import Iterable, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import PCR_MODELS, PhmmError, check
+
+Seq = "bytes | np.ndarray | Sequence[int]"
+
+
+def _u8(x) -> np.ndarray:
+    if isinstance(x, (bytes, bytearray, memoryview)):
+        return np.frombuffer(bytes(x), dtype=np.uint8)
+    if isinstance(x, str):
+        return np.frombuffer(x.encode(), dtype=np.uint8)
+    return np.ascontiguousarray(np.asarray(x, dtype=np.uint8))
+
+
+def _ptr(a: np.ndarray | None):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+@dataclass
+class Region:
+    """One active region: candidate haplotypes and reads with their per-base qualities."""
+
+    haplotypes: list
+    reads: list
+    quality: list
+    insertion_qualities: list
+    deletion_qualities: list
+    gap_contiguous_qualities: list
+
+    @property
+    def n_haps(self) -> int:
+        return len(self.haplotypes)
+
+    @property
+    def n_reads(self) -> int:
+        return len(self.reads)
+
+
+@dataclass
+class PackedBatch:
+    """Regions in the flat, concatenated layout of ``phmm_batch`` (include/phmm_b200.h)."""
+
+    n_haps: np.ndarray      # u32 [n_regions]
+    n_reads: np.ndarray     # u32 [n_regions]
+    hap_bases: np.ndarray   # u8
+    hap_off: np.ndarray     # u64 [sum(n_haps)+1]
+    read_bases: np.ndarray  # u8
+    read_qual: np.ndarray
+    read_ins: np.ndarray
+    read_del: np.ndarray
+    read_gcp: np.ndarray
+    read_off: np.ndarray    # u64 [sum(n_reads)+1]
+    _keep: list = field(default_factory=list, repr=False)
+
+    @property
+    def n_regions(self) -> int:
+        return int(self.n_haps.shape[0])
+
+    @property
+    def out_size(self) -> int:
+        return int(np.sum(self.n_haps.astype(np.uint64) * self.n_reads.astype(np.uint64)))
+
+    def out_offsets(self) -> np.ndarray:
+        """Start of each region's [hap][read] block in the flat output (n_regions+1 entries)."""
+        sizes = self.n_haps.astype(np.uint64) * self.n_reads.astype(np.uint64)
+        return np.concatenate([[0], np.cumsum(sizes)]).astype(np.uint64)
+
+    def cells(self) -> int:
+        """Sum over all pairs of read length x haplotype length."""
+        hl = np.diff(self.hap_off).astype(np.int64)
+        rl = np.diff(self.read_off).astype(np.int64)
+        total, h0, r0 = 0, 0, 0
+        for m, n in zip(self.n_haps.tolist(), self.n_reads.tolist()):
+            total += int(hl[h0:h0 + m].sum()) * int(rl[r0:r0 + n].sum())
+            h0 += m
+            r0 += n
+        return total
+
+    def region(self, g: int) -> Region:
+        """Region g back as sequences (for checks)."""
+        h0 = int(self.n_haps[:g].sum())
+        r0 = int(self.n_reads[:g].sum())
+        m, n = int(self.n_haps[g]), int(self.n_reads[g])
+        hs = [bytes(self.hap_bases[self.hap_off[h]:self.hap_off[h + 1]]) for h in range(h0, h0 + m)]
+        sl = [(int(self.read_off[r]), int(self.read_off[r + 1])) for r in range(r0, r0 + n)]
+        return Region(hs, [bytes(self.read_bases[a:b]) for a, b in sl], [bytes(self.read_qual[a:b]) for a, b in sl],
+                      [bytes(self.read_ins[a:b]) for a, b in sl], [bytes(self.read_del[a:b]) for a, b in sl],
+                      [bytes(self.read_gcp[a:b]) for a, b in sl])
+
+    @classmethod
+    def from_regions(cls, regions: Iterable[Region]) -> "PackedBatch":
+        regions = list(regions)
+        haps = [_u8(h) for r in regions for h in r.haplotypes]
+        reads = [_u8(x) for r in regions for x in r.reads]
+        cat = lambda parts: np.concatenate(parts) if parts else np.zeros(0, np.uint8)
+        qual = [_u8(x) for r in regions for x in r.quality]
+        ins = [_u8(x) for r in regions for x in r.insertion_qualities]
+        dele = [_u8(x) for r in regions for x in r.deletion_qualities]
+        gcp = [_u8(x) for r in regions for x in r.gap_contiguous_qualities]
+        for arr in (qual, ins, dele, gcp):
+            if [len(a) for a in arr] != [len(a) for a in reads]:
+                raise ValueError("every quality array must have its read's length")
+        off = lambda parts: np.concatenate([[0], np.cumsum([len(p) for p in parts])]).astype(np.uint64)
+        return cls(np.array([r.n_haps for r in regions], np.uint32), np.array([r.n_reads for r in regions], np.uint32),
+                   cat(haps), off(haps), cat(reads), cat(qual), cat(ins), cat(dele), cat(gcp), off(reads))
+
+    def pinned(self) -> "PackedBatch":
+        """A copy whose arrays live in page-locked host memory (fast DMA); uses torch for the pinning."""
+        import torch
+
+        def pin(a: np.ndarray) -> np.ndarray:
+            t = torch.empty(a.nbytes, dtype=torch.uint8, pin_memory=True)
+            v = t.numpy().view(a.dtype)[: a.size]
+            v[...] = a
+            keep.append(t)
+            return v
+
+        keep: list = []
+        pb = PackedBatch(*(pin(getattr(self, f)) for f in ("n_haps", "n_reads", "hap_bases", "hap_off", "read_bases",
+                                                           "read_qual", "read_ins", "read_del", "read_gcp", "read_off")))
+        pb._keep = keep
+        return pb
+
+    def subset(self, regions: Sequence[int]) -> "PackedBatch":
+        return PackedBatch.from_regions([self.region(g) for g in regions])
+
+    def as_c(self) -> _lib.Batch:
+        b = _lib.Batch()
+        b.n_regions = self.n_regions
+        b.n_haps = _ptr(self.n_haps)
+        b.n_reads = _ptr(self.n_reads)
+        b.hap_bases = _ptr(self.hap_bases)
+        b.hap_off = _ptr(self.hap_off)
+        b.read_bases = _ptr(self.read_bases)
+        b.read_qual = _ptr(self.read_qual)
+        b.read_ins = _ptr(self.read_ins)
+        b.read_del = _ptr(self.read_del)
+        b.read_gcp = _ptr(self.read_gcp)
+        b.read_off = _ptr(self.read_off)
+        return b
+
+
+class Engine:
+    """One engine per CUDA device (phmm_engine_create)."""
+
+    def __init__(self, device: int = 0, use_cuda_graph: bool = True, autotune: bool = True,
+                 hbm_budget_bytes: int = 0):
+        self._lib = _lib.load()
+        cfg = _lib.Config(device, int(use_cuda_graph), int(autotune), 0, hbm_budget_bytes, 0)
+        h = C.c_void_p()
+        check(self._lib.phmm_engine_create(C.byref(cfg), C.byref(h)))
+        self._h = h
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            check(self._lib.phmm_engine_destroy(self._h))
+            self._h = None
+
+    def __enter__(self) -> "Engine":
+        return self
+
+    def __exit__(self, *exc) -> None:
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def version() -> str:
+        return _lib.load().phmm_version().decode()
+
+    # ---- batched -----------------------------------------------------------------------
+    def compute(self, batch: PackedBatch, want_flags: bool = False, out: np.ndarray | None = None,
+                flags: np.ndarray | None = None):
+        """Every pair of every region; returns (likelihoods, flags or None, stats dict).
+
+        likelihoods is flat: region blocks in order, [hap][read] inside (see PackedBatch.out_offsets)."""
+        n = batch.out_size
+        if out is None:
+            out = np.empty(n, np.float64)
+        if want_flags and flags is None:
+            flags = np.empty(n, np.uint8)
+        st = _lib.Stats()
+        b = batch.as_c()
+        check(self._lib.phmm_compute_regions(self._h, C.byref(b), _ptr(out), _ptr(flags) if want_flags else None,
+                                             C.byref(st)))
+        return out, (flags if want_flags else None), st.as_dict()
+
+    def compute_regions(self, regions: Sequence[Region], want_flags: bool = False):
+        """List of [n_haps][n_reads] arrays, one per region."""
+        pb = PackedBatch.from_regions(regions)
+        out, fl, _ = self.compute(pb, want_flags)
+        offs = pb.out_offsets()
+        res = []
+        for g in range(pb.n_regions):
+            blk = out[offs[g]:offs[g + 1]].reshape(int(pb.n_haps[g]), int(pb.n_reads[g]))
+            res.append(blk if fl is None else (blk, fl[offs[g]:offs[g + 1]].reshape(blk.shape)))
+        return res
+
+    # ---- serving loop ------------------------------------------------------------------
+    def submit(self, region: PackedBatch, out: np.ndarray, flags: np.ndarray | None = None) -> int:
+        """Queues one region (region.n_regions == 1); out (and flags) must stay alive until wait()."""
+        t = C.c_uint64()
+        b = region.as_c()
+        check(self._lib.phmm_submit(self._h, C.byref(b), _ptr(out), _ptr(flags), C.byref(t)))
+        return t.value
+
+    def poll(self, ticket: int) -> bool:
+        d = C.c_int32()
+        check(self._lib.phmm_poll(self._h, ticket, C.byref(d)))
+        return bool(d.value)
+
+    def wait(self, ticket: int, timeout_us: int = -1):
+        """Blocks until done; returns (queued_us, total_us) and releases the ticket."""
+        q, t = C.c_double(), C.c_double()
+        check(self._lib.phmm_wait(self._h, ticket, timeout_us, C.byref(q), C.byref(t)))
+        return q.value, t.value
+
+    def cancel(self, ticket: int) -> None:
+        check(self._lib.phmm_cancel(self._h, ticket))
+
+    # ---- region API ----------------------------------------------------------------------
+    def call_region(self, haplotypes, reads, base_quals, mapq, min_quality_threshold: int = 18,
+                    pcr_option: str | int = "CONSERVATIVE"):
+        """call_pairhmm semantics; returns (matrix [n_haps][n_reads] with kept reads first, keep mask)."""
+        pcr = PCR_MODELS[pcr_option] if isinstance(pcr_option, str) else int(pcr_option)
+        hs = [_u8(h) for h in haplotypes]
+        rs = [_u8(r) for r in reads]
+        qs = [_u8(q) for q in base_quals]
+        cat = lambda parts: np.concatenate(parts) if parts else np.zeros(1, np.uint8)
+        off = lambda parts: np.concatenate([[0], np.cumsum([len(p) for p in parts])]).astype(np.uint64)
+        hb, hoff, rb, roff, qb = cat(hs), off(hs), cat(rs), off(rs), cat(qs)
+        mq = np.ascontiguousarray(np.asarray(mapq, np.uint8).reshape(-1))
+        if mq.size == 1 and len(rs) > 1:
+            mq = np.full(len(rs), mq[0], np.uint8)
+        out = np.empty(len(hs) * len(rs), np.float64)
+        keep = np.empty(len(rs), np.uint8)
+        nk = C.c_uint32()
+        st = self._lib.phmm_call_region(self._h, len(hs), _ptr(hb), _ptr(hoff), len(rs), _ptr(rb), _ptr(qb), _ptr(roff),
+                                        _ptr(mq), int(min_quality_threshold), pcr, _ptr(out), _ptr(keep), C.byref(nk))
+        check(st)
+        return out.reshape(len(hs), len(rs)), keep.astype(bool)
+
+
+_default_engine: Engine | None = None
+
+
+def default_engine() -> Engine:
+    global _default_engine
+    if _default_engine is None:
+        _default_engine = Engine()
+    return _default_engine
+
+
+def schedule_pairhmm(haplotypes, reads, quality, insertion_qualities, deletion_qualities, gap_contiguous_qualities,
+                     engine: Engine | None = None):
+    """Vector-API mirror: returns (ok, result) with result[read][hap] log10 likelihoods.
+
+    Like the reference, no quality capping or PCR model is applied; ok is False (and result
+    empty) when there are no haplotypes or no reads (roDV_schedule.cpp:179-181)."""
+    if len(haplotypes) == 0 or len(reads) == 0:
+        return False, np.zeros((0, 0))
+    eng = engine or default_engine()
+    reg = Region(list(haplotypes), list(reads), list(quality), list(insertion_qualities), list(deletion_qualities),
+                 list(gap_contiguous_qualities))
+    (mat,) = eng.compute_regions([reg])
+    return True, np.ascontiguousarray(mat.T)
+
+
+def call_pairhmm(haplotypes, reads, base_quals, mapq, min_quality_threshold: int = 18,
+                 pcr_option: str | int = "CONSERVATIVE", engine: Engine | None = None):
+    """HaplotypeCaller entry-point mirror: returns (result [hap][read], kept read indices).
+
+    As in the reference, result has one column per input read; the first len(kept) columns hold the
+    kept reads in order, the rest are NaN, and the caller erases the other reads."""
+    eng = engine or default_engine()
+    mat, keep = eng.call_region(haplotypes, reads, base_quals, mapq, min_quality_threshold, pcr_option)
+    return mat, np.nonzero(keep)[0]
+
+
+__all__ = ["Engine", "Region", "PackedBatch", "PhmmError", "schedule_pairhmm", "call_pairhmm", "default_engine"]
