@@ -1,0 +1,417 @@
+#!/usr/bin/env python
+"""PairHMM benchmark on one node: GCUPS of the batched engine on the 2,000-region uneven workload.
+
+One step = the whole PairHMM path over one batch of 2,000 active regions (reads U[10,500] of
+100-250 bp, 2-32 haplotypes of 150-600 bp; seeded synthetic data): the FP32 wavefront pass over
+every read x haplotype pair and the FP64 recompute of the pairs whose FP32 sum falls below 1e-28.
+
+  value      batched GCUPS with the batch already in HBM (device pipeline replayed, CUDA events)
+  e2e        the same through phmm_compute_regions from pinned host buffers (H2D of all reads and
+             haplotypes and D2H of all likelihoods inside every step)
+  plain      one region per call (the one-region-per-launch form), for the batched/plain ratio
+  latency    p50/p99 region latency of the serving loop under Poisson arrivals at 80% of capacity
+  roofline   the FP32 wavefront pass: 12 FLOP per cell against the device's measured FP32 FMA peak
+  cpu_baseline  the reference's own AVX PairHMM (compiled from its sources) on all host cores
+
+Multi-GPU: one process per GPU (torchrun); every rank runs its own 2,000 regions (regions are
+independent: weak scaling, no collective on the data path); value = all ranks' cells / max time.
+`--impl reference` times the reference's CPU implementation instead (rank 0 only).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from concurrent.futures import ThreadPoolExecutor
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "PairHMM GCUPS batched vs plain per-region, 1 B200, ≤1e-4 log10 err; p99 latency"
+WORKLOAD = ("2,000 batched uneven active regions in one launch sequence: reads U[10,500] per region of "
+            "length U[100,250], base quality Phred U[2,41], ins/del 45, GCP 10, 1% substitution errors; "
+            "haplotypes U[2,32] per region of 150-600 bp (SNP/indel edits of one window); FP32 with "
+            "FP64 recompute below 1e-28")
+FLOP_PER_CELL = 12  # 8 multiplies + 4 adds per cell (M, I, D updates)
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled every 200 ms while active."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait(5)
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[4:8]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def traffic_from_profiles() -> float | None:
+    """DRAM bytes per FP32-pass launch from the committed ncu summary (None if not captured)."""
+    p = ROOT / "profiles" / "fwd_f32_config1.md"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.strip().startswith("traffic_bytes_per_pass:"):
+            try:
+                return float(line.split(":", 1)[1].strip().split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+# ---- reference CPU arm -----------------------------------------------------------------------
+
+def reference_gcups(batch, regions, threads: int) -> tuple[float, float]:
+    """Runs the reference's schedule_pairhmm (AVX path) over `regions`, one region per worker thread
+    like HaplotypeCaller's region pool; returns (GCUPS, seconds)."""
+    from oracle import Ref
+
+    ref = Ref()
+    cells = sum(batch.subset([g]).cells() for g in regions)
+
+    def work(g):
+        return ref.schedule_region(batch, g, 0.02, 0.02)
+
+    with ThreadPoolExecutor(max_workers=threads, initializer=ref.init_thread) as ex:
+        t = time.perf_counter()
+        list(ex.map(work, regions))
+        dt = time.perf_counter() - t
+    return cells / dt / 1e9, dt
+
+
+def run_reference(args, rank: int, world: int) -> None:
+    if rank != 0:
+        return
+    from oracle import ref_available
+    from rovaca_b200 import synth
+
+    if not ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libphmm_ref.so was not built "
+                          "(needs the reference sources and oracle/build_ref.sh)"}), flush=True)
+        return
+    batch = synth.config1(seed=1)
+    cores = os.cpu_count() or 1
+    sample = list(range(64))
+    for _ in range(args.warmup):
+        reference_gcups(batch, sample[:8], cores)
+    times, cells = [], sum(batch.subset([g]).cells() for g in sample)
+    for _ in range(args.steps):
+        _, dt = reference_gcups(batch, sample, cores)
+        times.append(dt)
+    gcups = cells * len(times) / sum(times) / 1e9
+    line = {
+        "metric": METRIC, "value": round(gcups, 3), "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(1e3 * sum(times) / len(times), 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 recompute)", "data": "synthetic (seeded)",
+        "impl": "reference",
+        "config": {"workload": WORKLOAD, "regions_per_step": len(sample), "cells_per_step": cells},
+        "cpu_baseline": {"value": round(gcups, 3), "unit": "GCUPS", "cores": cores, "kind": "reference",
+                         "sample": f"regions 0-{len(sample) - 1} of the 2,000-region batch per step, one region "
+                                   "per thread, reference schedule_pairhmm (AVX-512 path when available)"},
+        "e2e": {"value": round(gcups, 3), "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---- our arm ----------------------------------------------------------------------------------
+
+def serving_latency(engine, batch, load: float, capacity_regions_per_s: float, seconds: float, seed: int):
+    """Poisson arrivals of the batch's regions at `load` x capacity; returns latency percentiles and
+    the sustained GCUPS of the completed requests."""
+    rng = np.random.default_rng(seed)
+    regions = [batch.subset([g]) for g in range(min(batch.n_regions, 400))]
+    cells = [r.cells() for r in regions]
+    rate = load * capacity_regions_per_s
+    outs, tickets, done_cells = [], [], 0
+    t0 = time.perf_counter()
+    next_t = t0
+    k = 0
+    while next_t - t0 < seconds:
+        now = time.perf_counter()
+        if now < next_t:
+            time.sleep(min(next_t - now, 0.002))
+            continue
+        r = regions[k % len(regions)]
+        out = np.empty(r.out_size)
+        tickets.append((engine.submit(r, out), k % len(regions)))
+        outs.append(out)
+        k += 1
+        next_t += rng.exponential(1.0 / rate)
+    lat = []
+    for t, g in tickets:
+        _, total_us = engine.wait(t)
+        lat.append(total_us / 1e3)
+        done_cells += cells[g]
+    elapsed = time.perf_counter() - t0
+    lat = np.array(lat)
+    return {"load": load, "offered_regions_per_s": round(rate, 1), "requests": len(lat),
+            "p50_ms": round(float(np.percentile(lat, 50)), 3), "p99_ms": round(float(np.percentile(lat, 99)), 3),
+            "sustained_gcups": round(done_cells / elapsed / 1e9, 2)}
+
+
+def run_resident_only(args) -> None:
+    """Profiling mode: only the device-resident replay (the launches the ncu summaries cover)."""
+    import torch
+
+    from rovaca_b200 import Engine, synth
+
+    torch.cuda.set_device(0)
+    batch = synth.config1(seed=1)
+    with Engine(device=0, use_cuda_graph=not args.no_graph) as engine:
+        with engine.resident(batch) as res:
+            res.run(args.warmup)
+            st = res.run(args.steps)
+    print(json.dumps({"mode": "resident", "graph": not args.no_graph, "steps": args.steps,
+                      "ms_per_step": st["device_ms"] / args.steps, "fp32_pass_ms": st["fp32_ms"],
+                      "fp64_pass_ms": st["fp64_ms"], "gcups": batch.cells() * args.steps / st["device_ms"] / 1e6,
+                      "kernel_launches": st["kernel_launches"]}), flush=True)
+
+
+def run_ours(args, rank: int, world: int, dist) -> None:
+    import torch
+
+    from rovaca_b200 import Engine, synth
+
+    device = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(device)
+    batch = synth.config1(seed=1 + rank)
+    cells = batch.cells()
+    engine = Engine(device=device, use_cuda_graph=not args.no_graph)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{device}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{device}")
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
+    # device-resident batched throughput
+    res = engine.resident(batch, want_flags=True)
+    res.run(args.warmup)
+    barrier()
+    with ClockSampler(device) as clk:
+        st = res.run(args.steps)
+        barrier()
+    dev_ms = max_over_ranks(st["device_ms"])
+    ms_per_step = dev_ms / args.steps
+    total_cells = sum_over_ranks(float(cells)) * args.steps
+    value = total_cells / (dev_ms / 1e3) / 1e9
+    fp32_pass_ms = max_over_ranks(st["fp32_ms"])
+    out, flags = res.results()
+    res.close()
+    f64_frac = float(flags.mean())
+    launches = int(st["kernel_launches"])
+
+    # end to end through the public API, pinned host buffers
+    pinned = batch.pinned()
+    out_e2e = np.empty(batch.out_size)
+    for _ in range(args.warmup):
+        engine.compute(pinned, out=out_e2e)
+    barrier()
+    with ClockSampler(device) as clk_e2e:
+        t = time.perf_counter()
+        for _ in range(args.steps):
+            engine.compute(pinned, out=out_e2e)
+        barrier()
+        e2e_s = max_over_ranks(time.perf_counter() - t)
+    e2e = total_cells / e2e_s / 1e9
+    same = bool(np.array_equal(out_e2e, out))
+    h2d = int(batch.read_bases.size * 5 + batch.hap_bases.size + batch.read_off.nbytes + batch.hap_off.nbytes +
+              batch.n_haps.nbytes + batch.n_reads.nbytes)
+    d2h = int(batch.out_size * 8)
+
+    line = None
+    if rank == 0:
+        # plain: one region per call, on a sample of regions
+        plain_regions = [pinned.subset([g]).pinned() for g in range(200)]
+        plain_cells = sum(r.cells() for r in plain_regions)
+        for r in plain_regions[:10]:
+            engine.compute(r)
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        plain_dev_ms = 0.0
+        for r in plain_regions:
+            _, _, s = engine.compute(r)
+            plain_dev_ms += s["device_ms"]
+        plain_s = time.perf_counter() - t
+        plain = plain_cells / plain_s / 1e9
+        plain_dev = plain_cells / (plain_dev_ms / 1e3) / 1e9
+
+        # accuracy on a seeded sample of regions against the all-FP64 oracle
+        from oracle import Oracle
+
+        orc = Oracle()
+        offs = batch.out_offsets()
+        sample = [3, 1000, 1997]
+        f64, _ = orc.batch(batch.subset(sample), fp64_only=True)
+        got = np.concatenate([out[offs[g]:offs[g + 1]] for g in sample])
+        max_err = float(np.max(np.abs(got - f64)))
+
+        # serving loop latency
+        cap = batch.n_regions / (e2e_s / args.steps)
+        lat = serving_latency(engine, batch, 0.8, cap, args.serve_seconds, seed=rank)
+
+        # roofline of the FP32 wavefront pass against the measured FP32 FMA peak
+        peak = engine.fp32_fma_peak()
+        achieved = cells * FLOP_PER_CELL / (st["fp32_ms"] / 1e3) / 1e12
+        traffic = traffic_from_profiles()
+
+        # CPU baseline: the reference's own PairHMM on all host cores, bounded sample
+        cpu = None
+        if world == 1:
+            from oracle import ref_available
+
+            cores = os.cpu_count() or 1
+            if ref_available():
+                sample_regions = list(range(64))
+                reference_gcups(batch, sample_regions[:4], cores)
+                g, dt = reference_gcups(batch, sample_regions, cores)
+                cpu = {"value": round(g, 3), "unit": "GCUPS", "cores": cores, "kind": "reference",
+                       "sample": f"regions 0-63 of the batch ({dt:.1f} s), one region per thread, reference "
+                                 "schedule_pairhmm AVX path compiled from its sources"}
+            else:
+                t = time.perf_counter()
+                sub = batch.subset([0, 1, 2, 3])
+                orc.batch(sub)
+                dt = time.perf_counter() - t
+                cpu = {"value": round(sub.cells() / dt / 1e9, 3), "unit": "GCUPS", "cores": 1, "kind": "port",
+                       "sample": "regions 0-3 through the scalar oracle (reference build unavailable)"}
+
+        clocks = clk.summary()
+        line = {
+            "metric": METRIC, "value": round(value, 2), "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 recompute)",
+            "data": "synthetic (seeded generator, one 2,000-region batch per rank)",
+            "config": {"workload": WORKLOAD, "regions": batch.n_regions, "pairs": int(batch.out_size),
+                       "cells_per_rank": int(cells), "l2": "inputs (~540 MB) larger than the 126 MB L2; no flush",
+                       "parallelism": f"regions sharded per rank x{world}, no collective"},
+            "e2e": {"value": round(e2e, 2), "unit": "GCUPS", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "ms_per_step": round(1e3 * e2e_s / args.steps, 3), "results_identical_to_resident": same},
+            "gpu_launches": launches,
+            "roofline": {"bound": "fp32", "achieved": round(achieved, 2), "peak": round(peak, 2), "unit": "TFLOP/s",
+                         "frac": round(achieved / peak, 4), "traffic": traffic,
+                         "kernel": "FP32 wavefront pass (fwd_f32 class kernels + prep), 12 FLOP/cell",
+                         "peak_source": "measured FP32 FMA throughput (phmm_fp32_fma_peak, 2 FLOP per FMA)"},
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+            "clocks_e2e": clk_e2e.summary(),
+            "plain": {"gcups_e2e": round(plain, 2), "gcups_device": round(plain_dev, 2), "regions": len(plain_regions),
+                      "form": "one region per phmm_compute_regions call"},
+            "batched_vs_plain": {"e2e": round(e2e / plain, 2), "device": round(value / world / plain_dev, 2)},
+            "fp32_pass_ms": round(fp32_pass_ms, 3),
+            "fp64_rerun_fraction": round(f64_frac, 5),
+            "max_abs_err_log10_vs_fp64": max_err,
+            "latency": lat,
+        }
+    engine.close()
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--serve-seconds", type=float, default=6.0)
+    ap.add_argument("--only", choices=["all", "resident"], default="all",
+                    help="resident: only the device-resident replay (for profiling)")
+    ap.add_argument("--no-graph", action="store_true", help="direct launches instead of CUDA-graph replay")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be at least 3")
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as tdist
+
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist = tdist
+    try:
+        if args.only == "resident":
+            run_resident_only(args)
+        elif args.impl == "reference":
+            run_reference(args, rank, world)
+        else:
+            run_ours(args, rank, world, dist)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

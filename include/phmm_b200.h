@@ -94,9 +94,10 @@ typedef struct phmm_stats {
     uint64_t work_items;    /* wavefront work items of the FP32 pass */
     uint64_t h2d_bytes;
     uint64_t d2h_bytes;
+    uint64_t kernel_launches; /* kernels this library launched for the call */
     double device_ms;       /* CUDA-event time of the device pipeline (prep + FP32 + FP64) */
-    double fp32_ms;         /* CUDA-event time of the FP32 wavefront kernel alone */
-    double fp64_ms;         /* CUDA-event time of the FP64 recompute kernel alone */
+    double fp32_ms;         /* CUDA-event time of the FP32 wavefront pass (prep included) */
+    double fp64_ms;         /* CUDA-event time of the FP64 recompute pass */
     double host_ms;         /* wall time of the whole call */
 } phmm_stats;
 
@@ -139,6 +140,25 @@ PHMM_API phmm_status phmm_call_region(phmm_engine* engine, uint32_t n_haps, cons
                              const uint64_t* read_off, const uint8_t* mapq, int32_t min_quality_threshold,
                              int32_t pcr_model, double* out, uint8_t* keep, uint32_t* n_kept);
 
+/* ---- device-resident batches ------------------------------------------------------------ */
+
+typedef struct phmm_resident phmm_resident;
+
+/* Uploads a batch once into a device arena of its own (reads and haplotypes stay in HBM). */
+PHMM_API phmm_status phmm_resident_create(phmm_engine* engine, const phmm_batch* batch, int32_t want_flags,
+                                          phmm_resident** out_resident);
+/* Recomputes the resident batch `iterations` times back to back with no host transfer; stats
+ * (optional) report the device time of all iterations together (CUDA events on the engine's
+ * stream) and the kernels launched. */
+PHMM_API phmm_status phmm_resident_run(phmm_resident* resident, int32_t iterations, phmm_stats* stats);
+/* Copies the latest results to the host (layout of phmm_compute_regions; flags may be NULL). */
+PHMM_API phmm_status phmm_resident_results(phmm_resident* resident, double* out, uint8_t* pair_flags);
+PHMM_API phmm_status phmm_resident_destroy(phmm_resident* resident);
+
+/* Measures the device's FP32 FMA throughput (independent FMA chains on every SM, about 50 ms),
+ * in TFLOP/s counting an FMA as 2 FLOPs: the peak the wavefront kernels are compared with. */
+PHMM_API phmm_status phmm_fp32_fma_peak(phmm_engine* engine, double* tflops);
+
 /* ---- host-only pieces of the region path (no GPU involved) ----------------------------- */
 
 /* Base qualities as the region API prepares them: min(q, mapq), below the threshold -> 6
@@ -153,6 +173,13 @@ PHMM_API int32_t phmm_host_tandem_repeat_length(const uint8_t* bases, uint32_t n
  * drop poorly modelled reads, compact kept reads into the first columns (NaN after them). */
 PHMM_API void phmm_host_normalize_filter(const double* lk_hap_read, uint32_t n_haps, uint32_t n_reads, const uint64_t* read_len,
                                 double* out, uint8_t* keep, uint32_t* n_kept);
+
+/* How a batch is cut into wavefront work, without running it (no GPU involved): per kernel class
+ * (class = variant * 9 + (read longer than 256 ? 8 : rows per lane - 1), variant 0 for pairs
+ * without 'N', 1 with), the number of work items and of pairs; and the batch's pairs and cells.
+ * Returns the same validation status phmm_compute_regions would. */
+PHMM_API phmm_status phmm_host_plan_summary(const phmm_batch* batch, uint32_t class_items[18], uint64_t class_pairs[18],
+                                            uint64_t* pairs, uint64_t* cells);
 
 /* ---- serving loop ----------------------------------------------------------------------- */
 

@@ -44,7 +44,10 @@ for isa in avx2 avx512; do
     cc "ref_kernels_$isa.o" "$HERE/ref_kernels.cpp" "${F[@]}"
 done
 cc schedule.o "$P/roDV_schedule.cpp" -mavx -mavx2
+cc internal.o "$P/pairhmm_internal.cpp" -mavx -mavx2
+cc memory_pool.o "$REF/src/haplotypecaller/common/utils/rovaca_memory_pool.cpp"
 cc ref_shim.o "$HERE/ref_shim.cpp" -mavx -mavx2
+cc ref_region.o "$HERE/ref_region.cpp" -mavx -mavx2
 cc ref_unreached.o "$HERE/ref_unreached.cpp" -mavx -mavx2
 wait
 g++ -shared -o "$OUT/libphmm_ref.so" "$TMP"/*.o -Wl,--no-undefined -lm

@@ -45,7 +45,8 @@ def build_ref(reference_root: str = "/root/reference") -> Path | None:
     """Builds oracle/_ref from the reference sources when they are present; returns the library."""
     if not Path(reference_root, "src/haplotypecaller/pairhmm").is_dir():
         return REF_LIB if REF_LIB.exists() else None
-    srcs = [HERE / "ref_shim.cpp", HERE / "ref_kernels.cpp", HERE / "ref_unreached.cpp", HERE / "build_ref.sh"]
+    srcs = [HERE / "ref_shim.cpp", HERE / "ref_kernels.cpp", HERE / "ref_region.cpp", HERE / "ref_unreached.cpp",
+            HERE / "build_ref.sh"]
     if REF_LIB.exists() and all(REF_LIB.stat().st_mtime >= s.stat().st_mtime for s in srcs):
         return REF_LIB
     subprocess.run(["bash", str(HERE / "build_ref.sh"), reference_root], check=True)

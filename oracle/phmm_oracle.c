@@ -300,11 +300,21 @@ static const float MIN_ACCEPTED = 1e-28f;                   /* roDV_schedule.cpp
 double oracle_log10_from_f32(float raw) { return log10((double)raw) - (double)LOG10_C_F; }
 double oracle_log10_from_f64(double raw) { return log10(raw) - LOG10_C_D; }
 
-/* All-FP64 oracle: log10 likelihood computed in double end to end (unfused, inter prior). */
+static int any_n(const uint8_t* p, uint32_t n)
+{
+    for (uint32_t i = 0; i < n; i++)
+        if (p[i] == 'N') return 1;
+    return 0;
+}
+
+/* All-FP64 oracle: log10 likelihood computed in double end to end with plain multiply/add.  A pair
+ * with an 'N' in its read or haplotype uses the model the reference applies to it (N matches
+ * every base, intra prior); other pairs the inter prior. */
 double oracle_log10_f64(const uint8_t* hap, uint32_t hl, const uint8_t* rd, uint32_t rl, const uint8_t* q,
                         const uint8_t* iq, const uint8_t* dq, const uint8_t* cq)
 {
-    return oracle_log10_from_f64(oracle_raw_f64(hap, hl, rd, rl, q, iq, dq, cq, ORACLE_INTER, ORACLE_UNFUSED));
+    const int kernel = (any_n(hap, hl) || any_n(rd, rl)) ? ORACLE_INTRA : ORACLE_INTER;
+    return oracle_log10_from_f64(oracle_raw_f64(hap, hl, rd, rl, q, iq, dq, cq, kernel, ORACLE_UNFUSED));
 }
 
 /* One pair with the reference's FP32 -> FP64 switch; *used_f64 reports which precision won. */

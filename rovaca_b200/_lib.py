@@ -45,7 +45,8 @@ class Batch(C.Structure):
 class Stats(C.Structure):
     _fields_ = [("regions", C.c_uint64), ("pairs", C.c_uint64), ("cells", C.c_uint64), ("pairs_f64", C.c_uint64),
                 ("work_items", C.c_uint64), ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64),
-                ("device_ms", C.c_double), ("fp32_ms", C.c_double), ("fp64_ms", C.c_double), ("host_ms", C.c_double)]
+                ("kernel_launches", C.c_uint64), ("device_ms", C.c_double), ("fp32_ms", C.c_double),
+                ("fp64_ms", C.c_double), ("host_ms", C.c_double)]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -75,6 +76,12 @@ def load() -> C.CDLL:
         "phmm_host_pcr_model": (None, [P, U32, P, I32]),
         "phmm_host_tandem_repeat_length": (I32, [P, U32, U32]),
         "phmm_host_normalize_filter": (None, [P, U32, U32, P, P, P, C.POINTER(U32)]),
+        "phmm_resident_create": (I32, [P, C.POINTER(Batch), I32, C.POINTER(P)]),
+        "phmm_resident_run": (I32, [P, I32, C.POINTER(Stats)]),
+        "phmm_resident_results": (I32, [P, P, P]),
+        "phmm_resident_destroy": (I32, [P]),
+        "phmm_fp32_fma_peak": (I32, [P, C.POINTER(D)]),
+        "phmm_host_plan_summary": (I32, [C.POINTER(Batch), P, P, C.POINTER(U64), C.POINTER(U64)]),
         "phmm_submit": (I32, [P, C.POINTER(Batch), P, P, C.POINTER(U64)]),
         "phmm_poll": (I32, [P, U64, C.POINTER(I32)]),
         "phmm_wait": (I32, [P, U64, I64, C.POINTER(D), C.POINTER(D)]),

@@ -7,6 +7,7 @@
 #include "../../include/phmm_b200.h"
 #include "phmm_capi_internal.h"
 #include "phmm_engine.h"
+#include "phmm_plan.h"
 
 namespace phmm {
 
@@ -108,6 +109,148 @@ phmm_status phmm_compute_regions(phmm_engine* engine, const phmm_batch* batch, d
     std::string err;
     phmm_status st = phmm::engine_of(engine)->compute(*batch, out, pair_flags, stats, err);
     if (st != PHMM_OK) return set_error(st, err);
+    return PHMM_OK;
+    PHMM_GUARD_END
+}
+
+}  // extern "C"
+
+struct phmm_resident {
+    phmm::Engine* eng = nullptr;
+    phmm::Slot* slot = nullptr;
+    phmm::Plan plan;
+    bool flags = false;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+};
+
+extern "C" {
+
+phmm_status phmm_resident_destroy(phmm_resident* r)
+{
+    PHMM_GUARD_BEGIN
+    phmm::clear_error();
+    if (!r) return set_error(PHMM_ERR_INVALID_ARGUMENT, "resident is null");
+    if (r->eng) cudaSetDevice(r->eng->device());
+    if (r->e0) cudaEventDestroy(r->e0);
+    if (r->e1) cudaEventDestroy(r->e1);
+    if (r->slot) r->eng->free_slot(r->slot);
+    delete r;
+    return PHMM_OK;
+    PHMM_GUARD_END
+}
+
+phmm_status phmm_resident_create(phmm_engine* engine, const phmm_batch* batch, int32_t want_flags,
+                                 phmm_resident** out_resident)
+{
+    PHMM_GUARD_BEGIN
+    phmm::clear_error();
+    if (!engine) return set_error(PHMM_ERR_NOT_INITIALIZED, "engine is null");
+    if (!batch || !out_resident) return set_error(PHMM_ERR_INVALID_ARGUMENT, "batch or out_resident is null");
+    *out_resident = nullptr;
+    auto* r = new phmm_resident();
+    r->eng = phmm::engine_of(engine);
+    r->flags = want_flags != 0;
+    std::string err;
+    phmm_status st = phmm::build_plan(*batch, phmm::PlanLimits(), r->plan, err);
+    if (st == PHMM_OK) st = r->eng->make_slot(1000, &r->slot, err);
+    if (st == PHMM_OK && (cudaEventCreate(&r->e0) != cudaSuccess || cudaEventCreate(&r->e1) != cudaSuccess)) {
+        err = "event creation failed";
+        st = PHMM_ERR_CUDA;
+    }
+    if (st == PHMM_OK) st = r->eng->upload(*r->slot, r->plan, *batch, err);
+    if (st == PHMM_OK) st = r->eng->run(*r->slot, r->plan, r->flags, false, err);
+    if (st == PHMM_OK && cudaStreamSynchronize(r->slot->main) != cudaSuccess) {
+        err = std::string("first run failed: ") + cudaGetErrorString(cudaGetLastError());
+        st = PHMM_ERR_CUDA;
+    }
+    if (st != PHMM_OK) {
+        phmm_resident_destroy(r);
+        return set_error(st, err);
+    }
+    *out_resident = r;
+    return PHMM_OK;
+    PHMM_GUARD_END
+}
+
+phmm_status phmm_resident_run(phmm_resident* r, int32_t iterations, phmm_stats* stats)
+{
+    PHMM_GUARD_BEGIN
+    phmm::clear_error();
+    if (!r || !r->slot) return set_error(PHMM_ERR_INVALID_ARGUMENT, "resident is null");
+    if (iterations < 1) return set_error(PHMM_ERR_INVALID_ARGUMENT, "iterations < 1");
+    std::string err;
+    cudaSetDevice(r->eng->device());
+    cudaStream_t m = r->slot->main;
+    if (cudaEventRecord(r->e0, m) != cudaSuccess) return set_error(PHMM_ERR_CUDA, "event record failed");
+    for (int i = 0; i < iterations; ++i) {
+        phmm_status st = r->eng->run(*r->slot, r->plan, r->flags, true, err);
+        if (st != PHMM_OK) return set_error(st, err);
+    }
+    cudaEventRecord(r->e1, m);
+    cudaError_t e = cudaEventSynchronize(r->e1);
+    if (e != cudaSuccess) return set_error(PHMM_ERR_CUDA, std::string("resident run: ") + cudaGetErrorString(e));
+    if (stats) {
+        float ms = 0, f32 = 0, f64 = 0;
+        cudaEventElapsedTime(&ms, r->e0, r->e1);
+        cudaEventElapsedTime(&f32, r->slot->ev_t0, r->slot->ev_t1);
+        cudaEventElapsedTime(&f64, r->slot->ev_t1, r->slot->ev_t2);
+        *stats = phmm_stats{};
+        stats->regions = r->plan.n_regions;
+        stats->pairs = r->plan.pairs * (uint64_t)iterations;
+        stats->cells = r->plan.cells * (uint64_t)iterations;
+        stats->work_items = r->plan.items.size();
+        stats->kernel_launches = r->slot->launches * (uint64_t)iterations;
+        stats->device_ms = ms;
+        stats->fp32_ms = f32;  // last iteration
+        stats->fp64_ms = f64;  // last iteration
+    }
+    return PHMM_OK;
+    PHMM_GUARD_END
+}
+
+phmm_status phmm_resident_results(phmm_resident* r, double* out, uint8_t* pair_flags)
+{
+    PHMM_GUARD_BEGIN
+    phmm::clear_error();
+    if (!r || !r->slot) return set_error(PHMM_ERR_INVALID_ARGUMENT, "resident is null");
+    if (pair_flags && !r->flags) return set_error(PHMM_ERR_INVALID_ARGUMENT, "resident batch was created without flags");
+    if (r->plan.out_total && !out) return set_error(PHMM_ERR_INVALID_ARGUMENT, "out is null");
+    std::string err;
+    cudaSetDevice(r->eng->device());
+    phmm_stats st{};
+    phmm_status s = r->eng->finish(*r->slot, r->plan, out, pair_flags, &st, err);
+    return s == PHMM_OK ? PHMM_OK : set_error(s, err);
+    PHMM_GUARD_END
+}
+
+phmm_status phmm_fp32_fma_peak(phmm_engine* engine, double* tflops)
+{
+    PHMM_GUARD_BEGIN
+    phmm::clear_error();
+    if (!engine) return set_error(PHMM_ERR_NOT_INITIALIZED, "engine is null");
+    if (!tflops) return set_error(PHMM_ERR_INVALID_ARGUMENT, "tflops is null");
+    std::string err;
+    phmm_status st = phmm::engine_of(engine)->fp32_fma_peak(tflops, err);
+    return st == PHMM_OK ? PHMM_OK : set_error(st, err);
+    PHMM_GUARD_END
+}
+
+phmm_status phmm_host_plan_summary(const phmm_batch* batch, uint32_t class_items[18], uint64_t class_pairs[18],
+                                   uint64_t* pairs, uint64_t* cells)
+{
+    PHMM_GUARD_BEGIN
+    phmm::clear_error();
+    if (!batch) return set_error(PHMM_ERR_INVALID_ARGUMENT, "batch is null");
+    phmm::Plan plan;
+    std::string err;
+    phmm_status st = phmm::build_plan(*batch, phmm::PlanLimits(), plan, err);
+    if (st != PHMM_OK) return set_error(st, err);
+    for (int c = 0; c < phmm::kPlanClasses; ++c) {
+        if (class_items) class_items[c] = plan.classes[c].n_items;
+        if (class_pairs) class_pairs[c] = plan.classes[c].rerun_cap;
+    }
+    if (pairs) *pairs = plan.pairs;
+    if (cells) *cells = plan.cells;
     return PHMM_OK;
     PHMM_GUARD_END
 }

@@ -44,6 +44,7 @@ size_t carve(const Capacity& c, char* base, Slot* s)
         return base ? base + at : nullptr;
     };
     char* desc = take(kDescBytes);
+    char* desc_pristine = take(kDescBytes);
     char* regions = take(c.regions * sizeof(RegionDesc));
     char* read_off = take((c.reads + 1) * sizeof(uint64_t));
     char* hap_off = take((c.haps + 1) * sizeof(uint64_t));
@@ -64,6 +65,7 @@ size_t carve(const Capacity& c, char* base, Slot* s)
     char* scratch = take(c.scratch_cols * 3 * sizeof(double));  // c.scratch_cols counts all warps' columns
     if (s) {
         s->d_desc = (BatchDesc*)desc;
+        s->d_desc_pristine = desc_pristine;
         s->d_classes = (ClassDesc*)(desc + sizeof(BatchDesc));
         s->d_status = (unsigned int*)(desc + sizeof(BatchDesc) + sizeof(ClassDesc) * kNumClasses);
         s->d_regions = (RegionDesc*)regions;
@@ -355,8 +357,10 @@ phmm_status Engine::launch_pipeline(Slot& s, bool want_flags, const Plan* plan, 
     const unsigned int scr_cols = s.cap.scratch_cols ? (unsigned int)(s.cap.scratch_cols / warps) : 0u;
     const unsigned int rec = plan ? cudaEventRecordDefault : cudaEventRecordExternal;
 
+    s.launches = 0;
     PHMM_CK(cudaEventRecordWithFlags(s.ev_t0, s.main, rec));
     PHMM_CK(launch_prep(s.d_desc, s.d_hb, s.d_codes_inter, s.d_codes_intra, s.d_out, v.pair_flags, sms_, s.main));
+    s.launches += 2;
     for (int pass = 0; pass < 2; ++pass) {
         const int precision = pass == 0 ? 32 : 64;
         PHMM_CK(cudaEventRecord(s.ev_fork, s.main));
@@ -376,6 +380,7 @@ phmm_status Engine::launch_pipeline(Slot& s, bool want_flags, const Plan* plan, 
             pc.scratch_cols = scr_cols;
             PHMM_CK(cudaStreamWaitEvent(s.side[c], s.ev_fork, 0));
             PHMM_CK(launch_fwd(precision, c, v, tf_, td_, pc, grid, s.side[c]));
+            ++s.launches;
             PHMM_CK(cudaEventRecord(s.ev_side[c], s.side[c]));
             PHMM_CK(cudaStreamWaitEvent(s.main, s.ev_side[c], 0));
         }
@@ -415,7 +420,7 @@ phmm_status Engine::capture_graph(Slot& s, bool want_flags, std::string& err)
     return PHMM_OK;
 }
 
-phmm_status Engine::enqueue(Slot& s, const Plan& plan, const phmm_batch& b, bool want_flags, std::string& err)
+phmm_status Engine::upload(Slot& s, const Plan& plan, const phmm_batch& b, std::string& err)
 {
     phmm_status st = ensure_capacity(s, plan, err);
     if (st != PHMM_OK) return st;
@@ -470,6 +475,15 @@ phmm_status Engine::enqueue(Slot& s, const Plan& plan, const phmm_batch& b, bool
     if (plan.hap_bases)
         PHMM_CK(cudaMemcpyAsync(s.d_hb, b.hap_bases + plan.hap_base0, plan.hap_bases, cudaMemcpyHostToDevice, m));
 
+    PHMM_CK(cudaMemcpyAsync(s.d_desc_pristine, s.d_desc, kDescBytes, cudaMemcpyDeviceToDevice, m));
+    return PHMM_OK;
+}
+
+phmm_status Engine::run(Slot& s, const Plan& plan, bool want_flags, bool restore, std::string& err)
+{
+    phmm_status st = PHMM_OK;
+    cudaStream_t m = s.main;
+    if (restore) PHMM_CK(cudaMemcpyAsync(s.d_desc, s.d_desc_pristine, kDescBytes, cudaMemcpyDeviceToDevice, m));
     if (cfg_.use_cuda_graph) {
         if (!s.graph || s.graph_flags != want_flags) {
             st = capture_graph(s, want_flags, err);
@@ -481,6 +495,13 @@ phmm_status Engine::enqueue(Slot& s, const Plan& plan, const phmm_batch& b, bool
         if (st != PHMM_OK) return st;
     }
     return PHMM_OK;
+}
+
+phmm_status Engine::enqueue(Slot& s, const Plan& plan, const phmm_batch& b, bool want_flags, std::string& err)
+{
+    phmm_status st = upload(s, plan, b, err);
+    if (st != PHMM_OK) return st;
+    return run(s, plan, want_flags, false, err);
 }
 
 phmm_status Engine::finish(Slot& s, const Plan& plan, double* out, uint8_t* pair_flags, phmm_stats* stats,
@@ -505,6 +526,7 @@ phmm_status Engine::finish(Slot& s, const Plan& plan, double* out, uint8_t* pair
         stats->cells = plan.cells;
         stats->pairs_f64 = f64;
         stats->work_items = plan.items.size();
+        stats->kernel_launches = s.launches;
         stats->h2d_bytes = plan.read_bases * 5 + plan.hap_bases;
         stats->d2h_bytes = plan.out_total * (sizeof(double) + (pair_flags ? 1 : 0));
         float a = 0, bms = 0, c2 = 0;
@@ -521,6 +543,31 @@ phmm_status Engine::finish(Slot& s, const Plan& plan, double* out, uint8_t* pair
               ((status & kStatusRerunOverflow) ? " (FP64 rerun list overflow)" : "");
         return PHMM_ERR_DEVICE_STATUS;
     }
+    return PHMM_OK;
+}
+
+phmm_status Engine::fp32_fma_peak(double* tflops, std::string& err)
+{
+    std::lock_guard<std::mutex> lk(mu_);
+    PHMM_CK(cudaSetDevice(dev_));
+    Slot& s = *default_slot_;
+    float* sink = nullptr;
+    PHMM_CK(cudaMalloc(&sink, sizeof(float) * sms_ * 64));
+    const int blocks = sms_ * 8, iters = 1 << 14;
+    launch_fma_peak(sink, blocks, 256, s.main);  // warm-up
+    cudaEventRecord(s.ev_t0, s.main);
+    launch_fma_peak(sink, blocks, iters, s.main);
+    cudaEventRecord(s.ev_t1, s.main);
+    cudaError_t e = cudaEventSynchronize(s.ev_t1);
+    float ms = 0;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, s.ev_t0, s.ev_t1);
+    cudaFree(sink);
+    if (e != cudaSuccess) {
+        err = std::string("FMA probe failed: ") + cudaGetErrorString(e);
+        return PHMM_ERR_CUDA;
+    }
+    const double flops = 2.0 * 16.0 * (double)iters * 256.0 * blocks;
+    *tflops = flops / (ms * 1e-3) / 1e12;
     return PHMM_OK;
 }
 

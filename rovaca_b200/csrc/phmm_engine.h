@@ -34,6 +34,7 @@ struct Slot {
     Capacity cap;
     // carved device pointers
     BatchDesc* d_desc = nullptr;
+    char* d_desc_pristine = nullptr;  // the batch's descriptor block as uploaded, for replays
     ClassDesc* d_classes = nullptr;
     unsigned int* d_status = nullptr;
     RegionDesc* d_regions = nullptr;
@@ -54,6 +55,7 @@ struct Slot {
                 ev_t3 = nullptr, ev_done = nullptr;
     cudaGraphExec_t graph = nullptr;
     bool graph_flags = false;        // the captured graph writes pair flags
+    uint64_t launches = 0;           // kernels launched by the last pipeline run
 };
 
 class Engine {
@@ -70,6 +72,11 @@ public:
     phmm_status enqueue(Slot& s, const Plan& plan, const phmm_batch& b, bool want_flags, std::string& err);
     phmm_status finish(Slot& s, const Plan& plan, double* out, uint8_t* pair_flags, phmm_stats* stats,
                        std::string& err);
+    // Upload only (descriptor, plan arrays, reads, haplotypes); then run the device pipeline, with
+    // restore = true resetting the descriptor from its pristine device copy first (replays).
+    phmm_status upload(Slot& s, const Plan& plan, const phmm_batch& b, std::string& err);
+    phmm_status run(Slot& s, const Plan& plan, bool want_flags, bool restore, std::string& err);
+    phmm_status fp32_fma_peak(double* tflops, std::string& err);
 
     int device() const { return dev_; }
     int num_sms() const { return sms_; }

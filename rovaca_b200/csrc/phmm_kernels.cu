@@ -148,6 +148,30 @@ __global__ void __launch_bounds__(kFwdBlock, 1) fwd_f64_kernel(BatchView b, Prob
 }
 
 // ------------------------------------------------------------------------------------------
+// FP32 FMA throughput probe: 16 independent FMA chains per thread on every SM.
+// ------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) fma_peak_kernel(float* sink, int iters, float a, float b)
+{
+    float x[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) x[k] = (float)(threadIdx.x + k) * 1e-3f;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int k = 0; k < 16; ++k) x[k] = __fmaf_rn(x[k], a, b);
+    }
+    float s = 0.f;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) s += x[k];
+    if (s == -1.0f) sink[blockIdx.x] = s;  // never true; keeps the chains alive
+}
+
+cudaError_t launch_fma_peak(float* sink, int blocks, int iters, cudaStream_t st)
+{
+    fma_peak_kernel<<<blocks, 256, 0, st>>>(sink, iters, 0.999f, 1e-4f);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------------------------
 // Class tables and host-side launch wrappers.
 // ------------------------------------------------------------------------------------------
 typedef void (*F32Kernel)(BatchView, ProbTables<float>, PassControl);

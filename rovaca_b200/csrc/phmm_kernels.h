@@ -25,5 +25,7 @@ cudaError_t launch_prep(const BatchDesc* desc, const uint8_t* hap_bases, uint32_
 cudaError_t launch_fwd(int precision, int cls, const BatchView& b, const ProbTables<float>& tf,
                        const ProbTables<double>& td, const PassControl& pc, int grid, cudaStream_t st);
 cudaError_t occupancy(int precision, int cls, int* blocks_per_sm);
+// 256-thread blocks, each thread running 16 independent FMA chains for iters steps.
+cudaError_t launch_fma_peak(float* sink, int blocks, int iters, cudaStream_t st);
 
 }  // namespace phmm

@@ -164,6 +164,17 @@ class PackedBatch:
         return b
 
 
+def plan_summary(batch: PackedBatch) -> dict:
+    """How the engine cuts a batch into work (host only): items and pairs per kernel class."""
+    lib = _lib.load()
+    items = np.zeros(18, np.uint32)
+    pairs = np.zeros(18, np.uint64)
+    tp, tc = C.c_uint64(), C.c_uint64()
+    b = batch.as_c()
+    check(lib.phmm_host_plan_summary(C.byref(b), _ptr(items), _ptr(pairs), C.byref(tp), C.byref(tc)))
+    return {"class_items": items, "class_pairs": pairs, "pairs": tp.value, "cells": tc.value}
+
+
 class Engine:
     """One engine per CUDA device (phmm_engine_create)."""
 
@@ -224,6 +235,16 @@ class Engine:
             res.append(blk if fl is None else (blk, fl[offs[g]:offs[g + 1]].reshape(blk.shape)))
         return res
 
+    # ---- device-resident batches -------------------------------------------------------
+    def resident(self, batch: PackedBatch, want_flags: bool = False) -> "ResidentBatch":
+        return ResidentBatch(self, batch, want_flags)
+
+    def fp32_fma_peak(self) -> float:
+        """Measured FP32 FMA throughput of the device, TFLOP/s (an FMA counts 2 FLOPs)."""
+        v = C.c_double()
+        check(self._lib.phmm_fp32_fma_peak(self._h, C.byref(v)))
+        return v.value
+
     # ---- serving loop ------------------------------------------------------------------
     def submit(self, region: PackedBatch, out: np.ndarray, flags: np.ndarray | None = None) -> int:
         """Queues one region (region.n_regions == 1); out (and flags) must stay alive until wait()."""
@@ -269,6 +290,47 @@ class Engine:
         return out.reshape(len(hs), len(rs)), keep.astype(bool)
 
 
+class ResidentBatch:
+    """A batch uploaded once; run() recomputes it from HBM with no host transfers."""
+
+    def __init__(self, engine: Engine, batch: PackedBatch, want_flags: bool = False):
+        self._lib = engine._lib
+        self.batch = batch
+        self.want_flags = want_flags
+        h = C.c_void_p()
+        b = batch.as_c()
+        check(self._lib.phmm_resident_create(engine._h, C.byref(b), int(want_flags), C.byref(h)))
+        self._h = h
+
+    def run(self, iterations: int = 1) -> dict:
+        st = _lib.Stats()
+        check(self._lib.phmm_resident_run(self._h, iterations, C.byref(st)))
+        return st.as_dict()
+
+    def results(self):
+        out = np.empty(self.batch.out_size, np.float64)
+        fl = np.empty(self.batch.out_size, np.uint8) if self.want_flags else None
+        check(self._lib.phmm_resident_results(self._h, _ptr(out), _ptr(fl)))
+        return out, fl
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            check(self._lib.phmm_resident_destroy(self._h))
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 _default_engine: Engine | None = None
 
 
@@ -305,4 +367,5 @@ def call_pairhmm(haplotypes, reads, base_quals, mapq, min_quality_threshold: int
     return mat, np.nonzero(keep)[0]
 
 
-__all__ = ["Engine", "Region", "PackedBatch", "PhmmError", "schedule_pairhmm", "call_pairhmm", "default_engine"]
+__all__ = ["Engine", "Region", "PackedBatch", "PhmmError", "schedule_pairhmm", "call_pairhmm", "default_engine",
+           "plan_summary"]

@@ -1,0 +1,82 @@
+"""Shared fixtures.  Tests marked ``gpu`` need a CUDA device (B200); the rest run on CPU."""
+from __future__ import annotations
+
+import json
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+ROOT = Path(__file__).resolve().parent.parent
+GOLDEN = Path(__file__).resolve().parent / "golden"
+sys.path.insert(0, str(ROOT))
+
+PACK_FIELDS = ("n_haps", "n_reads", "hap_bases", "hap_off", "read_bases", "read_qual", "read_ins", "read_del",
+               "read_gcp", "read_off")
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (runs on a B200)")
+
+
+@pytest.fixture(scope="session")
+def oracle():
+    from oracle import Oracle
+
+    return Oracle()
+
+
+@pytest.fixture(scope="session")
+def ref():
+    from oracle import Ref, build_ref
+
+    if build_ref() is None:
+        pytest.skip("reference build (oracle/_ref) not available here")
+    return Ref()
+
+
+@pytest.fixture(scope="session")
+def golden_cases():
+    return json.loads((GOLDEN / "golden_cases.json").read_text())["cases"]
+
+
+@pytest.fixture(scope="session")
+def ref_regions():
+    """{group: (PackedBatch, reference schedule_pairhmm log10 [hap][read] flat)} from the fixtures."""
+    from rovaca_b200.pairhmm import PackedBatch
+
+    z = np.load(GOLDEN / "ref_regions.npz")
+    groups = sorted({k.split(".")[0] for k in z.files})
+    return {g: (PackedBatch(*(z[f"{g}.{f}"] for f in PACK_FIELDS)), z[f"{g}.ref_log10"]) for g in groups}
+
+
+@pytest.fixture(scope="session")
+def engine():
+    from rovaca_b200 import Engine
+
+    eng = Engine(device=0)
+    yield eng
+    eng.close()
+
+
+@pytest.fixture(scope="session")
+def engine_direct():
+    """Same engine without CUDA-graph replay (only non-empty kernel classes launched)."""
+    from rovaca_b200 import Engine
+
+    eng = Engine(device=0, use_cuda_graph=False)
+    yield eng
+    eng.close()
+
+
+def case_tuple(c):
+    return (c["hap"].encode(), c["read"].encode(), bytes(c["q"]), bytes(c["i"]), bytes(c["d"]), bytes(c["c"]))
+
+
+def f32_of_hex(h: str) -> float:
+    return float(np.frombuffer(bytes.fromhex(h), ">f4")[0])
+
+
+def f64_of_hex(h: str) -> float:
+    return float(np.frombuffer(bytes.fromhex(h), ">f8")[0])

@@ -180,6 +180,36 @@ def main(reference_root: str = "/root/reference") -> None:
             arrays[f"{name}.{f}"] = getattr(pb, f)
         arrays[f"{name}.ref_log10"] = np.concatenate(outs)
     np.savez_compressed(HERE / "ref_regions.npz", **arrays)
+
+    # ---- region-path helpers: PCR model and tandem repeats (pairhmm_internal.cpp) ----------
+    import ctypes as C
+
+    lib = ref.lib
+    lib.ref_tandem_repeat.restype = C.c_int
+    prng = np.random.default_rng(4242)
+    reads = []
+    for k in range(120):
+        n = int(prng.integers(1, 160))
+        unit = prng.choice(list(b"ACGT"), int(prng.integers(1, 9)))
+        if k % 3 == 0:
+            s = prng.choice(list(b"ACGT"), n)
+        elif k % 3 == 1:
+            s = np.resize(unit, n)
+        else:
+            s = np.concatenate([prng.choice(list(b"ACGT"), 12), np.resize(unit, n), prng.choice(list(b"AC"), 9)])[:n]
+        reads.append(bytes(np.asarray(s, np.uint8)))
+    helpers = []
+    for s in reads:
+        n = len(s)
+        rec = {"bases": s.decode(), "repeat": [lib.ref_tandem_repeat(s, n, o, 1) for o in range(max(n - 1, 0))]}
+        for model, name in ((1, "HOSTILE"), (2, "AGGRESSIVE"), (3, "CONSERVATIVE")):
+            g = (C.c_uint8 * n)(*([45] * n))
+            lib.ref_pcr_model(s, n, g, model, 1)
+            rec[name] = list(bytes(g))
+        helpers.append(rec)
+    (HERE / "region_helpers.json").write_text(json.dumps({"source": "apply_pcr_error_model_rolling and "
+                                                          "find_tandem_repeat_units_rolling from oracle/_ref",
+                                                          "reads": helpers}))
     print(f"wrote {HERE / 'golden_cases.json'} ({len(allc)} cases) and {HERE / 'ref_regions.npz'} "
           f"({', '.join(f'{k}: {len(v)}' for k, v in groups.items())} regions)")
 

@@ -1,0 +1,173 @@
+"""Parity of the CUDA engine with the oracle and the reference, through the C ABI.
+
+Tolerances: the engine reproduces the reference's FP32/FP64 arithmetic exactly, so its log10 values
+equal the oracle's up to the last bits of the final double log10 (|diff| <= 1e-12, far below the
+6e-8 relative step between neighbouring FP32 sums, so equal values mean equal raw sums); against the
+all-FP64 oracle the bound is the 1e-4 log10 of the specification; against the reference's own output
+1e-5 (pairs the reference leaves to its intra kernel round the prior and the log once more)."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import case_tuple
+from rovaca_b200 import synth
+from rovaca_b200.pairhmm import PackedBatch, PhmmError, Region
+
+pytestmark = pytest.mark.gpu
+
+EXACT = 1e-12
+SPEC = 1e-4
+
+
+def _golden_batch(cases):
+    regs = [Region([c["hap"]], [c["read"]], [bytes(c["q"])], [bytes(c["i"])], [bytes(c["d"])], [bytes(c["c"])])
+            for c in cases]
+    return PackedBatch.from_regions(regs)
+
+
+def test_golden_vectors(engine, oracle, golden_cases):
+    pb = _golden_batch(golden_cases)
+    got, flags, _ = engine.compute(pb, want_flags=True)
+    for k, c in enumerate(golden_cases):
+        want, used = oracle.pair(*case_tuple(c))
+        assert abs(got[k] - c["expected"]) < 1e-5, (c["line"], got[k], c["expected"])
+        assert abs(got[k] - want) <= EXACT, (c["line"], got[k], want)
+        assert bool(flags[k]) == used
+
+
+@pytest.mark.parametrize("group", ["debug", "config0", "config1", "config2", "edge"])
+def test_reference_regions(engine, oracle, ref_regions, group):
+    pb, ref_out = ref_regions[group]
+    got, flags, stats = engine.compute(pb, want_flags=True)
+    want, used = oracle.batch(pb)
+    assert np.array_equal(np.isnan(got), np.isnan(want))
+    assert np.nanmax(np.abs(got - want)) <= EXACT
+    assert np.array_equal(flags.astype(bool), used)
+    assert stats["pairs_f64"] == int(used.sum())
+    # the reference's own schedule_pairhmm output
+    assert np.nanmax(np.abs(got - ref_out)) < 1e-5
+    # every FP32 -> FP64 decision equals the reference's, whichever of its kernels made it
+    routes = np.concatenate([oracle.schedule_region(pb, g)[1].reshape(-1) for g in range(pb.n_regions)])
+    ref_f64 = np.isin(routes, oracle.ROUTE_F64)
+    assert np.array_equal(flags.astype(bool), ref_f64), int(np.sum(flags.astype(bool) != ref_f64))
+    # the specification's bound against the all-FP64 oracle
+    f64, _ = oracle.batch(pb, fp64_only=True)
+    assert np.nanmax(np.abs(got - f64)) < SPEC
+
+
+def test_graph_and_direct_launch_agree(engine, engine_direct, ref_regions):
+    for group in ("debug", "edge", "config1"):
+        pb, _ = ref_regions[group]
+        a, fa, _ = engine.compute(pb, want_flags=True)
+        b, fb, _ = engine_direct.compute(pb, want_flags=True)
+        assert np.array_equal(a, b, equal_nan=True)
+        assert np.array_equal(fa, fb)
+
+
+def test_region_result_independent_of_batch(engine):
+    """Per-pair arithmetic does not depend on what else is in the batch."""
+    pb = synth.config1(12, seed=5)
+    full, _, _ = engine.compute(pb)
+    offs = pb.out_offsets()
+    for g in (0, 5, 11):
+        alone, _, _ = engine.compute(pb.subset([g]))
+        assert np.array_equal(alone, full[offs[g]:offs[g + 1]], equal_nan=True)
+    rev = pb.subset(list(range(pb.n_regions))[::-1])
+    back, _, _ = engine.compute(rev)
+    roffs = rev.out_offsets()
+    for g in range(pb.n_regions):
+        r = pb.n_regions - 1 - g
+        assert np.array_equal(back[roffs[r]:roffs[r + 1]], full[offs[g]:offs[g + 1]], equal_nan=True)
+
+
+def test_underflow_stress_region(engine, oracle):
+    """Config-2 regime: most pairs fall below 1e-28 in FP32 and are recomputed in FP64."""
+    pb = synth.config2(2, seed=21)
+    got, flags, stats = engine.compute(pb, want_flags=True)
+    want, used = oracle.batch(pb)
+    assert used.mean() > 0.5
+    assert np.array_equal(flags.astype(bool), used)
+    assert np.max(np.abs(got - want)) <= EXACT
+    f64, _ = oracle.batch(pb, fp64_only=True)
+    assert np.max(np.abs(got - f64)) < SPEC
+
+
+def test_empty_reads_and_haplotypes_give_nan(engine, oracle):
+    reg = Region([b"ACGTACGTAA", b"", b"ACGGT"], [b"ACGT", b"", b"CGTAC"],
+                 [b"\x1e" * 4, b"", b"\x1e" * 5], [b"\x2d" * 4, b"", b"\x2d" * 5], [b"\x2d" * 4, b"", b"\x2d" * 5],
+                 [b"\x0a" * 4, b"", b"\x0a" * 5])
+    pb = PackedBatch.from_regions([reg])
+    got, _, stats = engine.compute(pb)
+    m = got.reshape(3, 3)
+    assert np.isnan(m[1]).all() and np.isnan(m[:, 1]).all()
+    assert np.isfinite(m[[0, 2]][:, [0, 2]]).all()
+    want, _ = oracle.batch(pb)
+    assert np.nanmax(np.abs(got - want)) <= EXACT
+    assert stats["pairs"] == 4
+
+
+def test_regions_without_reads_or_haplotypes(engine):
+    regs = [Region([], [b"ACGT"], [b"\x1e" * 4], [b"-" * 4], [b"-" * 4], [b"\x0a" * 4]),
+            Region([b"ACGT"], [], [], [], [], []),
+            Region([b"ACGTT"], [b"ACGT"], [b"\x1e" * 4], [b"-" * 4], [b"-" * 4], [b"\x0a" * 4])]
+    got, _, _ = engine.compute(PackedBatch.from_regions(regs))
+    assert got.shape == (1,) and np.isfinite(got[0])
+
+
+def test_limits_are_rejected(engine):
+    reg = Region([b"A" * 1537], [b"ACGT"], [b"\x1e" * 4], [b"-" * 4], [b"-" * 4], [b"\x0a" * 4])
+    with pytest.raises(PhmmError) as e:
+        engine.compute(PackedBatch.from_regions([reg]))
+    assert e.value.name == "PHMM_ERR_LIMIT_EXCEEDED"
+
+
+def test_random_lengths_all_classes(engine, oracle):
+    """Read lengths 1..768 (every rows-per-lane class and multi-stripe), haplotypes 1..1536, with N."""
+    rng = np.random.default_rng(77)
+    acgt = np.frombuffer(b"ACGTN", np.uint8)
+    regs = []
+    for g in range(6):
+        H = [int(x) for x in rng.integers(1, 1537 if g == 0 else 400, int(rng.integers(1, 6)))]
+        base = acgt[rng.integers(0, 4, max(H) + 800)]
+        haps = [bytes(base[:h]) for h in H]
+        if g % 2:
+            hb = bytearray(haps[0])
+            hb[len(hb) // 2] = ord("N")
+            haps[0] = bytes(hb)
+        lens = [int(x) for x in rng.integers(1, 769 if g < 2 else 300, int(rng.integers(1, 12)))]
+        reads = []
+        for L in lens:
+            r = bytearray(base[int(rng.integers(0, 100)):][:L])
+            if rng.random() < 0.2:
+                r[int(rng.integers(0, len(r)))] = ord("N")
+            reads.append(bytes(r))
+        q = [rng.integers(2, 42, len(r)).astype(np.uint8).tobytes() for r in reads]
+        i = [rng.integers(10, 46, len(r)).astype(np.uint8).tobytes() for r in reads]
+        d = [rng.integers(10, 46, len(r)).astype(np.uint8).tobytes() for r in reads]
+        c = [rng.integers(5, 15, len(r)).astype(np.uint8).tobytes() for r in reads]
+        regs.append(Region(haps, reads, q, i, d, c))
+    pb = PackedBatch.from_regions(regs)
+    got, flags, _ = engine.compute(pb, want_flags=True)
+    want, used = oracle.batch(pb)
+    assert np.array_equal(np.isnan(got), np.isnan(want))
+    assert np.nanmax(np.abs(got - want)) <= EXACT
+    assert np.array_equal(flags.astype(bool), used)
+
+
+def test_full_size_batch_properties(engine, oracle):
+    """The benchmark batch (2,000 regions, ~5.7e11 cells): deterministic, every pair finite, and a
+    seeded sample of regions equal to the oracle."""
+    pb = synth.config1()
+    a, fa, sa = engine.compute(pb, want_flags=True)
+    b, fb, sb = engine.compute(pb, want_flags=True)
+    assert np.array_equal(a, b) and np.array_equal(fa, fb)
+    assert np.isfinite(a).all()
+    assert sa["pairs"] == pb.out_size and sa["pairs_f64"] == int(fa.sum())
+    offs = pb.out_offsets()
+    sample = [0, 777, 1999]
+    want, used = oracle.batch(pb.subset(sample))
+    got = np.concatenate([a[offs[g]:offs[g + 1]] for g in sample])
+    gflags = np.concatenate([fa[offs[g]:offs[g + 1]] for g in sample])
+    assert np.max(np.abs(got - want)) <= EXACT
+    assert np.array_equal(gflags.astype(bool), used)

@@ -1,0 +1,174 @@
+"""Serving loop (continuous batching) and the region API, through the C ABI."""
+from __future__ import annotations
+
+import threading
+
+import numpy as np
+import pytest
+
+from rovaca_b200 import Engine, synth
+from rovaca_b200._lib import PhmmError
+from rovaca_b200.pairhmm import PackedBatch, call_pairhmm, schedule_pairhmm
+
+pytestmark = pytest.mark.gpu
+
+
+def test_each_result_same_alone_and_in_the_mix(engine):
+    """Regions submitted concurrently from several threads, admitted while others run, give exactly
+    the likelihoods the same region gets alone."""
+    pb = synth.config1(40, seed=31)
+    alone = [engine.compute(pb.subset([g]))[0] for g in range(pb.n_regions)]
+    outs = [np.empty(a.size) for a in alone]
+    tickets = [None] * pb.n_regions
+    regions = [pb.subset([g]) for g in range(pb.n_regions)]
+
+    def producer(k0):
+        for g in range(k0, pb.n_regions, 4):
+            tickets[g] = engine.submit(regions[g], outs[g])
+
+    threads = [threading.Thread(target=producer, args=(k,)) for k in range(4)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    lat = [engine.wait(t) for t in tickets]
+    for g in range(pb.n_regions):
+        assert np.array_equal(outs[g], alone[g], equal_nan=True), g
+    assert all(total >= queued >= 0 for queued, total in lat)
+
+
+def test_flags_and_poll(engine, oracle):
+    pb = synth.config2(1, seed=41)
+    out = np.empty(pb.out_size)
+    fl = np.empty(pb.out_size, np.uint8)
+    t = engine.submit(pb, out, fl)
+    while not engine.poll(t):
+        pass
+    engine.wait(t)
+    want, used = oracle.batch(pb)
+    assert np.max(np.abs(out - want)) <= 1e-12
+    assert np.array_equal(fl.astype(bool), used)
+
+
+def test_cancel_and_timeout():
+    """With a budget that fits one request at a time, later requests wait in the queue and can be
+    cancelled; a zero timeout on an unfinished request reports TIMEOUT and keeps the ticket."""
+    pb = synth.config2(1, seed=51)  # one region needs about 0.47 MB of device data
+    one = PackedBatch.from_regions([pb.region(0)])
+    with Engine(hbm_budget_bytes=700 << 10) as eng:
+        outs = [np.empty(one.out_size) for _ in range(6)]
+        ts = [eng.submit(one, o) for o in outs]
+        cancelled = set()
+        for t in ts[3:]:
+            try:
+                eng.cancel(t)
+                cancelled.add(t)
+            except PhmmError:
+                pass  # already admitted
+        assert cancelled
+        released = set()
+        try:
+            eng.wait(ts[1], timeout_us=0)
+            released.add(ts[1])
+        except PhmmError as e:
+            assert e.name == "PHMM_ERR_TIMEOUT"
+        for t in ts:
+            if t in released:
+                continue
+            if t in cancelled:
+                with pytest.raises(PhmmError) as e:
+                    eng.wait(t)
+                assert e.value.name == "PHMM_ERR_CANCELLED"
+            else:
+                eng.wait(t)
+                assert np.isfinite(outs[ts.index(t)]).all()
+
+
+def test_oversized_request_is_rejected():
+    pb = synth.config2(1, seed=52)
+    with Engine(hbm_budget_bytes=100 << 10) as eng:
+        with pytest.raises(PhmmError) as e:
+            eng.submit(pb, np.empty(pb.out_size))
+        assert e.value.name == "PHMM_ERR_LIMIT_EXCEEDED"
+
+
+def test_schedule_pairhmm_vector_api(engine, oracle, ref_regions):
+    pb, ref_out = ref_regions["debug"]
+    offs = pb.out_offsets()
+    for g in range(pb.n_regions):
+        r = pb.region(g)
+        ok, res = schedule_pairhmm(r.haplotypes, r.reads, r.quality, r.insertion_qualities, r.deletion_qualities,
+                                   r.gap_contiguous_qualities, engine=engine)
+        assert ok and res.shape == (r.n_reads, r.n_haps)
+        want = ref_out[offs[g]:offs[g + 1]].reshape(r.n_haps, r.n_reads).T
+        assert np.max(np.abs(res - want)) < 1e-5
+    ok, _ = schedule_pairhmm([], [b"ACGT"], [b"\x1e" * 4], [b"-" * 4], [b"-" * 4], [b"\x0a" * 4], engine=engine)
+    assert not ok
+
+
+def _region_api_expected(oracle, haps, reads, quals, mapq, thr, pcr):
+    """call_pairhmm restated on the oracle: read preparation (roDV_schedule.cpp:540-609), FP32/FP64
+    likelihoods, normalise, drop poorly modelled reads, [hap][read] with kept reads first."""
+    import ctypes as C
+
+    from rovaca_b200 import _lib
+
+    lib = _lib.load()
+    lk = np.full((len(haps), len(reads)), np.nan)
+    for r, (rd, q) in enumerate(zip(reads, quals)):
+        n = len(rd)
+        qq = np.array([min(x, mapq[r]) for x in q], np.uint8)
+        qq = np.where(qq < thr, 6, qq).astype(np.uint8)
+        gop = (C.c_uint8 * n)(*([45] * n))
+        lib.phmm_host_pcr_model(rd, n, gop, pcr)  # pinned against the reference in test_host.py
+        for h, hp in enumerate(haps):
+            if n and len(hp):
+                lk[h, r], _ = oracle.pair(hp, rd, qq.tobytes(), bytes(gop), bytes(gop), bytes([10]) * n)
+    out = np.full_like(lk, np.nan)
+    keep = []
+    for r in range(len(reads)):
+        row = lk[:, r].copy()
+        best = row[0]
+        for v in row[1:]:
+            if best < v:
+                best = v
+        row = np.where(row < best - 4.5, best - 4.5, row)
+        fin = row[~np.isnan(row)]
+        b = fin.max() if fin.size else -np.inf
+        ok = not (b < min(2.0, np.ceil(len(reads[r]) * 0.02)) * -4.0)
+        keep.append(ok)
+        if ok:
+            out[:, sum(keep) - 1] = row
+    return out, np.array(keep)
+
+
+@pytest.mark.parametrize("pcr", ["NONE", "CONSERVATIVE", "HOSTILE"])
+def test_call_pairhmm_region_api(engine, oracle, pcr):
+    rng = np.random.default_rng({"NONE": 1, "CONSERVATIVE": 2, "HOSTILE": 3}[pcr])
+    base = bytes(np.frombuffer(b"ACGT", np.uint8)[rng.integers(0, 4, 420)])
+    base = base[:100] + b"ACACACACACAC" + base[100:200] + b"TTTTTTTT" + base[200:]
+    haps = [base[:400], base[:150] + b"G" + base[151:400], base[:300] + base[305:400]]
+    reads, quals = [], []
+    for k in range(24):
+        L = int(rng.integers(60, 160))
+        s = int(rng.integers(0, 400 - L))
+        r = bytearray(base[s:s + L])
+        if k % 7 == 3:
+            r = bytearray(np.frombuffer(b"ACGT", np.uint8)[rng.integers(0, 4, L)])  # unrelated read
+        reads.append(bytes(r))
+        quals.append(rng.integers(2, 45, L).astype(np.uint8).tobytes())
+    mapq = rng.integers(10, 61, len(reads)).astype(np.uint8)
+    mat, kept = call_pairhmm(haps, reads, quals, mapq, 18, pcr, engine=engine)
+    want, wkeep = _region_api_expected(oracle, haps, reads, quals, mapq, 18, {"NONE": 0, "CONSERVATIVE": 3,
+                                                                              "HOSTILE": 1}[pcr])
+    assert np.array_equal(kept, np.nonzero(wkeep)[0])
+    assert np.array_equal(np.isnan(mat), np.isnan(want))
+    assert np.nanmax(np.abs(mat - want)) <= 1e-12
+    assert len(kept) < len(reads)  # the unrelated reads are dropped
+
+
+def test_call_pairhmm_over_limits_returns_nan_matrix(engine):
+    haps = [b"A" * 1600]
+    with pytest.raises(PhmmError) as e:
+        call_pairhmm(haps, [b"ACGT"], [b"\x1e" * 4], [60], 18, "NONE", engine=engine)
+    assert e.value.name == "PHMM_ERR_LIMIT_EXCEEDED"

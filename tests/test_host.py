@@ -1,0 +1,237 @@
+"""CPU-only checks of the engine library: it loads, exports every declared entry point, refuses to
+run without a GPU, and its host-side logic (planning, read preparation, PCR model, post-processing)
+matches the reference."""
+from __future__ import annotations
+
+import ctypes as C
+import json
+import multiprocessing as mp
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+from rovaca_b200 import _lib
+from rovaca_b200.pairhmm import PackedBatch, Region, plan_summary
+
+
+def _region(haps, reads, q=30, ins=45, gcp=10):
+    return Region(haps, reads, [bytes([q]) * len(r) for r in reads], [bytes([ins]) * len(r) for r in reads],
+                  [bytes([ins]) * len(r) for r in reads], [bytes([gcp]) * len(r) for r in reads])
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _lib.load()
+    names = _lib.declared_symbols()
+    assert len(names) >= 15
+    for n in names:
+        assert hasattr(lib, n), n
+
+
+def test_status_strings_and_version():
+    lib = _lib.load()
+    for s in range(12):
+        assert lib.phmm_status_string(s)
+    assert b"sm_100a" in lib.phmm_version()
+
+
+def _create_engine_without_gpu(q):
+    try:
+        from rovaca_b200 import Engine
+
+        Engine()
+        q.put("created")
+    except _lib.PhmmError as e:
+        q.put(e.name)
+
+
+def test_engine_refuses_to_run_without_a_gpu():
+    """No CUDA device: engine creation fails loudly (no CPU fallback exists)."""
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    p = ctx.Process(target=_create_engine_without_gpu, args=(q,))
+    p.start()
+    p.join(120)
+    assert q.get(timeout=5) == "PHMM_ERR_NO_DEVICE"
+
+
+# ---- planning -------------------------------------------------------------------------------
+
+def cls(variant, k, multi=False):
+    return variant * 9 + (8 if multi else k - 1)
+
+
+def test_plan_rows_per_lane_follow_read_length():
+    hap = b"ACGT" * 100
+    reads = [hap[:n] for n in (1, 32, 33, 64, 100, 151, 200, 256)]
+    s = plan_summary(PackedBatch.from_regions([_region([hap, hap[3:]], reads)]))
+    want = {1: 2, 2: 2, 4: 1, 5: 1, 7: 1, 8: 1}  # K = ceil(R / 32): items per K (one item per read)
+    for k, n in want.items():
+        assert s["class_items"][cls(0, k)] == n, (k, s["class_items"])
+    assert s["pairs"] == 16
+    assert s["cells"] == sum(len(r) for r in reads) * (len(hap) + len(hap) - 3)
+
+
+def test_plan_long_reads_use_multi_stripe_class():
+    hap = b"ACGT" * 300
+    s = plan_summary(PackedBatch.from_regions([_region([hap], [hap[:257], hap[:768], hap[:256]])]))
+    assert s["class_items"][cls(0, 8, True)] == 2
+    assert s["class_items"][cls(0, 8)] == 1
+
+
+def test_plan_routes_n_pairs_to_the_intra_variant():
+    h = b"ACGTACGGTCA" * 10
+    hn = h[:20] + b"N" + h[21:]
+    r = [h[5:60], h[10:40] + b"N" + h[41:70], h[:30]]
+    s = plan_summary(PackedBatch.from_regions([_region([h, hn, h], r)]))
+    # read with N: every pair intra; reads without N: the N haplotype alone is intra
+    assert s["class_pairs"][9:].sum() == 3 + 2
+    assert s["class_pairs"][:9].sum() == 2 * 2
+    # a read without N streams [h] and [h] as two inter items split around the N haplotype
+    assert s["class_items"][:9].sum() == 4
+
+
+def test_plan_splits_long_haplotype_streams():
+    haps = [b"A" * 1500] * 20  # 30,000 columns, more than one stream (8192 max)
+    s = plan_summary(PackedBatch.from_regions([_region(haps, [b"A" * 100])]))
+    assert s["class_items"][cls(0, 4)] == 4  # 5 haplotypes (7500 columns) per item
+    assert s["pairs"] == 20
+
+
+def test_plan_skips_empty_reads_and_haplotypes():
+    s = plan_summary(PackedBatch.from_regions([_region([b"ACGT" * 10, b"", b"ACG"], [b"ACGT", b"", b"A" * 40])]))
+    assert s["pairs"] == 4  # 2 non-empty haplotypes x 2 non-empty reads
+
+
+def test_plan_rejects_regions_beyond_the_reference_limits():
+    ok = b"ACGT"
+    with pytest.raises(_lib.PhmmError) as e:
+        plan_summary(PackedBatch.from_regions([_region([b"A" * 1537], [ok])]))
+    assert e.value.name == "PHMM_ERR_LIMIT_EXCEEDED"
+    with pytest.raises(_lib.PhmmError) as e:
+        plan_summary(PackedBatch.from_regions([_region([ok], [b"A" * 769])]))
+    assert e.value.name == "PHMM_ERR_LIMIT_EXCEEDED"
+    with pytest.raises(_lib.PhmmError) as e:
+        plan_summary(PackedBatch.from_regions([_region([ok] * 4097, [ok])]))
+    assert e.value.name == "PHMM_ERR_LIMIT_EXCEEDED"
+    plan_summary(PackedBatch.from_regions([_region([b"A" * 1536] * 2, [b"A" * 768])]))
+
+
+def test_plan_rejects_bad_offsets():
+    pb = PackedBatch.from_regions([_region([b"ACGT", b"ACG"], [b"AC"])])
+    pb.hap_off = np.array([0, 4, 2], np.uint64)
+    with pytest.raises(_lib.PhmmError) as e:
+        plan_summary(pb)
+    assert e.value.name == "PHMM_ERR_INVALID_ARGUMENT"
+
+
+# ---- region-path host helpers ---------------------------------------------------------------
+
+def test_pcr_model_and_repeats_match_reference_fixture():
+    lib = _lib.load()
+    data = json.loads((GOLDEN / "region_helpers.json").read_text())["reads"]
+    assert len(data) >= 100
+    for rec in data:
+        s = rec["bases"].encode()
+        n = len(s)
+        got = [lib.phmm_host_tandem_repeat_length(s, n, o) for o in range(max(n - 1, 0))]
+        assert got == rec["repeat"], rec["bases"]
+        for model, name in ((1, "HOSTILE"), (2, "AGGRESSIVE"), (3, "CONSERVATIVE")):
+            g = (C.c_uint8 * n)(*([45] * n))
+            lib.phmm_host_pcr_model(s, n, g, model)
+            assert list(bytes(g)) == rec[name], (name, rec["bases"])
+
+
+def test_pcr_model_matches_reference_build_on_random_reads(ref):
+    lib = _lib.load()
+    ref.lib.ref_tandem_repeat.restype = C.c_int
+    rng = np.random.default_rng(3)
+    for t in range(300):
+        n = int(rng.integers(2, 120))
+        unit = rng.choice(list(b"ACGT"), int(rng.integers(1, 9)))
+        s = bytes(np.asarray(np.resize(unit, n) if t % 2 else rng.choice(list(b"ACGT"), n), np.uint8))
+        for o in range(n - 1):
+            assert lib.phmm_host_tandem_repeat_length(s, n, o) == ref.lib.ref_tandem_repeat(s, n, o, 1)
+        for model in (1, 2, 3):
+            g1 = (C.c_uint8 * n)(*([45] * n))
+            g2 = (C.c_uint8 * n)(*([45] * n))
+            lib.phmm_host_pcr_model(s, n, g1, model)
+            ref.lib.ref_pcr_model(s, n, g2, model, 1)
+            assert bytes(g1) == bytes(g2)
+
+
+def test_quality_preparation():
+    lib = _lib.load()
+    q = np.array([2, 5, 17, 18, 30, 45, 60], np.uint8)
+    out = np.empty_like(q)
+    lib.phmm_host_prepare_quals(q.ctypes.data_as(C.c_void_p), len(q), 40, 18, out.ctypes.data_as(C.c_void_p))
+    assert out.tolist() == [6, 6, 6, 18, 30, 40, 40]
+
+
+def _normalize_filter_expected(lk_hr, read_len):
+    """normalize_likelihoods + collect_poorly_modelled_indices + transpose (pairhmm_internal.cpp:23-44,
+    248-258,499-508), written out plainly."""
+    n_haps, n_reads = lk_hr.shape
+    out = np.full_like(lk_hr, np.nan)
+    keep = []
+    for r in range(n_reads):
+        row = lk_hr[:, r].copy()
+        best = row[0]
+        for v in row[1:]:
+            if best < v:
+                best = v
+        cmp = best - 4.5
+        row = np.where(row < cmp, cmp, row)
+        finite = row[~np.isnan(row)]
+        b = finite.max() if finite.size else -np.inf
+        if b < min(2.0, np.ceil(read_len[r] * 0.02)) * -4.0:
+            keep.append(False)
+        else:
+            keep.append(True)
+            out[:, sum(keep) - 1] = row
+    return out, np.array(keep)
+
+
+def test_normalize_and_filter_matches_restatement():
+    lib = _lib.load()
+    rng = np.random.default_rng(8)
+    for t in range(200):
+        nh, nr = int(rng.integers(1, 7)), int(rng.integers(1, 9))
+        lk = -rng.random((nh, nr)) * 30
+        if t % 5 == 0:
+            lk[int(rng.integers(0, nh)), int(rng.integers(0, nr))] = np.nan
+        rl = rng.integers(0, 300, nr).astype(np.uint64)
+        out = np.empty_like(lk)
+        keep = np.empty(nr, np.uint8)
+        nk = C.c_uint32()
+        lk_c = np.ascontiguousarray(lk)
+        lib.phmm_host_normalize_filter(lk_c.ctypes.data_as(C.c_void_p), nh, nr, rl.ctypes.data_as(C.c_void_p),
+                                       out.ctypes.data_as(C.c_void_p), keep.ctypes.data_as(C.c_void_p), C.byref(nk))
+        want, wkeep = _normalize_filter_expected(lk, rl)
+        assert np.array_equal(keep.astype(bool), wkeep)
+        assert nk.value == wkeep.sum()
+        assert np.array_equal(np.isnan(out), np.isnan(want))
+        assert np.array_equal(out[~np.isnan(out)], want[~np.isnan(want)])
+
+
+def test_normalize_matches_reference_build(ref):
+    lib = _lib.load()
+    rng = np.random.default_rng(9)
+    for t in range(100):
+        nh, nr = int(rng.integers(1, 7)), int(rng.integers(1, 9))
+        lk_rh = -rng.random((nr, nh)) * 30
+        want = lk_rh.copy()
+        ref.lib.ref_normalize(want.ctypes.data_as(C.c_void_p), nr, nh)
+        hr = np.ascontiguousarray(lk_rh.T)
+        out = np.empty_like(hr)
+        keep = np.empty(nr, np.uint8)
+        nk = C.c_uint32()
+        rl = np.full(nr, 10, np.uint64)  # threshold -4: every row's best is within 4.5 of itself
+        lib.phmm_host_normalize_filter(hr.ctypes.data_as(C.c_void_p), nh, nr, rl.ctypes.data_as(C.c_void_p),
+                                       out.ctypes.data_as(C.c_void_p), keep.ctypes.data_as(C.c_void_p), C.byref(nk))
+        kept = keep.astype(bool)
+        assert np.array_equal(out[:, : nk.value], want.T[:, kept])
