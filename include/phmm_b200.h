@@ -155,9 +155,10 @@ PHMM_API phmm_status phmm_resident_run(phmm_resident* resident, int32_t iteratio
 PHMM_API phmm_status phmm_resident_results(phmm_resident* resident, double* out, uint8_t* pair_flags);
 PHMM_API phmm_status phmm_resident_destroy(phmm_resident* resident);
 
-/* Measures the device's FP32 FMA throughput (independent FMA chains on every SM, about 50 ms),
- * in TFLOP/s counting an FMA as 2 FLOPs: the peak the wavefront kernels are compared with. */
-PHMM_API phmm_status phmm_fp32_fma_peak(phmm_engine* engine, double* tflops);
+/* Measures the device's FP32 FMA throughput (independent FMA chains on every SM, about 0.1 s),
+ * in TFLOP/s counting an FMA as 2 FLOPs, with scalar FFMA and with packed two-wide FFMA2
+ * instructions (either pointer may be NULL): the peak the wavefront kernels are compared with. */
+PHMM_API phmm_status phmm_fp32_fma_peak(phmm_engine* engine, double* scalar_tflops, double* packed_tflops);
 
 /* ---- host-only pieces of the region path (no GPU involved) ----------------------------- */
 
@@ -174,11 +175,16 @@ PHMM_API int32_t phmm_host_tandem_repeat_length(const uint8_t* bases, uint32_t n
 PHMM_API void phmm_host_normalize_filter(const double* lk_hap_read, uint32_t n_haps, uint32_t n_reads, const uint64_t* read_len,
                                 double* out, uint8_t* keep, uint32_t* n_kept);
 
-/* How a batch is cut into wavefront work, without running it (no GPU involved): per kernel class
- * (class = variant * 9 + (read longer than 256 ? 8 : rows per lane - 1), variant 0 for pairs
- * without 'N', 1 with), the number of work items and of pairs; and the batch's pairs and cells.
+/* How a batch is cut into wavefront work, without running it (no GPU involved).  With
+ * KH = ceil(read length / 32) (8 for reads longer than 256, which run in 256-row stripes):
+ *   class_items[27]: work items per FP32 kernel class, (multi-stripe ? 8 : KH - 1) plus 0 for pairs
+ *     without 'N' whose read has constant gap qualities, 9 for other pairs without 'N', 18 for pairs
+ *     with 'N'; an item is two reads (one when a region has an odd count) against a haplotype run;
+ *   class_pairs[18]: pairs per FP64 recompute class, (multi-stripe ? 8 : KH - 1) plus 9 for 'N'
+ *     pairs (the capacity reserved for pairs that underflow in FP32);
+ *   pairs, cells: totals of the batch.
  * Returns the same validation status phmm_compute_regions would. */
-PHMM_API phmm_status phmm_host_plan_summary(const phmm_batch* batch, uint32_t class_items[18], uint64_t class_pairs[18],
+PHMM_API phmm_status phmm_host_plan_summary(const phmm_batch* batch, uint32_t class_items[27], uint64_t class_pairs[18],
                                             uint64_t* pairs, uint64_t* cells);
 
 /* ---- serving loop ----------------------------------------------------------------------- */

@@ -80,7 +80,7 @@ def load() -> C.CDLL:
         "phmm_resident_run": (I32, [P, I32, C.POINTER(Stats)]),
         "phmm_resident_results": (I32, [P, P, P]),
         "phmm_resident_destroy": (I32, [P]),
-        "phmm_fp32_fma_peak": (I32, [P, C.POINTER(D)]),
+        "phmm_fp32_fma_peak": (I32, [P, C.POINTER(D), C.POINTER(D)]),
         "phmm_host_plan_summary": (I32, [C.POINTER(Batch), P, P, C.POINTER(U64), C.POINTER(U64)]),
         "phmm_submit": (I32, [P, C.POINTER(Batch), P, P, C.POINTER(U64)]),
         "phmm_poll": (I32, [P, U64, C.POINTER(I32)]),

@@ -223,19 +223,18 @@ phmm_status phmm_resident_results(phmm_resident* r, double* out, uint8_t* pair_f
     PHMM_GUARD_END
 }
 
-phmm_status phmm_fp32_fma_peak(phmm_engine* engine, double* tflops)
+phmm_status phmm_fp32_fma_peak(phmm_engine* engine, double* scalar_tflops, double* packed_tflops)
 {
     PHMM_GUARD_BEGIN
     phmm::clear_error();
     if (!engine) return set_error(PHMM_ERR_NOT_INITIALIZED, "engine is null");
-    if (!tflops) return set_error(PHMM_ERR_INVALID_ARGUMENT, "tflops is null");
     std::string err;
-    phmm_status st = phmm::engine_of(engine)->fp32_fma_peak(tflops, err);
+    phmm_status st = phmm::engine_of(engine)->fp32_fma_peak(scalar_tflops, packed_tflops, err);
     return st == PHMM_OK ? PHMM_OK : set_error(st, err);
     PHMM_GUARD_END
 }
 
-phmm_status phmm_host_plan_summary(const phmm_batch* batch, uint32_t class_items[18], uint64_t class_pairs[18],
+phmm_status phmm_host_plan_summary(const phmm_batch* batch, uint32_t class_items[27], uint64_t class_pairs[18],
                                    uint64_t* pairs, uint64_t* cells)
 {
     PHMM_GUARD_BEGIN
@@ -245,10 +244,10 @@ phmm_status phmm_host_plan_summary(const phmm_batch* batch, uint32_t class_items
     std::string err;
     phmm_status st = phmm::build_plan(*batch, phmm::PlanLimits(), plan, err);
     if (st != PHMM_OK) return set_error(st, err);
-    for (int c = 0; c < phmm::kPlanClasses; ++c) {
+    for (int c = 0; c < phmm::kClasses32; ++c)
         if (class_items) class_items[c] = plan.classes[c].n_items;
-        if (class_pairs) class_pairs[c] = plan.classes[c].rerun_cap;
-    }
+    for (int c = 0; c < phmm::kClasses64; ++c)
+        if (class_pairs) class_pairs[c] = plan.classes[phmm::kClasses32 + c].rerun_cap;
     if (pairs) *pairs = plan.pairs;
     if (cells) *cells = plan.cells;
     return PHMM_OK;

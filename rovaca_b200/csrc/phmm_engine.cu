@@ -182,7 +182,7 @@ phmm_status Engine::create(const phmm_config* cfg, Engine** out, std::string& er
     }
     e->sms_ = prop.multiProcessorCount;
     for (int p = 0; p < 2; ++p)
-        for (int c = 0; c < kNumClasses; ++c) {
+        for (int c = 0; c < (p == 0 ? kClasses32 : kClasses64); ++c) {
             int b = 0;
             PHMM_CKE(occupancy(p == 0 ? 32 : 64, c, &b));
             e->occ_[p][c] = std::max(b, 1);
@@ -277,17 +277,22 @@ void Engine::free_slot(Slot* s)
     delete s;
 }
 
-uint64_t Engine::arena_bytes_for(const Plan& plan) const
+uint64_t Engine::scratch_warps() const
 {
-    const uint64_t warps = (uint64_t)sms_ * occ_[1][8] * (kFwdBlock / kWarp);
-    return carve(need_of(plan, warps), nullptr, nullptr);
+    // Each resident warp of a multi-stripe class owns a scratch region of 24 bytes per column: two
+    // FP32 rows (one per read of the warp) or one FP64 row.
+    int occ = 1;
+    for (int c : {class32(kInter, 0, kMaxK, true), class32(kInter, 1, kMaxK, true), class32(kIntra, 1, kMaxK, true)})
+        occ = std::max(occ, occ_[0][c]);
+    for (int c : {class64(kInter, kMaxK, true), class64(kIntra, kMaxK, true)}) occ = std::max(occ, occ_[1][c]);
+    return (uint64_t)sms_ * occ * (kFwdBlock / kWarp);
 }
+
+uint64_t Engine::arena_bytes_for(const Plan& plan) const { return carve(need_of(plan, scratch_warps()), nullptr, nullptr); }
 
 phmm_status Engine::ensure_capacity(Slot& s, const Plan& plan, std::string& err)
 {
-    // multi-stripe scratch: one row per resident warp of the widest multi-stripe class
-    const uint64_t warps = (uint64_t)sms_ * std::max(occ_[0][8], occ_[1][8]) * (kFwdBlock / kWarp);
-    const Capacity need = need_of(plan, warps);
+    const Capacity need = need_of(plan, scratch_warps());
     if (s.dev && s.cap.covers(need)) return PHMM_OK;
     const Capacity nc = s.dev ? s.cap.grown_to(need) : need;
     PHMM_CK(cudaSetDevice(dev_));
@@ -353,7 +358,7 @@ phmm_status Engine::launch_pipeline(Slot& s, bool want_flags, const Plan* plan, 
     v.regions = s.d_regions;
     v.out = s.d_out;
     v.pair_flags = want_flags ? s.d_pair_flags : nullptr;
-    const uint64_t warps = (uint64_t)sms_ * std::max(occ_[0][8], occ_[1][8]) * (kFwdBlock / kWarp);
+    const uint64_t warps = scratch_warps();
     const unsigned int scr_cols = s.cap.scratch_cols ? (unsigned int)(s.cap.scratch_cols / warps) : 0u;
     const unsigned int rec = plan ? cudaEventRecordDefault : cudaEventRecordExternal;
 
@@ -364,15 +369,19 @@ phmm_status Engine::launch_pipeline(Slot& s, bool want_flags, const Plan* plan, 
     for (int pass = 0; pass < 2; ++pass) {
         const int precision = pass == 0 ? 32 : 64;
         PHMM_CK(cudaEventRecord(s.ev_fork, s.main));
-        for (int c = 0; c < kNumClasses; ++c) {
+        const int n_cls = pass == 0 ? kClasses32 : kClasses64;
+        const int slot0 = pass == 0 ? 0 : kClasses32;  // descriptor slot of the pass's first class
+        for (int c = 0; c < n_cls; ++c) {
             uint32_t work = 0;
             if (plan) {
-                work = pass == 0 ? plan->classes[c].n_items : plan->classes[c].rerun_cap;
+                work = pass == 0 ? plan->classes[c].n_items : plan->classes[slot0 + c].rerun_cap;
                 if (work == 0) continue;
             }
+            // FP32 items hold two reads (warps = items); FP64 claims are single pairs
             const int grid = plan ? grid_for(precision, c, work) : occ_[pass][c] * sms_;
             PassControl pc;
-            pc.cd = s.d_classes + c;
+            pc.cd = s.d_classes + slot0 + c;
+            pc.cd64 = s.d_classes + kClasses32;
             pc.items = s.d_items;
             pc.rerun = s.d_rerun;
             pc.status = s.d_status;
@@ -519,7 +528,7 @@ phmm_status Engine::finish(Slot& s, const Plan& plan, double* out, uint8_t* pair
     const ClassDesc* cls = (const ClassDesc*)(desc + sizeof(BatchDesc));
     const unsigned int status = *(const unsigned int*)(desc + sizeof(BatchDesc) + sizeof(ClassDesc) * kNumClasses);
     uint64_t f64 = 0;
-    for (int c = 0; c < kNumClasses; ++c) f64 += std::min(cls[c].rerun_count, cls[c].rerun_cap);
+    for (int c = kClasses32; c < kNumClasses; ++c) f64 += std::min(cls[c].rerun_count, cls[c].rerun_cap);
     if (stats) {
         stats->regions = plan.n_regions;
         stats->pairs = plan.pairs;
@@ -546,7 +555,7 @@ phmm_status Engine::finish(Slot& s, const Plan& plan, double* out, uint8_t* pair
     return PHMM_OK;
 }
 
-phmm_status Engine::fp32_fma_peak(double* tflops, std::string& err)
+phmm_status Engine::fp32_fma_peak(double* scalar_tflops, double* packed_tflops, std::string& err)
 {
     std::lock_guard<std::mutex> lk(mu_);
     PHMM_CK(cudaSetDevice(dev_));
@@ -554,20 +563,28 @@ phmm_status Engine::fp32_fma_peak(double* tflops, std::string& err)
     float* sink = nullptr;
     PHMM_CK(cudaMalloc(&sink, sizeof(float) * sms_ * 64));
     const int blocks = sms_ * 8, iters = 1 << 14;
-    launch_fma_peak(sink, blocks, 256, s.main);  // warm-up
-    cudaEventRecord(s.ev_t0, s.main);
-    launch_fma_peak(sink, blocks, iters, s.main);
-    cudaEventRecord(s.ev_t1, s.main);
-    cudaError_t e = cudaEventSynchronize(s.ev_t1);
-    float ms = 0;
-    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, s.ev_t0, s.ev_t1);
+    cudaError_t e = cudaSuccess;
+    for (int packed = 0; packed < 2 && e == cudaSuccess; ++packed) {
+        launch_fma_peak(sink, blocks, 256, packed != 0, s.main);  // warm-up
+        cudaEventRecord(s.ev_t0, s.main);
+        launch_fma_peak(sink, blocks, iters, packed != 0, s.main);
+        cudaEventRecord(s.ev_t1, s.main);
+        e = cudaEventSynchronize(s.ev_t1);
+        float ms = 0;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, s.ev_t0, s.ev_t1);
+        const double flops = 2.0 * 16.0 * (packed ? 2.0 : 1.0) * (double)iters * 256.0 * blocks;
+        const double tf = e == cudaSuccess ? flops / (ms * 1e-3) / 1e12 : 0.0;
+        if (packed) {
+            if (packed_tflops) *packed_tflops = tf;
+        } else if (scalar_tflops) {
+            *scalar_tflops = tf;
+        }
+    }
     cudaFree(sink);
     if (e != cudaSuccess) {
         err = std::string("FMA probe failed: ") + cudaGetErrorString(e);
         return PHMM_ERR_CUDA;
     }
-    const double flops = 2.0 * 16.0 * (double)iters * 256.0 * blocks;
-    *tflops = flops / (ms * 1e-3) / 1e12;
     return PHMM_OK;
 }
 

@@ -76,7 +76,7 @@ public:
     // restore = true resetting the descriptor from its pristine device copy first (replays).
     phmm_status upload(Slot& s, const Plan& plan, const phmm_batch& b, std::string& err);
     phmm_status run(Slot& s, const Plan& plan, bool want_flags, bool restore, std::string& err);
-    phmm_status fp32_fma_peak(double* tflops, std::string& err);
+    phmm_status fp32_fma_peak(double* scalar_tflops, double* packed_tflops, std::string& err);
 
     int device() const { return dev_; }
     int num_sms() const { return sms_; }
@@ -89,6 +89,7 @@ private:
     phmm_status launch_pipeline(Slot& s, bool want_flags, const Plan* plan, std::string& err);
     phmm_status capture_graph(Slot& s, bool want_flags, std::string& err);
     int grid_for(int precision, int cls, uint32_t work) const;
+    uint64_t scratch_warps() const;
 
     phmm_config cfg_{};
     int dev_ = 0;

@@ -6,8 +6,9 @@
 //   intra kernel (N wildcard)   (region API tests 'N' only, :422,:435)
 //   empty read or haplotype     src/haplotypecaller/pairhmm/roDV_schedule.cpp:460 (pair skipped,
 //                               its likelihood stays NaN, pairhmm_internal.cpp:593)
-// Instead of the reference's greedy SIMD grouping (roDV_schedule.cpp:87-142), every read becomes
-// one work item per run of its region's haplotypes: a warp streams all of them through the read.
+// Instead of the reference's greedy SIMD grouping (roDV_schedule.cpp:87-142), reads of a region are
+// paired (two reads per warp, equal kernel class) and each pair becomes one work item per run of
+// the region's haplotypes: the warp streams all of them through both reads.
 #include "phmm_plan.h"
 
 #include <algorithm>
@@ -18,6 +19,16 @@ namespace phmm {
 namespace {
 
 bool has_n(const uint8_t* p, uint64_t n) { return n > 0 && std::memchr(p, 'N', (size_t)n) != nullptr; }
+
+// True when every byte equals the first (OR of differences, so the loop vectorises).
+bool constant_run(const uint8_t* p, uint64_t n)
+{
+    if (n == 0) return true;
+    const uint8_t v = p[0];
+    uint8_t acc = 0;
+    for (uint64_t i = 1; i < n; ++i) acc |= (uint8_t)(p[i] ^ v);
+    return acc == 0;
+}
 
 struct Run {
     uint16_t lo, hi;
@@ -127,14 +138,19 @@ phmm_status build_plan(const phmm_batch& b, const PlanLimits& lim, Plan& plan, s
     for (uint64_t r = 0; r < nr; ++r)
         plan.read_flags[r] = has_n(rb + plan.read_off[r], plan.read_off[r + 1] - plan.read_off[r]);
 
-    // regions and work items, counted per (class, stream-length bucket) for a stable counting sort
+    // regions and work items, counted per (FP32 class, stream-length bucket) for a stable counting sort
     constexpr int kBuckets = 64;
     constexpr uint32_t kBucketCols = 128;
-    std::vector<uint32_t> count((size_t)kPlanClasses * kBuckets, 0);
+    std::vector<uint32_t> count((size_t)kClasses32 * kBuckets, 0);
     plan.regions.resize(b.n_regions);
     std::vector<Run> runs_split, runs_all, runs_split_m, runs_all_m;
     std::vector<WorkItem> raw;
     std::vector<uint32_t> raw_key;
+    struct ReadKey {
+        uint32_t key;  // (N, gap mode, stripes, kh) packed; reads with equal keys share a work item
+        uint32_t read;
+    };
+    std::vector<ReadKey> rk;
     uint64_t out_off = 0;
     uint32_t hap_begin = 0, read_begin = 0;
     for (uint32_t g = 0; g < b.n_regions; ++g) {
@@ -148,14 +164,31 @@ phmm_status build_plan(const phmm_batch& b, const PlanLimits& lim, Plan& plan, s
         rd.n_reads = N;
         const uint64_t* hoff = plan.hap_off.data() + hap_begin;
         const uint8_t* hfl = plan.hap_flags.data() + hap_begin;
-        bool runs_ready = false, runs_m_ready = false;
+        rk.clear();
         for (uint32_t r = 0; r < N; ++r) {
             const uint32_t gr = read_begin + r;
-            const uint64_t R = plan.read_off[gr + 1] - plan.read_off[gr];
+            const uint64_t a = plan.read_off[gr], R = plan.read_off[gr + 1] - a;
             if (R == 0) continue;
             const bool multi = R > (uint64_t)kWarp * kMaxK;
-            const int k = multi ? kMaxK : (int)((R + kWarp - 1) / kWarp);
-            const bool read_n = plan.read_flags[gr] & 1;
+            const uint32_t kh = multi ? kMaxK : (uint32_t)((R + kWarp - 1) / kWarp);
+            const uint32_t stripes = multi ? (uint32_t)((R + kWarp * kMaxK - 1) / (kWarp * kMaxK)) : 1;
+            const uint8_t* ib = b.read_ins + plan.read_base0 + a;
+            const uint8_t* db = b.read_del + plan.read_base0 + a;
+            const uint8_t* cb = b.read_gcp + plan.read_base0 + a;
+            const bool uniform = constant_run(ib, R) && constant_run(db, R) && constant_run(cb, R);
+            const uint32_t n_flag = plan.read_flags[gr] & 1;
+            rk.push_back({(n_flag << 20) | ((uniform ? 0u : 1u) << 19) | (stripes << 4) | kh, gr});
+        }
+        std::stable_sort(rk.begin(), rk.end(), [](const ReadKey& x, const ReadKey& y) { return x.key < y.key; });
+        bool runs_ready = false, runs_m_ready = false;
+        for (size_t k = 0; k < rk.size();) {
+            const uint32_t key = rk[k].key;
+            const uint32_t r0 = rk[k].read;
+            const uint32_t r1 = (k + 1 < rk.size() && rk[k + 1].key == key) ? rk[k + 1].read : kNoRead;
+            k += (r1 == kNoRead) ? 1 : 2;
+            const uint32_t kh = key & 0xf, stripes = (key >> 4) & 0x7fff;
+            const bool uniform = ((key >> 19) & 1) == 0, read_n = ((key >> 20) & 1) != 0;
+            const bool multi = stripes > 1;
             const std::vector<Run>* runs;
             if (!multi) {
                 if (!runs_ready) {
@@ -172,24 +205,30 @@ phmm_status build_plan(const phmm_batch& b, const PlanLimits& lim, Plan& plan, s
                 }
                 runs = read_n ? &runs_all_m : &runs_split_m;
             }
+            const uint64_t rows = (plan.read_off[r0 + 1] - plan.read_off[r0]) +
+                                  (r1 == kNoRead ? 0 : plan.read_off[r1 + 1] - plan.read_off[r1]);
+            const uint32_t nreads = r1 == kNoRead ? 1 : 2;
             for (const Run& run : *runs) {
                 WorkItem it{};
-                it.read = gr;
+                it.read[0] = r0;
+                it.read[1] = r1;
                 it.region = g;
                 it.hap_lo = run.lo;
                 it.hap_hi = run.hi;
-                it.k = (uint8_t)k;
-                it.stripes = (uint8_t)(multi ? (R + kWarp * kMaxK - 1) / (kWarp * kMaxK) : 1);
+                it.kh = (uint8_t)kh;
+                it.stripes = (uint8_t)stripes;
                 it.variant = read_n ? (uint8_t)kIntra : run.variant;
-                const int cls = plan_class(it.variant, k, multi);
+                it.pmode = (it.variant == kInter && uniform) ? 0 : 1;
+                const int c32 = class32(it.variant, it.pmode, (int)kh, multi);
                 const uint32_t bucket = std::min<uint32_t>(run.cols / kBucketCols, kBuckets - 1);
-                const uint32_t key = (uint32_t)cls * kBuckets + (kBuckets - 1 - bucket);  // longest first
+                const uint32_t skey = (uint32_t)c32 * kBuckets + (kBuckets - 1 - bucket);  // longest first
                 raw.push_back(it);
-                raw_key.push_back(key);
-                ++count[key];
-                plan.classes[cls].rerun_cap += run.hi - run.lo;
-                plan.pairs += run.hi - run.lo;
-                plan.cells += (uint64_t)run.cols * R;
+                raw_key.push_back(skey);
+                ++count[skey];
+                const uint32_t npairs = nreads * (uint32_t)(run.hi - run.lo);
+                plan.classes[kClasses32 + class64(it.variant, (int)kh, multi)].rerun_cap += npairs;
+                plan.pairs += npairs;
+                plan.cells += (uint64_t)run.cols * rows;
                 if (multi) plan.max_multi_stream = std::max(plan.max_multi_stream, run.cols);
             }
         }
@@ -208,15 +247,18 @@ phmm_status build_plan(const phmm_batch& b, const PlanLimits& lim, Plan& plan, s
         std::vector<uint32_t> pos(start.begin(), start.end() - 1);
         for (size_t i = 0; i < raw.size(); ++i) plan.items[pos[raw_key[i]]++] = raw[i];
     }
-    uint32_t rerun_off = 0;
-    for (int c = 0; c < kPlanClasses; ++c) {
+    for (int c = 0; c < kClasses32; ++c) {
         ClassDesc& cd = plan.classes[c];
         cd.item_off = start[(size_t)c * kBuckets];
         cd.n_items = start[(size_t)(c + 1) * kBuckets] - cd.item_off;
+    }
+    uint32_t rerun_off = 0;
+    for (int c = kClasses32; c < kPlanClasses; ++c) {
+        ClassDesc& cd = plan.classes[c];
         cd.rerun_off = rerun_off;
         rerun_off += cd.rerun_cap;
-        cd.claim32 = cd.claim64 = cd.rerun_count = 0;
     }
+    for (ClassDesc& cd : plan.classes) cd.claim32 = cd.claim64 = cd.rerun_count = 0;
     plan.rerun_slots = rerun_off;
     return PHMM_OK;
 }

@@ -11,7 +11,8 @@
 
 namespace phmm {
 
-constexpr int kPlanClasses = 18;  // same numbering as phmm_kernels.h
+// Descriptor slots: the 27 FP32 classes, then the 18 FP64 classes (numbering in phmm_types.h).
+constexpr int kPlanClasses = kClasses32 + kClasses64;
 
 struct PlanLimits {
     // Reference limits, roDV_schedule.cpp:70-73 (haplotype index <= 4095, read length <= 768,
@@ -34,7 +35,7 @@ struct Plan {
     std::vector<uint64_t> read_off, hap_off;  // rebased to start at 0
     std::vector<uint8_t> read_flags, hap_flags;
     std::vector<WorkItem> items;
-    std::vector<ClassDesc> classes;  // kPlanClasses
+    std::vector<ClassDesc> classes;  // kPlanClasses: FP32 classes (items), then FP64 (rerun segments)
     uint64_t rerun_slots = 0;
     uint32_t max_multi_stream = 0;   // longest stream among multi-stripe items (0 if none)
 };
@@ -42,6 +43,6 @@ struct Plan {
 // Returns PHMM_OK, PHMM_ERR_INVALID_ARGUMENT or PHMM_ERR_LIMIT_EXCEEDED (err holds the detail).
 phmm_status build_plan(const phmm_batch& b, const PlanLimits& lim, Plan& plan, std::string& err);
 
-inline int plan_class(int variant, int k, bool multi) { return variant * 9 + (multi ? 8 : k - 1); }
+
 
 }  // namespace phmm

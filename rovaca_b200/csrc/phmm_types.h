@@ -18,6 +18,19 @@ constexpr int kChunk = 8;         // steps per boundary-free fast chunk
 
 enum Variant : int { kInter = 0, kIntra = 1 };
 
+// Kernel classes.  FP64 (scalar, 32 lanes per read): variant * 9 + (multi ? 8 : K - 1) with
+// K = ceil(R / 32).  FP32 (packed, 16 lanes per read, KH = ceil(R / 32) row pairs per lane):
+// 0..8 inter with constant gap parameters, 9..17 inter per-row, 18..26 intra per-row, each
+// (multi ? 8 : KH - 1).
+constexpr int kClasses64 = 18;
+constexpr int kClasses32 = 27;
+PHMM_HD inline int class64(int variant, int k, bool multi) { return variant * 9 + (multi ? 8 : k - 1); }
+PHMM_HD inline int class32(int variant, int pmode, int kh, bool multi)
+{
+    const int base = variant == 1 ? 18 : (pmode == 0 ? 0 : 9);
+    return base + (multi ? 8 : kh - 1);
+}
+
 struct RegionDesc {               // 32 bytes
     uint64_t out_off;             // first likelihood of this region in the output
     uint32_t hap_begin;           // global index of the region's first haplotype
@@ -27,14 +40,17 @@ struct RegionDesc {               // 32 bytes
     uint32_t pad0, pad1;
 };
 
-struct WorkItem {                 // 16 bytes
-    uint32_t read;                // global read index
+// FP32 work item: two reads of one region (one per 16-lane group; read[1] may be kNoRead) against a
+// run of the region's haplotypes.
+constexpr uint32_t kNoRead = 0xffffffffu;
+struct WorkItem {                 // 20 bytes
+    uint32_t read[2];             // global read indices
     uint32_t region;
     uint16_t hap_lo, hap_hi;      // haplotype range inside the region, [lo, hi)
-    uint8_t k;                    // rows per lane
-    uint8_t stripes;              // 32*k-row stripes
+    uint8_t kh;                   // row pairs per lane (rows per 256-row stripe / 32)
+    uint8_t stripes;              // 256-row stripes (1 unless the reads are longer than 256)
     uint8_t variant;              // Variant
-    uint8_t pad;
+    uint8_t pmode;                // ParamMode of the FP32 kernel (0: gap parameters constant)
 };
 
 struct RerunEntry {               // 16 bytes: one pair whose FP32 sum fell below 1e-28
@@ -98,6 +114,7 @@ enum StatusBits : unsigned int {
 
 struct PassControl {
     ClassDesc* cd;                // this class's descriptor
+    ClassDesc* cd64;              // FP32 pass: descriptors of the FP64 classes (rerun segments)
     const WorkItem* items;        // all work items (class slice at cd->item_off)
     RerunEntry* rerun;            // all rerun slots (class segment at cd->rerun_off)
     unsigned int* status;         // StatusBits, OR-ed

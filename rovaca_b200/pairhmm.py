@@ -167,7 +167,7 @@ class PackedBatch:
 def plan_summary(batch: PackedBatch) -> dict:
     """How the engine cuts a batch into work (host only): items and pairs per kernel class."""
     lib = _lib.load()
-    items = np.zeros(18, np.uint32)
+    items = np.zeros(27, np.uint32)
     pairs = np.zeros(18, np.uint64)
     tp, tc = C.c_uint64(), C.c_uint64()
     b = batch.as_c()
@@ -239,11 +239,12 @@ class Engine:
     def resident(self, batch: PackedBatch, want_flags: bool = False) -> "ResidentBatch":
         return ResidentBatch(self, batch, want_flags)
 
-    def fp32_fma_peak(self) -> float:
-        """Measured FP32 FMA throughput of the device, TFLOP/s (an FMA counts 2 FLOPs)."""
-        v = C.c_double()
-        check(self._lib.phmm_fp32_fma_peak(self._h, C.byref(v)))
-        return v.value
+    def fp32_fma_peak(self) -> tuple[float, float]:
+        """Measured FP32 FMA throughput of the device, TFLOP/s (an FMA counts 2 FLOPs): with scalar
+        FFMA and with packed FFMA2 instructions."""
+        a, b = C.c_double(), C.c_double()
+        check(self._lib.phmm_fp32_fma_peak(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
 
     # ---- serving loop ------------------------------------------------------------------
     def submit(self, region: PackedBatch, out: np.ndarray, flags: np.ndarray | None = None) -> int:

@@ -61,17 +61,26 @@ def test_engine_refuses_to_run_without_a_gpu():
 
 # ---- planning -------------------------------------------------------------------------------
 
-def cls(variant, k, multi=False):
-    return variant * 9 + (8 if multi else k - 1)
+def cls(variant, kh, multi=False, uniform=True):
+    """FP32 kernel class: 0.. inter with constant gap qualities, 9.. inter per-row, 18.. intra."""
+    base = 18 if variant else (0 if uniform else 9)
+    return base + (8 if multi else kh - 1)
+
+
+def cls64(variant, kh, multi=False):
+    return variant * 9 + (8 if multi else kh - 1)
 
 
 def test_plan_rows_per_lane_follow_read_length():
     hap = b"ACGT" * 100
     reads = [hap[:n] for n in (1, 32, 33, 64, 100, 151, 200, 256)]
     s = plan_summary(PackedBatch.from_regions([_region([hap, hap[3:]], reads)]))
-    want = {1: 2, 2: 2, 4: 1, 5: 1, 7: 1, 8: 1}  # K = ceil(R / 32): items per K (one item per read)
+    # KH = ceil(R / 32) row pairs per lane; reads of equal KH share an item (two reads per warp)
+    want = {1: 1, 2: 1, 4: 1, 5: 1, 7: 1, 8: 1}
     for k, n in want.items():
         assert s["class_items"][cls(0, k)] == n, (k, s["class_items"])
+    assert s["class_items"].sum() == 6
+    assert s["class_pairs"][cls64(0, 1)] == 4 and s["class_pairs"][cls64(0, 8)] == 2
     assert s["pairs"] == 16
     assert s["cells"] == sum(len(r) for r in reads) * (len(hap) + len(hap) - 3)
 
@@ -91,8 +100,9 @@ def test_plan_routes_n_pairs_to_the_intra_variant():
     # read with N: every pair intra; reads without N: the N haplotype alone is intra
     assert s["class_pairs"][9:].sum() == 3 + 2
     assert s["class_pairs"][:9].sum() == 2 * 2
-    # a read without N streams [h] and [h] as two inter items split around the N haplotype
-    assert s["class_items"][:9].sum() == 4
+    # each read without N streams [h] and [h] as two inter items split around the N haplotype
+    assert s["class_items"][:18].sum() == 4
+    assert s["class_items"][18:].sum() == 3
 
 
 def test_plan_splits_long_haplotype_streams():
@@ -100,6 +110,19 @@ def test_plan_splits_long_haplotype_streams():
     s = plan_summary(PackedBatch.from_regions([_region(haps, [b"A" * 100])]))
     assert s["class_items"][cls(0, 4)] == 4  # 5 haplotypes (7500 columns) per item
     assert s["pairs"] == 20
+
+
+def test_plan_pairs_reads_and_gap_modes():
+    hap = b"ACGT" * 60
+    reads = [hap[k:k + 150] for k in range(5)]  # five reads of KH 5: items of 2 + 2 + 1
+    reg = _region([hap], reads)
+    s = plan_summary(PackedBatch.from_regions([reg]))
+    assert s["class_items"][cls(0, 5)] == 3 and s["pairs"] == 5
+    # varying gap-open qualities along a read select the per-row class
+    reg.insertion_qualities[0] = bytes([45] * 149 + [40])
+    s = plan_summary(PackedBatch.from_regions([reg]))
+    assert s["class_items"][cls(0, 5, uniform=False)] == 1
+    assert s["class_items"][cls(0, 5)] == 2
 
 
 def test_plan_skips_empty_reads_and_haplotypes():
