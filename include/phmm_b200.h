@@ -140,6 +140,21 @@ PHMM_API phmm_status phmm_call_region(phmm_engine* engine, uint32_t n_haps, cons
                              const uint64_t* read_off, const uint8_t* mapq, int32_t min_quality_threshold,
                              int32_t pcr_model, double* out, uint8_t* keep, uint32_t* n_kept);
 
+/* ---- batches without device allocation -------------------------------------------------- */
+
+/* Same computation and result layout as phmm_compute_regions, for callers that cannot call
+ * cudaMalloc (a process whose GPU memory belongs to another framework's pool allocator, or a host
+ * that forbids allocation on its worker threads): it allocates no device or pinned memory.  All
+ * device data of the call lives in a fixed 64 MiB array that is part of this library's device code
+ * (every GPU that loads the library holds it until the process exits).  A batch that needs more
+ * than that (about 100 regions of the benchmark's shape) is rejected with PHMM_ERR_LIMIT_EXCEEDED.
+ * Synchronous; calls on one device are serialised and share the array.  The first call on a device
+ * sets that device up (looks up the array's address, uploads the probability tables): make it
+ * before any stream capture on the device.  No counterpart in the reference: an addition of this
+ * library. */
+PHMM_API phmm_status phmm_compute_regions_noalloc(const phmm_batch* batch, double* out, uint8_t* pair_flags,
+                                                  int32_t device);
+
 /* ---- device-resident batches ------------------------------------------------------------ */
 
 typedef struct phmm_resident phmm_resident;

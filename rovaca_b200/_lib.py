@@ -81,6 +81,7 @@ def load() -> C.CDLL:
         "phmm_resident_results": (I32, [P, P, P]),
         "phmm_resident_destroy": (I32, [P]),
         "phmm_fp32_fma_peak": (I32, [P, C.POINTER(D), C.POINTER(D)]),
+        "phmm_compute_regions_noalloc": (I32, [C.POINTER(Batch), P, P, I32]),
         "phmm_host_plan_summary": (I32, [C.POINTER(Batch), P, P, C.POINTER(U64), C.POINTER(U64)]),
         "phmm_submit": (I32, [P, C.POINTER(Batch), P, P, C.POINTER(U64)]),
         "phmm_poll": (I32, [P, U64, C.POINTER(I32)]),

@@ -164,6 +164,18 @@ class PackedBatch:
         return b
 
 
+def compute_noalloc(batch: PackedBatch, device: int = 0, want_flags: bool = False):
+    """phmm_compute_regions_noalloc: the batch computation without any device allocation (for
+    callers that cannot call cudaMalloc); all device data lives in the library's fixed 64 MiB array.
+    Returns (likelihoods, flags or None) in the layout of Engine.compute."""
+    lib = _lib.load()
+    out = np.empty(batch.out_size, np.float64)
+    fl = np.empty(batch.out_size, np.uint8) if want_flags else None
+    b = batch.as_c()
+    check(lib.phmm_compute_regions_noalloc(C.byref(b), _ptr(out), _ptr(fl), device))
+    return out, fl
+
+
 def plan_summary(batch: PackedBatch) -> dict:
     """How the engine cuts a batch into work (host only): items and pairs per kernel class."""
     lib = _lib.load()
@@ -369,4 +381,4 @@ def call_pairhmm(haplotypes, reads, base_quals, mapq, min_quality_threshold: int
 
 
 __all__ = ["Engine", "Region", "PackedBatch", "PhmmError", "schedule_pairhmm", "call_pairhmm", "default_engine",
-           "plan_summary"]
+           "plan_summary", "compute_noalloc"]
