@@ -13,6 +13,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <thread>
 
 namespace phmm {
 
@@ -20,15 +21,8 @@ namespace {
 
 bool has_n(const uint8_t* p, uint64_t n) { return n > 0 && std::memchr(p, 'N', (size_t)n) != nullptr; }
 
-// True when every byte equals the first (OR of differences, so the loop vectorises).
-bool constant_run(const uint8_t* p, uint64_t n)
-{
-    if (n == 0) return true;
-    const uint8_t v = p[0];
-    uint8_t acc = 0;
-    for (uint64_t i = 1; i < n; ++i) acc |= (uint8_t)(p[i] ^ v);
-    return acc == 0;
-}
+// True when every byte equals the first: the array equals itself shifted by one.
+bool constant_run(const uint8_t* p, uint64_t n) { return n < 2 || std::memcmp(p, p + 1, (size_t)(n - 1)) == 0; }
 
 struct Run {
     uint16_t lo, hi;
@@ -133,119 +127,165 @@ phmm_status build_plan(const phmm_batch& b, const PlanLimits& lim, Plan& plan, s
     const uint8_t* rb = b.read_bases + plan.read_base0;
 
     plan.hap_flags.resize(nh);
-    for (uint64_t h = 0; h < nh; ++h) plan.hap_flags[h] = has_n(hb + plan.hap_off[h], plan.hap_off[h + 1] - plan.hap_off[h]);
     plan.read_flags.resize(nr);
-    for (uint64_t r = 0; r < nr; ++r)
-        plan.read_flags[r] = has_n(rb + plan.read_off[r], plan.read_off[r + 1] - plan.read_off[r]);
+    plan.regions.resize(b.n_regions);
+    {
+        uint64_t out_off = 0;
+        uint32_t hap_begin = 0, read_begin = 0;
+        for (uint32_t g = 0; g < b.n_regions; ++g) {
+            RegionDesc& rd = plan.regions[g];
+            rd = RegionDesc{};
+            rd.out_off = out_off;
+            rd.hap_begin = hap_begin;
+            rd.n_haps = b.n_haps[g];
+            rd.read_begin = read_begin;
+            rd.n_reads = b.n_reads[g];
+            out_off += (uint64_t)b.n_haps[g] * b.n_reads[g];
+            hap_begin += b.n_haps[g];
+            read_begin += b.n_reads[g];
+        }
+        plan.out_total = out_off;
+    }
 
-    // regions and work items, counted per (FP32 class, stream-length bucket) for a stable counting sort
+    // Regions are planned independently on host threads: N flags, gap modes, read pairing,
+    // haplotype runs and work items, each counted per (FP32 class, stream-length bucket).
     constexpr int kBuckets = 64;
     constexpr uint32_t kBucketCols = 128;
-    std::vector<uint32_t> count((size_t)kClasses32 * kBuckets, 0);
-    plan.regions.resize(b.n_regions);
-    std::vector<Run> runs_split, runs_all, runs_split_m, runs_all_m;
-    std::vector<WorkItem> raw;
-    std::vector<uint32_t> raw_key;
-    struct ReadKey {
-        uint32_t key;  // (N, gap mode, stripes, kh) packed; reads with equal keys share a work item
-        uint32_t read;
+    struct Part {
+        std::vector<WorkItem> raw;
+        std::vector<uint32_t> key;
+        std::vector<uint32_t> count;
+        uint64_t rerun_cap[kClasses64] = {};
+        uint64_t pairs = 0, cells = 0;
+        uint32_t max_multi = 0;
     };
-    std::vector<ReadKey> rk;
-    uint64_t out_off = 0;
-    uint32_t hap_begin = 0, read_begin = 0;
-    for (uint32_t g = 0; g < b.n_regions; ++g) {
-        const uint32_t M = b.n_haps[g], N = b.n_reads[g];
-        RegionDesc& rd = plan.regions[g];
-        rd = RegionDesc{};
-        rd.out_off = out_off;
-        rd.hap_begin = hap_begin;
-        rd.n_haps = M;
-        rd.read_begin = read_begin;
-        rd.n_reads = N;
-        const uint64_t* hoff = plan.hap_off.data() + hap_begin;
-        const uint8_t* hfl = plan.hap_flags.data() + hap_begin;
-        rk.clear();
-        for (uint32_t r = 0; r < N; ++r) {
-            const uint32_t gr = read_begin + r;
-            const uint64_t a = plan.read_off[gr], R = plan.read_off[gr + 1] - a;
-            if (R == 0) continue;
-            const bool multi = R > (uint64_t)kWarp * kMaxK;
-            const uint32_t kh = multi ? kMaxK : (uint32_t)((R + kWarp - 1) / kWarp);
-            const uint32_t stripes = multi ? (uint32_t)((R + kWarp * kMaxK - 1) / (kWarp * kMaxK)) : 1;
-            const uint8_t* ib = b.read_ins + plan.read_base0 + a;
-            const uint8_t* db = b.read_del + plan.read_base0 + a;
-            const uint8_t* cb = b.read_gcp + plan.read_base0 + a;
-            const bool uniform = constant_run(ib, R) && constant_run(db, R) && constant_run(cb, R);
-            const uint32_t n_flag = plan.read_flags[gr] & 1;
-            rk.push_back({(n_flag << 20) | ((uniform ? 0u : 1u) << 19) | (stripes << 4) | kh, gr});
-        }
-        std::stable_sort(rk.begin(), rk.end(), [](const ReadKey& x, const ReadKey& y) { return x.key < y.key; });
-        bool runs_ready = false, runs_m_ready = false;
-        for (size_t k = 0; k < rk.size();) {
-            const uint32_t key = rk[k].key;
-            const uint32_t r0 = rk[k].read;
-            const uint32_t r1 = (k + 1 < rk.size() && rk[k + 1].key == key) ? rk[k + 1].read : kNoRead;
-            k += (r1 == kNoRead) ? 1 : 2;
-            const uint32_t kh = key & 0xf, stripes = (key >> 4) & 0x7fff;
-            const bool uniform = ((key >> 19) & 1) == 0, read_n = ((key >> 20) & 1) != 0;
-            const bool multi = stripes > 1;
-            const std::vector<Run>* runs;
-            if (!multi) {
-                if (!runs_ready) {
-                    make_runs(hoff, hfl, M, lim.max_stream_single, true, runs_split);
-                    make_runs(hoff, hfl, M, lim.max_stream_single, false, runs_all);
-                    runs_ready = true;
-                }
-                runs = read_n ? &runs_all : &runs_split;
-            } else {
-                if (!runs_m_ready) {
-                    make_runs(hoff, hfl, M, lim.max_stream_multi, true, runs_split_m);
-                    make_runs(hoff, hfl, M, lim.max_stream_multi, false, runs_all_m);
-                    runs_m_ready = true;
-                }
-                runs = read_n ? &runs_all_m : &runs_split_m;
+    auto plan_range = [&](uint32_t g0, uint32_t g1, Part& part) {
+        part.count.assign((size_t)kClasses32 * kBuckets, 0);
+        std::vector<Run> runs_split, runs_all, runs_split_m, runs_all_m;
+        struct ReadKey {
+            uint32_t key;  // (N, gap mode, stripes, kh) packed; reads with equal keys share a work item
+            uint32_t read;
+        };
+        std::vector<ReadKey> rk;
+        for (uint32_t g = g0; g < g1; ++g) {
+            const RegionDesc& rd = plan.regions[g];
+            const uint32_t M = rd.n_haps, N = rd.n_reads, hap_begin = rd.hap_begin, read_begin = rd.read_begin;
+            for (uint32_t h = hap_begin; h < hap_begin + M; ++h)
+                plan.hap_flags[h] = has_n(hb + plan.hap_off[h], plan.hap_off[h + 1] - plan.hap_off[h]);
+            const uint64_t* hoff = plan.hap_off.data() + hap_begin;
+            const uint8_t* hfl = plan.hap_flags.data() + hap_begin;
+            rk.clear();
+            for (uint32_t r = 0; r < N; ++r) {
+                const uint32_t gr = read_begin + r;
+                const uint64_t a = plan.read_off[gr], R = plan.read_off[gr + 1] - a;
+                plan.read_flags[gr] = has_n(rb + a, R);
+                if (R == 0) continue;
+                const bool multi = R > (uint64_t)kWarp * kMaxK;
+                const uint32_t kh = multi ? kMaxK : (uint32_t)((R + kWarp - 1) / kWarp);
+                const uint32_t stripes = multi ? (uint32_t)((R + kWarp * kMaxK - 1) / (kWarp * kMaxK)) : 1;
+                const uint8_t* ib = b.read_ins + plan.read_base0 + a;
+                const uint8_t* db = b.read_del + plan.read_base0 + a;
+                const uint8_t* cb = b.read_gcp + plan.read_base0 + a;
+                const bool uniform = constant_run(ib, R) && constant_run(db, R) && constant_run(cb, R);
+                const uint32_t n_flag = plan.read_flags[gr] & 1;
+                rk.push_back({(n_flag << 20) | ((uniform ? 0u : 1u) << 19) | (stripes << 4) | kh, gr});
             }
-            const uint64_t rows = (plan.read_off[r0 + 1] - plan.read_off[r0]) +
-                                  (r1 == kNoRead ? 0 : plan.read_off[r1 + 1] - plan.read_off[r1]);
-            const uint32_t nreads = r1 == kNoRead ? 1 : 2;
-            for (const Run& run : *runs) {
-                WorkItem it{};
-                it.read[0] = r0;
-                it.read[1] = r1;
-                it.region = g;
-                it.hap_lo = run.lo;
-                it.hap_hi = run.hi;
-                it.kh = (uint8_t)kh;
-                it.stripes = (uint8_t)stripes;
-                it.variant = read_n ? (uint8_t)kIntra : run.variant;
-                it.pmode = (it.variant == kInter && uniform) ? 0 : 1;
-                const int c32 = class32(it.variant, it.pmode, (int)kh, multi);
-                const uint32_t bucket = std::min<uint32_t>(run.cols / kBucketCols, kBuckets - 1);
-                const uint32_t skey = (uint32_t)c32 * kBuckets + (kBuckets - 1 - bucket);  // longest first
-                raw.push_back(it);
-                raw_key.push_back(skey);
-                ++count[skey];
-                const uint32_t npairs = nreads * (uint32_t)(run.hi - run.lo);
-                plan.classes[kClasses32 + class64(it.variant, (int)kh, multi)].rerun_cap += npairs;
-                plan.pairs += npairs;
-                plan.cells += (uint64_t)run.cols * rows;
-                if (multi) plan.max_multi_stream = std::max(plan.max_multi_stream, run.cols);
+            std::stable_sort(rk.begin(), rk.end(), [](const ReadKey& x, const ReadKey& y) { return x.key < y.key; });
+            bool runs_ready = false, runs_m_ready = false;
+            for (size_t k = 0; k < rk.size();) {
+                const uint32_t key = rk[k].key;
+                const uint32_t r0 = rk[k].read;
+                const uint32_t r1 = (k + 1 < rk.size() && rk[k + 1].key == key) ? rk[k + 1].read : kNoRead;
+                k += (r1 == kNoRead) ? 1 : 2;
+                const uint32_t kh = key & 0xf, stripes = (key >> 4) & 0x7fff;
+                const bool uniform = ((key >> 19) & 1) == 0, read_n = ((key >> 20) & 1) != 0;
+                const bool multi = stripes > 1;
+                const std::vector<Run>* runs;
+                if (!multi) {
+                    if (!runs_ready) {
+                        make_runs(hoff, hfl, M, lim.max_stream_single, true, runs_split);
+                        make_runs(hoff, hfl, M, lim.max_stream_single, false, runs_all);
+                        runs_ready = true;
+                    }
+                    runs = read_n ? &runs_all : &runs_split;
+                } else {
+                    if (!runs_m_ready) {
+                        make_runs(hoff, hfl, M, lim.max_stream_multi, true, runs_split_m);
+                        make_runs(hoff, hfl, M, lim.max_stream_multi, false, runs_all_m);
+                        runs_m_ready = true;
+                    }
+                    runs = read_n ? &runs_all_m : &runs_split_m;
+                }
+                const uint64_t rows = (plan.read_off[r0 + 1] - plan.read_off[r0]) +
+                                      (r1 == kNoRead ? 0 : plan.read_off[r1 + 1] - plan.read_off[r1]);
+                const uint32_t nreads = r1 == kNoRead ? 1 : 2;
+                for (const Run& run : *runs) {
+                    WorkItem it{};
+                    it.read[0] = r0;
+                    it.read[1] = r1;
+                    it.region = g;
+                    it.hap_lo = run.lo;
+                    it.hap_hi = run.hi;
+                    it.kh = (uint8_t)kh;
+                    it.stripes = (uint8_t)stripes;
+                    it.variant = read_n ? (uint8_t)kIntra : run.variant;
+                    it.pmode = (it.variant == kInter && uniform) ? 0 : 1;
+                    const int c32 = class32(it.variant, it.pmode, (int)kh, multi);
+                    const uint32_t bucket = std::min<uint32_t>(run.cols / kBucketCols, kBuckets - 1);
+                    const uint32_t skey = (uint32_t)c32 * kBuckets + (kBuckets - 1 - bucket);  // longest first
+                    part.raw.push_back(it);
+                    part.key.push_back(skey);
+                    ++part.count[skey];
+                    const uint32_t npairs = nreads * (uint32_t)(run.hi - run.lo);
+                    part.rerun_cap[class64(it.variant, (int)kh, multi)] += npairs;
+                    part.pairs += npairs;
+                    part.cells += (uint64_t)run.cols * rows;
+                    if (multi) part.max_multi = std::max(part.max_multi, run.cols);
+                }
             }
         }
-        out_off += (uint64_t)M * N;
-        hap_begin += M;
-        read_begin += N;
+    };
+    const uint64_t work = plan.read_bases + plan.hap_bases;
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const unsigned nthreads = (unsigned)std::min<uint64_t>({hw, 32u, b.n_regions, work / (1u << 20) + 1});
+    std::vector<Part> parts(nthreads);
+    {
+        // contiguous region ranges with about equal bases each
+        std::vector<uint32_t> cut(nthreads + 1, b.n_regions);
+        cut[0] = 0;
+        uint64_t acc = 0;
+        unsigned t = 1;
+        for (uint32_t g = 0; g < b.n_regions && t < nthreads; ++g) {
+            const RegionDesc& rd = plan.regions[g];
+            acc += plan.read_off[rd.read_begin + rd.n_reads] - plan.read_off[rd.read_begin] +
+                   plan.hap_off[rd.hap_begin + rd.n_haps] - plan.hap_off[rd.hap_begin];
+            if (acc * nthreads >= work * t) cut[t++] = g + 1;
+        }
+        std::vector<std::thread> pool;
+        for (unsigned t2 = 1; t2 < nthreads; ++t2) pool.emplace_back(plan_range, cut[t2], cut[t2 + 1], std::ref(parts[t2]));
+        plan_range(cut[0], cut[1], parts[0]);
+        for (auto& th : pool) th.join();
     }
-    plan.out_total = out_off;
-    plan.empty_pairs = out_off - plan.pairs;
+    std::vector<uint32_t> count((size_t)kClasses32 * kBuckets, 0);
+    size_t n_items = 0;
+    for (const Part& p : parts) {
+        for (size_t i = 0; i < count.size(); ++i) count[i] += p.count[i];
+        for (int c = 0; c < kClasses64; ++c) plan.classes[kClasses32 + c].rerun_cap += (uint32_t)p.rerun_cap[c];
+        plan.pairs += p.pairs;
+        plan.cells += p.cells;
+        plan.max_multi_stream = std::max(plan.max_multi_stream, p.max_multi);
+        n_items += p.raw.size();
+    }
+    plan.empty_pairs = plan.out_total - plan.pairs;
 
-    // stable counting sort by key
+    // stable counting sort by key (parts in region order)
     std::vector<uint32_t> start(count.size() + 1, 0);
     for (size_t i = 0; i < count.size(); ++i) start[i + 1] = start[i] + count[i];
-    plan.items.resize(raw.size());
+    plan.items.resize(n_items);
     {
         std::vector<uint32_t> pos(start.begin(), start.end() - 1);
-        for (size_t i = 0; i < raw.size(); ++i) plan.items[pos[raw_key[i]]++] = raw[i];
+        for (const Part& p : parts)
+            for (size_t i = 0; i < p.raw.size(); ++i) plan.items[pos[p.key[i]]++] = p.raw[i];
     }
     for (int c = 0; c < kClasses32; ++c) {
         ClassDesc& cd = plan.classes[c];
