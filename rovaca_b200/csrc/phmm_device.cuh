@@ -36,6 +36,14 @@
 
 namespace phmm {
 
+// Steps per boundary-free chunk of the scalar sweep (the FP64 recompute), a build-time setting:
+// the double-precision cell update is about twice the code of the FP32 one, so the unrolled chunk
+// decides how much of the hot loop the instruction cache has to hold.
+#ifndef PHMM_CHUNK_SCALAR
+#define PHMM_CHUNK_SCALAR 8
+#endif
+constexpr int kChunkScalar = PHMM_CHUNK_SCALAR;
+
 // Explicitly rounded arithmetic: these are never contracted or reassociated by the compiler.
 __device__ __forceinline__ float rmul(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ float rfma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
@@ -63,6 +71,14 @@ struct Scale<double> {
     __device__ static double initial() { return 1.1235582092889474e307; }  // 2^1020
     __device__ static double log10_initial() { return 307.050595577260822; }
 };
+
+// Lane 0 claims the warp's next work index from a per-class counter.
+__device__ __forceinline__ unsigned int claim(unsigned int* counter, int lane)
+{
+    unsigned int idx = 0;
+    if (lane == 0) idx = atomicAdd(counter, 1u);
+    return __shfl_sync(0xffffffffu, idx, 0);
+}
 
 template <typename T>
 __device__ __forceinline__ T shfl_up1(T v)
@@ -121,7 +137,7 @@ __device__ __forceinline__ void cells(LaneRows<T, K>& L, uint32_t hc, T sM, T sI
 #pragma unroll
     for (int k = 0; k < K; ++k) {
         const T oM = L.Mp[k], oI = L.Ip[k], oD = L.Dp[k];
-        const T prior = (hc & L.rc[k]) ? L.pa[k] : L.pb[k];
+        const T prior = codes_match(hc, L.rc[k], V) ? L.pa[k] : L.pb[k];
         T s;
         if (V == kInter)
             s = ftz(rfma(diD, L.gm[k], ftz(rfma(diM, L.mm[k], ftz(rmul(diI, L.gm[k]))))));
@@ -258,16 +274,16 @@ __device__ void sweep(LaneRows<T, K>& L, const BatchView& b, const PassControl& 
         }
     };
 
-    for (int t0 = 0; t0 < steps; t0 += kChunk) {
-        // Lanes cover stream columns [t0-31, t0+kChunk-1] in this chunk.  Lane 31 trails, so its
-        // next boundary is the first boundary at or after t0-31: past the chunk means no lane
+    for (int t0 = 0; t0 < steps; t0 += kChunkScalar) {
+        // Lanes cover stream columns [t0-31, t0+kChunkScalar-1] in this chunk.  Lane 31 trails, so
+        // its next boundary is the first boundary at or after t0-31: past the chunk means no lane
         // meets a boundary and the chunk needs no per-step check.
         const int nb31 = __shfl_sync(0xffffffffu, nb, kWarp - 1);
-        if (nb31 >= t0 + kChunk && t0 + kChunk <= steps) {
+        if (nb31 >= t0 + kChunkScalar && t0 + kChunkScalar <= steps) {
 #pragma unroll
-            for (int u = 0; u < kChunk; ++u) step(t0 + u, false);
+            for (int u = 0; u < kChunkScalar; ++u) step(t0 + u, false);
         } else {
-            for (int u = 0; u < kChunk; ++u)
+            for (int u = 0; u < kChunkScalar; ++u)
                 if (t0 + u < steps) step(t0 + u, true);
         }
     }

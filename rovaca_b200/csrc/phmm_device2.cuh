@@ -125,7 +125,8 @@ __device__ __forceinline__ void cells2(LaneRows2<KH, PM>& L, uint32_t hcA, uint3
     for (int a = 0; a < KH; ++a) {
         const int r = PM == PM_ROW ? a : 0;
         const float2 oM = L.Mp[a], oI = L.Ip[a], oD = L.Dp[a];
-        const float2 prior = f2((hcA & L.rcA[a]) ? L.pa[a].x : L.pb[a].x, (hcB & L.rcB[a]) ? L.pa[a].y : L.pb[a].y);
+        const float2 prior = f2(codes_match(hcA, L.rcA[a], V) ? L.pa[a].x : L.pb[a].x,
+                                codes_match(hcB, L.rcB[a], V) ? L.pa[a].y : L.pb[a].y);
         float2 s;
         if (V == kInter)
             s = rfma2(dgD, L.gm[r], rfma2(dgM, L.mm[r], rmul2(dgI, L.gm[r])));

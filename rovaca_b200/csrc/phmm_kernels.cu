@@ -89,13 +89,6 @@ __device__ __forceinline__ void run_read(const BatchView& b, const ProbTables<T>
     }
 }
 
-__device__ __forceinline__ unsigned int claim(unsigned int* counter, int lane)
-{
-    unsigned int idx = 0;
-    if (lane == 0) idx = atomicAdd(counter, 1u);
-    return __shfl_sync(0xffffffffu, idx, 0);
-}
-
 // ------------------------------------------------------------------------------------------
 // FP32 pass for one class: two reads per warp against a run of haplotypes.
 // ------------------------------------------------------------------------------------------

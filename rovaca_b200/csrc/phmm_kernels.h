@@ -7,7 +7,10 @@
 
 namespace phmm {
 
-constexpr int kFwdBlock = 128;  // threads per block of the persistent wavefront kernels
+// Threads per block of the persistent wavefront kernels: one warp, so that resident warps are
+// limited by the register file at warp granularity (kernels with 170-250 registers per thread fit
+// 10-11 warps per SM instead of the 8 that four-warp blocks allow).
+constexpr int kFwdBlock = 32;
 
 // Kernel classes: see class32 / class64 in phmm_types.h.
 constexpr int kNumClasses = kClasses32 + kClasses64;  // descriptor slots: FP32 classes, then FP64

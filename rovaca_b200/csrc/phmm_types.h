@@ -14,7 +14,10 @@ namespace phmm {
 constexpr int kWarp = 32;
 constexpr int kMaxK = 8;          // rows per lane in one stripe (stripe = 256 rows)
 constexpr int kCodePad = 64;      // guard codes before/after the haplotype code stream
-constexpr int kChunk = 8;         // steps per boundary-free fast chunk
+#ifndef PHMM_CHUNK_PACKED
+#define PHMM_CHUNK_PACKED 8
+#endif
+constexpr int kChunk = PHMM_CHUNK_PACKED;  // steps per boundary-free fast chunk of the FP32 sweep
 
 enum Variant : int { kInter = 0, kIntra = 1 };
 
@@ -122,21 +125,27 @@ struct PassControl {
     unsigned int scratch_cols;    // columns per warp scratch row
 };
 
-// Per-byte match codes.  A pair matches at (i, j) when code(read[i]) & code(hap[j]) != 0.
-// Inter variant (pairs without 'N'): raw byte equality, as pairhmm_inter.cpp:166-168 compares
-// bytes; A, C, G, T get one bit each and other letters a distinct bit of their own.
+// Per-byte match codes.
+// Inter variant (pairs without 'N'): the code is the byte itself and a pair matches at (i, j) when
+// code(read[i]) == code(hap[j]), the raw byte compare of pairhmm_inter.cpp:166-168.
 // Intra variant (pairs with an 'N'): the reference's base classes (common.h:42-55, letters other
-// than A/C/G/T/N fall in A's class) with N matching everything (pairhmm_impl.cpp:26-42).
+// than A/C/G/T/N fall in A's class) as one bit each, N matching everything (pairhmm_impl.cpp:26-42);
+// a pair matches when code(read[i]) & code(hap[j]) != 0.
 PHMM_HD inline uint32_t match_code(uint8_t b, int variant)
 {
+    if (variant == kInter) return b;
     switch (b) {
-    case 'A': return 1u;
     case 'C': return 2u;
     case 'G': return 4u;
     case 'T': return 8u;
-    case 'N': return variant == kIntra ? 0xffffffffu : (1u << (4 + ('N' % 28)));
-    default: return variant == kIntra ? 1u : (1u << (4 + (b % 28)));
+    case 'N': return 0xffffffffu;
+    default: return 1u;
     }
+}
+
+PHMM_HD inline bool codes_match(uint32_t hc, uint32_t rc, int variant)
+{
+    return variant == kInter ? hc == rc : (hc & rc) != 0u;
 }
 
 }  // namespace phmm

@@ -155,6 +155,33 @@ def test_random_lengths_all_classes(engine, oracle):
     assert np.array_equal(flags.astype(bool), used)
 
 
+def test_bytes_outside_acgtn(engine, oracle):
+    """Lower-case and IUPAC letters: pairs without 'N' compare raw bytes (so 'a' and 'E', or 'R' and
+    'R', are told apart or matched exactly as bytes), pairs with 'N' use the reference's base classes."""
+    rng = np.random.default_rng(91)
+    alphabet = np.frombuffer(b"ACGTACGTACGTacgtRYKMSWEBDHV", np.uint8)
+    regs = []
+    for g in range(4):
+        base = alphabet[rng.integers(0, len(alphabet), 700)]
+        haps = [bytes(base[s:s + int(rng.integers(40, 300))]) for s in rng.integers(0, 300, 3)]
+        reads = []
+        for L in rng.integers(20, 260, 9):
+            r = bytearray(base[int(rng.integers(0, 300)):][:int(L)])
+            if g % 2 and rng.random() < 0.4:
+                r[int(rng.integers(0, len(r)))] = ord("N")
+            reads.append(bytes(r))
+        q = [rng.integers(2, 42, len(r)).astype(np.uint8).tobytes() for r in reads]
+        i = [rng.integers(10, 46, len(r)).astype(np.uint8).tobytes() for r in reads]
+        d = [rng.integers(10, 46, len(r)).astype(np.uint8).tobytes() for r in reads]
+        c = [rng.integers(5, 15, len(r)).astype(np.uint8).tobytes() for r in reads]
+        regs.append(Region(haps, reads, q, i, d, c))
+    pb = PackedBatch.from_regions(regs)
+    got, flags, _ = engine.compute(pb, want_flags=True)
+    want, used = oracle.batch(pb)
+    assert np.nanmax(np.abs(got - want)) <= EXACT
+    assert np.array_equal(flags.astype(bool), used)
+
+
 def test_full_size_batch_properties(engine, oracle):
     """The benchmark batch (2,000 regions, ~5.7e11 cells): deterministic, every pair finite, and a
     seeded sample of regions equal to the oracle."""
