@@ -27,6 +27,7 @@ import subprocess
 import sys
 import threading
 import time
+import ctypes as C
 from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
@@ -171,37 +172,58 @@ def run_reference(args, rank: int, world: int) -> None:
 # ---- our arm ----------------------------------------------------------------------------------
 
 def serving_latency(engine, batch, load: float, capacity_regions_per_s: float, seconds: float, seed: int):
-    """Poisson arrivals of the batch's regions at `load` x capacity; returns latency percentiles and
-    the sustained GCUPS of the completed requests."""
+    """Poisson arrivals of the batch's regions at `load` x capacity; returns latency percentiles,
+    the sustained GCUPS of the completed requests and the serving loop's own counters."""
+    from rovaca_b200 import _lib
+
+    lib = _lib.load()
     rng = np.random.default_rng(seed)
     regions = [batch.subset([g]) for g in range(min(batch.n_regions, 400))]
+    structs = [r.as_c() for r in regions]
     cells = [r.cells() for r in regions]
+    sizes = [r.out_size for r in regions]
     rate = load * capacity_regions_per_s
+    gaps = rng.exponential(1.0 / rate, int(rate * seconds * 1.5) + 16)
+    before = engine.server_stats()
     outs, tickets, done_cells = [], [], 0
     t0 = time.perf_counter()
     next_t = t0
     k = 0
+    lag = 0.0  # how far submission fell behind the arrival schedule (host-side stalls)
     while next_t - t0 < seconds:
         now = time.perf_counter()
         if now < next_t:
             time.sleep(min(next_t - now, 0.002))
             continue
-        r = regions[k % len(regions)]
-        out = np.empty(r.out_size)
-        tickets.append((engine.submit(r, out), k % len(regions)))
+        lag = max(lag, now - next_t)
+        g = k % len(regions)
+        out = np.empty(sizes[g])
+        t = C.c_uint64()
+        rc = lib.phmm_submit(engine._h, C.byref(structs[g]), out.ctypes.data, None, C.byref(t))
+        if rc != 0:
+            raise RuntimeError(f"phmm_submit failed: {rc}")
+        tickets.append((t.value, g))
         outs.append(out)
+        next_t += gaps[k % len(gaps)]
         k += 1
-        next_t += rng.exponential(1.0 / rate)
     lat = []
     for t, g in tickets:
         _, total_us = engine.wait(t)
         lat.append(total_us / 1e3)
         done_cells += cells[g]
     elapsed = time.perf_counter() - t0
+    after = engine.server_stats()
     lat = np.array(lat)
+    batches = after["batches"] - before["batches"]
     return {"load": load, "offered_regions_per_s": round(rate, 1), "requests": len(lat),
             "p50_ms": round(float(np.percentile(lat, 50)), 3), "p99_ms": round(float(np.percentile(lat, 99)), 3),
-            "sustained_gcups": round(done_cells / elapsed / 1e9, 2)}
+            "sustained_gcups": round(done_cells / elapsed / 1e9, 2),
+            "batches": batches,
+            "mean_batch_regions": round((after["requests_done"] - before["requests_done"]) / max(batches, 1), 1),
+            "mean_batch_ms": round((after["batch_ms"] - before["batch_ms"]) / max(batches, 1), 2),
+            "mean_batch_device_ms": round((after["device_ms"] - before["device_ms"]) / max(batches, 1), 2),
+            "max_batch_ms_so_far": round(after["max_batch_ms"], 2), "max_queue_ms_so_far": round(after["max_queue_ms"], 2),
+            "max_submit_lag_ms": round(lag * 1e3, 2)}
 
 
 def run_resident_only(args) -> None:
@@ -316,7 +338,8 @@ def run_ours(args, rank: int, world: int, dist) -> None:
 
         # serving loop latency
         cap = batch.n_regions / (e2e_s / args.steps)
-        lat = serving_latency(engine, batch, 0.8, cap, args.serve_seconds, seed=rank)
+        lat = [serving_latency(engine, batch, load, cap, args.serve_seconds, seed=rank)
+               for load in (0.25, 0.5, 0.8, 0.95)]
 
         # roofline of the FP32 wavefront pass against the measured FP32 FMA peak
         peak_scalar, peak_packed = engine.fp32_fma_peak()
@@ -372,7 +395,8 @@ def run_ours(args, rank: int, world: int, dist) -> None:
             "fp32_pass_ms": round(fp32_pass_ms, 3),
             "fp64_rerun_fraction": round(f64_frac, 5),
             "max_abs_err_log10_vs_fp64": max_err,
-            "latency": lat,
+            "latency": next(x for x in lat if x["load"] == 0.8),
+            "latency_by_load": lat,
         }
     engine.close()
     if line is not None:

@@ -223,6 +223,23 @@ PHMM_API phmm_status phmm_wait(phmm_engine* engine, phmm_ticket ticket, int64_t 
 /* Cancels a request that has not been admitted to the device yet. */
 PHMM_API phmm_status phmm_cancel(phmm_engine* engine, phmm_ticket ticket);
 
+/* Counters of the serving loop since the engine's first submit (no reference counterpart: the
+ * reference's region pool keeps no statistics). */
+typedef struct phmm_server_stats {
+    uint64_t requests_submitted;
+    uint64_t requests_done;       /* completed or failed after admission */
+    uint64_t batches;             /* device batches formed from the queue */
+    uint64_t max_batch_regions;
+    uint64_t queue_peak;          /* longest queue seen at submit */
+    uint64_t cells_done;
+    double batch_ms;              /* summed wall time of the batches, admission to results scattered */
+    double device_ms;             /* summed device time of the batches' launch sequences */
+    double max_batch_ms;          /* longest batch, admission to results scattered */
+    double max_queue_ms;          /* longest wait of a request between submit and admission */
+} phmm_server_stats;
+
+PHMM_API phmm_status phmm_server_stats_get(phmm_engine* engine, phmm_server_stats* stats);
+
 #ifdef __cplusplus
 }
 #endif

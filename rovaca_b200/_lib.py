@@ -52,6 +52,16 @@ class Stats(C.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class ServerStats(C.Structure):
+    _fields_ = [("requests_submitted", C.c_uint64), ("requests_done", C.c_uint64), ("batches", C.c_uint64),
+                ("max_batch_regions", C.c_uint64), ("queue_peak", C.c_uint64), ("cells_done", C.c_uint64),
+                ("batch_ms", C.c_double), ("device_ms", C.c_double), ("max_batch_ms", C.c_double),
+                ("max_queue_ms", C.c_double)]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 _lib = None
 
 
@@ -87,6 +97,7 @@ def load() -> C.CDLL:
         "phmm_poll": (I32, [P, U64, C.POINTER(I32)]),
         "phmm_wait": (I32, [P, U64, I64, C.POINTER(D), C.POINTER(D)]),
         "phmm_cancel": (I32, [P, U64]),
+        "phmm_server_stats_get": (I32, [P, P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -288,7 +288,10 @@ uint64_t Engine::scratch_warps() const
     return (uint64_t)sms_ * occ * (kFwdBlock / kWarp);
 }
 
-uint64_t Engine::arena_bytes_for(const Plan& plan) const { return carve(need_of(plan, scratch_warps()), nullptr, nullptr); }
+uint64_t Engine::scratch_bytes() const
+{
+    return scratch_warps() * (uint64_t)PlanLimits().max_stream_multi * 3 * sizeof(double);
+}
 
 phmm_status Engine::ensure_capacity(Slot& s, const Plan& plan, std::string& err)
 {

@@ -81,7 +81,8 @@ public:
     int device() const { return dev_; }
     int num_sms() const { return sms_; }
     const phmm_config& config() const { return cfg_; }
-    uint64_t arena_bytes_for(const Plan& plan) const;
+    uint64_t scratch_bytes() const;  // device bytes of the stripe scratch rows (multi-stripe reads)
+    PlanLimits plan_limits() const { return PlanLimits(); }
 
 private:
     Engine() = default;

@@ -62,10 +62,9 @@ void make_runs(const uint64_t* hoff, const uint8_t* hflags, uint32_t n, uint32_t
 
 }  // namespace
 
-phmm_status build_plan(const phmm_batch& b, const PlanLimits& lim, Plan& plan, std::string& err)
+phmm_status scan_batch(const phmm_batch& b, const PlanLimits& lim, BatchScan& s, std::string& err)
 {
-    plan = Plan();
-    plan.classes.assign(kPlanClasses, ClassDesc{});
+    s = BatchScan();
     if (b.n_regions == 0) return PHMM_OK;
     if (!b.n_haps || !b.n_reads || !b.hap_off || !b.read_off) {
         err = "batch: n_haps, n_reads, hap_off and read_off are required";
@@ -85,44 +84,73 @@ phmm_status build_plan(const phmm_batch& b, const PlanLimits& lim, Plan& plan, s
         err = "batch: more than 2^32 haplotypes or reads";
         return PHMM_ERR_INVALID_ARGUMENT;
     }
-    plan.n_regions = b.n_regions;
-    plan.n_haps = (uint32_t)nh;
-    plan.n_reads = (uint32_t)nr;
-
-    // offsets: monotone, rebased to 0, lengths within the limits
-    plan.hap_base0 = b.hap_off[0];
-    plan.read_base0 = b.read_off[0];
-    plan.hap_off.resize(nh + 1);
-    plan.read_off.resize(nr + 1);
-    for (uint64_t h = 0; h <= nh; ++h) {
-        if (h > 0 && b.hap_off[h] < b.hap_off[h - 1]) {
-            err = "hap_off is not non-decreasing at " + std::to_string(h);
-            return PHMM_ERR_INVALID_ARGUMENT;
+    s.n_haps = (uint32_t)nh;
+    s.n_reads = (uint32_t)nr;
+    s.hap_base0 = b.hap_off[0];
+    s.read_base0 = b.read_off[0];
+    // offsets non-decreasing, lengths within the limits; per region the non-empty pairs and cells
+    uint64_t h = 0, r = 0;
+    for (uint32_t g = 0; g < b.n_regions; ++g) {
+        uint64_t hcols = 0, hnon = 0, rrows = 0, rnon = 0;
+        for (uint32_t k = 0; k < b.n_haps[g]; ++k, ++h) {
+            if (b.hap_off[h + 1] < b.hap_off[h]) {
+                err = "hap_off is not non-decreasing at " + std::to_string(h + 1);
+                return PHMM_ERR_INVALID_ARGUMENT;
+            }
+            const uint64_t H = b.hap_off[h + 1] - b.hap_off[h];
+            if (H > lim.max_hap_len) {
+                err = "haplotype " + std::to_string(h) + " longer than " + std::to_string(lim.max_hap_len);
+                return PHMM_ERR_LIMIT_EXCEEDED;
+            }
+            hcols += H;
+            hnon += H > 0;
         }
-        plan.hap_off[h] = b.hap_off[h] - plan.hap_base0;
-        if (h > 0 && plan.hap_off[h] - plan.hap_off[h - 1] > lim.max_hap_len) {
-            err = "haplotype " + std::to_string(h - 1) + " longer than " + std::to_string(lim.max_hap_len);
-            return PHMM_ERR_LIMIT_EXCEEDED;
+        for (uint32_t k = 0; k < b.n_reads[g]; ++k, ++r) {
+            if (b.read_off[r + 1] < b.read_off[r]) {
+                err = "read_off is not non-decreasing at " + std::to_string(r + 1);
+                return PHMM_ERR_INVALID_ARGUMENT;
+            }
+            const uint64_t R = b.read_off[r + 1] - b.read_off[r];
+            if (R > lim.max_read_len) {
+                err = "read " + std::to_string(r) + " longer than " + std::to_string(lim.max_read_len);
+                return PHMM_ERR_LIMIT_EXCEEDED;
+            }
+            rrows += R;
+            rnon += R > 0;
         }
+        s.out_total += (uint64_t)b.n_haps[g] * b.n_reads[g];
+        s.pairs += hnon * rnon;
+        s.cells += hcols * rrows;
     }
-    for (uint64_t r = 0; r <= nr; ++r) {
-        if (r > 0 && b.read_off[r] < b.read_off[r - 1]) {
-            err = "read_off is not non-decreasing at " + std::to_string(r);
-            return PHMM_ERR_INVALID_ARGUMENT;
-        }
-        plan.read_off[r] = b.read_off[r] - plan.read_base0;
-        if (r > 0 && plan.read_off[r] - plan.read_off[r - 1] > lim.max_read_len) {
-            err = "read " + std::to_string(r - 1) + " longer than " + std::to_string(lim.max_read_len);
-            return PHMM_ERR_LIMIT_EXCEEDED;
-        }
-    }
-    plan.hap_bases = plan.hap_off[nh];
-    plan.read_bases = plan.read_off[nr];
-    if ((plan.hap_bases > 0 && !b.hap_bases) ||
-        (plan.read_bases > 0 && (!b.read_bases || !b.read_qual || !b.read_ins || !b.read_del || !b.read_gcp))) {
+    s.hap_bases = b.hap_off[nh] - s.hap_base0;
+    s.read_bases = b.read_off[nr] - s.read_base0;
+    if ((s.hap_bases > 0 && !b.hap_bases) ||
+        (s.read_bases > 0 && (!b.read_bases || !b.read_qual || !b.read_ins || !b.read_del || !b.read_gcp))) {
         err = "batch: sequence or quality pointer is null";
         return PHMM_ERR_INVALID_ARGUMENT;
     }
+    return PHMM_OK;
+}
+
+phmm_status build_plan(const phmm_batch& b, const PlanLimits& lim, Plan& plan, std::string& err)
+{
+    plan = Plan();
+    plan.classes.assign(kPlanClasses, ClassDesc{});
+    BatchScan sc;
+    const phmm_status st = scan_batch(b, lim, sc, err);
+    if (st != PHMM_OK || b.n_regions == 0) return st;
+    const uint64_t nh = sc.n_haps, nr = sc.n_reads;
+    plan.n_regions = b.n_regions;
+    plan.n_haps = sc.n_haps;
+    plan.n_reads = sc.n_reads;
+    plan.hap_base0 = sc.hap_base0;
+    plan.read_base0 = sc.read_base0;
+    plan.hap_off.resize(nh + 1);
+    plan.read_off.resize(nr + 1);
+    for (uint64_t h = 0; h <= nh; ++h) plan.hap_off[h] = b.hap_off[h] - plan.hap_base0;
+    for (uint64_t r = 0; r <= nr; ++r) plan.read_off[r] = b.read_off[r] - plan.read_base0;
+    plan.hap_bases = sc.hap_bases;
+    plan.read_bases = sc.read_bases;
     const uint8_t* hb = b.hap_bases + plan.hap_base0;
     const uint8_t* rb = b.read_bases + plan.read_base0;
 

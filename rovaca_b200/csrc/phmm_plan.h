@@ -40,9 +40,20 @@ struct Plan {
     uint32_t max_multi_stream = 0;   // longest stream among multi-stripe items (0 if none)
 };
 
-// Returns PHMM_OK, PHMM_ERR_INVALID_ARGUMENT or PHMM_ERR_LIMIT_EXCEEDED (err holds the detail).
+// Sizes of a batch, from one validating pass over its counts and offsets (no copies).
+struct BatchScan {
+    uint32_t n_haps = 0, n_reads = 0;
+    uint64_t hap_base0 = 0, read_base0 = 0;  // hap_off[0], read_off[0]
+    uint64_t hap_bases = 0, read_bases = 0, out_total = 0;
+    uint64_t pairs = 0, cells = 0;           // pairs with a non-empty read and haplotype, their cells
+};
+
+// Validation shared by every entry point: counts, non-decreasing offsets, the reference limits and
+// the pointers the batch needs.  Returns PHMM_OK, PHMM_ERR_INVALID_ARGUMENT or
+// PHMM_ERR_LIMIT_EXCEEDED (err holds the detail).
+phmm_status scan_batch(const phmm_batch& b, const PlanLimits& lim, BatchScan& s, std::string& err);
+
+// scan_batch, then the full plan.  Same return codes.
 phmm_status build_plan(const phmm_batch& b, const PlanLimits& lim, Plan& plan, std::string& err);
-
-
 
 }  // namespace phmm

@@ -2,10 +2,10 @@
 //
 // The reference runs one PairHMM call per active region on each of --nthreads pool workers
 // (haplotypecaller_engine.cpp:119,254; haplotypecaller.cpp:105).  Here those calls become
-// requests: phmm_submit copies the region and queues it; kSlots worker threads each own a device
-// slot (arena, streams, captured graph).  A worker that is free takes every queued request that
-// fits the HBM budget and the per-batch cell cap, runs them as one batch, scatters the results and
-// signals the requests.  While one slot's batch is on the GPU the next worker is already forming
+// requests: phmm_submit validates and copies the region and queues it; kSlots worker threads each
+// own a device slot (arena, streams, captured graph) and pinned staging buffers.  A worker that is
+// free takes every queued request that fits the HBM budget and the per-batch cell cap, gathers them
+// into its pinned buffer, runs them as one batch, scatters the results and signals the requests.  While one slot's batch is on the GPU the next worker is already forming
 // and launching the next one, so requests that arrive meanwhile are admitted as soon as a slot and
 // budget are free, and their kernels overlap with the running ones on the device.  Each pair's
 // arithmetic does not depend on what it was batched with, so a region's likelihoods are the same
@@ -26,6 +26,7 @@
 #include "../../include/phmm_b200.h"
 #include "phmm_capi_internal.h"
 #include "phmm_engine.h"
+#include "phmm_plan.h"
 
 namespace phmm {
 
@@ -33,7 +34,7 @@ namespace {
 
 using Clock = std::chrono::steady_clock;
 
-constexpr int kSlots = 3;                           // batches in flight at once
+constexpr int kSlots = 3;                            // batches in flight at once
 constexpr uint64_t kMaxBatchCells = 200000000000ull;  // bound on one batch's work (~0.1 s on B200)
 constexpr size_t kMaxQueued = 1u << 20;
 
@@ -44,16 +45,42 @@ struct Request {
     ReqState state = ReqState::Queued;
     phmm_status status = PHMM_OK;
     std::string error;
-    // owned copy of the region
+    // owned copy of the region: haplotype bases, then read bases, quals, ins, del, gcp
     uint32_t n_haps = 0, n_reads = 0;
-    std::vector<uint8_t> hap_bases, read_bases, q, ins, del, gcp;
-    std::vector<uint64_t> hap_off, read_off;
+    uint64_t hap_bases = 0, read_bases = 0;
+    std::vector<uint8_t> data;
+    std::vector<uint64_t> hap_off, read_off;  // rebased to 0
     double* out = nullptr;
     uint8_t* flags = nullptr;
     uint64_t out_n = 0;
     uint64_t cells = 0;
     uint64_t bytes = 0;  // device footprint estimate for admission
     Clock::time_point t_submit, t_admit, t_done;
+};
+
+// Page-locked host buffer that grows on demand (device copies from it are asynchronous DMA).
+struct PinnedBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    bool reserve(size_t n)
+    {
+        if (n <= bytes) return true;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        bytes = 0;
+        const size_t want = std::max(n, n / 2 * 3);
+        if (cudaMallocHost(&p, want) != cudaSuccess) {
+            cudaGetLastError();
+            p = nullptr;
+            return false;
+        }
+        bytes = want;
+        return true;
+    }
+    ~PinnedBuf()
+    {
+        if (p) cudaFreeHost(p);
+    }
 };
 
 struct Server {
@@ -67,6 +94,7 @@ struct Server {
     uint64_t budget = 0, in_use = 0;
     bool stop = false;
     std::vector<std::thread> workers;
+    phmm_server_stats stats{};         // guarded by mu
 
     void worker(int idx);
 };
@@ -79,6 +107,11 @@ uint64_t footprint(uint64_t read_bases, uint64_t hap_bases, uint64_t pairs, uint
     return read_bases * 5 + hap_bases * 9 + pairs * (8 + 1 + 16) + n_reads * 17 + n_haps * 9 + 4096;
 }
 
+double ms_between(Clock::time_point a, Clock::time_point b)
+{
+    return std::chrono::duration<double, std::milli>(b - a).count();
+}
+
 void Server::worker(int idx)
 {
     cudaSetDevice(eng->device());
@@ -88,12 +121,10 @@ void Server::worker(int idx)
     std::vector<std::shared_ptr<Request>> batch;
     std::vector<uint32_t> nh, nr;
     std::vector<uint64_t> hoff, roff;
-    std::vector<uint8_t> hb, rb, rq, ri, rd, rc;
-    std::vector<double> out;
-    std::vector<uint8_t> flags;
+    PinnedBuf in_buf, out_buf;
     for (;;) {
         batch.clear();
-        uint64_t batch_bytes = 0;
+        uint64_t batch_bytes = 0, hap_total = 0, read_total = 0, out_total = 0, cells = 0;
         {
             std::unique_lock<std::mutex> lk(mu);
             cv_work.wait(lk, [&] { return stop || (!queue.empty() && in_use + queue.front()->bytes <= budget); });
@@ -102,7 +133,7 @@ void Server::worker(int idx)
             // slots together then stay within the budget.  A request alone always fits (checked at
             // submit).
             const uint64_t batch_cap = budget / kSlots;
-            uint64_t cells = 0;
+            const auto now = Clock::now();
             while (!queue.empty()) {
                 auto& r = queue.front();
                 const bool fits = in_use + batch_bytes + r->bytes <= budget &&
@@ -110,69 +141,75 @@ void Server::worker(int idx)
                 if (!fits || (!batch.empty() && cells + r->cells > kMaxBatchCells)) break;
                 batch_bytes += r->bytes;
                 cells += r->cells;
+                hap_total += r->hap_bases;
+                read_total += r->read_bases;
+                out_total += r->out_n;
                 r->state = ReqState::Running;
-                r->t_admit = Clock::now();
+                r->t_admit = now;
                 batch.push_back(r);
                 queue.pop_front();
             }
             in_use += batch_bytes;
         }
         if (batch.empty()) continue;
+        const auto t_start = Clock::now();
         phmm_status st = mk;
         std::string berr = err;
+        double device_ms = 0.0;
+        bool want_flags = false;
+        for (auto& r : batch) want_flags |= r->flags != nullptr;
+        // the admitted regions go into the slot's pinned buffers: haplotype bases, then the five
+        // read arrays in; likelihoods (and flags) out
+        if (st == PHMM_OK && !(in_buf.reserve(hap_total + 5 * read_total + 16) &&
+                               out_buf.reserve(out_total * (sizeof(double) + (want_flags ? 1 : 0)) + 16))) {
+            st = PHMM_ERR_OUT_OF_MEMORY;
+            berr = "pinned staging for a batch of " + std::to_string(batch.size()) + " regions";
+        }
         if (st == PHMM_OK) {
-            // concatenate the admitted regions into one batch
+            uint8_t* hb = (uint8_t*)in_buf.p;
+            uint8_t* rd[5];
+            for (int k = 0; k < 5; ++k) rd[k] = hb + hap_total + (uint64_t)k * read_total;
             nh.clear();
             nr.clear();
             hoff.assign(1, 0);
             roff.assign(1, 0);
-            hb.clear();
-            rb.clear();
-            rq.clear();
-            ri.clear();
-            rd.clear();
-            rc.clear();
-            uint64_t out_total = 0;
-            bool want_flags = false;
+            uint64_t ho = 0, ro = 0;
             for (auto& r : batch) {
                 nh.push_back(r->n_haps);
                 nr.push_back(r->n_reads);
-                for (uint32_t h = 0; h < r->n_haps; ++h) hoff.push_back(hb.size() + r->hap_off[h + 1]);
-                for (uint32_t k = 0; k < r->n_reads; ++k) roff.push_back(rb.size() + r->read_off[k + 1]);
-                hb.insert(hb.end(), r->hap_bases.begin(), r->hap_bases.end());
-                rb.insert(rb.end(), r->read_bases.begin(), r->read_bases.end());
-                rq.insert(rq.end(), r->q.begin(), r->q.end());
-                ri.insert(ri.end(), r->ins.begin(), r->ins.end());
-                rd.insert(rd.end(), r->del.begin(), r->del.end());
-                rc.insert(rc.end(), r->gcp.begin(), r->gcp.end());
-                out_total += r->out_n;
-                want_flags |= r->flags != nullptr;
+                for (uint32_t h = 0; h < r->n_haps; ++h) hoff.push_back(ho + r->hap_off[h + 1]);
+                for (uint32_t k = 0; k < r->n_reads; ++k) roff.push_back(ro + r->read_off[k + 1]);
+                if (r->hap_bases) std::memcpy(hb + ho, r->data.data(), r->hap_bases);
+                for (int k = 0; k < 5 && r->read_bases; ++k)
+                    std::memcpy(rd[k] + ro, r->data.data() + r->hap_bases + (uint64_t)k * r->read_bases, r->read_bases);
+                ho += r->hap_bases;
+                ro += r->read_bases;
             }
             phmm_batch b{};
             b.n_regions = (uint32_t)batch.size();
             b.n_haps = nh.data();
             b.n_reads = nr.data();
-            b.hap_bases = hb.data();
+            b.hap_bases = hb;
             b.hap_off = hoff.data();
-            b.read_bases = rb.data();
-            b.read_qual = rq.data();
-            b.read_ins = ri.data();
-            b.read_del = rd.data();
-            b.read_gcp = rc.data();
+            b.read_bases = rd[0];
+            b.read_qual = rd[1];
+            b.read_ins = rd[2];
+            b.read_del = rd[3];
+            b.read_gcp = rd[4];
             b.read_off = roff.data();
             Plan plan;
-            st = build_plan(b, PlanLimits(), plan, berr);
+            st = build_plan(b, eng->plan_limits(), plan, berr);
             if (st == PHMM_OK) st = eng->enqueue(*slot, plan, b, want_flags, berr);
-            if (st == PHMM_OK) {
-                out.resize(out_total);
-                flags.resize(want_flags ? out_total : 0);
-                st = eng->finish(*slot, plan, out.data(), want_flags ? flags.data() : nullptr, nullptr, berr);
-            }
+            double* out = (double*)out_buf.p;
+            uint8_t* flags = want_flags ? (uint8_t*)(out + out_total) : nullptr;
+            phmm_stats ps{};
+            if (st == PHMM_OK) st = eng->finish(*slot, plan, out, flags, &ps, berr);
+            device_ms = ps.device_ms;
             if (st == PHMM_OK) {
                 uint64_t o = 0;
                 for (auto& r : batch) {
-                    if (r->out_n) std::memcpy(r->out, out.data() + o, r->out_n * sizeof(double));
-                    if (r->flags && r->out_n) std::memcpy(r->flags, flags.data() + o, r->out_n);
+                    if (r->out_n) std::memcpy(r->out, out + o, r->out_n * sizeof(double));
+                    if (r->flags && r->out_n) std::memcpy(r->flags, flags + o, r->out_n);
                     o += r->out_n;
                 }
             }
@@ -185,15 +222,17 @@ void Server::worker(int idx)
                 r->error = st == PHMM_OK ? std::string() : berr;
                 r->state = ReqState::Done;
                 r->t_done = now;
-                // inputs are no longer needed
-                std::vector<uint8_t>().swap(r->hap_bases);
-                std::vector<uint8_t>().swap(r->read_bases);
-                std::vector<uint8_t>().swap(r->q);
-                std::vector<uint8_t>().swap(r->ins);
-                std::vector<uint8_t>().swap(r->del);
-                std::vector<uint8_t>().swap(r->gcp);
+                std::vector<uint8_t>().swap(r->data);  // inputs are no longer needed
+                stats.max_queue_ms = std::max(stats.max_queue_ms, ms_between(r->t_submit, r->t_admit));
             }
             in_use -= batch_bytes;
+            stats.batches += 1;
+            stats.requests_done += batch.size();
+            stats.cells_done += cells;
+            stats.max_batch_regions = std::max<uint64_t>(stats.max_batch_regions, batch.size());
+            stats.batch_ms += ms_between(t_start, now);
+            stats.device_ms += device_ms;
+            stats.max_batch_ms = std::max(stats.max_batch_ms, ms_between(t_start, now));
         }
         cv_done.notify_all();
         cv_work.notify_all();
@@ -252,35 +291,39 @@ phmm_status server_submit(phmm_engine* engine, const phmm_batch& b, double* out,
         err = "a request holds exactly one region (n_regions == 1)";
         return PHMM_ERR_INVALID_ARGUMENT;
     }
-    // validate with the planner's rules before queueing (limits, offsets)
-    Plan plan;
-    phmm_status st = build_plan(b, PlanLimits(), plan, err);
+    // validate with the planner's rules before queueing (limits, offsets, pointers)
+    BatchScan sc;
+    phmm_status st = scan_batch(b, PlanLimits(), sc, err);
     if (st != PHMM_OK) return st;
-    if (plan.out_total && !out) {
+    if (sc.out_total && !out) {
         err = "out is null";
         return PHMM_ERR_INVALID_ARGUMENT;
     }
     auto r = std::make_shared<Request>();
-    r->n_haps = b.n_haps[0];
-    r->n_reads = b.n_reads[0];
-    r->hap_off = plan.hap_off;
-    r->read_off = plan.read_off;
-    r->hap_bases.assign(b.hap_bases ? b.hap_bases + plan.hap_base0 : nullptr,
-                        b.hap_bases ? b.hap_bases + plan.hap_base0 + plan.hap_bases : nullptr);
-    auto cp = [&](std::vector<uint8_t>& dst, const uint8_t* src) {
-        dst.assign(src ? src + plan.read_base0 : nullptr, src ? src + plan.read_base0 + plan.read_bases : nullptr);
-    };
-    cp(r->read_bases, b.read_bases);
-    cp(r->q, b.read_qual);
-    cp(r->ins, b.read_ins);
-    cp(r->del, b.read_del);
-    cp(r->gcp, b.read_gcp);
+    r->n_haps = sc.n_haps;
+    r->n_reads = sc.n_reads;
+    r->hap_bases = sc.hap_bases;
+    r->read_bases = sc.read_bases;
+    r->hap_off.resize(sc.n_haps + 1);
+    r->read_off.resize(sc.n_reads + 1);
+    for (uint32_t h = 0; h <= sc.n_haps; ++h) r->hap_off[h] = b.hap_off[h] - sc.hap_base0;
+    for (uint32_t k = 0; k <= sc.n_reads; ++k) r->read_off[k] = b.read_off[k] - sc.read_base0;
+    r->data.resize(sc.hap_bases + 5 * sc.read_bases);
+    if (sc.hap_bases) std::memcpy(r->data.data(), b.hap_bases + sc.hap_base0, sc.hap_bases);
+    const uint8_t* src[5] = {b.read_bases, b.read_qual, b.read_ins, b.read_del, b.read_gcp};
+    for (int k = 0; k < 5 && sc.read_bases; ++k)
+        std::memcpy(r->data.data() + sc.hap_bases + (uint64_t)k * sc.read_bases, src[k] + sc.read_base0, sc.read_bases);
     r->out = out;
     r->flags = flags;
-    r->out_n = plan.out_total;
-    r->cells = plan.cells;
-    r->bytes = footprint(plan.read_bases, plan.hap_bases, plan.out_total, plan.n_reads, plan.n_haps);
-    if (plan.max_multi_stream) r->bytes += engine_of(engine)->arena_bytes_for(plan);
+    r->out_n = sc.out_total;
+    r->cells = sc.cells;
+    r->bytes = footprint(sc.read_bases, sc.hap_bases, sc.out_total, sc.n_reads, sc.n_haps);
+    // a read longer than one stripe needs the per-warp scratch rows
+    for (uint32_t k = 0; k < sc.n_reads; ++k)
+        if (r->read_off[k + 1] - r->read_off[k] > (uint64_t)kWarp * kMaxK) {
+            r->bytes += engine_of(engine)->scratch_bytes();
+            break;
+        }
     Server* s = server_for(engine, true);
     if (r->bytes > s->budget) {
         err = "region needs about " + std::to_string(r->bytes) + " device bytes, more than the HBM budget of " +
@@ -301,6 +344,8 @@ phmm_status server_submit(phmm_engine* engine, const phmm_batch& b, double* out,
         r->t_submit = Clock::now();
         s->tickets[r->id] = r;
         s->queue.push_back(r);
+        s->stats.requests_submitted += 1;
+        s->stats.queue_peak = std::max<uint64_t>(s->stats.queue_peak, s->queue.size());
         *ticket = r->id;
     }
     s->cv_work.notify_one();
@@ -381,6 +426,19 @@ phmm_status phmm_wait(phmm_engine* engine, phmm_ticket ticket, int64_t timeout_u
     std::string err;
     phmm_status st = phmm::server_wait(engine, ticket, timeout_us, true, queued_us, total_us, err);
     return st == PHMM_OK ? PHMM_OK : set_error(st, err);
+}
+
+phmm_status phmm_server_stats_get(phmm_engine* engine, phmm_server_stats* stats)
+{
+    phmm::clear_error();
+    if (!engine) return set_error(PHMM_ERR_NOT_INITIALIZED, "engine is null");
+    if (!stats) return set_error(PHMM_ERR_INVALID_ARGUMENT, "stats is null");
+    *stats = phmm_server_stats{};
+    phmm::Server* s = phmm::server_for(engine, false);
+    if (!s) return PHMM_OK;
+    std::lock_guard<std::mutex> lk(s->mu);
+    *stats = s->stats;
+    return PHMM_OK;
 }
 
 phmm_status phmm_cancel(phmm_engine* engine, phmm_ticket ticket)

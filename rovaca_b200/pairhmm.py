@@ -280,6 +280,12 @@ class Engine:
     def cancel(self, ticket: int) -> None:
         check(self._lib.phmm_cancel(self._h, ticket))
 
+    def server_stats(self) -> dict:
+        """Counters of the serving loop (phmm_server_stats_get)."""
+        st = _lib.ServerStats()
+        check(self._lib.phmm_server_stats_get(self._h, C.byref(st)))
+        return st.as_dict()
+
     # ---- region API ----------------------------------------------------------------------
     def call_region(self, haplotypes, reads, base_quals, mapq, min_quality_threshold: int = 18,
                     pcr_option: str | int = "CONSERVATIVE"):

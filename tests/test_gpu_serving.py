@@ -35,6 +35,9 @@ def test_each_result_same_alone_and_in_the_mix(engine):
     for g in range(pb.n_regions):
         assert np.array_equal(outs[g], alone[g], equal_nan=True), g
     assert all(total >= queued >= 0 for queued, total in lat)
+    st = engine.server_stats()
+    assert st["requests_submitted"] >= pb.n_regions and st["requests_done"] >= pb.n_regions
+    assert 1 <= st["batches"] <= st["requests_done"] and st["cells_done"] >= pb.cells()
 
 
 def test_flags_and_poll(engine, oracle):
