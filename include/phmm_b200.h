@@ -65,7 +65,8 @@ typedef struct phmm_engine phmm_engine;
 typedef struct phmm_config {
     int32_t device;            /* CUDA device ordinal */
     int32_t use_cuda_graph;    /* 1: replay the device-side batch pipeline from a captured CUDA graph */
-    int32_t autotune;          /* 1: pick launch shapes by timing candidates on first use */
+    int32_t autotune;          /* 1: run the tile-shape autotuner at creation (once per device and
+                                  process; later engines reuse its table); 0: default shapes */
     int32_t reserved0;
     uint64_t hbm_budget_bytes; /* serving-loop admission budget for resident region data; 0 = 40 GiB */
     uint64_t reserved1;
@@ -190,17 +191,64 @@ PHMM_API int32_t phmm_host_tandem_repeat_length(const uint8_t* bases, uint32_t n
 PHMM_API void phmm_host_normalize_filter(const double* lk_hap_read, uint32_t n_haps, uint32_t n_reads, const uint64_t* read_len,
                                 double* out, uint8_t* keep, uint32_t* n_kept);
 
-/* How a batch is cut into wavefront work, without running it (no GPU involved).  With
- * KH = ceil(read length / 32) (8 for reads longer than 256, which run in 256-row stripes):
- *   class_items[27]: work items per FP32 kernel class, (multi-stripe ? 8 : KH - 1) plus 0 for pairs
- *     without 'N' whose read has constant gap qualities, 9 for other pairs without 'N', 18 for pairs
- *     with 'N'; an item is two reads (one when a region has an odd count) against a haplotype run;
- *   class_pairs[18]: pairs per FP64 recompute class, (multi-stripe ? 8 : KH - 1) plus 9 for 'N'
- *     pairs (the capacity reserved for pairs that underflow in FP32);
+/* ---- tile shapes and the autotuner (no reference counterpart) ---------------------------------
+ *
+ * The FP32 pass runs every read in a tile shape chosen by its mode and read-length bucket:
+ *   mode 0: pairs without 'N' whose read has constant insertion/deletion/gap qualities,
+ *   mode 1: other pairs without 'N', mode 2: pairs with 'N';
+ *   bucket b = ceil(read length / 32), 1..24;
+ *   shape: rows_per_lane KH (16 lanes per read hold 32 * KH rows) in one stripe (KH >= b), or
+ *          multi_stripe with 4 <= KH < b, the read running as ceil(length / (32 * KH)) stripes.
+ * FP32 kernel class = mode * 13 + (multi_stripe ? 4 + KH : KH - 1); FP64 recompute class =
+ * ('N' ? 9 : 0) + (length > 256 ? 8 : b - 1).  Results do not depend on the shapes. */
+#define PHMM_TILE_MODES 3
+#define PHMM_LEN_BUCKETS 24
+#define PHMM_FP32_CLASSES 39
+#define PHMM_FP64_CLASSES 18
+
+typedef struct phmm_tile_table {
+    uint8_t rows_per_lane[PHMM_TILE_MODES][PHMM_LEN_BUCKETS];
+    uint8_t multi_stripe[PHMM_TILE_MODES][PHMM_LEN_BUCKETS];
+} phmm_tile_table;
+
+/* One candidate shape the autotuner timed. */
+typedef struct phmm_tune_entry {
+    uint8_t mode, bucket, rows_per_lane, multi_stripe;
+    uint8_t chosen;               /* 1: installed for (mode, bucket) */
+    uint8_t reserved[3];
+    float gcups;                  /* FP32 pass throughput on the calibration batch */
+} phmm_tune_entry;
+
+#define PHMM_TUNE_MAX_ENTRIES 512
+typedef struct phmm_tune_report {
+    uint32_t n_entries;
+    uint32_t reserved;
+    double seconds;               /* wall time of the tuning run */
+    phmm_tune_entry entries[PHMM_TUNE_MAX_ENTRIES];
+} phmm_tune_report;
+
+/* Default shapes: the smallest single stripe up to 256 rows, 256-row stripes beyond. */
+PHMM_API void phmm_tile_table_default(phmm_tile_table* table);
+PHMM_API phmm_status phmm_engine_get_tiles(phmm_engine* engine, phmm_tile_table* table);
+/* Installs a table for batches planned from now on (PHMM_ERR_INVALID_ARGUMENT if a shape cannot
+ * hold its bucket). */
+PHMM_API phmm_status phmm_engine_set_tiles(phmm_engine* engine, const phmm_tile_table* table);
+/* Times the candidate shapes of every (mode, bucket) on synthetic calibration batches on the
+ * engine's device, installs the fastest and reports every measurement (report may be NULL).
+ * An engine created with config.autotune = 1 runs this once per device and process at creation. */
+PHMM_API phmm_status phmm_engine_autotune(phmm_engine* engine, phmm_tune_report* report);
+
+/* How a batch is cut into wavefront work, without running it (no GPU involved), under `tiles`
+ * (NULL: the default table):
+ *   class_items[39]: work items per FP32 kernel class (numbering above); an item is two reads (one
+ *     when a region has an odd count) of one shape against a haplotype run;
+ *   class_pairs[18]: pairs per FP64 recompute class (the capacity reserved for pairs that
+ *     underflow in FP32);
  *   pairs, cells: totals of the batch.
  * Returns the same validation status phmm_compute_regions would. */
-PHMM_API phmm_status phmm_host_plan_summary(const phmm_batch* batch, uint32_t class_items[27], uint64_t class_pairs[18],
-                                            uint64_t* pairs, uint64_t* cells);
+PHMM_API phmm_status phmm_host_plan_summary(const phmm_batch* batch, const phmm_tile_table* tiles,
+                                            uint32_t class_items[PHMM_FP32_CLASSES],
+                                            uint64_t class_pairs[PHMM_FP64_CLASSES], uint64_t* pairs, uint64_t* cells);
 
 /* ---- serving loop ----------------------------------------------------------------------- */
 

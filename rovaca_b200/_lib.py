@@ -52,6 +52,44 @@ class Stats(C.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+TILE_MODES, LEN_BUCKETS, FP32_CLASSES, FP64_CLASSES = 3, 24, 39, 18
+
+
+class TileTable(C.Structure):
+    """phmm_tile_table: row pairs per lane and multi-stripe flag per (mode, read-length bucket)."""
+    _fields_ = [("rows_per_lane", (C.c_uint8 * LEN_BUCKETS) * TILE_MODES),
+                ("multi_stripe", (C.c_uint8 * LEN_BUCKETS) * TILE_MODES)]
+
+    def as_arrays(self):
+        import numpy as np
+        kh = np.array([[self.rows_per_lane[m][b] for b in range(LEN_BUCKETS)] for m in range(TILE_MODES)], np.uint8)
+        mu = np.array([[self.multi_stripe[m][b] for b in range(LEN_BUCKETS)] for m in range(TILE_MODES)], np.uint8)
+        return kh, mu
+
+    @classmethod
+    def from_arrays(cls, kh, multi) -> "TileTable":
+        t = cls()
+        for m in range(TILE_MODES):
+            for b in range(LEN_BUCKETS):
+                t.rows_per_lane[m][b] = int(kh[m][b])
+                t.multi_stripe[m][b] = int(multi[m][b])
+        return t
+
+
+class TuneEntry(C.Structure):
+    _fields_ = [("mode", C.c_uint8), ("bucket", C.c_uint8), ("rows_per_lane", C.c_uint8),
+                ("multi_stripe", C.c_uint8), ("chosen", C.c_uint8), ("reserved", C.c_uint8 * 3),
+                ("gcups", C.c_float)]
+
+
+TUNE_MAX_ENTRIES = 512
+
+
+class TuneReport(C.Structure):
+    _fields_ = [("n_entries", C.c_uint32), ("reserved", C.c_uint32), ("seconds", C.c_double),
+                ("entries", TuneEntry * TUNE_MAX_ENTRIES)]
+
+
 class ServerStats(C.Structure):
     _fields_ = [("requests_submitted", C.c_uint64), ("requests_done", C.c_uint64), ("batches", C.c_uint64),
                 ("max_batch_regions", C.c_uint64), ("queue_peak", C.c_uint64), ("cells_done", C.c_uint64),
@@ -92,7 +130,11 @@ def load() -> C.CDLL:
         "phmm_resident_destroy": (I32, [P]),
         "phmm_fp32_fma_peak": (I32, [P, C.POINTER(D), C.POINTER(D)]),
         "phmm_compute_regions_noalloc": (I32, [C.POINTER(Batch), P, P, I32]),
-        "phmm_host_plan_summary": (I32, [C.POINTER(Batch), P, P, C.POINTER(U64), C.POINTER(U64)]),
+        "phmm_host_plan_summary": (I32, [C.POINTER(Batch), P, P, P, C.POINTER(U64), C.POINTER(U64)]),
+        "phmm_tile_table_default": (None, [P]),
+        "phmm_engine_get_tiles": (I32, [P, P]),
+        "phmm_engine_set_tiles": (I32, [P, P]),
+        "phmm_engine_autotune": (I32, [P, P]),
         "phmm_submit": (I32, [P, C.POINTER(Batch), P, P, C.POINTER(U64)]),
         "phmm_poll": (I32, [P, U64, C.POINTER(I32)]),
         "phmm_wait": (I32, [P, U64, I64, C.POINTER(D), C.POINTER(D)]),

@@ -1,5 +1,6 @@
 // extern "C" entry points of include/phmm_b200.h.  No exception crosses this boundary: every
 // entry point catches, records the detail for phmm_last_error() and returns a status.
+#include <cstring>
 #include <exception>
 #include <new>
 #include <string>
@@ -8,6 +9,11 @@
 #include "phmm_capi_internal.h"
 #include "phmm_engine.h"
 #include "phmm_plan.h"
+
+static_assert(sizeof(phmm_tile_table) == sizeof(phmm::TileTable), "tile table layouts differ");
+static_assert(PHMM_FP32_CLASSES == phmm::kClasses32 && PHMM_FP64_CLASSES == phmm::kClasses64 &&
+                  PHMM_TILE_MODES == phmm::kModes32 && PHMM_LEN_BUCKETS == phmm::kLenBuckets,
+              "class counts differ between the C ABI and the kernels");
 
 namespace phmm {
 
@@ -151,7 +157,8 @@ phmm_status phmm_resident_create(phmm_engine* engine, const phmm_batch* batch, i
     r->eng = phmm::engine_of(engine);
     r->flags = want_flags != 0;
     std::string err;
-    phmm_status st = phmm::build_plan(*batch, phmm::PlanLimits(), r->plan, err);
+    const phmm::TileTable tiles = r->eng->tiles();
+    phmm_status st = phmm::build_plan(*batch, phmm::Engine::limits_with(tiles), r->plan, err);
     if (st == PHMM_OK) st = r->eng->make_slot(1000, &r->slot, err);
     if (st == PHMM_OK && (cudaEventCreate(&r->e0) != cudaSuccess || cudaEventCreate(&r->e1) != cudaSuccess)) {
         err = "event creation failed";
@@ -234,7 +241,8 @@ phmm_status phmm_fp32_fma_peak(phmm_engine* engine, double* scalar_tflops, doubl
     PHMM_GUARD_END
 }
 
-phmm_status phmm_host_plan_summary(const phmm_batch* batch, uint32_t class_items[27], uint64_t class_pairs[18],
+phmm_status phmm_host_plan_summary(const phmm_batch* batch, const phmm_tile_table* tiles,
+                                   uint32_t class_items[PHMM_FP32_CLASSES], uint64_t class_pairs[PHMM_FP64_CLASSES],
                                    uint64_t* pairs, uint64_t* cells)
 {
     PHMM_GUARD_BEGIN
@@ -242,7 +250,9 @@ phmm_status phmm_host_plan_summary(const phmm_batch* batch, uint32_t class_items
     if (!batch) return set_error(PHMM_ERR_INVALID_ARGUMENT, "batch is null");
     phmm::Plan plan;
     std::string err;
-    phmm_status st = phmm::build_plan(*batch, phmm::PlanLimits(), plan, err);
+    phmm::TileTable t = phmm::TileTable::defaults();
+    if (tiles) std::memcpy(&t, tiles, sizeof(t));
+    phmm_status st = phmm::build_plan(*batch, phmm::Engine::limits_with(t), plan, err);
     if (st != PHMM_OK) return set_error(st, err);
     for (int c = 0; c < phmm::kClasses32; ++c)
         if (class_items) class_items[c] = plan.classes[c].n_items;
@@ -251,6 +261,50 @@ phmm_status phmm_host_plan_summary(const phmm_batch* batch, uint32_t class_items
     if (pairs) *pairs = plan.pairs;
     if (cells) *cells = plan.cells;
     return PHMM_OK;
+    PHMM_GUARD_END
+}
+
+void phmm_tile_table_default(phmm_tile_table* table)
+{
+    if (!table) return;
+    const phmm::TileTable t = phmm::TileTable::defaults();
+    std::memcpy(table, &t, sizeof(t));
+}
+
+phmm_status phmm_engine_get_tiles(phmm_engine* engine, phmm_tile_table* table)
+{
+    PHMM_GUARD_BEGIN
+    phmm::clear_error();
+    if (!engine) return set_error(PHMM_ERR_NOT_INITIALIZED, "engine is null");
+    if (!table) return set_error(PHMM_ERR_INVALID_ARGUMENT, "table is null");
+    const phmm::TileTable t = phmm::engine_of(engine)->tiles();
+    std::memcpy(table, &t, sizeof(t));
+    return PHMM_OK;
+    PHMM_GUARD_END
+}
+
+phmm_status phmm_engine_set_tiles(phmm_engine* engine, const phmm_tile_table* table)
+{
+    PHMM_GUARD_BEGIN
+    phmm::clear_error();
+    if (!engine) return set_error(PHMM_ERR_NOT_INITIALIZED, "engine is null");
+    if (!table) return set_error(PHMM_ERR_INVALID_ARGUMENT, "table is null");
+    phmm::TileTable t;
+    std::memcpy(&t, table, sizeof(t));
+    std::string err;
+    phmm_status st = phmm::engine_of(engine)->set_tiles(t, err);
+    return st == PHMM_OK ? PHMM_OK : set_error(st, err);
+    PHMM_GUARD_END
+}
+
+phmm_status phmm_engine_autotune(phmm_engine* engine, phmm_tune_report* report)
+{
+    PHMM_GUARD_BEGIN
+    phmm::clear_error();
+    if (!engine) return set_error(PHMM_ERR_NOT_INITIALIZED, "engine is null");
+    std::string err;
+    phmm_status st = phmm::engine_of(engine)->autotune(report, err);
+    return st == PHMM_OK ? PHMM_OK : set_error(st, err);
     PHMM_GUARD_END
 }
 

@@ -223,6 +223,10 @@ phmm_status Engine::create(const phmm_config* cfg, Engine** out, std::string& er
 #undef PHMM_CKE
     phmm_status st = e->make_slot(0, &e->default_slot_, err);
     if (st != PHMM_OK) return fail(st);
+    if (e->cfg_.autotune) {
+        st = autotune_once(*e, err);
+        if (st != PHMM_OK) return fail(st);
+    }
     *out = e;
     return PHMM_OK;
 }
@@ -282,8 +286,8 @@ uint64_t Engine::scratch_warps() const
     // Each resident warp of a multi-stripe class owns a scratch region of 24 bytes per column: two
     // FP32 rows (one per read of the warp) or one FP64 row.
     int occ = 1;
-    for (int c : {class32(kInter, 0, kMaxK, true), class32(kInter, 1, kMaxK, true), class32(kIntra, 1, kMaxK, true)})
-        occ = std::max(occ, occ_[0][c]);
+    for (int c = 0; c < kClasses32; ++c)
+        if (class32_multi(c)) occ = std::max(occ, occ_[0][c]);
     for (int c : {class64(kInter, kMaxK, true), class64(kIntra, kMaxK, true)}) occ = std::max(occ, occ_[1][c]);
     return (uint64_t)sms_ * occ * (kFwdBlock / kWarp);
 }
@@ -343,7 +347,32 @@ int Engine::grid_for(int precision, int cls, uint32_t work) const
     return std::max(need, 1);
 }
 
-phmm_status Engine::launch_pipeline(Slot& s, bool want_flags, const Plan* plan, std::string& err)
+namespace {
+
+// FP32 classes that can append reruns to FP64 class c64 under tile table t: the shapes of every
+// read-length bucket whose reads belong to c64, in each mode that can produce the class's variant
+// (a read without 'N' runs in the intra variant against haplotypes with 'N').
+void fp64_sources(const TileTable& t, int c64, bool src[kClasses32])
+{
+    for (int c = 0; c < kClasses32; ++c) src[c] = false;
+    const int variant = c64 / 9;
+    for (int b = 1; b <= kLenBuckets; ++b) {
+        if (class64_for_len(variant, (uint64_t)b * kWarp) != c64) continue;
+        for (int m = 0; m < kModes32; ++m) {
+            const int kh = t.kh[m][b - 1];
+            const bool multi = t.multi[m][b - 1] != 0;
+            if (variant == kInter) {
+                if (m < 2) src[class32(kInter, m, kh, multi)] = true;
+            } else {
+                src[class32(kIntra, 1, kh, multi)] = true;
+            }
+        }
+    }
+}
+
+}  // namespace
+
+phmm_status Engine::launch_pipeline(Slot& s, bool want_flags, const Plan* plan, const TileTable& tiles, std::string& err)
 {
     // plan == nullptr: graph capture (every class launched, persistent full grids).
     BatchView v;
@@ -369,9 +398,13 @@ phmm_status Engine::launch_pipeline(Slot& s, bool want_flags, const Plan* plan, 
     PHMM_CK(cudaEventRecordWithFlags(s.ev_t0, s.main, rec));
     PHMM_CK(launch_prep(s.d_desc, s.d_hb, s.d_codes_inter, s.d_codes_intra, s.d_out, v.pair_flags, sms_, s.main));
     s.launches += 2;
+    PHMM_CK(cudaEventRecord(s.ev_fork, s.main));
+    // Each class runs on its own stream.  An FP64 class reads the rerun list that its FP32 source
+    // classes append to, so it waits for those classes only and overlaps with the FP32 classes
+    // still running.
+    bool launched[kNumClasses] = {};
     for (int pass = 0; pass < 2; ++pass) {
         const int precision = pass == 0 ? 32 : 64;
-        PHMM_CK(cudaEventRecord(s.ev_fork, s.main));
         const int n_cls = pass == 0 ? kClasses32 : kClasses64;
         const int slot0 = pass == 0 ? 0 : kClasses32;  // descriptor slot of the pass's first class
         for (int c = 0; c < n_cls; ++c) {
@@ -390,18 +423,27 @@ phmm_status Engine::launch_pipeline(Slot& s, bool want_flags, const Plan* plan, 
             pc.status = s.d_status;
             pc.scratch = s.d_scratch;
             pc.scratch_cols = scr_cols;
-            PHMM_CK(cudaStreamWaitEvent(s.side[c], s.ev_fork, 0));
-            PHMM_CK(launch_fwd(precision, c, v, tf_, td_, pc, grid, s.side[c]));
+            cudaStream_t st = s.side[slot0 + c];
+            PHMM_CK(cudaStreamWaitEvent(st, s.ev_fork, 0));
+            if (pass == 1) {
+                bool src[kClasses32];
+                fp64_sources(tiles, c, src);
+                for (int k = 0; k < kClasses32; ++k)
+                    if (src[k] && launched[k]) PHMM_CK(cudaStreamWaitEvent(st, s.ev_side[k], 0));
+            }
+            PHMM_CK(launch_fwd(precision, c, v, tf_, td_, pc, grid, st));
             ++s.launches;
-            PHMM_CK(cudaEventRecord(s.ev_side[c], s.side[c]));
-            PHMM_CK(cudaStreamWaitEvent(s.main, s.ev_side[c], 0));
+            launched[slot0 + c] = true;
+            PHMM_CK(cudaEventRecord(s.ev_side[slot0 + c], st));
         }
+        for (int c = 0; c < n_cls; ++c)
+            if (launched[slot0 + c]) PHMM_CK(cudaStreamWaitEvent(s.main, s.ev_side[slot0 + c], 0));
         PHMM_CK(cudaEventRecordWithFlags(pass == 0 ? s.ev_t1 : s.ev_t2, s.main, rec));
     }
     return PHMM_OK;
 }
 
-phmm_status Engine::capture_graph(Slot& s, bool want_flags, std::string& err)
+phmm_status Engine::capture_graph(Slot& s, bool want_flags, const TileTable& tiles, std::string& err)
 {
     if (s.graph) {
         cudaGraphExecDestroy(s.graph);
@@ -410,7 +452,7 @@ phmm_status Engine::capture_graph(Slot& s, bool want_flags, std::string& err)
     cudaGraph_t g = nullptr;
     PHMM_CK(cudaStreamBeginCapture(s.main, cudaStreamCaptureModeThreadLocal));
     std::string lerr;
-    phmm_status st = launch_pipeline(s, want_flags, nullptr, lerr);
+    phmm_status st = launch_pipeline(s, want_flags, nullptr, tiles, lerr);
     cudaError_t e = cudaStreamEndCapture(s.main, &g);
     if (st != PHMM_OK) {
         if (g) cudaGraphDestroy(g);
@@ -429,6 +471,7 @@ phmm_status Engine::capture_graph(Slot& s, bool want_flags, std::string& err)
         return PHMM_ERR_CUDA;
     }
     s.graph_flags = want_flags;
+    s.graph_tiles = tiles;
     return PHMM_OK;
 }
 
@@ -497,13 +540,13 @@ phmm_status Engine::run(Slot& s, const Plan& plan, bool want_flags, bool restore
     cudaStream_t m = s.main;
     if (restore) PHMM_CK(cudaMemcpyAsync(s.d_desc, s.d_desc_pristine, kDescBytes, cudaMemcpyDeviceToDevice, m));
     if (cfg_.use_cuda_graph) {
-        if (!s.graph || s.graph_flags != want_flags) {
-            st = capture_graph(s, want_flags, err);
+        if (!s.graph || s.graph_flags != want_flags || std::memcmp(&s.graph_tiles, &plan.tiles, sizeof(TileTable)) != 0) {
+            st = capture_graph(s, want_flags, plan.tiles, err);
             if (st != PHMM_OK) return st;
         }
         PHMM_CK(cudaGraphLaunch(s.graph, m));
     } else {
-        st = launch_pipeline(s, want_flags, &plan, err);
+        st = launch_pipeline(s, want_flags, &plan, plan.tiles, err);
         if (st != PHMM_OK) return st;
     }
     return PHMM_OK;
@@ -596,7 +639,8 @@ phmm_status Engine::compute(const phmm_batch& b, double* out, uint8_t* pair_flag
     const auto t0 = std::chrono::steady_clock::now();
     std::lock_guard<std::mutex> lk(mu_);
     Plan plan;
-    phmm_status st = build_plan(b, PlanLimits(), plan, err);
+    const TileTable t = tiles();
+    phmm_status st = build_plan(b, limits_with(t), plan, err);
     if (st != PHMM_OK) return st;
     if (plan.out_total && !out) {
         err = "out is null";
@@ -607,6 +651,72 @@ phmm_status Engine::compute(const phmm_batch& b, double* out, uint8_t* pair_flag
     st = finish(*default_slot_, plan, out, pair_flags, stats, err);
     if (stats) stats->host_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     return st;
+}
+
+TileTable Engine::tiles() const
+{
+    std::lock_guard<std::mutex> lk(tiles_mu_);
+    return tiles_;
+}
+
+phmm_status Engine::set_tiles(const TileTable& t, std::string& err)
+{
+    if (!t.valid(err)) return PHMM_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lk(tiles_mu_);
+    tiles_ = t;
+    return PHMM_OK;
+}
+
+phmm_status Engine::time_fp32_class(Slot& s, const Plan& plan, int cls, int reps, float* best_ms, std::string& err)
+{
+    PHMM_CK(cudaSetDevice(dev_));
+    BatchView v{};
+    v.read_bases = s.d_rb;
+    v.read_q = s.d_rq;
+    v.read_i = s.d_ri;
+    v.read_d = s.d_rd;
+    v.read_c = s.d_rc;
+    v.read_off = s.d_read_off;
+    v.read_flags = s.d_read_flags;
+    v.hap_off = s.d_hap_off;
+    v.codes_inter = s.d_codes_inter;
+    v.codes_intra = s.d_codes_intra;
+    v.hap_flags = s.d_hap_flags;
+    v.regions = s.d_regions;
+    v.out = s.d_out;
+    v.pair_flags = nullptr;
+    const uint64_t warps = scratch_warps();
+    PassControl pc;
+    pc.cd = s.d_classes + cls;
+    pc.cd64 = s.d_classes + kClasses32;
+    pc.items = s.d_items;
+    pc.rerun = s.d_rerun;
+    pc.status = s.d_status;
+    pc.scratch = s.d_scratch;
+    pc.scratch_cols = s.cap.scratch_cols ? (unsigned int)(s.cap.scratch_cols / warps) : 0u;
+    const int grid = grid_for(32, cls, plan.classes[cls].n_items);
+    cudaStream_t m = s.main;
+    float best = 0.f;
+    for (int r = 0; r < reps; ++r) {
+        // fresh claim counters, rerun segments, codes and outputs for every repetition
+        PHMM_CK(cudaMemcpyAsync(s.d_desc, s.d_desc_pristine, kDescBytes, cudaMemcpyDeviceToDevice, m));
+        PHMM_CK(launch_prep(s.d_desc, s.d_hb, s.d_codes_inter, s.d_codes_intra, s.d_out, nullptr, sms_, m));
+        PHMM_CK(cudaEventRecord(s.ev_t0, m));
+        PHMM_CK(launch_fwd(32, cls, v, tf_, td_, pc, grid, m));
+        PHMM_CK(cudaEventRecord(s.ev_t1, m));
+        PHMM_CK(cudaEventSynchronize(s.ev_t1));
+        float ms = 0.f;
+        PHMM_CK(cudaEventElapsedTime(&ms, s.ev_t0, s.ev_t1));
+        if (r == 0 || ms < best) best = ms;
+    }
+    unsigned int status = 0;
+    PHMM_CK(cudaMemcpy(&status, s.d_status, sizeof(status), cudaMemcpyDeviceToHost));
+    if (status != 0) {
+        err = "kernel status word " + std::to_string(status) + " while timing class " + std::to_string(cls);
+        return PHMM_ERR_DEVICE_STATUS;
+    }
+    *best_ms = best;
+    return PHMM_OK;
 }
 
 }  // namespace phmm

@@ -55,6 +55,7 @@ struct Slot {
                 ev_t3 = nullptr, ev_done = nullptr;
     cudaGraphExec_t graph = nullptr;
     bool graph_flags = false;        // the captured graph writes pair flags
+    TileTable graph_tiles{};         // tile table whose FP64 dependencies the graph encodes
     uint64_t launches = 0;           // kernels launched by the last pipeline run
 };
 
@@ -78,17 +79,31 @@ public:
     phmm_status run(Slot& s, const Plan& plan, bool want_flags, bool restore, std::string& err);
     phmm_status fp32_fma_peak(double* scalar_tflops, double* packed_tflops, std::string& err);
 
+    // FP32 tile shapes used for new plans (thread-safe copy / replace).
+    TileTable tiles() const;
+    phmm_status set_tiles(const TileTable& t, std::string& err);
+    // Planner limits with a tile table (t must outlive the returned limits).
+    static PlanLimits limits_with(const TileTable& t)
+    {
+        PlanLimits l;
+        l.tiles = &t;
+        return l;
+    }
+    // Measures the FP32 pass of one class alone on an uploaded plan: best of `reps` launches (ms).
+    phmm_status time_fp32_class(Slot& s, const Plan& plan, int cls, int reps, float* best_ms, std::string& err);
+    // Runs the tile-shape autotuner and installs its table (phmm_tune.cpp).
+    phmm_status autotune(phmm_tune_report* report, std::string& err);
+
     int device() const { return dev_; }
     int num_sms() const { return sms_; }
     const phmm_config& config() const { return cfg_; }
     uint64_t scratch_bytes() const;  // device bytes of the stripe scratch rows (multi-stripe reads)
-    PlanLimits plan_limits() const { return PlanLimits(); }
 
 private:
     Engine() = default;
     phmm_status ensure_capacity(Slot& s, const Plan& plan, std::string& err);
-    phmm_status launch_pipeline(Slot& s, bool want_flags, const Plan* plan, std::string& err);
-    phmm_status capture_graph(Slot& s, bool want_flags, std::string& err);
+    phmm_status launch_pipeline(Slot& s, bool want_flags, const Plan* plan, const TileTable& tiles, std::string& err);
+    phmm_status capture_graph(Slot& s, bool want_flags, const TileTable& tiles, std::string& err);
     int grid_for(int precision, int cls, uint32_t work) const;
     uint64_t scratch_warps() const;
 
@@ -102,6 +117,12 @@ private:
     ProbTables<double> td_{};
     Slot* default_slot_ = nullptr;
     std::mutex mu_;
+    mutable std::mutex tiles_mu_;
+    TileTable tiles_ = TileTable::defaults();
 };
+
+// Installs the table tuned for this engine's device earlier in the process, or runs the autotuner
+// (phmm_tune.cpp).
+phmm_status autotune_once(Engine& e, std::string& err);
 
 }  // namespace phmm

@@ -1,14 +1,15 @@
-// PairHMM kernels for sm_100a: haplotype code preparation, the persistent FP32 wavefront pass and
-// the persistent FP64 recompute pass.  Device arithmetic lives in phmm_device.cuh.
+// PairHMM kernels for sm_100a: haplotype code preparation, the persistent FP64 recompute pass, the
+// FMA throughput probes and the launch wrappers of every class.  Device arithmetic lives in
+// phmm_device.cuh (scalar) and phmm_device2.cuh (packed FP32); the FP32 class kernels are in
+// phmm_fwd32.cuh, instantiated per mode in phmm_fwd32_m0/m1/m2.cu.
 //
-// Every kernel class (precision, rows per lane, variant, FP32 gap-parameter mode) is its own kernel,
-// so each gets the register allocation its own live state needs instead of the union of all paths.
-// Work items are grouped by class on the host.  FP32 runs the packed two-reads-per-warp path of
-// phmm_device2.cuh; the FP64 recompute runs the scalar one-read-per-warp path of phmm_device.cuh.
+// Every kernel class (precision, rows per lane, variant, FP32 gap-parameter mode, stripe mode) is
+// its own kernel, so each gets the register allocation its own live state needs instead of the
+// union of all paths.  Work items are grouped by class on the host.
 #include <cuda_runtime.h>
 
 #include "phmm_device.cuh"
-#include "phmm_device2.cuh"
+#include "phmm_fwd32.cuh"
 #include "phmm_kernels.h"
 
 namespace phmm {
@@ -90,80 +91,6 @@ __device__ __forceinline__ void run_read(const BatchView& b, const ProbTables<T>
 }
 
 // ------------------------------------------------------------------------------------------
-// FP32 pass for one class: two reads per warp against a run of haplotypes.
-// ------------------------------------------------------------------------------------------
-template <int KH, int V, int PM, bool MULTI>
-__device__ __forceinline__ void run_pair2(const BatchView& b, const ProbTables<float>& tb, const PassControl& pc,
-                                          const SweepOut& so, uint32_t g_lo, uint32_t g_hi, int lane, int stripes,
-                                          float* scr)
-{
-    constexpr int SR = 2 * kLanesPerRead * KH;  // rows per stripe (32 virtual lanes x KH)
-    const int l = lane & (kLanesPerRead - 1);
-    LaneRows2<KH, PM> L;
-    uint64_t roff = 0;
-    int R = 0;
-    if (so.read != kNoRead) {
-        roff = b.read_off[so.read];
-        R = (int)(b.read_off[so.read + 1] - roff);
-    }
-    const int S = MULTI ? stripes : 1;
-    const int Tcols = (int)(b.hap_off[g_hi] - b.hap_off[g_lo]);
-    // Both groups run the sweep together (full-warp shuffles), so a planning error in either skips
-    // the item for both; its pairs stay NaN and the status word reports it.
-    const bool bad = (so.read != kNoRead && R <= 0) || R > SR * S || (MULTI && (S < 2 || Tcols > (int)pc.scratch_cols));
-    if (__any_sync(0xffffffffu, bad)) {
-        if (lane == 0) atomicOr(pc.status, kStatusBadItem);
-        return;
-    }
-    const int pad = SR * S - R;
-    if (!MULTI) {
-        load_rows2<KH, V, PM>(L, b, tb, roff, R, 0, pad, l);
-        sweep2<KH, V, PM, false, false>(L, b, pc, so, g_lo, g_hi, scr, lane, 2 * l * KH <= pad);
-    } else {
-        for (int s = 0; s < S; ++s) {
-            load_rows2<KH, V, PM>(L, b, tb, roff, R, s * SR, pad, l);
-            const bool aboveA = (s == 0) && (2 * l * KH <= pad);
-            if (s == 0)
-                sweep2<KH, V, PM, false, true>(L, b, pc, so, g_lo, g_hi, scr, lane, aboveA);
-            else if (s == S - 1)
-                sweep2<KH, V, PM, true, false>(L, b, pc, so, g_lo, g_hi, scr, lane, aboveA);
-            else
-                sweep2<KH, V, PM, true, true>(L, b, pc, so, g_lo, g_hi, scr, lane, aboveA);
-            __syncwarp();  // lane 15's scratch row is read by lane 0 of the group in the next stripe
-        }
-    }
-}
-
-template <int KH, int V, int PM, bool MULTI>
-__global__ void __launch_bounds__(kFwdBlock, 1) fwd_f32_kernel(BatchView b, ProbTables<float> tb, PassControl pc)
-{
-    const int lane = threadIdx.x & (kWarp - 1);
-    const int group = lane / kLanesPerRead;
-    const unsigned int warp_id = (blockIdx.x * blockDim.x + threadIdx.x) / kWarp;
-    float* scr = MULTI ? (float*)pc.scratch + ((size_t)warp_id * 2 + group) * pc.scratch_cols * 3 : nullptr;
-    const unsigned int n = pc.cd->n_items;
-    const WorkItem* items = pc.items + pc.cd->item_off;
-    // underflowed pairs go to the FP64 class with the same rows per lane and variant
-    PassControl pr = pc;
-    pr.cd = pc.cd64 + class64(V, KH, MULTI);
-    for (;;) {
-        const unsigned int idx = claim(&pc.cd->claim32, lane);
-        if (idx >= n) break;
-        const WorkItem it = items[idx];
-        const RegionDesc rg = b.regions[it.region];
-        SweepOut so;
-        so.out = b.out;
-        so.pair_flags = b.pair_flags;
-        so.read = it.read[group];
-        so.out_base = rg.out_off + (uint64_t)it.hap_lo * rg.n_reads + (so.read - rg.read_begin);
-        so.out_stride = rg.n_reads;
-        so.fp32_pass = true;
-        run_pair2<KH, V, PM, MULTI>(b, tb, pr, so, rg.hap_begin + it.hap_lo, rg.hap_begin + it.hap_hi, lane,
-                                    it.stripes, scr);
-    }
-}
-
-// ------------------------------------------------------------------------------------------
 // FP64 pass for one class over the pairs its FP32 pass flagged, one pair per claim.
 // ------------------------------------------------------------------------------------------
 template <int K, int V, bool MULTI>
@@ -236,20 +163,13 @@ cudaError_t launch_fma_peak(float* sink, int blocks, int iters, bool packed, cud
 // ------------------------------------------------------------------------------------------
 // Class tables and host-side launch wrappers.
 // ------------------------------------------------------------------------------------------
-typedef void (*F32Kernel)(BatchView, ProbTables<float>, PassControl);
 typedef void (*F64Kernel)(BatchView, ProbTables<double>, PassControl);
 
-#define PHMM_ROW32(V, PM)                                                                                 \
-    fwd_f32_kernel<1, V, PM, false>, fwd_f32_kernel<2, V, PM, false>, fwd_f32_kernel<3, V, PM, false>,    \
-        fwd_f32_kernel<4, V, PM, false>, fwd_f32_kernel<5, V, PM, false>, fwd_f32_kernel<6, V, PM, false>, \
-        fwd_f32_kernel<7, V, PM, false>, fwd_f32_kernel<8, V, PM, false>, fwd_f32_kernel<8, V, PM, true>
 #define PHMM_ROW64(V)                                                                                     \
     fwd_f64_kernel<1, V, false>, fwd_f64_kernel<2, V, false>, fwd_f64_kernel<3, V, false>,                \
         fwd_f64_kernel<4, V, false>, fwd_f64_kernel<5, V, false>, fwd_f64_kernel<6, V, false>,            \
         fwd_f64_kernel<7, V, false>, fwd_f64_kernel<8, V, false>, fwd_f64_kernel<8, V, true>
 
-static const F32Kernel kF32[kClasses32] = {PHMM_ROW32(kInter, PM_ALL), PHMM_ROW32(kInter, PM_ROW),
-                                           PHMM_ROW32(kIntra, PM_ROW)};
 static const F64Kernel kF64[kClasses64] = {PHMM_ROW64(kInter), PHMM_ROW64(kIntra)};
 
 cudaError_t launch_prep(const BatchDesc* desc, const uint8_t* hap_bases, uint32_t* codes_inter, uint32_t* codes_intra,
@@ -265,17 +185,25 @@ cudaError_t launch_fwd(int precision, int cls, const BatchView& b, const ProbTab
                        const ProbTables<double>& td, const PassControl& pc, int grid, cudaStream_t st)
 {
     if (cls < 0 || cls >= (precision == 32 ? kClasses32 : kClasses64) || grid <= 0) return cudaErrorInvalidValue;
-    if (precision == 32)
-        kF32[cls]<<<grid, kFwdBlock, 0, st>>>(b, tf, pc);
-    else
-        kF64[cls]<<<grid, kFwdBlock, 0, st>>>(b, td, pc);
+    if (precision == 32) {
+        const int mode = cls / kShapes32, shape = cls % kShapes32;
+        if (mode == 0) return launch_f32_mode0(shape, b, tf, pc, grid, st);
+        if (mode == 1) return launch_f32_mode1(shape, b, tf, pc, grid, st);
+        return launch_f32_mode2(shape, b, tf, pc, grid, st);
+    }
+    kF64[cls]<<<grid, kFwdBlock, 0, st>>>(b, td, pc);
     return cudaGetLastError();
 }
 
 cudaError_t occupancy(int precision, int cls, int* blocks_per_sm)
 {
     if (cls < 0 || cls >= (precision == 32 ? kClasses32 : kClasses64)) return cudaErrorInvalidValue;
-    if (precision == 32) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kF32[cls], kFwdBlock, 0);
+    if (precision == 32) {
+        const int mode = cls / kShapes32, shape = cls % kShapes32;
+        if (mode == 0) return occupancy_f32_mode0(shape, blocks_per_sm);
+        if (mode == 1) return occupancy_f32_mode1(shape, blocks_per_sm);
+        return occupancy_f32_mode2(shape, blocks_per_sm);
+    }
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kF64[cls], kFwdBlock, 0);
 }
 

@@ -19,8 +19,8 @@ constexpr int kNumClasses = kClasses32 + kClasses64;  // descriptor slots: FP32 
 // with every size read from the device-side batch descriptor.
 cudaError_t launch_prep(const BatchDesc* desc, const uint8_t* hap_bases, uint32_t* codes_inter, uint32_t* codes_intra,
                         double* out, uint8_t* flags, int num_sms, cudaStream_t st);
-// precision 32: FP32 pass of class `cls` (0..26) over its work items; precision 64: FP64 pass of
-// class `cls` (0..17) over its rerun segment.
+// precision 32: FP32 pass of class `cls` (0..kClasses32-1) over its work items; precision 64: FP64
+// pass of class `cls` (0..kClasses64-1) over its rerun segment.
 cudaError_t launch_fwd(int precision, int cls, const BatchView& b, const ProbTables<float>& tf,
                        const ProbTables<double>& td, const PassControl& pc, int grid, cudaStream_t st);
 cudaError_t occupancy(int precision, int cls, int* blocks_per_sm);

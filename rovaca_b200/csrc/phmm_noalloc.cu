@@ -232,7 +232,7 @@ phmm_status run(const phmm_batch& b, double* out, uint8_t* flags, int32_t device
         for (int c = 0; c < n_cls; ++c) {
             const uint32_t work = pass == 0 ? plan.classes[c].n_items : plan.classes[slot0 + c].rerun_cap;
             if (work == 0) continue;
-            const bool multi = (c % 9) == 8;
+            const bool multi = pass == 0 ? class32_multi(c) : (c % 9) == 8;
             const int wpb = kFwdBlock / kWarp;
             int grid = std::min<int>((int)((work + wpb - 1) / wpb), d.occ[pass][c] * d.sms);
             if (multi) grid = std::min(grid, kNoAllocMultiWarps / wpb);

@@ -62,6 +62,35 @@ void make_runs(const uint64_t* hoff, const uint8_t* hflags, uint32_t n, uint32_t
 
 }  // namespace
 
+TileTable TileTable::defaults()
+{
+    TileTable t{};
+    for (int m = 0; m < kModes32; ++m)
+        for (int b = 1; b <= kLenBuckets; ++b) {
+            t.kh[m][b - 1] = (uint8_t)std::min(b, kMaxK);
+            t.multi[m][b - 1] = b > kMaxK ? 1 : 0;
+        }
+    return t;
+}
+
+bool TileTable::valid(std::string& err) const
+{
+    for (int m = 0; m < kModes32; ++m)
+        for (int b = 1; b <= kLenBuckets; ++b) {
+            const int k = kh[m][b - 1];
+            const bool mu = multi[m][b - 1] != 0;
+            const bool ok = mu ? (k >= kMinMultiKH && k <= kMaxK && k < b) : (k >= b && k <= kMaxK);
+            if (!ok) {
+                err = "tile shape of mode " + std::to_string(m) + ", bucket " + std::to_string(b) + " (reads of " +
+                      std::to_string(32 * (b - 1) + 1) + "-" + std::to_string(32 * b) + " bases): " +
+                      (mu ? "multi-stripe" : "single-stripe") + " with " + std::to_string(k) +
+                      " row pairs per lane cannot hold it";
+                return false;
+            }
+        }
+    return true;
+}
+
 phmm_status scan_batch(const phmm_batch& b, const PlanLimits& lim, BatchScan& s, std::string& err)
 {
     s = BatchScan();
@@ -136,6 +165,9 @@ phmm_status build_plan(const phmm_batch& b, const PlanLimits& lim, Plan& plan, s
 {
     plan = Plan();
     plan.classes.assign(kPlanClasses, ClassDesc{});
+    plan.tiles = lim.tiles ? *lim.tiles : TileTable::defaults();
+    if (lim.tiles && !plan.tiles.valid(err)) return PHMM_ERR_INVALID_ARGUMENT;
+    const TileTable& tiles = plan.tiles;
     BatchScan sc;
     const phmm_status st = scan_batch(b, lim, sc, err);
     if (st != PHMM_OK || b.n_regions == 0) return st;
@@ -191,7 +223,7 @@ phmm_status build_plan(const phmm_batch& b, const PlanLimits& lim, Plan& plan, s
         part.count.assign((size_t)kClasses32 * kBuckets, 0);
         std::vector<Run> runs_split, runs_all, runs_split_m, runs_all_m;
         struct ReadKey {
-            uint32_t key;  // (N, gap mode, stripes, kh) packed; reads with equal keys share a work item
+            uint32_t key;  // (N, gap mode, multi, stripes, kh) packed; reads with equal keys share an item
             uint32_t read;
         };
         std::vector<ReadKey> rk;
@@ -208,15 +240,18 @@ phmm_status build_plan(const phmm_batch& b, const PlanLimits& lim, Plan& plan, s
                 const uint64_t a = plan.read_off[gr], R = plan.read_off[gr + 1] - a;
                 plan.read_flags[gr] = has_n(rb + a, R);
                 if (R == 0) continue;
-                const bool multi = R > (uint64_t)kWarp * kMaxK;
-                const uint32_t kh = multi ? kMaxK : (uint32_t)((R + kWarp - 1) / kWarp);
-                const uint32_t stripes = multi ? (uint32_t)((R + kWarp * kMaxK - 1) / (kWarp * kMaxK)) : 1;
                 const uint8_t* ib = b.read_ins + plan.read_base0 + a;
                 const uint8_t* db = b.read_del + plan.read_base0 + a;
                 const uint8_t* cb = b.read_gcp + plan.read_base0 + a;
                 const bool uniform = constant_run(ib, R) && constant_run(db, R) && constant_run(cb, R);
                 const uint32_t n_flag = plan.read_flags[gr] & 1;
-                rk.push_back({(n_flag << 20) | ((uniform ? 0u : 1u) << 19) | (stripes << 4) | kh, gr});
+                const int mode = n_flag ? 2 : (uniform ? 0 : 1);
+                const int bucket = len_bucket(R);
+                const uint32_t kh = tiles.kh[mode][bucket - 1];
+                const bool multi = tiles.multi[mode][bucket - 1] != 0;
+                const uint32_t stripes = multi ? (uint32_t)((R + kWarp * kh - 1) / (kWarp * kh)) : 1;
+                rk.push_back({(n_flag << 22) | ((uniform ? 0u : 1u) << 21) | ((multi ? 1u : 0u) << 20) | (stripes << 4) | kh,
+                              gr});
             }
             std::stable_sort(rk.begin(), rk.end(), [](const ReadKey& x, const ReadKey& y) { return x.key < y.key; });
             bool runs_ready = false, runs_m_ready = false;
@@ -225,9 +260,9 @@ phmm_status build_plan(const phmm_batch& b, const PlanLimits& lim, Plan& plan, s
                 const uint32_t r0 = rk[k].read;
                 const uint32_t r1 = (k + 1 < rk.size() && rk[k + 1].key == key) ? rk[k + 1].read : kNoRead;
                 k += (r1 == kNoRead) ? 1 : 2;
-                const uint32_t kh = key & 0xf, stripes = (key >> 4) & 0x7fff;
-                const bool uniform = ((key >> 19) & 1) == 0, read_n = ((key >> 20) & 1) != 0;
-                const bool multi = stripes > 1;
+                const uint32_t kh = key & 0xf, stripes = (key >> 4) & 0xffff;
+                const bool uniform = ((key >> 21) & 1) == 0, read_n = ((key >> 22) & 1) != 0;
+                const bool multi = ((key >> 20) & 1) != 0;
                 const std::vector<Run>* runs;
                 if (!multi) {
                     if (!runs_ready) {
@@ -244,8 +279,9 @@ phmm_status build_plan(const phmm_batch& b, const PlanLimits& lim, Plan& plan, s
                     }
                     runs = read_n ? &runs_all_m : &runs_split_m;
                 }
-                const uint64_t rows = (plan.read_off[r0 + 1] - plan.read_off[r0]) +
-                                      (r1 == kNoRead ? 0 : plan.read_off[r1 + 1] - plan.read_off[r1]);
+                const uint64_t R0 = plan.read_off[r0 + 1] - plan.read_off[r0];
+                const uint64_t R1 = r1 == kNoRead ? 0 : plan.read_off[r1 + 1] - plan.read_off[r1];
+                const uint64_t rows = R0 + R1;
                 const uint32_t nreads = r1 == kNoRead ? 1 : 2;
                 for (const Run& run : *runs) {
                     WorkItem it{};
@@ -265,7 +301,9 @@ phmm_status build_plan(const phmm_batch& b, const PlanLimits& lim, Plan& plan, s
                     part.key.push_back(skey);
                     ++part.count[skey];
                     const uint32_t npairs = nreads * (uint32_t)(run.hi - run.lo);
-                    part.rerun_cap[class64(it.variant, (int)kh, multi)] += npairs;
+                    // each read's pairs may go to the FP64 class of its own length
+                    part.rerun_cap[class64_for_len(it.variant, R0)] += run.hi - run.lo;
+                    if (r1 != kNoRead) part.rerun_cap[class64_for_len(it.variant, R1)] += run.hi - run.lo;
                     part.pairs += npairs;
                     part.cells += (uint64_t)run.cols * rows;
                     if (multi) part.max_multi = std::max(part.max_multi, run.cols);

@@ -11,8 +11,19 @@
 
 namespace phmm {
 
-// Descriptor slots: the 27 FP32 classes, then the 18 FP64 classes (numbering in phmm_types.h).
+// Descriptor slots: the FP32 classes, then the FP64 classes (numbering in phmm_types.h).
 constexpr int kPlanClasses = kClasses32 + kClasses64;
+
+// FP32 tile shape of every (mode, read-length bucket): kh row pairs per lane, single stripe
+// (kh >= bucket) or multi-stripe (kMinMultiKH <= kh < bucket, stripes = ceil(R / (32 * kh))).
+// Modes as in phmm_types.h: 0 inter with constant gap qualities, 1 inter per-row, 2 intra.
+struct TileTable {
+    uint8_t kh[kModes32][kLenBuckets];
+    uint8_t multi[kModes32][kLenBuckets];
+    // smallest single stripe up to 256 rows, 256-row stripes beyond
+    static TileTable defaults();
+    bool valid(std::string& err) const;
+};
 
 struct PlanLimits {
     // Reference limits, roDV_schedule.cpp:70-73 (haplotype index <= 4095, read length <= 768,
@@ -24,6 +35,8 @@ struct PlanLimits {
     // multi-stripe item (bounded by the per-warp scratch row).
     uint32_t max_stream_single = 8192;
     uint32_t max_stream_multi = 4096;
+    // FP32 tile shapes (null: TileTable::defaults())
+    const TileTable* tiles = nullptr;
 };
 
 struct Plan {
@@ -38,6 +51,7 @@ struct Plan {
     std::vector<ClassDesc> classes;  // kPlanClasses: FP32 classes (items), then FP64 (rerun segments)
     uint64_t rerun_slots = 0;
     uint32_t max_multi_stream = 0;   // longest stream among multi-stripe items (0 if none)
+    TileTable tiles{};               // the shapes the items were planned with
 };
 
 // Sizes of a batch, from one validating pass over its counts and offsets (no copies).

@@ -198,7 +198,8 @@ void Server::worker(int idx)
             b.read_gcp = rd[4];
             b.read_off = roff.data();
             Plan plan;
-            st = build_plan(b, eng->plan_limits(), plan, berr);
+            const TileTable tiles = eng->tiles();
+            st = build_plan(b, Engine::limits_with(tiles), plan, berr);
             if (st == PHMM_OK) st = eng->enqueue(*slot, plan, b, want_flags, berr);
             double* out = (double*)out_buf.p;
             uint8_t* flags = want_flags ? (uint8_t*)(out + out_total) : nullptr;

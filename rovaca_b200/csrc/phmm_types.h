@@ -21,17 +21,40 @@ constexpr int kChunk = PHMM_CHUNK_PACKED;  // steps per boundary-free fast chunk
 
 enum Variant : int { kInter = 0, kIntra = 1 };
 
-// Kernel classes.  FP64 (scalar, 32 lanes per read): variant * 9 + (multi ? 8 : K - 1) with
-// K = ceil(R / 32).  FP32 (packed, 16 lanes per read, KH = ceil(R / 32) row pairs per lane):
-// 0..8 inter with constant gap parameters, 9..17 inter per-row, 18..26 intra per-row, each
-// (multi ? 8 : KH - 1).
-constexpr int kClasses64 = 18;
-constexpr int kClasses32 = 27;
-PHMM_HD inline int class64(int variant, int k, bool multi) { return variant * 9 + (multi ? 8 : k - 1); }
+// Read-length buckets: bucket = ceil(R / 32), 1..24 for the reference's R <= 768.
+constexpr int kLenBuckets = 24;
+PHMM_HD inline int len_bucket(uint64_t R) { return (int)((R + kWarp - 1) / kWarp); }
+
+// FP32 kernel classes (packed path: 16 lanes per read, two reads per warp).  A class is a mode
+//   0: inter, gap qualities constant along the read;  1: inter, per-row;  2: intra (pairs with 'N')
+// and a tile shape: KH row pairs per lane in one stripe of 32*KH rows (KH = 1..8), or stripes of
+// 32*KH rows linked through per-warp scratch rows (KH = 4..8).  Which shape a read-length bucket
+// runs in is a per-engine table (default: the smallest single stripe, 256-row stripes beyond).
+constexpr int kMinMultiKH = 4;
+constexpr int kShapes32 = kMaxK + (kMaxK - kMinMultiKH + 1);  // 8 single-stripe + 5 multi-stripe
+constexpr int kModes32 = 3;
+constexpr int kClasses32 = kModes32 * kShapes32;
+PHMM_HD inline int mode32(int variant, int pmode) { return variant == 1 ? 2 : pmode; }
+PHMM_HD inline int shape32(int kh, bool multi) { return multi ? kMaxK + kh - kMinMultiKH : kh - 1; }
 PHMM_HD inline int class32(int variant, int pmode, int kh, bool multi)
 {
-    const int base = variant == 1 ? 18 : (pmode == 0 ? 0 : 9);
-    return base + (multi ? 8 : kh - 1);
+    return mode32(variant, pmode) * kShapes32 + shape32(kh, multi);
+}
+PHMM_HD inline bool class32_multi(int c) { return c % kShapes32 >= kMaxK; }
+PHMM_HD inline int class32_kh(int c)
+{
+    const int s = c % kShapes32;
+    return s < kMaxK ? s + 1 : s - kMaxK + kMinMultiKH;
+}
+
+// FP64 recompute classes (scalar path, one read per warp): variant * 9 + (multi ? 8 : K - 1) with
+// K = ceil(R / 32) rows per lane, multi for R > 256 (stripes of 256 rows).  A pair's FP64 class
+// depends only on its read length, whatever FP32 shape computed it.
+constexpr int kClasses64 = 18;
+PHMM_HD inline int class64(int variant, int k, bool multi) { return variant * 9 + (multi ? 8 : k - 1); }
+PHMM_HD inline int class64_for_len(int variant, uint64_t R)
+{
+    return R > (uint64_t)kWarp * kMaxK ? class64(variant, kMaxK, true) : class64(variant, len_bucket(R), false);
 }
 
 struct RegionDesc {               // 32 bytes
@@ -50,8 +73,8 @@ struct WorkItem {                 // 20 bytes
     uint32_t read[2];             // global read indices
     uint32_t region;
     uint16_t hap_lo, hap_hi;      // haplotype range inside the region, [lo, hi)
-    uint8_t kh;                   // row pairs per lane (rows per 256-row stripe / 32)
-    uint8_t stripes;              // 256-row stripes (1 unless the reads are longer than 256)
+    uint8_t kh;                   // row pairs per lane: a stripe holds 32 * kh rows
+    uint8_t stripes;              // stripes per read (1 for single-stripe shapes)
     uint8_t variant;              // Variant
     uint8_t pmode;                // ParamMode of the FP32 kernel (0: gap parameters constant)
 };

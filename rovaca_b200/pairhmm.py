@@ -176,15 +176,34 @@ def compute_noalloc(batch: PackedBatch, device: int = 0, want_flags: bool = Fals
     return out, fl
 
 
-def plan_summary(batch: PackedBatch) -> dict:
-    """How the engine cuts a batch into work (host only): items and pairs per kernel class."""
+def plan_summary(batch: PackedBatch, tiles: "_lib.TileTable | None" = None) -> dict:
+    """How the engine cuts a batch into work (host only): items per FP32 class and pairs per FP64
+    class, under a tile table (default shapes when None)."""
     lib = _lib.load()
-    items = np.zeros(27, np.uint32)
-    pairs = np.zeros(18, np.uint64)
+    items = np.zeros(_lib.FP32_CLASSES, np.uint32)
+    pairs = np.zeros(_lib.FP64_CLASSES, np.uint64)
     tp, tc = C.c_uint64(), C.c_uint64()
     b = batch.as_c()
-    check(lib.phmm_host_plan_summary(C.byref(b), _ptr(items), _ptr(pairs), C.byref(tp), C.byref(tc)))
+    check(lib.phmm_host_plan_summary(C.byref(b), C.byref(tiles) if tiles is not None else None, _ptr(items),
+                                     _ptr(pairs), C.byref(tp), C.byref(tc)))
     return {"class_items": items, "class_pairs": pairs, "pairs": tp.value, "cells": tc.value}
+
+
+def default_tiles() -> "_lib.TileTable":
+    """phmm_tile_table_default: smallest single stripe up to 256 rows, 256-row stripes beyond."""
+    t = _lib.TileTable()
+    _lib.load().phmm_tile_table_default(C.byref(t))
+    return t
+
+
+def class32(mode: int, kh: int, multi: bool = False) -> int:
+    """FP32 kernel class of a mode (0 inter constant gaps, 1 inter per-row, 2 intra) and shape."""
+    return mode * 13 + (4 + kh if multi else kh - 1)
+
+
+def class64(intra: bool, read_len: int) -> int:
+    """FP64 recompute class of a pair from its variant and read length."""
+    return (9 if intra else 0) + (8 if read_len > 256 else (read_len + 31) // 32 - 1)
 
 
 class Engine:
@@ -279,6 +298,23 @@ class Engine:
 
     def cancel(self, ticket: int) -> None:
         check(self._lib.phmm_cancel(self._h, ticket))
+
+    def tiles(self) -> "_lib.TileTable":
+        t = _lib.TileTable()
+        check(self._lib.phmm_engine_get_tiles(self._h, C.byref(t)))
+        return t
+
+    def set_tiles(self, table: "_lib.TileTable") -> None:
+        check(self._lib.phmm_engine_set_tiles(self._h, C.byref(table)))
+
+    def autotune(self) -> dict:
+        """Runs the tile-shape autotuner now; returns its measurements (the table is installed)."""
+        rep = _lib.TuneReport()
+        check(self._lib.phmm_engine_autotune(self._h, C.byref(rep)))
+        entries = [{"mode": e.mode, "bucket": e.bucket, "rows_per_lane": e.rows_per_lane,
+                    "multi_stripe": bool(e.multi_stripe), "chosen": bool(e.chosen), "gcups": round(e.gcups, 1)}
+                   for e in rep.entries[:rep.n_entries]]
+        return {"seconds": rep.seconds, "entries": entries}
 
     def server_stats(self) -> dict:
         """Counters of the serving loop (phmm_server_stats_get)."""

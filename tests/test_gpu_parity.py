@@ -198,3 +198,90 @@ def test_full_size_batch_properties(engine, oracle):
     gflags = np.concatenate([fa[offs[g]:offs[g + 1]] for g in sample])
     assert np.max(np.abs(got - want)) <= EXACT
     assert np.array_equal(gflags.astype(bool), used)
+
+
+def _all_length_batch(seed):
+    """Reads of every length bucket 1..24 (with and without N, constant and per-row gap
+    qualities) against a few haplotypes."""
+    rng = np.random.default_rng(seed)
+    acgt = np.frombuffer(b"ACGT", np.uint8)
+    regs = []
+    for g in range(3):
+        base = acgt[rng.integers(0, 4, 2000)]
+        haps = [bytes(base[s:s + int(rng.integers(100, 700))]) for s in rng.integers(0, 600, 4)]
+        if g == 2:
+            hb = bytearray(haps[1])
+            hb[10] = ord("N")
+            haps[1] = bytes(hb)
+        reads, ins = [], []
+        for bucket in range(1, 25):
+            for k in range(2):
+                L = int(rng.integers(32 * (bucket - 1) + 1, 32 * bucket + 1))
+                r = bytearray(base[int(rng.integers(0, 1000)):][:L])
+                if (bucket + k + g) % 5 == 0:
+                    r[len(r) // 2] = ord("N")
+                reads.append(bytes(r))
+                ins.append(bytes([45] * L) if k == 0 else rng.integers(30, 46, L).astype(np.uint8).tobytes())
+        q = [rng.integers(5, 42, len(r)).astype(np.uint8).tobytes() for r in reads]
+        d = [bytes([45] * len(r)) for r in reads]
+        c = [bytes([10] * len(r)) for r in reads]
+        regs.append(Region(haps, reads, q, ins, d, c))
+    return PackedBatch.from_regions(regs)
+
+
+def _table(shape_of_bucket):
+    from rovaca_b200 import _lib
+    from rovaca_b200.pairhmm import default_tiles
+
+    kh, mu = default_tiles().as_arrays()
+    for m in range(3):
+        for b in range(1, 25):
+            s = shape_of_bucket(m, b)
+            if s is not None:
+                kh[m, b - 1], mu[m, b - 1] = s
+    return _lib.TileTable.from_arrays(kh, mu)
+
+
+def test_every_tile_shape_gives_identical_results(oracle):
+    """Every FP32 kernel class (13 shapes x 3 modes) computes the same bits: the same batch under
+    tables that move each bucket to each multi-stripe shape that can hold it."""
+    from rovaca_b200 import Engine
+
+    pb = _all_length_batch(7)
+    want, used = oracle.batch(pb)
+    with Engine(device=0, autotune=False, use_cuda_graph=False) as eng:
+        base, fb, _ = eng.compute(pb, want_flags=True)
+        assert np.nanmax(np.abs(base - want)) <= EXACT
+        assert np.array_equal(fb.astype(bool), used)
+        for kh in range(4, 9):
+            eng.set_tiles(_table(lambda m, b, kh=kh: (kh, 1) if kh < b else None))
+            got, fg, _ = eng.compute(pb, want_flags=True)
+            assert np.array_equal(got, base, equal_nan=True), kh
+            assert np.array_equal(fg, fb), kh
+    # a captured graph is captured again for a new table (its FP64 dependencies follow the shapes)
+    with Engine(device=0, autotune=False, use_cuda_graph=True) as eng:
+        a, _, _ = eng.compute(pb)
+        assert np.array_equal(a, base, equal_nan=True)
+        eng.set_tiles(_table(lambda m, b: (4, 1) if b > 4 else None))
+        got, fg, _ = eng.compute(pb, want_flags=True)
+        assert np.array_equal(got, base, equal_nan=True) and np.array_equal(fg, fb)
+
+
+def test_autotune_installs_a_valid_table(engine_direct):
+    from rovaca_b200 import Engine
+
+    with Engine(device=0, autotune=False) as eng:
+        rep = eng.autotune()
+        assert rep["seconds"] > 0 and rep["entries"]
+        kh, mu = eng.tiles().as_arrays()
+        chosen = [e for e in rep["entries"] if e["chosen"]]
+        tuned = {(e["mode"], e["bucket"]) for e in rep["entries"]}
+        assert {(e["mode"], e["bucket"]) for e in chosen} == tuned  # one winner per tuned bucket
+        for e in chosen:
+            assert kh[e["mode"], e["bucket"] - 1] == e["rows_per_lane"]
+            assert bool(mu[e["mode"], e["bucket"] - 1]) == e["multi_stripe"]
+        assert all(e["gcups"] > 0 for e in rep["entries"])
+        pb = synth.config1(6, seed=3)
+        a, _, _ = eng.compute(pb)
+        b, _, _ = engine_direct.compute(pb)
+        assert np.array_equal(a, b, equal_nan=True)

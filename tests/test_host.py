@@ -12,7 +12,7 @@ import pytest
 
 from conftest import GOLDEN
 from rovaca_b200 import _lib
-from rovaca_b200.pairhmm import PackedBatch, Region, plan_summary
+from rovaca_b200.pairhmm import PackedBatch, Region, class32, class64, default_tiles, plan_summary
 
 
 def _region(haps, reads, q=30, ins=45, gcp=10):
@@ -62,9 +62,10 @@ def test_engine_refuses_to_run_without_a_gpu():
 # ---- planning -------------------------------------------------------------------------------
 
 def cls(variant, kh, multi=False, uniform=True):
-    """FP32 kernel class: 0.. inter with constant gap qualities, 9.. inter per-row, 18.. intra."""
-    base = 18 if variant else (0 if uniform else 9)
-    return base + (8 if multi else kh - 1)
+    """FP32 kernel class: mode (0 inter with constant gap qualities, 1 inter per-row, 2 intra) x 13
+    shapes (single stripe KH 1..8, multi-stripe KH 4..8)."""
+    mode = 2 if variant else (0 if uniform else 1)
+    return class32(mode, kh, multi)
 
 
 def cls64(variant, kh, multi=False):
@@ -101,8 +102,8 @@ def test_plan_routes_n_pairs_to_the_intra_variant():
     assert s["class_pairs"][9:].sum() == 3 + 2
     assert s["class_pairs"][:9].sum() == 2 * 2
     # each read without N streams [h] and [h] as two inter items split around the N haplotype
-    assert s["class_items"][:18].sum() == 4
-    assert s["class_items"][18:].sum() == 3
+    assert s["class_items"][:26].sum() == 4
+    assert s["class_items"][26:].sum() == 3
 
 
 def test_plan_splits_long_haplotype_streams():
@@ -123,6 +124,32 @@ def test_plan_pairs_reads_and_gap_modes():
     s = plan_summary(PackedBatch.from_regions([reg]))
     assert s["class_items"][cls(0, 5, uniform=False)] == 1
     assert s["class_items"][cls(0, 5)] == 2
+
+
+def test_tile_table_shapes_route_reads():
+    """A tile table moves a read-length bucket to a multi-stripe shape; FP64 classes follow the read
+    length whatever the FP32 shape; invalid shapes are rejected."""
+    hap = b"ACGT" * 100
+    reads = [hap[:200], hap[:210], hap[:240], hap[:100]]  # buckets 7, 7, 8, 4
+    pb = PackedBatch.from_regions([_region([hap, hap[5:]], reads)])
+    d = plan_summary(pb)
+    assert d["class_items"][cls(0, 7)] == 1 and d["class_items"][cls(0, 8)] == 1 and d["class_items"][cls(0, 4)] == 1
+    kh, mu = default_tiles().as_arrays()
+    assert list(kh[0, :10]) == [1, 2, 3, 4, 5, 6, 7, 8, 8, 8] and list(mu[0, :10]) == [0] * 8 + [1, 1]
+    kh[0, 6], mu[0, 6] = 4, 1  # bucket 7 (193-224 rows): two 128-row stripes
+    kh[0, 7], mu[0, 7] = 5, 1  # bucket 8 (225-256 rows): two 160-row stripes
+    s = plan_summary(pb, _lib.TileTable.from_arrays(kh, mu))
+    assert s["class_items"][cls(0, 4, True)] == 1 and s["class_items"][cls(0, 5, True)] == 1
+    assert s["class_items"][cls(0, 4)] == 1 and s["class_items"].sum() == 3
+    assert np.array_equal(s["class_pairs"], d["class_pairs"])
+    assert s["class_pairs"][class64(False, 200)] == 4 and s["class_pairs"][class64(False, 240)] == 2
+    assert s["cells"] == d["cells"] and s["pairs"] == d["pairs"]
+    for b, k, m in ((6, 7, 1), (6, 6, 0), (3, 3, 1)):  # multi needs 4 <= KH < bucket, single KH >= bucket
+        kh2, mu2 = default_tiles().as_arrays()
+        kh2[0, b], mu2[0, b] = k, m
+        with pytest.raises(_lib.PhmmError) as e:
+            plan_summary(pb, _lib.TileTable.from_arrays(kh2, mu2))
+        assert e.value.name == "PHMM_ERR_INVALID_ARGUMENT"
 
 
 def test_plan_skips_empty_reads_and_haplotypes():
