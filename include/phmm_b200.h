@@ -135,7 +135,9 @@ PHMM_API phmm_status phmm_compute_regions(phmm_engine* engine, const phmm_batch*
  *   5. reads whose best likelihood is below -4 * min(2, ceil(0.02 * len)) are dropped.
  * out    : [n_haps][n_reads] doubles; column k holds the k-th kept read, trailing columns NaN.
  * keep   : [n_reads] bytes, 1 where the read was kept (the caller erases the others, in order).
- * n_kept : number of kept reads. */
+ * n_kept : number of kept reads.
+ * Steps 1-3 and 4-5 run on the GPU around the likelihood kernels (only bases, raw qualities and
+ * MAPQ are uploaded); concurrent calls are batched by the serving loop (phmm_submit_region). */
 PHMM_API phmm_status phmm_call_region(phmm_engine* engine, uint32_t n_haps, const uint8_t* hap_bases, const uint64_t* hap_off,
                              uint32_t n_reads, const uint8_t* read_bases, const uint8_t* read_qual,
                              const uint64_t* read_off, const uint8_t* mapq, int32_t min_quality_threshold,
@@ -260,6 +262,26 @@ typedef uint64_t phmm_ticket;
  * batched with whatever else is in flight.  Thread-safe. */
 PHMM_API phmm_status phmm_submit(phmm_engine* engine, const phmm_batch* region, double* out, uint8_t* pair_flags,
                         phmm_ticket* ticket);
+/* One region for the region API (phmm_call_region's inputs). */
+typedef struct phmm_region_input {
+    uint32_t n_haps;
+    const uint8_t* hap_bases;
+    const uint64_t* hap_off;    /* [n_haps + 1] */
+    uint32_t n_reads;
+    const uint8_t* read_bases;
+    const uint8_t* read_qual;   /* raw base qualities */
+    const uint64_t* read_off;   /* [n_reads + 1] */
+    const uint8_t* mapq;        /* [n_reads] */
+    int32_t min_quality_threshold;
+    int32_t pcr_model;          /* phmm_pcr_model */
+} phmm_region_input;
+
+/* Submits one region with phmm_call_region's semantics; the read preparation (quality cap, gap
+ * qualities, PCR model) and the post-processing (normalise, drop poorly modelled reads, kept reads
+ * first) run on the GPU.  out [n_haps][n_reads], keep [n_reads] and n_kept must stay valid until
+ * the request completes (phmm_wait).  Inputs are copied before the call returns.  Thread-safe. */
+PHMM_API phmm_status phmm_submit_region(phmm_engine* engine, const phmm_region_input* region, double* out, uint8_t* keep,
+                                        uint32_t* n_kept, phmm_ticket* ticket);
 /* *done = 1 once the request's results are in out (or it failed / was cancelled). */
 PHMM_API phmm_status phmm_poll(phmm_engine* engine, phmm_ticket ticket, int32_t* done);
 /* Blocks up to timeout_us (negative = forever).  Once the request is done it returns the request's

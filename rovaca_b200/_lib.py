@@ -90,6 +90,14 @@ class TuneReport(C.Structure):
                 ("entries", TuneEntry * TUNE_MAX_ENTRIES)]
 
 
+class RegionInput(C.Structure):
+    """phmm_region_input: one region for the region API."""
+    _fields_ = [("n_haps", C.c_uint32), ("hap_bases", C.c_void_p), ("hap_off", C.c_void_p),
+                ("n_reads", C.c_uint32), ("read_bases", C.c_void_p), ("read_qual", C.c_void_p),
+                ("read_off", C.c_void_p), ("mapq", C.c_void_p), ("min_quality_threshold", C.c_int32),
+                ("pcr_model", C.c_int32)]
+
+
 class ServerStats(C.Structure):
     _fields_ = [("requests_submitted", C.c_uint64), ("requests_done", C.c_uint64), ("batches", C.c_uint64),
                 ("max_batch_regions", C.c_uint64), ("queue_peak", C.c_uint64), ("cells_done", C.c_uint64),
@@ -136,6 +144,7 @@ def load() -> C.CDLL:
         "phmm_engine_set_tiles": (I32, [P, P]),
         "phmm_engine_autotune": (I32, [P, P]),
         "phmm_submit": (I32, [P, C.POINTER(Batch), P, P, C.POINTER(U64)]),
+        "phmm_submit_region": (I32, [P, P, P, P, C.POINTER(U32), C.POINTER(U64)]),
         "phmm_poll": (I32, [P, U64, C.POINTER(I32)]),
         "phmm_wait": (I32, [P, U64, I64, C.POINTER(D), C.POINTER(D)]),
         "phmm_cancel": (I32, [P, U64]),

@@ -5,7 +5,9 @@
 //   plan arrays       regions, read_off, hap_off, read/hap N flags, work items
 //   read data         bases, q, ins, del, gcp (1 byte per base each)
 //   haplotypes        bases, then two u32 match-code streams with guard codes on both ends
-//   results           likelihoods (f64), pair flags (u8), FP64 rerun slots (16 B per pair)
+//   region API        MAPQ and kept flag per read, kept count per region
+//   results           likelihoods (f64), pair flags (u8), normalised likelihoods (f64, region API),
+//                     FP64 rerun slots (16 B per pair)
 //   scratch           per-warp stripe row for reads longer than 256 (3 values per column)
 // The arena only grows; all kernel arguments are arena pointers, so a graph captured for an arena
 // replays for every batch that fits it.
@@ -15,6 +17,7 @@
 #include <chrono>
 #include <cstring>
 
+#include "phmm_regionk.h"
 #include "phmm_tables.h"
 
 namespace phmm {
@@ -57,10 +60,14 @@ size_t carve(const Capacity& c, char* base, Slot* s)
     char* rd = take(c.read_bases);
     char* rc = take(c.read_bases);
     char* hb = take(c.hap_bases);
+    char* mapq = take(c.reads);
+    char* keep = take(c.reads);
+    char* nkept = take(c.regions * sizeof(uint32_t));
     char* ci = take((c.hap_bases + 2 * kCodePad) * sizeof(uint32_t));
     char* ca = take((c.hap_bases + 2 * kCodePad) * sizeof(uint32_t));
     char* out = take(c.out * sizeof(double));
     char* pf = take(c.out);
+    char* out2 = take(c.out * sizeof(double));
     char* rerun = take(c.rerun * sizeof(RerunEntry));
     char* scratch = take(c.scratch_cols * 3 * sizeof(double));  // c.scratch_cols counts all warps' columns
     if (s) {
@@ -80,6 +87,10 @@ size_t carve(const Capacity& c, char* base, Slot* s)
         s->d_rd = (uint8_t*)rd;
         s->d_rc = (uint8_t*)rc;
         s->d_hb = (uint8_t*)hb;
+        s->d_mapq = (uint8_t*)mapq;
+        s->d_keep = (uint8_t*)keep;
+        s->d_nkept = (uint32_t*)nkept;
+        s->d_out2 = (double*)out2;
         s->d_codes_inter = (uint32_t*)ci;
         s->d_codes_intra = (uint32_t*)ca;
         s->d_out = (double*)out;
@@ -349,6 +360,25 @@ int Engine::grid_for(int precision, int cls, uint32_t work) const
 
 namespace {
 
+RegionApiView region_view(const Slot& s)
+{
+    RegionApiView rv;
+    rv.desc = s.d_desc;
+    rv.regions = s.d_regions;
+    rv.read_off = s.d_read_off;
+    rv.read_bases = s.d_rb;
+    rv.read_q = s.d_rq;
+    rv.read_i = s.d_ri;
+    rv.read_d = s.d_rd;
+    rv.read_c = s.d_rc;
+    rv.mapq = s.d_mapq;
+    rv.lk = s.d_out;
+    rv.out = s.d_out2;
+    rv.keep = s.d_keep;
+    rv.n_kept = s.d_nkept;
+    return rv;
+}
+
 // FP32 classes that can append reruns to FP64 class c64 under tile table t: the shapes of every
 // read-length bucket whose reads belong to c64, in each mode that can produce the class's variant
 // (a read without 'N' runs in the intra variant against haplotypes with 'N').
@@ -398,6 +428,11 @@ phmm_status Engine::launch_pipeline(Slot& s, bool want_flags, const Plan* plan, 
     PHMM_CK(cudaEventRecordWithFlags(s.ev_t0, s.main, rec));
     PHMM_CK(launch_prep(s.d_desc, s.d_hb, s.d_codes_inter, s.d_codes_intra, s.d_out, v.pair_flags, sms_, s.main));
     s.launches += 2;
+    const RegionApiView rv = region_view(s);
+    if (!plan || plan->region_api) {
+        PHMM_CK(launch_read_prep(rv, sms_, s.main));
+        ++s.launches;
+    }
     PHMM_CK(cudaEventRecord(s.ev_fork, s.main));
     // Each class runs on its own stream.  An FP64 class reads the rerun list that its FP32 source
     // classes append to, so it waits for those classes only and overlaps with the FP32 classes
@@ -438,6 +473,10 @@ phmm_status Engine::launch_pipeline(Slot& s, bool want_flags, const Plan* plan, 
         }
         for (int c = 0; c < n_cls; ++c)
             if (launched[slot0 + c]) PHMM_CK(cudaStreamWaitEvent(s.main, s.ev_side[slot0 + c], 0));
+        if (pass == 1 && (!plan || plan->region_api)) {
+            PHMM_CK(launch_post_region(rv, sms_, s.main));
+            ++s.launches;
+        }
         PHMM_CK(cudaEventRecordWithFlags(pass == 0 ? s.ev_t1 : s.ev_t2, s.main, rec));
     }
     return PHMM_OK;
@@ -475,8 +514,12 @@ phmm_status Engine::capture_graph(Slot& s, bool want_flags, const TileTable& til
     return PHMM_OK;
 }
 
-phmm_status Engine::upload(Slot& s, const Plan& plan, const phmm_batch& b, std::string& err)
+phmm_status Engine::upload(Slot& s, const Plan& plan, const phmm_batch& b, std::string& err, const uint8_t* mapq)
 {
+    if (plan.region_api && plan.n_reads && !mapq) {
+        err = "region-API batch without MAPQ";
+        return PHMM_ERR_INVALID_ARGUMENT;
+    }
     phmm_status st = ensure_capacity(s, plan, err);
     if (st != PHMM_OK) return st;
     PHMM_CK(cudaSetDevice(dev_));
@@ -496,6 +539,8 @@ phmm_status Engine::upload(Slot& s, const Plan& plan, const phmm_batch& b, std::
     bd.n_reads = plan.n_reads;
     bd.n_haps = plan.n_haps;
     bd.n_items = (uint32_t)plan.items.size();
+    bd.read_bases_total = plan.read_bases;
+    bd.region_api = plan.region_api ? plan.n_regions : 0;
     char* desc = p;
     std::memcpy(desc, &bd, sizeof(bd));
     std::memcpy(desc + sizeof(bd), plan.classes.data(), sizeof(ClassDesc) * kNumClasses);
@@ -523,13 +568,17 @@ phmm_status Engine::upload(Slot& s, const Plan& plan, const phmm_batch& b, std::
     if (rb) {
         PHMM_CK(cudaMemcpyAsync(s.d_rb, b.read_bases + plan.read_base0, rb, cudaMemcpyHostToDevice, m));
         PHMM_CK(cudaMemcpyAsync(s.d_rq, b.read_qual + plan.read_base0, rb, cudaMemcpyHostToDevice, m));
-        PHMM_CK(cudaMemcpyAsync(s.d_ri, b.read_ins + plan.read_base0, rb, cudaMemcpyHostToDevice, m));
-        PHMM_CK(cudaMemcpyAsync(s.d_rd, b.read_del + plan.read_base0, rb, cudaMemcpyHostToDevice, m));
-        PHMM_CK(cudaMemcpyAsync(s.d_rc, b.read_gcp + plan.read_base0, rb, cudaMemcpyHostToDevice, m));
+        if (!plan.region_api) {  // region API: the device writes the gap qualities
+            PHMM_CK(cudaMemcpyAsync(s.d_ri, b.read_ins + plan.read_base0, rb, cudaMemcpyHostToDevice, m));
+            PHMM_CK(cudaMemcpyAsync(s.d_rd, b.read_del + plan.read_base0, rb, cudaMemcpyHostToDevice, m));
+            PHMM_CK(cudaMemcpyAsync(s.d_rc, b.read_gcp + plan.read_base0, rb, cudaMemcpyHostToDevice, m));
+        }
     }
     if (plan.hap_bases)
         PHMM_CK(cudaMemcpyAsync(s.d_hb, b.hap_bases + plan.hap_base0, plan.hap_bases, cudaMemcpyHostToDevice, m));
 
+    if (plan.region_api && plan.n_reads)
+        PHMM_CK(cudaMemcpyAsync(s.d_mapq, mapq, plan.n_reads, cudaMemcpyHostToDevice, m));
     PHMM_CK(cudaMemcpyAsync(s.d_desc_pristine, s.d_desc, kDescBytes, cudaMemcpyDeviceToDevice, m));
     return PHMM_OK;
 }
@@ -552,21 +601,28 @@ phmm_status Engine::run(Slot& s, const Plan& plan, bool want_flags, bool restore
     return PHMM_OK;
 }
 
-phmm_status Engine::enqueue(Slot& s, const Plan& plan, const phmm_batch& b, bool want_flags, std::string& err)
+phmm_status Engine::enqueue(Slot& s, const Plan& plan, const phmm_batch& b, bool want_flags, std::string& err,
+                            const uint8_t* mapq)
 {
-    phmm_status st = upload(s, plan, b, err);
+    phmm_status st = upload(s, plan, b, err, mapq);
     if (st != PHMM_OK) return st;
     return run(s, plan, want_flags, false, err);
 }
 
 phmm_status Engine::finish(Slot& s, const Plan& plan, double* out, uint8_t* pair_flags, phmm_stats* stats,
-                           std::string& err)
+                           std::string& err, uint8_t* keep, uint32_t* n_kept)
 {
     cudaStream_t m = s.main;
     char* desc = s.pinned;  // reuse the staged descriptor block for the read-back
     PHMM_CK(cudaMemcpyAsync(desc, s.d_desc, kDescBytes, cudaMemcpyDeviceToHost, m));
+    if (plan.region_api) {
+        if (plan.n_reads && keep) PHMM_CK(cudaMemcpyAsync(keep, s.d_keep, plan.n_reads, cudaMemcpyDeviceToHost, m));
+        if (plan.n_regions && n_kept)
+            PHMM_CK(cudaMemcpyAsync(n_kept, s.d_nkept, plan.n_regions * sizeof(uint32_t), cudaMemcpyDeviceToHost, m));
+    }
     if (plan.out_total) {
-        PHMM_CK(cudaMemcpyAsync(out, s.d_out, plan.out_total * sizeof(double), cudaMemcpyDeviceToHost, m));
+        PHMM_CK(cudaMemcpyAsync(out, plan.region_api ? s.d_out2 : s.d_out, plan.out_total * sizeof(double),
+                                cudaMemcpyDeviceToHost, m));
         if (pair_flags) PHMM_CK(cudaMemcpyAsync(pair_flags, s.d_pair_flags, plan.out_total, cudaMemcpyDeviceToHost, m));
     }
     PHMM_CK(cudaEventRecord(s.ev_t3, m));

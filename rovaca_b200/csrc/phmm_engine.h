@@ -46,6 +46,10 @@ struct Slot {
     uint8_t* d_pair_flags = nullptr;
     uint8_t *d_rb = nullptr, *d_rq = nullptr, *d_ri = nullptr, *d_rd = nullptr, *d_rc = nullptr;
     uint8_t* d_hb = nullptr;
+    uint8_t* d_mapq = nullptr;       // region API: MAPQ per read
+    double* d_out2 = nullptr;        // region API: normalised likelihoods, kept reads first
+    uint8_t* d_keep = nullptr;       // region API: kept flag per read
+    uint32_t* d_nkept = nullptr;     // region API: kept reads per region
     uint32_t *d_codes_inter = nullptr, *d_codes_intra = nullptr;
     void* d_scratch = nullptr;
     // execution
@@ -70,12 +74,17 @@ public:
     // Pieces used by the serving loop (phmm_serve.cpp), each on a caller-owned slot.
     phmm_status make_slot(int id, Slot** out, std::string& err);
     void free_slot(Slot* s);
-    phmm_status enqueue(Slot& s, const Plan& plan, const phmm_batch& b, bool want_flags, std::string& err);
+    // mapq: MAPQ per read, region-API plans only (their raw qualities are prepared on the device).
+    phmm_status enqueue(Slot& s, const Plan& plan, const phmm_batch& b, bool want_flags, std::string& err,
+                        const uint8_t* mapq = nullptr);
+    // Region-API plans: out receives the normalised matrices (kept reads first), keep the kept flag
+    // of every read and n_kept the kept reads of every region.
     phmm_status finish(Slot& s, const Plan& plan, double* out, uint8_t* pair_flags, phmm_stats* stats,
-                       std::string& err);
+                       std::string& err, uint8_t* keep = nullptr, uint32_t* n_kept = nullptr);
     // Upload only (descriptor, plan arrays, reads, haplotypes); then run the device pipeline, with
     // restore = true resetting the descriptor from its pristine device copy first (replays).
-    phmm_status upload(Slot& s, const Plan& plan, const phmm_batch& b, std::string& err);
+    phmm_status upload(Slot& s, const Plan& plan, const phmm_batch& b, std::string& err,
+                       const uint8_t* mapq = nullptr);
     phmm_status run(Slot& s, const Plan& plan, bool want_flags, bool restore, std::string& err);
     phmm_status fp32_fma_peak(double* scalar_tflops, double* packed_tflops, std::string& err);
 

@@ -153,8 +153,10 @@ phmm_status scan_batch(const phmm_batch& b, const PlanLimits& lim, BatchScan& s,
     }
     s.hap_bases = b.hap_off[nh] - s.hap_base0;
     s.read_bases = b.read_off[nr] - s.read_base0;
+    const bool gaps_needed = lim.region_api == nullptr;
     if ((s.hap_bases > 0 && !b.hap_bases) ||
-        (s.read_bases > 0 && (!b.read_bases || !b.read_qual || !b.read_ins || !b.read_del || !b.read_gcp))) {
+        (s.read_bases > 0 && (!b.read_bases || !b.read_qual ||
+                              (gaps_needed && (!b.read_ins || !b.read_del || !b.read_gcp))))) {
         err = "batch: sequence or quality pointer is null";
         return PHMM_ERR_INVALID_ARGUMENT;
     }
@@ -166,6 +168,7 @@ phmm_status build_plan(const phmm_batch& b, const PlanLimits& lim, Plan& plan, s
     plan = Plan();
     plan.classes.assign(kPlanClasses, ClassDesc{});
     plan.tiles = lim.tiles ? *lim.tiles : TileTable::defaults();
+    plan.region_api = lim.region_api != nullptr;
     if (lim.tiles && !plan.tiles.valid(err)) return PHMM_ERR_INVALID_ARGUMENT;
     const TileTable& tiles = plan.tiles;
     BatchScan sc;
@@ -200,6 +203,10 @@ phmm_status build_plan(const phmm_batch& b, const PlanLimits& lim, Plan& plan, s
             rd.n_haps = b.n_haps[g];
             rd.read_begin = read_begin;
             rd.n_reads = b.n_reads[g];
+            if (lim.region_api) {
+                rd.api = kRegionApi | ((uint32_t)(lim.region_api[g].pcr & 0xff) << 8);
+                rd.min_quality = lim.region_api[g].min_quality;
+            }
             out_off += (uint64_t)b.n_haps[g] * b.n_reads[g];
             hap_begin += b.n_haps[g];
             read_begin += b.n_reads[g];
@@ -240,10 +247,16 @@ phmm_status build_plan(const phmm_batch& b, const PlanLimits& lim, Plan& plan, s
                 const uint64_t a = plan.read_off[gr], R = plan.read_off[gr + 1] - a;
                 plan.read_flags[gr] = has_n(rb + a, R);
                 if (R == 0) continue;
-                const uint8_t* ib = b.read_ins + plan.read_base0 + a;
-                const uint8_t* db = b.read_del + plan.read_base0 + a;
-                const uint8_t* cb = b.read_gcp + plan.read_base0 + a;
-                const bool uniform = constant_run(ib, R) && constant_run(db, R) && constant_run(cb, R);
+                // region API: gap qualities are constant unless a PCR model caps them
+                bool uniform;
+                if (lim.region_api) {
+                    uniform = lim.region_api[g].pcr == PHMM_PCR_NONE;
+                } else {
+                    const uint8_t* ib = b.read_ins + plan.read_base0 + a;
+                    const uint8_t* db = b.read_del + plan.read_base0 + a;
+                    const uint8_t* cb = b.read_gcp + plan.read_base0 + a;
+                    uniform = constant_run(ib, R) && constant_run(db, R) && constant_run(cb, R);
+                }
                 const uint32_t n_flag = plan.read_flags[gr] & 1;
                 const int mode = n_flag ? 2 : (uniform ? 0 : 1);
                 const int bucket = len_bucket(R);

@@ -25,6 +25,13 @@ struct TileTable {
     bool valid(std::string& err) const;
 };
 
+// Region-API parameters of one region (call_pairhmm semantics): reads arrive with raw base
+// qualities and are prepared on the device.
+struct RegionApiParams {
+    int32_t min_quality;  // base qualities below this become 6
+    int32_t pcr;          // phmm_pcr_model
+};
+
 struct PlanLimits {
     // Reference limits, roDV_schedule.cpp:70-73 (haplotype index <= 4095, read length <= 768,
     // haplotype length <= 1536).
@@ -37,6 +44,9 @@ struct PlanLimits {
     uint32_t max_stream_multi = 4096;
     // FP32 tile shapes (null: TileTable::defaults())
     const TileTable* tiles = nullptr;
+    // Non-null: every region of the batch uses the region API, with these parameters [n_regions];
+    // the batch's gap-quality arrays are not read (the device writes them).
+    const RegionApiParams* region_api = nullptr;
 };
 
 struct Plan {
@@ -52,6 +62,7 @@ struct Plan {
     uint64_t rerun_slots = 0;
     uint32_t max_multi_stream = 0;   // longest stream among multi-stripe items (0 if none)
     TileTable tiles{};               // the shapes the items were planned with
+    bool region_api = false;         // every region uses the region API (device read prep and post)
 };
 
 // Sizes of a batch, from one validating pass over its counts and offsets (no copies).

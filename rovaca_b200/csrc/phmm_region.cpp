@@ -12,8 +12,10 @@
 //   normalise (cap at best-4.5)  src/haplotypecaller/pairhmm/pairhmm_internal.cpp:248-258
 //   poorly modelled reads        src/haplotypecaller/pairhmm/pairhmm_internal.cpp:23-44,489-497
 //   transpose to [hap][read]     src/haplotypecaller/pairhmm/pairhmm_internal.cpp:499-508
-// The likelihoods themselves go through the serving loop, so concurrent callers (the reference's
-// region thread pool) are batched together on the GPU.
+// phmm_call_region runs the whole path on the GPU through the serving loop (device read preparation
+// and post-processing in phmm_regionk.cu), so concurrent callers (the reference's region thread
+// pool) are batched together.  The host functions below compute the same steps; they are exported
+// for tests and for callers that prepare reads themselves.
 #include <cmath>
 #include <cstring>
 #include <limits>
@@ -30,6 +32,8 @@ phmm_status server_submit(phmm_engine* engine, const phmm_batch& b, double* out,
                           std::string& err);
 phmm_status server_wait(phmm_engine* engine, phmm_ticket ticket, int64_t timeout_us, bool release, double* queued_us,
                         double* total_us, std::string& err);
+phmm_status server_submit_region(phmm_engine* engine, const phmm_region_input& in, double* out, uint8_t* keep,
+                                 uint32_t* n_kept, phmm_ticket* ticket, std::string& err);
 
 namespace {
 
@@ -185,55 +189,25 @@ phmm_status phmm_call_region(phmm_engine* engine, uint32_t n_haps, const uint8_t
             for (uint32_t r = 0; r < n_reads; ++r) keep[r] = 1;
             *n_kept = n_reads;
         };
-        const uint64_t rb0 = read_off[0], rbn = read_off[n_reads];
-        if (rbn < rb0) {
-            fail_matrix();
-            return set_error(PHMM_ERR_INVALID_ARGUMENT, "read_off is not non-decreasing");
-        }
-        const uint64_t nb = rbn - rb0;
-        if (nb && (!read_bases || !read_qual)) {
-            fail_matrix();
-            return set_error(PHMM_ERR_INVALID_ARGUMENT, "read arrays are null");
-        }
-        std::vector<uint8_t> q(nb), gop(nb, phmm::kDefaultGapOpen), gcp(nb, phmm::kDefaultGapCont);
-        std::vector<uint64_t> roff(n_reads + 1), rlen(n_reads);
-        for (uint32_t r = 0; r <= n_reads; ++r) roff[r] = read_off[r] - rb0;
-        for (uint32_t r = 0; r < n_reads; ++r) {
-            if (roff[r + 1] < roff[r]) {
-                fail_matrix();
-                return set_error(PHMM_ERR_INVALID_ARGUMENT, "read_off is not non-decreasing");
-            }
-            const uint64_t a = roff[r], n = roff[r + 1] - roff[r];
-            rlen[r] = n;
-            if (n > 768) {  // reference limit, roDV_schedule.cpp:73,457
-                fail_matrix();
-                return set_error(PHMM_ERR_LIMIT_EXCEEDED, "read " + std::to_string(r) + " longer than 768");
-            }
-            phmm::prepare_read_quals(read_qual + rb0 + a, (int)n, mapq[r], min_quality_threshold, q.data() + a);
-            phmm::apply_pcr_model(read_bases + rb0 + a, (int)n, gop.data() + a, pcr_model);
-        }
-        phmm_batch b{};
-        b.n_regions = 1;
-        b.n_haps = &n_haps;
-        b.n_reads = &n_reads;
-        b.hap_bases = hap_bases;
-        b.hap_off = hap_off;
-        b.read_bases = read_bases ? read_bases + rb0 : nullptr;
-        b.read_qual = q.data();
-        b.read_ins = gop.data();
-        b.read_del = gop.data();  // deletion aliases the (capped) insertion gap-open
-        b.read_gcp = gcp.data();
-        b.read_off = roff.data();
-        std::vector<double> lk(total);
+        phmm_region_input in{};
+        in.n_haps = n_haps;
+        in.hap_bases = hap_bases;
+        in.hap_off = hap_off;
+        in.n_reads = n_reads;
+        in.read_bases = read_bases;
+        in.read_qual = read_qual;
+        in.read_off = read_off;
+        in.mapq = mapq;
+        in.min_quality_threshold = min_quality_threshold;
+        in.pcr_model = pcr_model;
         std::string err;
         phmm_ticket t = 0;
-        phmm_status st = phmm::server_submit(engine, b, lk.data(), nullptr, &t, err);
+        phmm_status st = phmm::server_submit_region(engine, in, out, keep, n_kept, &t, err);
         if (st == PHMM_OK) st = phmm::server_wait(engine, t, -1, true, nullptr, nullptr, err);
         if (st != PHMM_OK) {
             fail_matrix();
             return set_error(st, err);
         }
-        phmm::normalize_and_filter(lk.data(), n_haps, n_reads, rlen.data(), out, keep, n_kept);
         return PHMM_OK;
     } catch (const std::bad_alloc&) {
         return set_error(PHMM_ERR_OUT_OF_MEMORY, "host allocation failed");

@@ -52,6 +52,13 @@ struct Request {
     std::vector<uint64_t> hap_off, read_off;  // rebased to 0
     double* out = nullptr;
     uint8_t* flags = nullptr;
+    // region API (call_pairhmm semantics): data holds haplotype bases, read bases and raw base
+    // qualities; the device prepares the reads and post-processes the likelihoods
+    bool region_api = false;
+    std::vector<uint8_t> mapq;
+    RegionApiParams params{};
+    uint8_t* keep = nullptr;
+    uint32_t* n_kept = nullptr;
     uint64_t out_n = 0;
     uint64_t cells = 0;
     uint64_t bytes = 0;  // device footprint estimate for admission
@@ -121,6 +128,7 @@ void Server::worker(int idx)
     std::vector<std::shared_ptr<Request>> batch;
     std::vector<uint32_t> nh, nr;
     std::vector<uint64_t> hoff, roff;
+    std::vector<RegionApiParams> params;
     PinnedBuf in_buf, out_buf;
     for (;;) {
         batch.clear();
@@ -136,6 +144,8 @@ void Server::worker(int idx)
             const auto now = Clock::now();
             while (!queue.empty()) {
                 auto& r = queue.front();
+                // a batch holds requests of one kind (region API or plain likelihoods)
+                if (!batch.empty() && r->region_api != batch.front()->region_api) break;
                 const bool fits = in_use + batch_bytes + r->bytes <= budget &&
                                   (batch.empty() || batch_bytes + r->bytes <= batch_cap);
                 if (!fits || (!batch.empty() && cells + r->cells > kMaxBatchCells)) break;
@@ -158,17 +168,26 @@ void Server::worker(int idx)
         double device_ms = 0.0;
         bool want_flags = false;
         for (auto& r : batch) want_flags |= r->flags != nullptr;
-        // the admitted regions go into the slot's pinned buffers: haplotype bases, then the five
-        // read arrays in; likelihoods (and flags) out
-        if (st == PHMM_OK && !(in_buf.reserve(hap_total + 5 * read_total + 16) &&
-                               out_buf.reserve(out_total * (sizeof(double) + (want_flags ? 1 : 0)) + 16))) {
+        const bool api = batch.front()->region_api;
+        const int read_arrays = api ? 2 : 5;  // region API: bases and raw qualities only
+        uint64_t reads_total = 0;
+        for (auto& r : batch) reads_total += r->n_reads;
+        // the admitted regions go into the slot's pinned buffers: haplotype bases, then the read
+        // arrays (and MAPQ) in; likelihoods (and flags, or kept flags and counts) out
+        const size_t in_bytes = hap_total + read_arrays * read_total + (api ? reads_total : 0) + 16;
+        const size_t out_bytes = out_total * sizeof(double) + (want_flags ? out_total : 0) +
+                                 (api ? reads_total + batch.size() * sizeof(uint32_t) + 16 : 0) + 16;
+        if (st == PHMM_OK && !(in_buf.reserve(in_bytes) && out_buf.reserve(out_bytes))) {
             st = PHMM_ERR_OUT_OF_MEMORY;
             berr = "pinned staging for a batch of " + std::to_string(batch.size()) + " regions";
         }
         if (st == PHMM_OK) {
             uint8_t* hb = (uint8_t*)in_buf.p;
-            uint8_t* rd[5];
-            for (int k = 0; k < 5; ++k) rd[k] = hb + hap_total + (uint64_t)k * read_total;
+            uint8_t* rd[5] = {};
+            for (int k = 0; k < read_arrays; ++k) rd[k] = hb + hap_total + (uint64_t)k * read_total;
+            uint8_t* mq = hb + hap_total + (uint64_t)read_arrays * read_total;
+            uint64_t mo = 0;
+            params.clear();
             nh.clear();
             nr.clear();
             hoff.assign(1, 0);
@@ -180,8 +199,13 @@ void Server::worker(int idx)
                 for (uint32_t h = 0; h < r->n_haps; ++h) hoff.push_back(ho + r->hap_off[h + 1]);
                 for (uint32_t k = 0; k < r->n_reads; ++k) roff.push_back(ro + r->read_off[k + 1]);
                 if (r->hap_bases) std::memcpy(hb + ho, r->data.data(), r->hap_bases);
-                for (int k = 0; k < 5 && r->read_bases; ++k)
+                for (int k = 0; k < read_arrays && r->read_bases; ++k)
                     std::memcpy(rd[k] + ro, r->data.data() + r->hap_bases + (uint64_t)k * r->read_bases, r->read_bases);
+                if (api) {
+                    if (r->n_reads) std::memcpy(mq + mo, r->mapq.data(), r->n_reads);
+                    mo += r->n_reads;
+                    params.push_back(r->params);
+                }
                 ho += r->hap_bases;
                 ro += r->read_bases;
             }
@@ -199,19 +223,29 @@ void Server::worker(int idx)
             b.read_off = roff.data();
             Plan plan;
             const TileTable tiles = eng->tiles();
-            st = build_plan(b, Engine::limits_with(tiles), plan, berr);
-            if (st == PHMM_OK) st = eng->enqueue(*slot, plan, b, want_flags, berr);
+            PlanLimits lim = Engine::limits_with(tiles);
+            if (api) lim.region_api = params.data();
+            st = build_plan(b, lim, plan, berr);
+            if (st == PHMM_OK) st = eng->enqueue(*slot, plan, b, want_flags, berr, api ? mq : nullptr);
             double* out = (double*)out_buf.p;
             uint8_t* flags = want_flags ? (uint8_t*)(out + out_total) : nullptr;
+            uint32_t* kept_n = api ? (uint32_t*)(out + out_total) : nullptr;
+            uint8_t* keep = api ? (uint8_t*)(kept_n + batch.size()) : nullptr;
             phmm_stats ps{};
-            if (st == PHMM_OK) st = eng->finish(*slot, plan, out, flags, &ps, berr);
+            if (st == PHMM_OK) st = eng->finish(*slot, plan, out, flags, &ps, berr, keep, kept_n);
             device_ms = ps.device_ms;
             if (st == PHMM_OK) {
-                uint64_t o = 0;
-                for (auto& r : batch) {
+                uint64_t o = 0, ko = 0;
+                for (size_t i = 0; i < batch.size(); ++i) {
+                    auto& r = batch[i];
                     if (r->out_n) std::memcpy(r->out, out + o, r->out_n * sizeof(double));
                     if (r->flags && r->out_n) std::memcpy(r->flags, flags + o, r->out_n);
+                    if (api) {
+                        if (r->n_reads) std::memcpy(r->keep, keep + ko, r->n_reads);
+                        *r->n_kept = kept_n[i];
+                    }
                     o += r->out_n;
+                    ko += r->n_reads;
                 }
             }
         }
@@ -284,6 +318,38 @@ void server_release(phmm_engine* e)
     for (auto& t : s->workers) t.join();
 }
 
+// Queues a prepared request (admission checks against the HBM budget).
+phmm_status enqueue_request(phmm_engine* engine, const std::shared_ptr<Request>& r, phmm_ticket* ticket,
+                            std::string& err)
+{
+    Server* s = server_for(engine, true);
+    if (r->bytes > s->budget) {
+        err = "region needs about " + std::to_string(r->bytes) + " device bytes, more than the HBM budget of " +
+              std::to_string(s->budget);
+        return PHMM_ERR_LIMIT_EXCEEDED;
+    }
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (s->stop) {
+            err = "engine is shutting down";
+            return PHMM_ERR_NOT_INITIALIZED;
+        }
+        if (s->queue.size() >= kMaxQueued) {
+            err = "serving queue is full";
+            return PHMM_ERR_QUEUE_FULL;
+        }
+        r->id = s->next_id++;
+        r->t_submit = Clock::now();
+        s->tickets[r->id] = r;
+        s->queue.push_back(r);
+        s->stats.requests_submitted += 1;
+        s->stats.queue_peak = std::max<uint64_t>(s->stats.queue_peak, s->queue.size());
+        *ticket = r->id;
+    }
+    s->cv_work.notify_one();
+    return PHMM_OK;
+}
+
 // Submits a copy of one region; used by phmm_submit and the region API.
 phmm_status server_submit(phmm_engine* engine, const phmm_batch& b, double* out, uint8_t* flags, phmm_ticket* ticket,
                           std::string& err)
@@ -325,32 +391,72 @@ phmm_status server_submit(phmm_engine* engine, const phmm_batch& b, double* out,
             r->bytes += engine_of(engine)->scratch_bytes();
             break;
         }
-    Server* s = server_for(engine, true);
-    if (r->bytes > s->budget) {
-        err = "region needs about " + std::to_string(r->bytes) + " device bytes, more than the HBM budget of " +
-              std::to_string(s->budget);
-        return PHMM_ERR_LIMIT_EXCEEDED;
+    return enqueue_request(engine, r, ticket, err);
+}
+
+// Submits one region with call_pairhmm semantics: raw base qualities and MAPQ are copied, the
+// device prepares the reads and post-processes the likelihoods.
+phmm_status server_submit_region(phmm_engine* engine, const phmm_region_input& in, double* out, uint8_t* keep,
+                                 uint32_t* n_kept, phmm_ticket* ticket, std::string& err)
+{
+    if (!in.hap_off || !in.read_off || (in.n_reads && (!in.mapq || !keep)) || !n_kept) {
+        err = "null argument";
+        return PHMM_ERR_INVALID_ARGUMENT;
     }
-    {
-        std::lock_guard<std::mutex> lk(s->mu);
-        if (s->stop) {
-            err = "engine is shutting down";
-            return PHMM_ERR_NOT_INITIALIZED;
-        }
-        if (s->queue.size() >= kMaxQueued) {
-            err = "serving queue is full";
-            return PHMM_ERR_QUEUE_FULL;
-        }
-        r->id = s->next_id++;
-        r->t_submit = Clock::now();
-        s->tickets[r->id] = r;
-        s->queue.push_back(r);
-        s->stats.requests_submitted += 1;
-        s->stats.queue_peak = std::max<uint64_t>(s->stats.queue_peak, s->queue.size());
-        *ticket = r->id;
+    if (in.pcr_model < PHMM_PCR_NONE || in.pcr_model > PHMM_PCR_CONSERVATIVE) {
+        err = "pcr_model out of range";
+        return PHMM_ERR_INVALID_ARGUMENT;
     }
-    s->cv_work.notify_one();
-    return PHMM_OK;
+    phmm_batch b{};
+    b.n_regions = 1;
+    b.n_haps = &in.n_haps;
+    b.n_reads = &in.n_reads;
+    b.hap_bases = in.hap_bases;
+    b.hap_off = in.hap_off;
+    b.read_bases = in.read_bases;
+    b.read_qual = in.read_qual;
+    b.read_off = in.read_off;
+    RegionApiParams params{in.min_quality_threshold, in.pcr_model};
+    PlanLimits lim;
+    lim.region_api = &params;
+    BatchScan sc;
+    phmm_status st = scan_batch(b, lim, sc, err);
+    if (st != PHMM_OK) return st;
+    if (sc.out_total && !out) {
+        err = "out is null";
+        return PHMM_ERR_INVALID_ARGUMENT;
+    }
+    auto r = std::make_shared<Request>();
+    r->region_api = true;
+    r->params = params;
+    r->n_haps = sc.n_haps;
+    r->n_reads = sc.n_reads;
+    r->hap_bases = sc.hap_bases;
+    r->read_bases = sc.read_bases;
+    r->hap_off.resize(sc.n_haps + 1);
+    r->read_off.resize(sc.n_reads + 1);
+    for (uint32_t h = 0; h <= sc.n_haps; ++h) r->hap_off[h] = in.hap_off[h] - sc.hap_base0;
+    for (uint32_t k = 0; k <= sc.n_reads; ++k) r->read_off[k] = in.read_off[k] - sc.read_base0;
+    r->data.resize(sc.hap_bases + 2 * sc.read_bases);
+    if (sc.hap_bases) std::memcpy(r->data.data(), in.hap_bases + sc.hap_base0, sc.hap_bases);
+    if (sc.read_bases) {
+        std::memcpy(r->data.data() + sc.hap_bases, in.read_bases + sc.read_base0, sc.read_bases);
+        std::memcpy(r->data.data() + sc.hap_bases + sc.read_bases, in.read_qual + sc.read_base0, sc.read_bases);
+    }
+    r->mapq.assign(in.mapq, in.mapq + sc.n_reads);
+    r->out = out;
+    r->keep = keep;
+    r->n_kept = n_kept;
+    r->out_n = sc.out_total;
+    r->cells = sc.cells;
+    r->bytes = footprint(sc.read_bases, sc.hap_bases, sc.out_total, sc.n_reads, sc.n_haps) + sc.out_total * 8 +
+               sc.n_reads * 2;
+    for (uint32_t k = 0; k < sc.n_reads; ++k)
+        if (r->read_off[k + 1] - r->read_off[k] > (uint64_t)kWarp * kMaxK) {
+            r->bytes += engine_of(engine)->scratch_bytes();
+            break;
+        }
+    return enqueue_request(engine, r, ticket, err);
 }
 
 phmm_status server_wait(phmm_engine* engine, phmm_ticket ticket, int64_t timeout_us, bool release, double* queued_us,
@@ -396,6 +502,23 @@ phmm_status phmm_submit(phmm_engine* engine, const phmm_batch* region, double* o
         if (!region || !ticket) return set_error(PHMM_ERR_INVALID_ARGUMENT, "region or ticket is null");
         std::string err;
         phmm_status st = phmm::server_submit(engine, *region, out, pair_flags, ticket, err);
+        return st == PHMM_OK ? PHMM_OK : set_error(st, err);
+    } catch (const std::bad_alloc&) {
+        return set_error(PHMM_ERR_OUT_OF_MEMORY, "host allocation failed");
+    } catch (const std::exception& ex) {
+        return set_error(PHMM_ERR_INTERNAL, ex.what());
+    }
+}
+
+phmm_status phmm_submit_region(phmm_engine* engine, const phmm_region_input* region, double* out, uint8_t* keep,
+                               uint32_t* n_kept, phmm_ticket* ticket)
+{
+    try {
+        phmm::clear_error();
+        if (!engine) return set_error(PHMM_ERR_NOT_INITIALIZED, "engine is null");
+        if (!region || !ticket) return set_error(PHMM_ERR_INVALID_ARGUMENT, "region or ticket is null");
+        std::string err;
+        phmm_status st = phmm::server_submit_region(engine, *region, out, keep, n_kept, ticket, err);
         return st == PHMM_OK ? PHMM_OK : set_error(st, err);
     } catch (const std::bad_alloc&) {
         return set_error(PHMM_ERR_OUT_OF_MEMORY, "host allocation failed");

@@ -63,8 +63,11 @@ struct RegionDesc {               // 32 bytes
     uint32_t n_haps;
     uint32_t read_begin;          // global index of the region's first read
     uint32_t n_reads;
-    uint32_t pad0, pad1;
+    uint32_t api;                 // kRegionApi: reads prepared and results post-processed on device;
+                                  // bits 8-15: PCR model
+    int32_t min_quality;          // region API: base qualities below this become 6
 };
+constexpr uint32_t kRegionApi = 1u;
 
 // FP32 work item: two reads of one region (one per 16-lane group; read[1] may be kNoRead) against a
 // run of the region's haplotypes.
@@ -112,6 +115,7 @@ struct BatchView {
     uint8_t* pair_flags;          // may be null
 };
 
+
 // Per-class launch descriptor, in device memory so that a captured launch sequence can be
 // replayed for any batch that fits the arena (the host rewrites the descriptors, not the graph).
 struct ClassDesc {                // 32 bytes
@@ -129,7 +133,27 @@ struct ClassDesc {                // 32 bytes
 struct BatchDesc {
     uint64_t hap_bases_total;     // haplotype bases (length of the code streams without guards)
     uint64_t out_total;           // likelihoods in the output
+    uint64_t read_bases_total;
     uint32_t n_regions, n_reads, n_haps, n_items;
+    uint32_t region_api;          // regions with kRegionApi (0: the read-prep and post kernels idle)
+    uint32_t pad;
+};
+
+// Region-API device arrays (read preparation in, post-processed results out).
+struct RegionApiView {
+    const BatchDesc* desc;
+    const RegionDesc* regions;
+    const uint64_t* read_off;
+    const uint8_t* read_bases;
+    uint8_t* read_q;              // in: raw base qualities; out: capped
+    uint8_t* read_i;              // out: gap-open (PCR-capped)
+    uint8_t* read_d;              // out: = read_i
+    uint8_t* read_c;              // out: gap continuation
+    const uint8_t* mapq;          // [n_reads]
+    const double* lk;             // likelihoods [hap][read] per region
+    double* out;                  // normalised, kept reads first, NaN after
+    uint8_t* keep;                // [n_reads]
+    uint32_t* n_kept;             // [n_regions]
 };
 
 // Status bits a kernel raises instead of touching memory it should not.

@@ -323,6 +323,12 @@ class Engine:
         return st.as_dict()
 
     # ---- region API ----------------------------------------------------------------------
+    def submit_region(self, haplotypes, reads, base_quals, mapq, min_quality_threshold: int = 18,
+                      pcr_option: str | int = "CONSERVATIVE") -> "RegionTicket":
+        """phmm_submit_region: queues one region with call_pairhmm semantics (read preparation and
+        post-processing on the GPU); RegionTicket.wait() returns what call_region returns."""
+        return RegionTicket(self, haplotypes, reads, base_quals, mapq, min_quality_threshold, pcr_option)
+
     def call_region(self, haplotypes, reads, base_quals, mapq, min_quality_threshold: int = 18,
                     pcr_option: str | int = "CONSERVATIVE"):
         """call_pairhmm semantics; returns (matrix [n_haps][n_reads] with kept reads first, keep mask)."""
@@ -343,6 +349,40 @@ class Engine:
                                         _ptr(mq), int(min_quality_threshold), pcr, _ptr(out), _ptr(keep), C.byref(nk))
         check(st)
         return out.reshape(len(hs), len(rs)), keep.astype(bool)
+
+
+class RegionTicket:
+    """A region submitted with phmm_submit_region; keeps its buffers alive until wait()."""
+
+    def __init__(self, engine: Engine, haplotypes, reads, base_quals, mapq, min_quality_threshold, pcr_option):
+        pcr = PCR_MODELS[pcr_option] if isinstance(pcr_option, str) else int(pcr_option)
+        hs = [_u8(h) for h in haplotypes]
+        rs = [_u8(r) for r in reads]
+        qs = [_u8(q) for q in base_quals]
+        cat = lambda parts: np.concatenate(parts) if parts else np.zeros(1, np.uint8)
+        off = lambda parts: np.concatenate([[0], np.cumsum([len(p) for p in parts])]).astype(np.uint64)
+        self._keepalive = (cat(hs), off(hs), cat(rs), off(rs), cat(qs))
+        hb, hoff, rb, roff, qb = self._keepalive
+        mq = np.ascontiguousarray(np.asarray(mapq, np.uint8).reshape(-1))
+        if mq.size == 1 and len(rs) > 1:
+            mq = np.full(len(rs), mq[0], np.uint8)
+        self._mq = mq
+        self.n_haps, self.n_reads = len(hs), len(rs)
+        self.out = np.empty(self.n_haps * self.n_reads, np.float64)
+        self.keep = np.empty(self.n_reads, np.uint8)
+        self.n_kept = C.c_uint32()
+        inp = _lib.RegionInput(self.n_haps, hb.ctypes.data, hoff.ctypes.data, self.n_reads, rb.ctypes.data,
+                               qb.ctypes.data, roff.ctypes.data, mq.ctypes.data, int(min_quality_threshold), pcr)
+        self._engine = engine
+        t = C.c_uint64()
+        check(engine._lib.phmm_submit_region(engine._h, C.byref(inp), _ptr(self.out), _ptr(self.keep),
+                                             C.byref(self.n_kept), C.byref(t)))
+        self.ticket = t.value
+
+    def wait(self):
+        """Blocks until done; returns (matrix [n_haps][n_reads] with kept reads first, keep mask)."""
+        self._engine.wait(self.ticket)
+        return self.out.reshape(self.n_haps, self.n_reads), self.keep.astype(bool)
 
 
 class ResidentBatch:

@@ -175,3 +175,98 @@ def test_call_pairhmm_over_limits_returns_nan_matrix(engine):
     with pytest.raises(PhmmError) as e:
         call_pairhmm(haps, [b"ACGT"], [b"\x1e" * 4], [60], 18, "NONE", engine=engine)
     assert e.value.name == "PHMM_ERR_LIMIT_EXCEEDED"
+
+
+def _host_region_path(engine, haps, reads, quals, mapq, thr, pcr):
+    """The region API computed with the host-side preparation and post-processing (the exported
+    phmm_host_* functions) around phmm_compute_regions: the device path must give the same bits."""
+    import ctypes as C
+
+    from rovaca_b200 import _lib
+    from rovaca_b200.pairhmm import Region
+
+    lib = _lib.load()
+    qs, gops = [], []
+    for rd, q, mq in zip(reads, quals, mapq):
+        n = len(rd)
+        qq = (C.c_uint8 * max(n, 1))()
+        lib.phmm_host_prepare_quals(q, n, int(mq), thr, qq)
+        gop = (C.c_uint8 * max(n, 1))(*([45] * max(n, 1)))
+        lib.phmm_host_pcr_model(rd, n, gop, pcr)
+        qs.append(bytes(qq)[:n])
+        gops.append(bytes(gop)[:n])
+    pb = PackedBatch.from_regions([Region(haps, reads, qs, gops, gops, [bytes([10]) * len(r) for r in reads])])
+    lk, _, _ = engine.compute(pb)
+    out = np.empty(len(haps) * len(reads))
+    keep = np.empty(len(reads), np.uint8)
+    nk = C.c_uint32()
+    rlen = np.array([len(r) for r in reads], np.uint64)
+    lib.phmm_host_normalize_filter(lk.ctypes.data, len(haps), len(reads), rlen.ctypes.data, out.ctypes.data,
+                                   keep.ctypes.data, C.byref(nk))
+    return out.reshape(len(haps), len(reads)), keep.astype(bool)
+
+
+def _repeat_region(rng, n_reads, max_len):
+    """Haplotypes and reads rich in tandem repeats of unit lengths 1-9."""
+    acgt = np.frombuffer(b"ACGT", np.uint8)
+    parts = []
+    for _ in range(30):
+        unit = bytes(acgt[rng.integers(0, 4, int(rng.integers(1, 10)))])
+        parts.append(unit * int(rng.integers(1, 25)))
+        parts.append(bytes(acgt[rng.integers(0, 4, int(rng.integers(0, 12)))]))
+    base = b"".join(parts)[:1500]
+    haps = [base[:1000], base[3:1003], base[:500] + base[507:1010]]
+    reads, quals = [], []
+    for _ in range(n_reads):
+        L = int(rng.integers(1, max_len + 1))
+        s = int(rng.integers(0, max(1, len(base) - L)))
+        r = bytearray(base[s:s + L])
+        if rng.random() < 0.1 and L:
+            r[int(rng.integers(0, L))] = ord("N")
+        reads.append(bytes(r))
+        quals.append(rng.integers(0, 50, L).astype(np.uint8).tobytes())
+    mapq = rng.integers(0, 70, n_reads).astype(np.uint8)
+    return haps, reads, quals, mapq
+
+
+@pytest.mark.parametrize("pcr", [0, 1, 2, 3])
+def test_device_region_path_equals_host_preparation(engine, pcr):
+    """Quality cap, gap qualities and the PCR tandem-repeat cap computed on the GPU, and the
+    normalise/filter/compact step after it, give exactly the host functions' results."""
+    rng = np.random.default_rng(100 + pcr)
+    for thr, max_len in ((18, 768), (5, 200), (40, 300)):
+        haps, reads, quals, mapq = _repeat_region(rng, 40, max_len)
+        got, keep = engine.call_region(haps, reads, quals, mapq, thr, pcr)
+        want, wkeep = _host_region_path(engine, haps, reads, quals, mapq, thr, pcr)
+        assert np.array_equal(keep, wkeep)
+        assert np.array_equal(got, want, equal_nan=True)
+        assert 0 < keep.sum() < len(reads)
+
+
+def test_region_and_plain_requests_mix(engine):
+    """Region-API and plain requests submitted together from several threads: each gets the result
+    it gets alone (the loop batches each kind separately)."""
+    rng = np.random.default_rng(7)
+    regions = [_repeat_region(rng, 20, 250) for _ in range(12)]
+    alone = [engine.call_region(h, r, q, m, 18, 3) for h, r, q, m in regions]
+    pb = synth.config1(12, seed=9)
+    plain_alone = [engine.compute(pb.subset([g]))[0] for g in range(pb.n_regions)]
+    outs = [np.empty(x.size) for x in plain_alone]
+    tickets, rts = [None] * 12, [None] * 12
+
+    def producer(k0):
+        for g in range(k0, 12, 3):
+            rts[g] = engine.submit_region(*regions[g], 18, 3)
+            tickets[g] = engine.submit(pb.subset([g]), outs[g])
+
+    threads = [threading.Thread(target=producer, args=(k,)) for k in range(3)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    for g in range(12):
+        mat, keep = rts[g].wait()
+        engine.wait(tickets[g])
+        assert np.array_equal(mat, alone[g][0], equal_nan=True)
+        assert np.array_equal(keep, alone[g][1])
+        assert np.array_equal(outs[g], plain_alone[g], equal_nan=True)
