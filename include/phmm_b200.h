@@ -276,11 +276,31 @@ typedef struct phmm_region_input {
     int32_t pcr_model;          /* phmm_pcr_model */
 } phmm_region_input;
 
+/* Genotyping events of one region: each event is a set of alleles with every haplotype mapped to
+ * one of them (or to none), as HaplotypeCaller maps haplotypes to the alleles of a variant site.
+ * On the GPU, after the region's reads are normalised and filtered:
+ *   allele likelihood (read, allele) = max over the allele's haplotypes (-inf if it has none)
+ *     (AlleleLikelihoods::marginal_likelihoods_direct, genotype/allele_likelihoods.hpp:702-730);
+ *   diploid genotype likelihoods, genotype (a <= b) at index b(b+1)/2 + a, and the most likely
+ *   genotype (first maximum) (GenotypeLikelihoodCalculator, genotype_likelihood_calculator.cpp:59-100).
+ * Only these come back to the host when the matrix itself is not asked for. */
+typedef struct phmm_region_events {
+    uint32_t n_events;
+    const uint8_t* n_alleles;    /* [n_events], 1..49 */
+    const int8_t* hap_allele;    /* [n_events][n_haps]: allele index of each haplotype, -1 for none */
+    double* genotype_lk;         /* out: [sum over events of n_alleles (n_alleles + 1) / 2] log10 */
+    int32_t* best_genotype;      /* out: [n_events] */
+    double* allele_lk;           /* out, optional: [sum of n_alleles][n_reads], kept reads first, NaN after */
+} phmm_region_events;
+
 /* Submits one region with phmm_call_region's semantics; the read preparation (quality cap, gap
- * qualities, PCR model) and the post-processing (normalise, drop poorly modelled reads, kept reads
- * first) run on the GPU.  out [n_haps][n_reads], keep [n_reads] and n_kept must stay valid until
- * the request completes (phmm_wait).  Inputs are copied before the call returns.  Thread-safe. */
-PHMM_API phmm_status phmm_submit_region(phmm_engine* engine, const phmm_region_input* region, double* out, uint8_t* keep,
+ * qualities, PCR model), the post-processing (normalise, drop poorly modelled reads, kept reads
+ * first) and, when events is not NULL, the genotyping of its events run on the GPU.  out
+ * [n_haps][n_reads] may be NULL when only the genotyping results are wanted.  Output buffers must
+ * stay valid until the request completes (phmm_wait); inputs are copied before the call returns.
+ * Thread-safe. */
+PHMM_API phmm_status phmm_submit_region(phmm_engine* engine, const phmm_region_input* region,
+                                        const phmm_region_events* events, double* out, uint8_t* keep,
                                         uint32_t* n_kept, phmm_ticket* ticket);
 /* *done = 1 once the request's results are in out (or it failed / was cancelled). */
 PHMM_API phmm_status phmm_poll(phmm_engine* engine, phmm_ticket ticket, int32_t* done);

@@ -98,6 +98,12 @@ class RegionInput(C.Structure):
                 ("pcr_model", C.c_int32)]
 
 
+class RegionEvents(C.Structure):
+    """phmm_region_events: genotyping events of one region."""
+    _fields_ = [("n_events", C.c_uint32), ("n_alleles", C.c_void_p), ("hap_allele", C.c_void_p),
+                ("genotype_lk", C.c_void_p), ("best_genotype", C.c_void_p), ("allele_lk", C.c_void_p)]
+
+
 class ServerStats(C.Structure):
     _fields_ = [("requests_submitted", C.c_uint64), ("requests_done", C.c_uint64), ("batches", C.c_uint64),
                 ("max_batch_regions", C.c_uint64), ("queue_peak", C.c_uint64), ("cells_done", C.c_uint64),
@@ -144,7 +150,7 @@ def load() -> C.CDLL:
         "phmm_engine_set_tiles": (I32, [P, P]),
         "phmm_engine_autotune": (I32, [P, P]),
         "phmm_submit": (I32, [P, C.POINTER(Batch), P, P, C.POINTER(U64)]),
-        "phmm_submit_region": (I32, [P, P, P, P, C.POINTER(U32), C.POINTER(U64)]),
+        "phmm_submit_region": (I32, [P, P, P, P, P, C.POINTER(U32), C.POINTER(U64)]),
         "phmm_poll": (I32, [P, U64, C.POINTER(I32)]),
         "phmm_wait": (I32, [P, U64, I64, C.POINTER(D), C.POINTER(D)]),
         "phmm_cancel": (I32, [P, U64]),

@@ -68,6 +68,11 @@ size_t carve(const Capacity& c, char* base, Slot* s)
     char* out = take(c.out * sizeof(double));
     char* pf = take(c.out);
     char* out2 = take(c.out * sizeof(double));
+    char* events = take(c.events * sizeof(EventDesc));
+    char* hap_allele = take(c.hap_allele);
+    char* allele_lk = take(c.allele_lk * sizeof(double));
+    char* gl = take(c.gl * sizeof(double));
+    char* best = take(c.events * sizeof(int32_t));
     char* rerun = take(c.rerun * sizeof(RerunEntry));
     char* scratch = take(c.scratch_cols * 3 * sizeof(double));  // c.scratch_cols counts all warps' columns
     if (s) {
@@ -91,6 +96,11 @@ size_t carve(const Capacity& c, char* base, Slot* s)
         s->d_keep = (uint8_t*)keep;
         s->d_nkept = (uint32_t*)nkept;
         s->d_out2 = (double*)out2;
+        s->d_events = (EventDesc*)events;
+        s->d_hap_allele = (int8_t*)hap_allele;
+        s->d_allele_lk = (double*)allele_lk;
+        s->d_gl = (double*)gl;
+        s->d_best = (int32_t*)best;
         s->d_codes_inter = (uint32_t*)ci;
         s->d_codes_intra = (uint32_t*)ca;
         s->d_out = (double*)out;
@@ -105,7 +115,8 @@ size_t carve(const Capacity& c, char* base, Slot* s)
 size_t pinned_bytes_for(const Capacity& c)
 {
     return align_up(kDescBytes) + align_up(c.regions * sizeof(RegionDesc)) + align_up((c.reads + 1) * 8) +
-           align_up((c.haps + 1) * 8) + align_up(c.reads) + align_up(c.haps) + align_up(c.items * sizeof(WorkItem));
+           align_up((c.haps + 1) * 8) + align_up(c.reads) + align_up(c.haps) + align_up(c.items * sizeof(WorkItem)) +
+           align_up(c.events * sizeof(EventDesc)) + align_up(c.hap_allele);
 }
 
 Capacity need_of(const Plan& p, uint64_t scratch_warps)
@@ -120,6 +131,10 @@ Capacity need_of(const Plan& p, uint64_t scratch_warps)
     c.rerun = p.rerun_slots;
     c.out = p.out_total;
     c.scratch_cols = p.max_multi_stream ? scratch_warps * (uint64_t)PlanLimits().max_stream_multi : 0;
+    c.events = p.events.size();
+    c.hap_allele = p.hap_allele.size();
+    c.allele_lk = p.allele_lk_total;
+    c.gl = p.gl_total;
     return c;
 }
 
@@ -129,7 +144,8 @@ bool Capacity::covers(const Capacity& o) const
 {
     return regions >= o.regions && reads >= o.reads && haps >= o.haps && read_bases >= o.read_bases &&
            hap_bases >= o.hap_bases && items >= o.items && rerun >= o.rerun && out >= o.out &&
-           scratch_cols >= o.scratch_cols;
+           scratch_cols >= o.scratch_cols && events >= o.events && hap_allele >= o.hap_allele &&
+           allele_lk >= o.allele_lk && gl >= o.gl;
 }
 
 Capacity Capacity::grown_to(const Capacity& need) const
@@ -145,6 +161,10 @@ Capacity Capacity::grown_to(const Capacity& need) const
     c.rerun = g(rerun, need.rerun);
     c.out = g(out, need.out);
     c.scratch_cols = std::max(scratch_cols, need.scratch_cols);
+    c.events = g(events, need.events);
+    c.hap_allele = g(hap_allele, need.hap_allele);
+    c.allele_lk = g(allele_lk, need.allele_lk);
+    c.gl = g(gl, need.gl);
     return c;
 }
 
@@ -203,7 +223,8 @@ phmm_status Engine::create(const phmm_config* cfg, Engine** out, std::string& er
     const HostTables<float>& hf = host_tables_f32();
     const HostTables<double>& hd = host_tables_f64();
     const size_t nf = 5 * 128 + 128 * 128;
-    const size_t bytes = nf * sizeof(float) + nf * sizeof(double);
+    const std::vector<double>& jac = genotype_jacobian();
+    const size_t bytes = nf * sizeof(float) + nf * sizeof(double) + jac.size() * sizeof(double);
     PHMM_CKE(cudaMalloc(&e->d_tables_, bytes));
     std::vector<char> host(bytes);
     float* f = (float*)host.data();
@@ -225,12 +246,15 @@ phmm_status Engine::create(const phmm_config* cfg, Engine** out, std::string& er
     dp = put(dp, hd.pmis_inter);
     dp = put(dp, hd.pmis_intra);
     dp = put(dp, hd.gapm);
-    put(dp, hd.mm);
+    dp = put(dp, hd.mm);
+    put(dp, jac);
     PHMM_CKE(cudaMemcpy(e->d_tables_, host.data(), bytes, cudaMemcpyHostToDevice));
     const float* df = (const float*)e->d_tables_;
     const double* dd = (const double*)((const char*)e->d_tables_ + nf * sizeof(float));
     e->tf_ = ProbTables<float>{df, df + 128, df + 256, df + 384, df + 512, df + 640};
     e->td_ = ProbTables<double>{dd, dd + 128, dd + 256, dd + 384, dd + 512, dd + 640};
+    e->d_jacobian_ = dd + nf;
+    e->log10_two_ = host_log10_two();
 #undef PHMM_CKE
     phmm_status st = e->make_slot(0, &e->default_slot_, err);
     if (st != PHMM_OK) return fail(st);
@@ -360,9 +384,16 @@ int Engine::grid_for(int precision, int cls, uint32_t work) const
 
 namespace {
 
-RegionApiView region_view(const Slot& s)
+RegionApiView region_view(const Slot& s, const double* jacobian, double log10_two)
 {
     RegionApiView rv;
+    rv.events = s.d_events;
+    rv.hap_allele = s.d_hap_allele;
+    rv.allele_lk = s.d_allele_lk;
+    rv.gl = s.d_gl;
+    rv.best = s.d_best;
+    rv.jacobian = jacobian;
+    rv.log10_two = log10_two;
     rv.desc = s.d_desc;
     rv.regions = s.d_regions;
     rv.read_off = s.d_read_off;
@@ -428,7 +459,7 @@ phmm_status Engine::launch_pipeline(Slot& s, bool want_flags, const Plan* plan, 
     PHMM_CK(cudaEventRecordWithFlags(s.ev_t0, s.main, rec));
     PHMM_CK(launch_prep(s.d_desc, s.d_hb, s.d_codes_inter, s.d_codes_intra, s.d_out, v.pair_flags, sms_, s.main));
     s.launches += 2;
-    const RegionApiView rv = region_view(s);
+    const RegionApiView rv = region_view(s, d_jacobian_, log10_two_);
     if (!plan || plan->region_api) {
         PHMM_CK(launch_read_prep(rv, sms_, s.main));
         ++s.launches;
@@ -476,6 +507,10 @@ phmm_status Engine::launch_pipeline(Slot& s, bool want_flags, const Plan* plan, 
         if (pass == 1 && (!plan || plan->region_api)) {
             PHMM_CK(launch_post_region(rv, sms_, s.main));
             ++s.launches;
+            if (!plan || !plan->events.empty()) {
+                PHMM_CK(launch_genotype(rv, sms_, s.main));
+                ++s.launches;
+            }
         }
         PHMM_CK(cudaEventRecordWithFlags(pass == 0 ? s.ev_t1 : s.ev_t2, s.main, rec));
     }
@@ -541,6 +576,7 @@ phmm_status Engine::upload(Slot& s, const Plan& plan, const phmm_batch& b, std::
     bd.n_items = (uint32_t)plan.items.size();
     bd.read_bases_total = plan.read_bases;
     bd.region_api = plan.region_api ? plan.n_regions : 0;
+    bd.n_events = (uint32_t)plan.events.size();
     char* desc = p;
     std::memcpy(desc, &bd, sizeof(bd));
     std::memcpy(desc + sizeof(bd), plan.classes.data(), sizeof(ClassDesc) * kNumClasses);
@@ -552,6 +588,8 @@ phmm_status Engine::upload(Slot& s, const Plan& plan, const phmm_batch& b, std::
     char* h_read_flags = stage(plan.read_flags.data(), plan.read_flags.size());
     char* h_hap_flags = stage(plan.hap_flags.data(), plan.hap_flags.size());
     char* h_items = stage(plan.items.data(), plan.items.size() * sizeof(WorkItem));
+    char* h_events = stage(plan.events.data(), plan.events.size() * sizeof(EventDesc));
+    char* h_hap_allele = stage(plan.hap_allele.data(), plan.hap_allele.size());
 
     cudaStream_t m = s.main;
     PHMM_CK(cudaMemcpyAsync(s.d_desc, desc, kDescBytes, cudaMemcpyHostToDevice, m));
@@ -579,6 +617,10 @@ phmm_status Engine::upload(Slot& s, const Plan& plan, const phmm_batch& b, std::
 
     if (plan.region_api && plan.n_reads)
         PHMM_CK(cudaMemcpyAsync(s.d_mapq, mapq, plan.n_reads, cudaMemcpyHostToDevice, m));
+    if (!plan.events.empty()) {
+        PHMM_CK(cudaMemcpyAsync(s.d_events, h_events, plan.events.size() * sizeof(EventDesc), cudaMemcpyHostToDevice, m));
+        PHMM_CK(cudaMemcpyAsync(s.d_hap_allele, h_hap_allele, plan.hap_allele.size(), cudaMemcpyHostToDevice, m));
+    }
     PHMM_CK(cudaMemcpyAsync(s.d_desc_pristine, s.d_desc, kDescBytes, cudaMemcpyDeviceToDevice, m));
     return PHMM_OK;
 }
@@ -610,7 +652,8 @@ phmm_status Engine::enqueue(Slot& s, const Plan& plan, const phmm_batch& b, bool
 }
 
 phmm_status Engine::finish(Slot& s, const Plan& plan, double* out, uint8_t* pair_flags, phmm_stats* stats,
-                           std::string& err, uint8_t* keep, uint32_t* n_kept)
+                           std::string& err, uint8_t* keep, uint32_t* n_kept, double* gl, int32_t* best,
+                           double* allele_lk)
 {
     cudaStream_t m = s.main;
     char* desc = s.pinned;  // reuse the staged descriptor block for the read-back
@@ -620,7 +663,14 @@ phmm_status Engine::finish(Slot& s, const Plan& plan, double* out, uint8_t* pair
         if (plan.n_regions && n_kept)
             PHMM_CK(cudaMemcpyAsync(n_kept, s.d_nkept, plan.n_regions * sizeof(uint32_t), cudaMemcpyDeviceToHost, m));
     }
-    if (plan.out_total) {
+    if (!plan.events.empty()) {
+        if (gl) PHMM_CK(cudaMemcpyAsync(gl, s.d_gl, plan.gl_total * sizeof(double), cudaMemcpyDeviceToHost, m));
+        if (best) PHMM_CK(cudaMemcpyAsync(best, s.d_best, plan.events.size() * sizeof(int32_t), cudaMemcpyDeviceToHost, m));
+        if (allele_lk)
+            PHMM_CK(cudaMemcpyAsync(allele_lk, s.d_allele_lk, plan.allele_lk_total * sizeof(double),
+                                    cudaMemcpyDeviceToHost, m));
+    }
+    if (plan.out_total && out) {
         PHMM_CK(cudaMemcpyAsync(out, plan.region_api ? s.d_out2 : s.d_out, plan.out_total * sizeof(double),
                                 cudaMemcpyDeviceToHost, m));
         if (pair_flags) PHMM_CK(cudaMemcpyAsync(pair_flags, s.d_pair_flags, plan.out_total, cudaMemcpyDeviceToHost, m));

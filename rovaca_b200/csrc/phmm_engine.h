@@ -20,6 +20,7 @@ namespace phmm {
 struct Capacity {
     uint64_t regions = 0, reads = 0, haps = 0, read_bases = 0, hap_bases = 0, items = 0, rerun = 0, out = 0;
     uint64_t scratch_cols = 0;
+    uint64_t events = 0, hap_allele = 0, allele_lk = 0, gl = 0;
     bool covers(const Capacity& o) const;
     Capacity grown_to(const Capacity& need) const;
 };
@@ -50,6 +51,11 @@ struct Slot {
     double* d_out2 = nullptr;        // region API: normalised likelihoods, kept reads first
     uint8_t* d_keep = nullptr;       // region API: kept flag per read
     uint32_t* d_nkept = nullptr;     // region API: kept reads per region
+    EventDesc* d_events = nullptr;   // genotyping events
+    int8_t* d_hap_allele = nullptr;
+    double* d_allele_lk = nullptr;
+    double* d_gl = nullptr;
+    int32_t* d_best = nullptr;
     uint32_t *d_codes_inter = nullptr, *d_codes_intra = nullptr;
     void* d_scratch = nullptr;
     // execution
@@ -79,8 +85,11 @@ public:
                         const uint8_t* mapq = nullptr);
     // Region-API plans: out receives the normalised matrices (kept reads first), keep the kept flag
     // of every read and n_kept the kept reads of every region.
+    // Genotyping outputs (plans with events): gl [gl_total], best [events], allele_lk (optional).
+    // out may be null to skip the likelihood matrix.
     phmm_status finish(Slot& s, const Plan& plan, double* out, uint8_t* pair_flags, phmm_stats* stats,
-                       std::string& err, uint8_t* keep = nullptr, uint32_t* n_kept = nullptr);
+                       std::string& err, uint8_t* keep = nullptr, uint32_t* n_kept = nullptr, double* gl = nullptr,
+                       int32_t* best = nullptr, double* allele_lk = nullptr);
     // Upload only (descriptor, plan arrays, reads, haplotypes); then run the device pipeline, with
     // restore = true resetting the descriptor from its pristine device copy first (replays).
     phmm_status upload(Slot& s, const Plan& plan, const phmm_batch& b, std::string& err,
@@ -124,6 +133,8 @@ private:
     void* d_tables_ = nullptr;
     ProbTables<float> tf_{};
     ProbTables<double> td_{};
+    const double* d_jacobian_ = nullptr;  // genotyping Jacobian table (inside d_tables_)
+    double log10_two_ = 0.0;
     Slot* default_slot_ = nullptr;
     std::mutex mu_;
     mutable std::mutex tiles_mu_;

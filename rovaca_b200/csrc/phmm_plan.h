@@ -63,6 +63,10 @@ struct Plan {
     uint32_t max_multi_stream = 0;   // longest stream among multi-stripe items (0 if none)
     TileTable tiles{};               // the shapes the items were planned with
     bool region_api = false;         // every region uses the region API (device read prep and post)
+    // genotyping events of region-API regions (filled by the caller after planning)
+    std::vector<EventDesc> events;
+    std::vector<int8_t> hap_allele;
+    uint64_t allele_lk_total = 0, gl_total = 0;
 };
 
 // Sizes of a batch, from one validating pass over its counts and offsets (no copies).

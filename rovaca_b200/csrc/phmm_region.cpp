@@ -32,8 +32,8 @@ phmm_status server_submit(phmm_engine* engine, const phmm_batch& b, double* out,
                           std::string& err);
 phmm_status server_wait(phmm_engine* engine, phmm_ticket ticket, int64_t timeout_us, bool release, double* queued_us,
                         double* total_us, std::string& err);
-phmm_status server_submit_region(phmm_engine* engine, const phmm_region_input& in, double* out, uint8_t* keep,
-                                 uint32_t* n_kept, phmm_ticket* ticket, std::string& err);
+phmm_status server_submit_region(phmm_engine* engine, const phmm_region_input& in, const phmm_region_events* events,
+                                 double* out, uint8_t* keep, uint32_t* n_kept, phmm_ticket* ticket, std::string& err);
 
 namespace {
 
@@ -202,7 +202,7 @@ phmm_status phmm_call_region(phmm_engine* engine, uint32_t n_haps, const uint8_t
         in.pcr_model = pcr_model;
         std::string err;
         phmm_ticket t = 0;
-        phmm_status st = phmm::server_submit_region(engine, in, out, keep, n_kept, &t, err);
+        phmm_status st = phmm::server_submit_region(engine, in, nullptr, out, keep, n_kept, &t, err);
         if (st == PHMM_OK) st = phmm::server_wait(engine, t, -1, true, nullptr, nullptr, err);
         if (st != PHMM_OK) {
             fail_matrix();

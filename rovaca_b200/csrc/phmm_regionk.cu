@@ -12,6 +12,8 @@
 //   normalise: cap each read at best - 4.5                src/haplotypecaller/pairhmm/pairhmm_internal.cpp:248-258
 //   drop poorly modelled reads                            src/haplotypecaller/pairhmm/pairhmm_internal.cpp:23-44
 //   [hap][read], kept reads first                         src/haplotypecaller/pairhmm/pairhmm_internal.cpp:489-508
+//   haplotype -> allele marginalisation (max)             src/haplotypecaller/genotype/allele_likelihoods.hpp:702-730
+//   diploid genotype likelihoods                          src/haplotypecaller/genotype/genotype_likelihood_calculator.cpp:59-100
 // The host functions of phmm_region.cpp compute the same values and are what the tests compare to.
 #include <cuda_runtime.h>
 
@@ -178,7 +180,91 @@ __global__ void __launch_bounds__(kPostThreads) post_region_kernel(RegionApiView
     }
 }
 
+// MathUtils::approximate_log10sum_log10(a, b) (common/utils/math_utils.cpp:280-290) with the
+// Jacobian table of math_utils.h:209-242: the larger value plus the tabulated correction at the
+// rounded difference, none beyond a difference of 8.
+__device__ __forceinline__ double approx_log10sum(double a, double b, const double* jac)
+{
+    if (a > b) {
+        const double t = a;
+        a = b;
+        b = t;
+    }
+    if (a == -__longlong_as_double(0x7ff0000000000000ll)) return b;
+    const double diff = __dsub_rn(b, a);
+    constexpr double kInvStep = 1.0 / 0.0001;
+    return __dadd_rn(b, diff < 8.0 ? jac[(size_t)round(__dmul_rn(diff, kInvStep))] : 0.0);
+}
+
+// One block per event: allele likelihoods are the maximum over the event's haplotypes of each
+// allele (AlleleLikelihoods::marginal_likelihoods_direct, genotype/allele_likelihoods.hpp:702-730;
+// -inf when an allele has no haplotype, NaN never wins), over the region's kept reads.  Diploid
+// genotype g = (a <= b), g = b(b+1)/2 + a, gets
+//   GL = sum_r v_r - K log10(2),  v_r = lk(r,a) + log10(2) if a == b else log10sum(lk(r,a), lk(r,b)),
+// summed from 0 in read order (GenotypeLikelihoodCalculator, genotype_likelihood_calculator.cpp:
+// 59-100 and .h:90-142).  The most likely genotype is the first maximum.
+__global__ void __launch_bounds__(kPostThreads) genotype_kernel(RegionApiView v)
+{
+    const BatchDesc* d = v.desc;
+    const uint32_t n_events = d->n_events;
+    if (n_events == 0) return;
+    const double ninf = -__longlong_as_double(0x7ff0000000000000ll);
+    const double nan = __longlong_as_double(0x7ff8000000000000ll);
+    for (uint32_t e = blockIdx.x; e < n_events; e += gridDim.x) {
+        const EventDesc ev = v.events[e];
+        const RegionDesc rg = v.regions[ev.region];
+        const uint32_t M = rg.n_haps, N = rg.n_reads, A = ev.n_alleles;
+        const uint32_t K = v.n_kept[ev.region];
+        const double* lk = v.out + rg.out_off;  // normalised, kept reads first
+        const int8_t* map = v.hap_allele + ev.hap_allele_off;
+        double* alk = v.allele_lk + ev.allele_lk_off;
+        for (uint64_t i = threadIdx.x; i < (uint64_t)A * N; i += blockDim.x) {
+            const uint32_t a = (uint32_t)(i / N), r = (uint32_t)(i % N);
+            double best = ninf;
+            if (r < K) {
+                for (uint32_t h = 0; h < M; ++h)
+                    if (map[h] == (int8_t)a) {
+                        const double x = lk[(uint64_t)h * N + r];
+                        if (x > best) best = x;
+                    }
+            } else {
+                best = nan;
+            }
+            alk[i] = best;
+        }
+        __syncthreads();
+        const uint32_t G = A * (A + 1) / 2;
+        double* gl = v.gl + ev.gl_off;
+        for (uint32_t g = threadIdx.x; g < G; g += blockDim.x) {
+            uint32_t b = 0;
+            while ((b + 1) * (b + 2) / 2 <= g) ++b;
+            const uint32_t a = g - b * (b + 1) / 2;
+            const double* la = alk + (uint64_t)a * N;
+            const double* lb = alk + (uint64_t)b * N;
+            double sum = 0.0;
+            for (uint32_t r = 0; r < K; ++r)
+                sum = __dadd_rn(sum, a == b ? __dadd_rn(la[r], v.log10_two) : approx_log10sum(la[r], lb[r], v.jacobian));
+            // explicit roundings: no fused multiply-add, as the host computes it
+            gl[g] = __dsub_rn(sum, __dmul_rn((double)K, v.log10_two));
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int32_t arg = 0;
+            for (uint32_t g = 1; g < G; ++g)
+                if (gl[g] > gl[arg]) arg = (int32_t)g;
+            v.best[e] = arg;
+        }
+        __syncthreads();
+    }
+}
+
 }  // namespace
+
+cudaError_t launch_genotype(const RegionApiView& v, int num_sms, cudaStream_t st)
+{
+    genotype_kernel<<<num_sms * 2, kPostThreads, 0, st>>>(v);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_read_prep(const RegionApiView& v, int num_sms, cudaStream_t st)
 {

@@ -10,5 +10,7 @@ namespace phmm {
 
 cudaError_t launch_read_prep(const RegionApiView& v, int num_sms, cudaStream_t st);
 cudaError_t launch_post_region(const RegionApiView& v, int num_sms, cudaStream_t st);
+// After launch_post_region: allele likelihoods, diploid genotype likelihoods and calls per event.
+cudaError_t launch_genotype(const RegionApiView& v, int num_sms, cudaStream_t st);
 
 }  // namespace phmm

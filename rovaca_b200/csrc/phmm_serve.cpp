@@ -59,6 +59,13 @@ struct Request {
     RegionApiParams params{};
     uint8_t* keep = nullptr;
     uint32_t* n_kept = nullptr;
+    // genotyping events of a region-API request
+    std::vector<uint8_t> n_alleles;
+    std::vector<int8_t> hap_allele;
+    double* gl = nullptr;
+    int32_t* best = nullptr;
+    double* allele_lk = nullptr;
+    uint64_t gl_n = 0, allele_lk_n = 0;
     uint64_t out_n = 0;
     uint64_t cells = 0;
     uint64_t bytes = 0;  // device footprint estimate for admission
@@ -175,8 +182,18 @@ void Server::worker(int idx)
         // the admitted regions go into the slot's pinned buffers: haplotype bases, then the read
         // arrays (and MAPQ) in; likelihoods (and flags, or kept flags and counts) out
         const size_t in_bytes = hap_total + read_arrays * read_total + (api ? reads_total : 0) + 16;
+        uint64_t gl_total = 0, alk_total = 0, n_events = 0;
+        bool want_out = false, want_alk = false;
+        for (auto& r : batch) {
+            gl_total += r->gl_n;
+            alk_total += r->allele_lk_n;
+            n_events += r->n_alleles.size();
+            want_out |= r->out != nullptr;
+            want_alk |= r->allele_lk != nullptr;
+        }
         const size_t out_bytes = out_total * sizeof(double) + (want_flags ? out_total : 0) +
-                                 (api ? reads_total + batch.size() * sizeof(uint32_t) + 16 : 0) + 16;
+                                 (api ? reads_total + batch.size() * sizeof(uint32_t) + 16 : 0) +
+                                 (gl_total + alk_total) * sizeof(double) + n_events * sizeof(int32_t) + 64;
         if (st == PHMM_OK && !(in_buf.reserve(in_bytes) && out_buf.reserve(out_bytes))) {
             st = PHMM_ERR_OUT_OF_MEMORY;
             berr = "pinned staging for a batch of " + std::to_string(batch.size()) + " regions";
@@ -226,26 +243,62 @@ void Server::worker(int idx)
             PlanLimits lim = Engine::limits_with(tiles);
             if (api) lim.region_api = params.data();
             st = build_plan(b, lim, plan, berr);
+            if (st == PHMM_OK && n_events) {
+                // events of the batch, in request order
+                uint64_t gl_o = 0, alk_o = 0;
+                for (size_t i = 0; i < batch.size(); ++i) {
+                    auto& r = batch[i];
+                    for (size_t e = 0; e < r->n_alleles.size(); ++e) {
+                        EventDesc ev{};
+                        ev.region = (uint32_t)i;
+                        ev.n_alleles = r->n_alleles[e];
+                        ev.hap_allele_off = plan.hap_allele.size();
+                        ev.gl_off = gl_o;
+                        ev.allele_lk_off = alk_o;
+                        plan.hap_allele.insert(plan.hap_allele.end(), r->hap_allele.begin() + e * r->n_haps,
+                                               r->hap_allele.begin() + (e + 1) * r->n_haps);
+                        gl_o += (uint64_t)ev.n_alleles * (ev.n_alleles + 1) / 2;
+                        alk_o += (uint64_t)ev.n_alleles * r->n_reads;
+                        plan.events.push_back(ev);
+                    }
+                }
+                plan.gl_total = gl_o;
+                plan.allele_lk_total = alk_o;
+            }
             if (st == PHMM_OK) st = eng->enqueue(*slot, plan, b, want_flags, berr, api ? mq : nullptr);
             double* out = (double*)out_buf.p;
             uint8_t* flags = want_flags ? (uint8_t*)(out + out_total) : nullptr;
-            uint32_t* kept_n = api ? (uint32_t*)(out + out_total) : nullptr;
+            double* gl = out + out_total;
+            double* alk = gl + gl_total;
+            int32_t* best = (int32_t*)(alk + alk_total);
+            uint32_t* kept_n = api ? (uint32_t*)(best + n_events) : nullptr;
             uint8_t* keep = api ? (uint8_t*)(kept_n + batch.size()) : nullptr;
+            if (want_flags) flags = (uint8_t*)(best + n_events);  // plain batches have no events
             phmm_stats ps{};
-            if (st == PHMM_OK) st = eng->finish(*slot, plan, out, flags, &ps, berr, keep, kept_n);
+            if (st == PHMM_OK)
+                st = eng->finish(*slot, plan, (!api || want_out) ? out : nullptr, flags, &ps, berr, keep, kept_n,
+                                 n_events ? gl : nullptr, n_events ? best : nullptr, want_alk ? alk : nullptr);
             device_ms = ps.device_ms;
             if (st == PHMM_OK) {
-                uint64_t o = 0, ko = 0;
+                uint64_t o = 0, ko = 0, go = 0, ao = 0, eo = 0;
                 for (size_t i = 0; i < batch.size(); ++i) {
                     auto& r = batch[i];
-                    if (r->out_n) std::memcpy(r->out, out + o, r->out_n * sizeof(double));
+                    if (r->out && r->out_n) std::memcpy(r->out, out + o, r->out_n * sizeof(double));
                     if (r->flags && r->out_n) std::memcpy(r->flags, flags + o, r->out_n);
                     if (api) {
                         if (r->n_reads) std::memcpy(r->keep, keep + ko, r->n_reads);
                         *r->n_kept = kept_n[i];
                     }
+                    if (!r->n_alleles.empty()) {
+                        std::memcpy(r->gl, gl + go, r->gl_n * sizeof(double));
+                        std::memcpy(r->best, best + eo, r->n_alleles.size() * sizeof(int32_t));
+                        if (r->allele_lk) std::memcpy(r->allele_lk, alk + ao, r->allele_lk_n * sizeof(double));
+                    }
                     o += r->out_n;
                     ko += r->n_reads;
+                    go += r->gl_n;
+                    ao += r->allele_lk_n;
+                    eo += r->n_alleles.size();
                 }
             }
         }
@@ -396,8 +449,8 @@ phmm_status server_submit(phmm_engine* engine, const phmm_batch& b, double* out,
 
 // Submits one region with call_pairhmm semantics: raw base qualities and MAPQ are copied, the
 // device prepares the reads and post-processes the likelihoods.
-phmm_status server_submit_region(phmm_engine* engine, const phmm_region_input& in, double* out, uint8_t* keep,
-                                 uint32_t* n_kept, phmm_ticket* ticket, std::string& err)
+phmm_status server_submit_region(phmm_engine* engine, const phmm_region_input& in, const phmm_region_events* events,
+                                 double* out, uint8_t* keep, uint32_t* n_kept, phmm_ticket* ticket, std::string& err)
 {
     if (!in.hap_off || !in.read_off || (in.n_reads && (!in.mapq || !keep)) || !n_kept) {
         err = "null argument";
@@ -422,12 +475,43 @@ phmm_status server_submit_region(phmm_engine* engine, const phmm_region_input& i
     BatchScan sc;
     phmm_status st = scan_batch(b, lim, sc, err);
     if (st != PHMM_OK) return st;
-    if (sc.out_total && !out) {
+    const uint32_t n_events = events ? events->n_events : 0;
+    if (sc.out_total && !out && n_events == 0) {
         err = "out is null";
+        return PHMM_ERR_INVALID_ARGUMENT;
+    }
+    if (n_events && (!events->n_alleles || (sc.n_haps && !events->hap_allele) || !events->genotype_lk ||
+                     !events->best_genotype)) {
+        err = "events: n_alleles, hap_allele, genotype_lk and best_genotype are required";
         return PHMM_ERR_INVALID_ARGUMENT;
     }
     auto r = std::make_shared<Request>();
     r->region_api = true;
+    for (uint32_t e = 0; e < n_events; ++e) {
+        const uint32_t A = events->n_alleles[e];
+        if (A < 1 || A > kMaxAlleles) {
+            err = "event " + std::to_string(e) + ": " + std::to_string(A) + " alleles (1.." + std::to_string(kMaxAlleles) +
+                  " supported)";
+            return PHMM_ERR_LIMIT_EXCEEDED;
+        }
+        for (uint32_t h = 0; h < sc.n_haps; ++h) {
+            const int8_t a = events->hap_allele[(uint64_t)e * sc.n_haps + h];
+            if (a < -1 || a >= (int)A) {
+                err = "event " + std::to_string(e) + ": haplotype " + std::to_string(h) + " mapped to allele " +
+                      std::to_string(a) + " of " + std::to_string(A);
+                return PHMM_ERR_INVALID_ARGUMENT;
+            }
+        }
+        r->gl_n += (uint64_t)A * (A + 1) / 2;
+        r->allele_lk_n += (uint64_t)A * sc.n_reads;
+    }
+    if (n_events) {
+        r->n_alleles.assign(events->n_alleles, events->n_alleles + n_events);
+        r->hap_allele.assign(events->hap_allele, events->hap_allele + (uint64_t)n_events * sc.n_haps);
+        r->gl = events->genotype_lk;
+        r->best = events->best_genotype;
+        r->allele_lk = events->allele_lk;
+    }
     r->params = params;
     r->n_haps = sc.n_haps;
     r->n_reads = sc.n_reads;
@@ -450,7 +534,7 @@ phmm_status server_submit_region(phmm_engine* engine, const phmm_region_input& i
     r->out_n = sc.out_total;
     r->cells = sc.cells;
     r->bytes = footprint(sc.read_bases, sc.hap_bases, sc.out_total, sc.n_reads, sc.n_haps) + sc.out_total * 8 +
-               sc.n_reads * 2;
+               sc.n_reads * 2 + r->hap_allele.size() + (r->gl_n + r->allele_lk_n) * 8 + n_events * 36;
     for (uint32_t k = 0; k < sc.n_reads; ++k)
         if (r->read_off[k + 1] - r->read_off[k] > (uint64_t)kWarp * kMaxK) {
             r->bytes += engine_of(engine)->scratch_bytes();
@@ -510,15 +594,15 @@ phmm_status phmm_submit(phmm_engine* engine, const phmm_batch* region, double* o
     }
 }
 
-phmm_status phmm_submit_region(phmm_engine* engine, const phmm_region_input* region, double* out, uint8_t* keep,
-                               uint32_t* n_kept, phmm_ticket* ticket)
+phmm_status phmm_submit_region(phmm_engine* engine, const phmm_region_input* region, const phmm_region_events* events,
+                               double* out, uint8_t* keep, uint32_t* n_kept, phmm_ticket* ticket)
 {
     try {
         phmm::clear_error();
         if (!engine) return set_error(PHMM_ERR_NOT_INITIALIZED, "engine is null");
         if (!region || !ticket) return set_error(PHMM_ERR_INVALID_ARGUMENT, "region or ticket is null");
         std::string err;
-        phmm_status st = phmm::server_submit_region(engine, *region, out, keep, n_kept, ticket, err);
+        phmm_status st = phmm::server_submit_region(engine, *region, events, out, keep, n_kept, ticket, err);
         return st == PHMM_OK ? PHMM_OK : set_error(st, err);
     } catch (const std::bad_alloc&) {
         return set_error(PHMM_ERR_OUT_OF_MEMORY, "host allocation failed");

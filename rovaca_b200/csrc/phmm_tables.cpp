@@ -113,4 +113,16 @@ const HostTables<double>& host_tables_f64()
     return t;
 }
 
+const std::vector<double>& genotype_jacobian()
+{
+    static const std::vector<double> t = [] {
+        std::vector<double> x(kJacSize);
+        for (int k = 0; k < kJacSize; ++k) x[k] = std::log10(1.0 + std::pow(10.0, -kJacStep * (double)k));
+        return x;
+    }();
+    return t;
+}
+
+double host_log10_two() { return std::log10(2.0); }
+
 }  // namespace phmm

@@ -18,4 +18,9 @@ struct HostTables {
 const HostTables<float>& host_tables_f32();
 const HostTables<double>& host_tables_f64();
 
+// The genotyping Jacobian table, log10(1 + 10^(-k * 1e-4)) for k = 0..80000 in double
+// (common/utils/math_utils.h:209-242), and log10(2) from the host math library (Log10Cache).
+const std::vector<double>& genotype_jacobian();
+double host_log10_two();
+
 }  // namespace phmm

@@ -136,8 +136,19 @@ struct BatchDesc {
     uint64_t read_bases_total;
     uint32_t n_regions, n_reads, n_haps, n_items;
     uint32_t region_api;          // regions with kRegionApi (0: the read-prep and post kernels idle)
-    uint32_t pad;
+    uint32_t n_events;            // genotyping events of region-API regions (0: genotype kernel idle)
 };
+
+// One genotyping event of a region-API region: a set of alleles, each haplotype mapped to one of
+// them or to none.
+struct EventDesc {                // 32 bytes
+    uint32_t region;
+    uint32_t n_alleles;           // 1..kMaxAlleles
+    uint64_t hap_allele_off;      // int8 allele of each of the region's haplotypes (-1: none)
+    uint64_t gl_off;              // first diploid genotype likelihood, n_alleles*(n_alleles+1)/2 of them
+    uint64_t allele_lk_off;       // first allele likelihood: [n_alleles][region's n_reads]
+};
+constexpr uint32_t kMaxAlleles = 49;  // the reference's genotype tables stop below 50 alleles
 
 // Region-API device arrays (read preparation in, post-processed results out).
 struct RegionApiView {
@@ -154,6 +165,14 @@ struct RegionApiView {
     double* out;                  // normalised, kept reads first, NaN after
     uint8_t* keep;                // [n_reads]
     uint32_t* n_kept;             // [n_regions]
+    // genotyping (events of the regions)
+    const EventDesc* events;
+    const int8_t* hap_allele;
+    double* allele_lk;            // marginal likelihoods, kept reads first, NaN after
+    double* gl;                   // diploid genotype log10 likelihoods
+    int32_t* best;                // most likely genotype per event
+    const double* jacobian;       // log10(1 + 10^(-k/10000)), k = 0..80000
+    double log10_two;             // log10(2) as the host's math library gives it
 };
 
 // Status bits a kernel raises instead of touching memory it should not.

@@ -324,10 +324,14 @@ class Engine:
 
     # ---- region API ----------------------------------------------------------------------
     def submit_region(self, haplotypes, reads, base_quals, mapq, min_quality_threshold: int = 18,
-                      pcr_option: str | int = "CONSERVATIVE") -> "RegionTicket":
+                      pcr_option: str | int = "CONSERVATIVE", events=None, want_matrix: bool = True,
+                      want_allele_lk: bool = False) -> "RegionTicket":
         """phmm_submit_region: queues one region with call_pairhmm semantics (read preparation and
-        post-processing on the GPU); RegionTicket.wait() returns what call_region returns."""
-        return RegionTicket(self, haplotypes, reads, base_quals, mapq, min_quality_threshold, pcr_option)
+        post-processing on the GPU).  events: optional list of (n_alleles, allele of each haplotype,
+        -1 for none) to genotype on the GPU.  RegionTicket.wait() returns (matrix or None, keep mask)
+        and RegionTicket.genotypes() the per-event results."""
+        return RegionTicket(self, haplotypes, reads, base_quals, mapq, min_quality_threshold, pcr_option, events,
+                            want_matrix, want_allele_lk)
 
     def call_region(self, haplotypes, reads, base_quals, mapq, min_quality_threshold: int = 18,
                     pcr_option: str | int = "CONSERVATIVE"):
@@ -354,35 +358,65 @@ class Engine:
 class RegionTicket:
     """A region submitted with phmm_submit_region; keeps its buffers alive until wait()."""
 
-    def __init__(self, engine: Engine, haplotypes, reads, base_quals, mapq, min_quality_threshold, pcr_option):
+    def __init__(self, engine: Engine, haplotypes, reads, base_quals, mapq, min_quality_threshold, pcr_option,
+                 events=None, want_matrix: bool = True, want_allele_lk: bool = False):
         pcr = PCR_MODELS[pcr_option] if isinstance(pcr_option, str) else int(pcr_option)
         hs = [_u8(h) for h in haplotypes]
         rs = [_u8(r) for r in reads]
         qs = [_u8(q) for q in base_quals]
         cat = lambda parts: np.concatenate(parts) if parts else np.zeros(1, np.uint8)
         off = lambda parts: np.concatenate([[0], np.cumsum([len(p) for p in parts])]).astype(np.uint64)
-        self._keepalive = (cat(hs), off(hs), cat(rs), off(rs), cat(qs))
+        self._keepalive = [cat(hs), off(hs), cat(rs), off(rs), cat(qs)]
         hb, hoff, rb, roff, qb = self._keepalive
         mq = np.ascontiguousarray(np.asarray(mapq, np.uint8).reshape(-1))
         if mq.size == 1 and len(rs) > 1:
             mq = np.full(len(rs), mq[0], np.uint8)
-        self._mq = mq
+        self._keepalive.append(mq)
         self.n_haps, self.n_reads = len(hs), len(rs)
-        self.out = np.empty(self.n_haps * self.n_reads, np.float64)
-        self.keep = np.empty(self.n_reads, np.uint8)
+        self.out = np.empty(self.n_haps * self.n_reads, np.float64) if want_matrix else None
+        self.keep = np.empty(max(self.n_reads, 1), np.uint8)
         self.n_kept = C.c_uint32()
         inp = _lib.RegionInput(self.n_haps, hb.ctypes.data, hoff.ctypes.data, self.n_reads, rb.ctypes.data,
                                qb.ctypes.data, roff.ctypes.data, mq.ctypes.data, int(min_quality_threshold), pcr)
+        self.events = None
+        ev_ptr = None
+        if events:
+            na = np.array([int(a) for a, _ in events], np.uint8)
+            ha = np.ascontiguousarray(np.array([np.asarray(m, np.int8).reshape(-1) for _, m in events], np.int8))
+            n_gl = int(sum(int(a) * (int(a) + 1) // 2 for a in na))
+            self.gl = np.empty(max(n_gl, 1), np.float64)
+            self.best = np.empty(len(na), np.int32)
+            self.allele_lk = np.empty(max(int(na.astype(np.int64).sum()) * self.n_reads, 1)) if want_allele_lk else None
+            self._keepalive += [na, ha]
+            self.events = _lib.RegionEvents(len(na), na.ctypes.data, ha.ctypes.data, self.gl.ctypes.data,
+                                            self.best.ctypes.data,
+                                            self.allele_lk.ctypes.data if want_allele_lk else None)
+            self._n_alleles = na
+            ev_ptr = C.byref(self.events)
         self._engine = engine
         t = C.c_uint64()
-        check(engine._lib.phmm_submit_region(engine._h, C.byref(inp), _ptr(self.out), _ptr(self.keep),
+        check(engine._lib.phmm_submit_region(engine._h, C.byref(inp), ev_ptr, _ptr(self.out), _ptr(self.keep),
                                              C.byref(self.n_kept), C.byref(t)))
         self.ticket = t.value
 
     def wait(self):
-        """Blocks until done; returns (matrix [n_haps][n_reads] with kept reads first, keep mask)."""
+        """Blocks until done; returns (matrix [n_haps][n_reads] with kept reads first or None, keep mask)."""
         self._engine.wait(self.ticket)
-        return self.out.reshape(self.n_haps, self.n_reads), self.keep.astype(bool)
+        mat = self.out.reshape(self.n_haps, self.n_reads) if self.out is not None else None
+        return mat, self.keep[:self.n_reads].astype(bool)
+
+    def genotypes(self):
+        """Per event: (genotype log10 likelihoods, most likely genotype, allele likelihoods or None)."""
+        res, go, ao = [], 0, 0
+        for a in self._n_alleles.astype(int):
+            g = a * (a + 1) // 2
+            alk = None
+            if self.allele_lk is not None:
+                alk = self.allele_lk[ao:ao + a * self.n_reads].reshape(a, self.n_reads)
+            res.append((self.gl[go:go + g].copy(), int(self.best[len(res)]), alk))
+            go += g
+            ao += a * self.n_reads
+        return res
 
 
 class ResidentBatch:

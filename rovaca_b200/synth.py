@@ -145,3 +145,72 @@ def make(config: int, scale: float = 1.0, seed: int | None = None) -> PackedBatc
     if config == 4:
         return config4(max(1, int(round(200_000 * scale))), **kw)
     raise ValueError(f"no generator for config {config}")
+
+
+def genotyping_regions(n_regions: int, seed: int = 5, depth: int = 40, read_len: int = 150,
+                       window: tuple[int, int] = (300, 400), sites: tuple[int, int] = (1, 3)):
+    """Regions with known variant sites for the genotyping path, one diploid sample each.
+
+    Each region: a reference window with 1-3 variant sites (a SNP, or an insertion or deletion of
+    1-6 bases) at distinct positions and a true genotype per site (0/0, 0/1 or 1/1, the two true
+    haplotypes phased at random); candidate haplotypes are the reference and every combination of
+    alternate alleles; reads of `read_len` come from the two true haplotypes at uniform offsets with
+    1% substitution errors and base qualities U[10,40].  Each site is one event with alleles
+    {ref, alt}; a haplotype maps to the alt allele when it carries the site's alternate.
+    Returns dicts with haplotypes, reads, quals, mapq, events [(2, allele of each haplotype)] and
+    truth (genotype index per site: 0 hom-ref, 1 het, 2 hom-alt)."""
+    rng = np.random.default_rng([seed, 5])
+    out = []
+    for _ in range(n_regions):
+        L = int(rng.integers(window[0], window[1] + 1))
+        ref = rng.integers(0, 4, L + read_len).astype(np.uint8)
+        n_sites = int(rng.integers(sites[0], sites[1] + 1))
+        pos = np.sort(rng.choice(np.arange(20, L - 20, 25), n_sites, replace=False))
+        kinds = []
+        for p in pos:
+            k = rng.integers(0, 3)
+            if k == 0:
+                kinds.append(("snp", int(p), int((ref[p] + rng.integers(1, 4)) % 4)))
+            elif k == 1:
+                kinds.append(("ins", int(p), rng.integers(0, 4, int(rng.integers(1, 7))).astype(np.uint8)))
+            else:
+                kinds.append(("del", int(p), int(rng.integers(1, 7))))
+
+        def build(carry):
+            s, last = [], 0
+            for (kind, p, x), c in zip(kinds, carry):
+                if not c:
+                    continue
+                s.append(ref[last:p])
+                if kind == "snp":
+                    s.append(np.array([x], np.uint8))
+                    last = p + 1
+                elif kind == "ins":
+                    s.append(ref[p:p + 1])
+                    s.append(x)
+                    last = p + 1
+                else:
+                    s.append(ref[p:p + 1])
+                    last = p + 1 + x
+            s.append(ref[last:L])
+            return np.concatenate(s)
+
+        combos = [tuple((m >> i) & 1 for i in range(n_sites)) for m in range(1 << n_sites)]
+        haps = [build(c) for c in combos]
+        truth = [int(g) for g in rng.integers(0, 3, n_sites)]
+        phase = [(0, 0) if g == 0 else ((1, 1) if g == 2 else ((0, 1) if rng.random() < 0.5 else (1, 0))) for g in truth]
+        true_haps = [combos.index(tuple(ph[k] for ph in phase)) for k in range(2)]
+        reads, quals = [], []
+        for _ in range(depth):
+            h = haps[true_haps[int(rng.integers(0, 2))]]
+            ext = np.concatenate([h, ref[L:]])
+            o = int(rng.integers(0, max(1, len(h) - read_len + 1)))
+            r = ext[o:o + read_len].copy()
+            flip = rng.random(len(r)) < 0.01
+            r[flip] = (r[flip] + rng.integers(1, 4, int(flip.sum()))) % 4
+            reads.append(ACGT[r].tobytes())
+            quals.append(rng.integers(10, 41, len(r)).astype(np.uint8).tobytes())
+        events = [(2, np.array([c[i] for c in combos], np.int8)) for i in range(n_sites)]
+        out.append({"haplotypes": [ACGT[h].tobytes() for h in haps], "reads": reads, "quals": quals,
+                    "mapq": np.full(depth, 60, np.uint8), "events": events, "truth": truth})
+    return out

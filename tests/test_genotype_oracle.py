@@ -1,0 +1,61 @@
+"""The genotyping restatement of the checker (oracle/genotype.py) against the reference's own
+definition of diploid genotype likelihoods (genotype/test/genotype_likelihood_calculator_unit_test.cpp:
+86-130: GL = sum_r [log10sum_c(lk(r, a_c) + log10(count_c)) - log10(2)], accepted within 1e-4) and
+its genotype order.  No GPU."""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+from oracle import genotype as G
+
+
+def _unit_test_gl(alk: np.ndarray, a: int, b: int) -> float:
+    comps = [(a, 2)] if a == b else [(a, 1), (b, 1)]
+    total = 0.0
+    for r in range(alk.shape[1]):
+        vals = [alk[x, r] + math.log10(c) for x, c in comps]
+        m = max(vals)
+        s = m + math.log10(sum(10.0 ** (v - m) for v in vals)) if m != -math.inf else -math.inf
+        total += s - math.log10(2)
+    return total
+
+
+@pytest.mark.parametrize("alleles", [1, 2, 5, 6])
+@pytest.mark.parametrize("reads", [0, 1, 10, 100])
+def test_genotype_likelihoods_match_reference_definition(alleles, reads):
+    rng = np.random.default_rng(alleles * 1000 + reads)
+    alk = -rng.exponential(3.0, (alleles, reads))
+    gl = G.genotype_likelihoods(alk)
+    assert len(gl) == alleles * (alleles + 1) // 2
+    for b in range(alleles):
+        for a in range(b + 1):
+            assert abs(gl[b * (b + 1) // 2 + a] - _unit_test_gl(alk, a, b)) < 1e-4
+
+
+def test_genotype_order_is_vcf_order():
+    # (0,0) (0,1) (1,1) (0,2) (1,2) (2,2): an allele with all the support wins at its hom index
+    alk = np.array([[-9.0] * 20, [-9.0] * 20, [-0.1] * 20])
+    gl = G.genotype_likelihoods(alk)
+    assert G.best_genotype(gl) == 5
+    alk[1, :10], alk[2, :10] = -0.1, -9.0  # half the reads for allele 1, half for allele 2
+    assert G.best_genotype(G.genotype_likelihoods(alk)) == 4  # het (1,2)
+
+
+def test_approximate_log10sum_accuracy_and_edges():
+    rng = np.random.default_rng(3)
+    for _ in range(2000):
+        a, b = -rng.exponential(5.0, 2)
+        exact = math.log10(10 ** a + 10 ** b)
+        assert abs(G.approx_log10sum(a, b) - exact) < 1e-4
+    assert G.approx_log10sum(-math.inf, -2.0) == -2.0
+    assert G.approx_log10sum(-1.0, -20.0) == -1.0  # difference beyond 8: the larger value
+
+
+def test_marginalisation_takes_the_best_haplotype_and_skips_nan():
+    norm = np.array([[-1.0, -3.0, np.nan], [-2.0, np.nan, np.nan], [-0.5, -4.0, np.nan]])
+    alk = G.marginalize(norm, 2, [0, 0, 1], 3)
+    assert alk[0].tolist() == [-1.0, -3.0] and alk[1].tolist() == [-0.5, -4.0]
+    assert alk[2].tolist() == [-math.inf, -math.inf]

@@ -270,3 +270,77 @@ def test_region_and_plain_requests_mix(engine):
         assert np.array_equal(mat, alone[g][0], equal_nan=True)
         assert np.array_equal(keep, alone[g][1])
         assert np.array_equal(outs[g], plain_alone[g], equal_nan=True)
+
+
+def _oracle_region_lk(oracle, haps, reads, quals, mapq, thr, pcr, fp64_only):
+    """Region-API likelihoods [hap][read] from the oracle: host read preparation, then the oracle's
+    FP32/FP64 switch (or all-FP64)."""
+    import ctypes as C
+
+    from rovaca_b200 import _lib
+    from rovaca_b200.pairhmm import Region
+
+    lib = _lib.load()
+    qs, gops = [], []
+    for rd, q, mq in zip(reads, quals, mapq):
+        n = len(rd)
+        qq = (C.c_uint8 * max(n, 1))()
+        lib.phmm_host_prepare_quals(q, n, int(mq), thr, qq)
+        gop = (C.c_uint8 * max(n, 1))(*([45] * max(n, 1)))
+        lib.phmm_host_pcr_model(rd, n, gop, pcr)
+        qs.append(bytes(qq)[:n])
+        gops.append(bytes(gop)[:n])
+    pb = PackedBatch.from_regions([Region(haps, reads, qs, gops, gops, [bytes([10]) * len(r) for r in reads])])
+    lk, _ = oracle.batch(pb, fp64_only=fp64_only)
+    return lk.reshape(len(haps), len(reads))
+
+
+def test_genotyping_on_device_and_concordance(engine, oracle):
+    """Allele marginalisation and diploid genotype likelihoods on the GPU equal the checker's
+    restatement on the same normalised matrix bit for bit, and the genotype calls equal those made
+    from all-FP64 likelihoods (identical final genotypes)."""
+    from oracle import genotype as G
+
+    regions = synth.genotyping_regions(16, seed=11)
+    tickets = [engine.submit_region(r["haplotypes"], r["reads"], r["quals"], r["mapq"], 18, 3, events=r["events"],
+                                    want_allele_lk=True) for r in regions]
+    max_gl_diff, calls, truth_hits = 0.0, 0, 0
+    for r, t in zip(regions, tickets):
+        mat, keep = t.wait()
+        got = t.genotypes()
+        K = int(keep.sum())
+        for (A, ha), (gl, best, alk) in zip(r["events"], got):
+            walk = G.marginalize(mat, K, list(ha), A)
+            assert np.array_equal(alk[:, :K], walk)
+            assert np.isnan(alk[:, K:]).all()
+            wgl = G.genotype_likelihoods(walk)
+            assert np.array_equal(gl, wgl)
+            assert best == G.best_genotype(wgl)
+        # concordance with genotypes from all-FP64 likelihoods
+        lk64 = _oracle_region_lk(oracle, r["haplotypes"], r["reads"], r["quals"], r["mapq"], 18, 3, True)
+        res64, _, keep64 = G.genotype_region(lk64, [len(x) for x in r["reads"]], r["events"])
+        assert np.array_equal(keep64, keep)
+        for (gl, best, _), (gl64, best64, _), truth in zip(got, res64, r["truth"]):
+            assert best == best64
+            max_gl_diff = max(max_gl_diff, float(np.max(np.abs(gl - gl64))))
+            calls += 1
+            truth_hits += int(best == (0 if truth == 0 else (1 if truth == 1 else 2)))
+    assert max_gl_diff < 1e-3, max_gl_diff
+    assert truth_hits >= 0.9 * calls  # the synthetic truth is recovered at depth 40
+
+
+def test_genotyping_only_results_come_back(engine):
+    """With no matrix requested, only keep flags, genotype likelihoods and calls return."""
+    r = synth.genotyping_regions(1, seed=12)[0]
+    full = engine.submit_region(r["haplotypes"], r["reads"], r["quals"], r["mapq"], 18, 0, events=r["events"])
+    lean = engine.submit_region(r["haplotypes"], r["reads"], r["quals"], r["mapq"], 18, 0, events=r["events"],
+                                want_matrix=False)
+    m1, k1 = full.wait()
+    m2, k2 = lean.wait()
+    assert m2 is None and np.array_equal(k1, k2)
+    for (g1, b1, _), (g2, b2, _) in zip(full.genotypes(), lean.genotypes()):
+        assert np.array_equal(g1, g2) and b1 == b2
+    with pytest.raises(PhmmError) as e:
+        engine.submit_region(r["haplotypes"], r["reads"], r["quals"], r["mapq"], 18, 0,
+                             events=[(50, np.zeros(len(r["haplotypes"]), np.int8))])
+    assert e.value.name == "PHMM_ERR_LIMIT_EXCEEDED"
