@@ -163,7 +163,6 @@ struct SweepOut {
     uint64_t out_base;            // output index of the stream's first haplotype
     uint32_t out_stride;          // output index step between consecutive haplotypes
     uint32_t read;                // global read index (for the rerun list)
-    bool fp32_pass;               // append underflowed pairs to the rerun list
 };
 
 // Sweep one stripe over the column stream of haplotypes [g_lo, g_hi) (global indices).
@@ -197,22 +196,6 @@ __device__ void sweep(LaneRows<T, K>& L, const BatchView& b, const PassControl& 
                 const T tot = ftz(radd(sumM, sumI));
                 const uint64_t oi = so.out_base + (uint64_t)(cur - g_lo) * so.out_stride;
                 so.out[oi] = log10((double)tot) - Scale<T>::log10_initial();
-                if (so.fp32_pass) {
-                    const bool under = (double)tot < (double)1e-28f;
-                    if (under) {
-                        const unsigned int slot = atomicAdd(&pc.cd->rerun_count, 1u);
-                        if (slot < pc.cd->rerun_cap) {
-                            RerunEntry e;
-                            e.out_idx = oi;
-                            e.read = so.read;
-                            e.hap = cur;
-                            pc.rerun[pc.cd->rerun_off + slot] = e;
-                        } else {
-                            atomicOr(pc.status, kStatusRerunOverflow);
-                        }
-                    }
-                    if (so.pair_flags) so.pair_flags[oi] = under ? 1 : 0;
-                }
             }
             ++cur;
         }

@@ -193,6 +193,26 @@ __device__ void sweep2(LaneRows2<KH, PM>& L, const BatchView& b, const PassContr
             nbA = 0x7fffffff;
         }
     };
+    // Writer lane: the open run of consecutive underflowed haplotypes (first haplotype, its output).
+    uint32_t run_lo = 0xffffffffu;
+    uint64_t run_oi = 0;
+    auto close_run = [&](uint32_t end) {
+        if (run_lo == 0xffffffffu) return;
+        const unsigned int slot = atomicAdd(&pc.cd->rerun_count, 1u);
+        if (slot < pc.cd->rerun_cap) {
+            RerunEntry e;
+            e.out_idx = run_oi;
+            e.read = so.read;
+            e.hap = run_lo;
+            e.n_haps = end - run_lo;
+            e.out_stride = so.out_stride;
+            pc.rerun[pc.cd->rerun_off + slot] = e;
+            atomicAdd(&pc.cd->rerun_pairs, end - run_lo);
+        } else {
+            atomicOr(pc.status, kStatusRerunOverflow);
+        }
+        run_lo = 0xffffffffu;
+    };
     auto boundaryB = [&]() {
         if (startedB) {
             if (writer && !TO_SCR) {
@@ -201,17 +221,14 @@ __device__ void sweep2(LaneRows2<KH, PM>& L, const BatchView& b, const PassContr
                 so.out[oi] = log10((double)tot) - Scale<float>::log10_initial();
                 const bool under = (double)tot < (double)1e-28f;
                 if (under) {
-                    const unsigned int slot = atomicAdd(&pc.cd->rerun_count, 1u);
-                    if (slot < pc.cd->rerun_cap) {
-                        RerunEntry e;
-                        e.out_idx = oi;
-                        e.read = so.read;
-                        e.hap = curB;
-                        pc.rerun[pc.cd->rerun_off + slot] = e;
-                    } else {
-                        atomicOr(pc.status, kStatusRerunOverflow);
+                    if (run_lo == 0xffffffffu) {
+                        run_lo = curB;
+                        run_oi = oi;
                     }
+                } else {
+                    close_run(curB);
                 }
+                if (curB + 1 == g_hi) close_run(g_hi);
                 if (so.pair_flags) so.pair_flags[oi] = under ? 1 : 0;
             }
             ++curB;

@@ -680,7 +680,7 @@ phmm_status Engine::finish(Slot& s, const Plan& plan, double* out, uint8_t* pair
     const ClassDesc* cls = (const ClassDesc*)(desc + sizeof(BatchDesc));
     const unsigned int status = *(const unsigned int*)(desc + sizeof(BatchDesc) + sizeof(ClassDesc) * kNumClasses);
     uint64_t f64 = 0;
-    for (int c = kClasses32; c < kNumClasses; ++c) f64 += std::min(cls[c].rerun_count, cls[c].rerun_cap);
+    for (int c = kClasses32; c < kNumClasses; ++c) f64 += cls[c].rerun_pairs;
     if (stats) {
         stats->regions = plan.n_regions;
         stats->pairs = plan.pairs;

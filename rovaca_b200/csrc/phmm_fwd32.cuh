@@ -78,7 +78,6 @@ __global__ void __launch_bounds__(kFwdBlock, 1) fwd_f32_kernel(BatchView b, Prob
         so.read = it.read[group];
         so.out_base = rg.out_off + (uint64_t)it.hap_lo * rg.n_reads + (so.read - rg.read_begin);
         so.out_stride = rg.n_reads;
-        so.fp32_pass = true;
         run_pair2<KH, V, PM, MULTI>(b, tb, pc, so, rg.hap_begin + it.hap_lo, rg.hap_begin + it.hap_hi, lane,
                                     it.stripes, scr);
     }

@@ -91,7 +91,8 @@ __device__ __forceinline__ void run_read(const BatchView& b, const ProbTables<T>
 }
 
 // ------------------------------------------------------------------------------------------
-// FP64 pass for one class over the pairs its FP32 pass flagged, one pair per claim.
+// FP64 pass for one class over the runs of underflowed pairs the FP32 pass appended, one run per
+// claim, streamed through the read like an FP32 work item.
 // ------------------------------------------------------------------------------------------
 template <int K, int V, bool MULTI>
 __global__ void __launch_bounds__(kFwdBlock, 1) fwd_f64_kernel(BatchView b, ProbTables<double> tb, PassControl pc)
@@ -109,10 +110,9 @@ __global__ void __launch_bounds__(kFwdBlock, 1) fwd_f64_kernel(BatchView b, Prob
         so.out = b.out;
         so.pair_flags = nullptr;
         so.out_base = e.out_idx;
-        so.out_stride = 0;
+        so.out_stride = e.out_stride;
         so.read = e.read;
-        so.fp32_pass = false;
-        run_read<double, K, V, MULTI>(b, tb, pc, so, e.hap, e.hap + 1, lane, scr);
+        run_read<double, K, V, MULTI>(b, tb, pc, so, e.hap, e.hap + e.n_haps, lane, scr);
     }
 }
 

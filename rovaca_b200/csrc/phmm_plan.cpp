@@ -377,7 +377,7 @@ phmm_status build_plan(const phmm_batch& b, const PlanLimits& lim, Plan& plan, s
         cd.rerun_off = rerun_off;
         rerun_off += cd.rerun_cap;
     }
-    for (ClassDesc& cd : plan.classes) cd.claim32 = cd.claim64 = cd.rerun_count = 0;
+    for (ClassDesc& cd : plan.classes) cd.claim32 = cd.claim64 = cd.rerun_count = cd.rerun_pairs = 0;
     plan.rerun_slots = rerun_off;
     return PHMM_OK;
 }

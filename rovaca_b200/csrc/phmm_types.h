@@ -82,10 +82,14 @@ struct WorkItem {                 // 20 bytes
     uint8_t pmode;                // ParamMode of the FP32 kernel (0: gap parameters constant)
 };
 
-struct RerunEntry {               // 16 bytes: one pair whose FP32 sum fell below 1e-28
-    uint64_t out_idx;
+// A run of consecutive haplotypes of one work item whose FP32 sums all fell below 1e-28 against
+// one read: the FP64 pass streams them through the read like an FP32 work item.
+struct RerunEntry {               // 24 bytes
+    uint64_t out_idx;             // likelihood of the first pair
     uint32_t read;                // global read index
-    uint32_t hap;                 // global haplotype index
+    uint32_t hap;                 // global index of the first haplotype
+    uint32_t n_haps;              // haplotypes in the run
+    uint32_t out_stride;          // output index step between consecutive haplotypes
 };
 
 template <typename T>
@@ -122,11 +126,11 @@ struct ClassDesc {                // 32 bytes
     uint32_t item_off;            // first work item of the class
     uint32_t n_items;
     uint32_t rerun_off;           // first slot of the class's FP64 rerun segment
-    uint32_t rerun_cap;           // = pairs of the class, so the segment cannot overflow
+    uint32_t rerun_cap;           // = pairs of the class (runs <= pairs), so it cannot overflow
     uint32_t claim32;             // FP32 claim counter (zeroed before each batch)
     uint32_t claim64;             // FP64 claim counter
-    uint32_t rerun_count;         // pairs appended to the rerun segment
-    uint32_t pad;
+    uint32_t rerun_count;         // runs appended to the rerun segment
+    uint32_t rerun_pairs;         // pairs in those runs
 };
 
 // Batch-wide sizes, in device memory for the same reason.
