@@ -223,7 +223,10 @@ def serving_latency(engine, batch, load: float, capacity_regions_per_s: float, s
             "mean_batch_ms": round((after["batch_ms"] - before["batch_ms"]) / max(batches, 1), 2),
             "mean_batch_device_ms": round((after["device_ms"] - before["device_ms"]) / max(batches, 1), 2),
             "max_batch_ms_so_far": round(after["max_batch_ms"], 2), "max_queue_ms_so_far": round(after["max_queue_ms"], 2),
-            "max_submit_lag_ms": round(lag * 1e3, 2)}
+            "max_submit_lag_ms": round(lag * 1e3, 2),
+            "arena_grows": after["arena_grows"] - before["arena_grows"],
+            "graph_captures": after["graph_captures"] - before["graph_captures"],
+            "max_setup_ms_so_far": round(after["max_setup_ms"], 2), "max_host_ms_so_far": round(after["max_host_ms"], 2)}
 
 
 def run_resident_only(args) -> None:

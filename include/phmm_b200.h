@@ -326,6 +326,10 @@ typedef struct phmm_server_stats {
     double device_ms;             /* summed device time of the batches' launch sequences */
     double max_batch_ms;          /* longest batch, admission to results scattered */
     double max_queue_ms;          /* longest wait of a request between submit and admission */
+    uint64_t arena_grows;         /* device arena (re)allocations of the serving slots */
+    uint64_t graph_captures;      /* CUDA graph captures of the serving slots */
+    double max_setup_ms;          /* longest arena growth + graph capture inside one batch */
+    double max_host_ms;           /* longest host part of one batch (gather, plan, scatter) */
 } phmm_server_stats;
 
 PHMM_API phmm_status phmm_server_stats_get(phmm_engine* engine, phmm_server_stats* stats);

@@ -318,18 +318,32 @@ void Engine::free_slot(Slot* s)
 
 uint64_t Engine::scratch_warps() const
 {
-    // Each resident warp of a multi-stripe class owns a scratch region of 24 bytes per column: two
-    // FP32 rows (one per read of the warp) or one FP64 row.
-    int occ = 1;
+    // Each resident warp of a multi-stripe class owns a scratch row of 24 bytes per column: two
+    // FP32 rows (one per read of the warp) or one FP64 row.  Classes that can run at the same time
+    // need disjoint rows: the FP32 multi-stripe classes run one after another on a chained stream
+    // and share the first region; each FP64 multi-stripe class (inter, intra) has its own, since it
+    // overlaps the FP32 pass.
+    return scratch_offset_warps(3);
+}
+
+uint64_t Engine::scratch_offset_warps(int region) const
+{
+    int occ32 = 1;
     for (int c = 0; c < kClasses32; ++c)
-        if (class32_multi(c)) occ = std::max(occ, occ_[0][c]);
-    for (int c : {class64(kInter, kMaxK, true), class64(kIntra, kMaxK, true)}) occ = std::max(occ, occ_[1][c]);
-    return (uint64_t)sms_ * occ * (kFwdBlock / kWarp);
+        if (class32_multi(c)) occ32 = std::max(occ32, occ_[0][c]);
+    const uint64_t w32 = (uint64_t)sms_ * occ32 * (kFwdBlock / kWarp);
+    const uint64_t w64i = (uint64_t)sms_ * occ_[1][class64(kInter, kMaxK, true)] * (kFwdBlock / kWarp);
+    const uint64_t w64n = (uint64_t)sms_ * occ_[1][class64(kIntra, kMaxK, true)] * (kFwdBlock / kWarp);
+    // region 0: FP32 multi-stripe classes; 1: FP64 inter multi-stripe; 2: FP64 intra multi-stripe
+    if (region == 0) return 0;
+    if (region == 1) return w32;
+    if (region == 2) return w32 + w64i;
+    return w32 + w64i + w64n;
 }
 
 uint64_t Engine::scratch_bytes() const
 {
-    return scratch_warps() * (uint64_t)PlanLimits().max_stream_multi * 3 * sizeof(double);
+    return scratch_offset_warps(3) * (uint64_t)PlanLimits().max_stream_multi * 3 * sizeof(double);
 }
 
 phmm_status Engine::ensure_capacity(Slot& s, const Plan& plan, std::string& err)
@@ -337,6 +351,13 @@ phmm_status Engine::ensure_capacity(Slot& s, const Plan& plan, std::string& err)
     const Capacity need = need_of(plan, scratch_warps());
     if (s.dev && s.cap.covers(need)) return PHMM_OK;
     const Capacity nc = s.dev ? s.cap.grown_to(need) : need;
+    const auto t0 = std::chrono::steady_clock::now();
+    ++s.arena_grows;
+    struct Timer {
+        Slot& s;
+        std::chrono::steady_clock::time_point t0;
+        ~Timer() { s.setup_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count(); }
+    } timer{s, t0};
     PHMM_CK(cudaSetDevice(dev_));
     if (s.main) PHMM_CK(cudaStreamSynchronize(s.main));
     if (s.graph) {
@@ -469,6 +490,7 @@ phmm_status Engine::launch_pipeline(Slot& s, bool want_flags, const Plan* plan, 
     // classes append to, so it waits for those classes only and overlaps with the FP32 classes
     // still running.
     bool launched[kNumClasses] = {};
+    int prev_multi = -1;
     for (int pass = 0; pass < 2; ++pass) {
         const int precision = pass == 0 ? 32 : 64;
         const int n_cls = pass == 0 ? kClasses32 : kClasses64;
@@ -487,10 +509,14 @@ phmm_status Engine::launch_pipeline(Slot& s, bool want_flags, const Plan* plan, 
             pc.items = s.d_items;
             pc.rerun = s.d_rerun;
             pc.status = s.d_status;
-            pc.scratch = s.d_scratch;
+            const bool multi = pass == 0 ? class32_multi(c) : c % 9 == 8;
+            const int region = pass == 0 ? 0 : (c / 9 == kInter ? 1 : 2);
+            pc.scratch = multi ? (void*)((char*)s.d_scratch + scratch_offset_warps(region) * scr_cols * 24) : nullptr;
             pc.scratch_cols = scr_cols;
             cudaStream_t st = s.side[slot0 + c];
             PHMM_CK(cudaStreamWaitEvent(st, s.ev_fork, 0));
+            // FP32 multi-stripe classes share one scratch region: each waits for the previous one
+            if (pass == 0 && multi && prev_multi >= 0) PHMM_CK(cudaStreamWaitEvent(st, s.ev_side[prev_multi], 0));
             if (pass == 1) {
                 bool src[kClasses32];
                 fp64_sources(tiles, c, src);
@@ -501,6 +527,7 @@ phmm_status Engine::launch_pipeline(Slot& s, bool want_flags, const Plan* plan, 
             ++s.launches;
             launched[slot0 + c] = true;
             PHMM_CK(cudaEventRecord(s.ev_side[slot0 + c], st));
+            if (pass == 0 && multi) prev_multi = c;
         }
         for (int c = 0; c < n_cls; ++c)
             if (launched[slot0 + c]) PHMM_CK(cudaStreamWaitEvent(s.main, s.ev_side[slot0 + c], 0));
@@ -523,6 +550,13 @@ phmm_status Engine::capture_graph(Slot& s, bool want_flags, const TileTable& til
         cudaGraphExecDestroy(s.graph);
         s.graph = nullptr;
     }
+    const auto t0 = std::chrono::steady_clock::now();
+    ++s.graph_captures;
+    struct Timer {
+        Slot& s;
+        std::chrono::steady_clock::time_point t0;
+        ~Timer() { s.setup_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count(); }
+    } timer{s, t0};
     cudaGraph_t g = nullptr;
     PHMM_CK(cudaStreamBeginCapture(s.main, cudaStreamCaptureModeThreadLocal));
     std::string lerr;
@@ -798,7 +832,7 @@ phmm_status Engine::time_fp32_class(Slot& s, const Plan& plan, int cls, int reps
     pc.items = s.d_items;
     pc.rerun = s.d_rerun;
     pc.status = s.d_status;
-    pc.scratch = s.d_scratch;
+    pc.scratch = s.d_scratch;  // the FP32 multi-stripe region
     pc.scratch_cols = s.cap.scratch_cols ? (unsigned int)(s.cap.scratch_cols / warps) : 0u;
     const int grid = grid_for(32, cls, plan.classes[cls].n_items);
     cudaStream_t m = s.main;

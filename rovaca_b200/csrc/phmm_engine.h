@@ -67,6 +67,9 @@ struct Slot {
     bool graph_flags = false;        // the captured graph writes pair flags
     TileTable graph_tiles{};         // tile table whose FP64 dependencies the graph encodes
     uint64_t launches = 0;           // kernels launched by the last pipeline run
+    uint64_t arena_grows = 0;        // arena (re)allocations
+    uint64_t graph_captures = 0;
+    double setup_ms = 0.0;           // wall time spent growing the arena and capturing graphs
 };
 
 class Engine {
@@ -124,6 +127,8 @@ private:
     phmm_status capture_graph(Slot& s, bool want_flags, const TileTable& tiles, std::string& err);
     int grid_for(int precision, int cls, uint32_t work) const;
     uint64_t scratch_warps() const;
+    // First warp row of scratch region r (0 FP32 multi-stripe, 1 FP64 inter, 2 FP64 intra; 3: total).
+    uint64_t scratch_offset_warps(int region) const;
 
     phmm_config cfg_{};
     int dev_ = 0;

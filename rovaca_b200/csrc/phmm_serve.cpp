@@ -170,6 +170,9 @@ void Server::worker(int idx)
         }
         if (batch.empty()) continue;
         const auto t_start = Clock::now();
+        const uint64_t grows0 = slot ? slot->arena_grows : 0, caps0 = slot ? slot->graph_captures : 0;
+        const double setup0 = slot ? slot->setup_ms : 0.0;
+        double wait_ms = 0.0;  // time blocked on the device in finish()
         phmm_status st = mk;
         std::string berr = err;
         double device_ms = 0.0;
@@ -275,10 +278,12 @@ void Server::worker(int idx)
             uint8_t* keep = api ? (uint8_t*)(kept_n + batch.size()) : nullptr;
             if (want_flags) flags = (uint8_t*)(best + n_events);  // plain batches have no events
             phmm_stats ps{};
+            const auto t_fin = Clock::now();
             if (st == PHMM_OK)
                 st = eng->finish(*slot, plan, (!api || want_out) ? out : nullptr, flags, &ps, berr, keep, kept_n,
                                  n_events ? gl : nullptr, n_events ? best : nullptr, want_alk ? alk : nullptr);
             device_ms = ps.device_ms;
+            wait_ms = ms_between(t_fin, Clock::now());
             if (st == PHMM_OK) {
                 uint64_t o = 0, ko = 0, go = 0, ao = 0, eo = 0;
                 for (size_t i = 0; i < batch.size(); ++i) {
@@ -321,6 +326,13 @@ void Server::worker(int idx)
             stats.batch_ms += ms_between(t_start, now);
             stats.device_ms += device_ms;
             stats.max_batch_ms = std::max(stats.max_batch_ms, ms_between(t_start, now));
+            if (slot) {
+                stats.arena_grows += slot->arena_grows - grows0;
+                stats.graph_captures += slot->graph_captures - caps0;
+                stats.max_setup_ms = std::max(stats.max_setup_ms, slot->setup_ms - setup0);
+                stats.max_host_ms =
+                    std::max(stats.max_host_ms, ms_between(t_start, now) - wait_ms - (slot->setup_ms - setup0));
+            }
         }
         cv_done.notify_all();
         cv_work.notify_all();
