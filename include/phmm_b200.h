@@ -171,6 +171,12 @@ PHMM_API phmm_status phmm_resident_create(phmm_engine* engine, const phmm_batch*
 PHMM_API phmm_status phmm_resident_run(phmm_resident* resident, int32_t iterations, phmm_stats* stats);
 /* Copies the latest results to the host (layout of phmm_compute_regions; flags may be NULL). */
 PHMM_API phmm_status phmm_resident_results(phmm_resident* resident, double* out, uint8_t* pair_flags);
+/* Runs the resident batch once with every kernel class alone (one after another on one stream,
+ * CUDA events around each launch) for per-kernel timing: class_ms[57] (FP32 classes 0..38, then
+ * FP64 classes; 0 for classes without work) and class_cells[57] (cells of the FP32 classes' work
+ * items; 0 for FP64 classes, whose work is only known on the device).  The results equal those of
+ * phmm_resident_run. */
+PHMM_API phmm_status phmm_resident_profile(phmm_resident* resident, float* class_ms, uint64_t* class_cells);
 PHMM_API phmm_status phmm_resident_destroy(phmm_resident* resident);
 
 /* Measures the device's FP32 FMA throughput (independent FMA chains on every SM, about 0.1 s),

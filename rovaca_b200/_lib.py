@@ -152,6 +152,7 @@ def load() -> C.CDLL:
         "phmm_engine_autotune": (I32, [P, P]),
         "phmm_submit": (I32, [P, C.POINTER(Batch), P, P, C.POINTER(U64)]),
         "phmm_submit_region": (I32, [P, P, P, P, P, C.POINTER(U32), C.POINTER(U64)]),
+        "phmm_resident_profile": (I32, [P, P, P]),
         "phmm_poll": (I32, [P, U64, C.POINTER(I32)]),
         "phmm_wait": (I32, [P, U64, I64, C.POINTER(D), C.POINTER(D)]),
         "phmm_cancel": (I32, [P, U64]),

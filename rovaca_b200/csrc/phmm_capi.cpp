@@ -215,6 +215,33 @@ phmm_status phmm_resident_run(phmm_resident* r, int32_t iterations, phmm_stats* 
     PHMM_GUARD_END
 }
 
+phmm_status phmm_resident_profile(phmm_resident* r, float* class_ms, uint64_t* class_cells)
+{
+    PHMM_GUARD_BEGIN
+    phmm::clear_error();
+    if (!r || !r->slot) return set_error(PHMM_ERR_INVALID_ARGUMENT, "resident is null");
+    if (!class_ms) return set_error(PHMM_ERR_INVALID_ARGUMENT, "class_ms is null");
+    std::string err;
+    phmm_status st = r->eng->profile_classes(*r->slot, r->plan, class_ms, err);
+    if (st != PHMM_OK) return set_error(st, err);
+    if (class_cells) {
+        const phmm::Plan& p = r->plan;
+        for (int c = 0; c < phmm::kNumClasses; ++c) class_cells[c] = 0;
+        for (int c = 0; c < phmm::kClasses32; ++c)
+            for (uint32_t i = p.classes[c].item_off; i < p.classes[c].item_off + p.classes[c].n_items; ++i) {
+                const phmm::WorkItem& it = p.items[i];
+                const phmm::RegionDesc& rg = p.regions[it.region];
+                const uint64_t cols = p.hap_off[rg.hap_begin + it.hap_hi] - p.hap_off[rg.hap_begin + it.hap_lo];
+                uint64_t rows = 0;
+                for (int k = 0; k < 2; ++k)
+                    if (it.read[k] != phmm::kNoRead) rows += p.read_off[it.read[k] + 1] - p.read_off[it.read[k]];
+                class_cells[c] += rows * cols;
+            }
+    }
+    return PHMM_OK;
+    PHMM_GUARD_END
+}
+
 phmm_status phmm_resident_results(phmm_resident* r, double* out, uint8_t* pair_flags)
 {
     PHMM_GUARD_BEGIN

@@ -148,6 +148,25 @@ bool Capacity::covers(const Capacity& o) const
            allele_lk >= o.allele_lk && gl >= o.gl;
 }
 
+Capacity Capacity::max_of(const Capacity& a, const Capacity& b)
+{
+    Capacity c;
+    c.regions = std::max(a.regions, b.regions);
+    c.reads = std::max(a.reads, b.reads);
+    c.haps = std::max(a.haps, b.haps);
+    c.read_bases = std::max(a.read_bases, b.read_bases);
+    c.hap_bases = std::max(a.hap_bases, b.hap_bases);
+    c.items = std::max(a.items, b.items);
+    c.rerun = std::max(a.rerun, b.rerun);
+    c.out = std::max(a.out, b.out);
+    c.scratch_cols = std::max(a.scratch_cols, b.scratch_cols);
+    c.events = std::max(a.events, b.events);
+    c.hap_allele = std::max(a.hap_allele, b.hap_allele);
+    c.allele_lk = std::max(a.allele_lk, b.allele_lk);
+    c.gl = std::max(a.gl, b.gl);
+    return c;
+}
+
 Capacity Capacity::grown_to(const Capacity& need) const
 {
     auto g = [](uint64_t cur, uint64_t want) { return want <= cur ? cur : std::max(want, cur + cur / 2); };
@@ -346,9 +365,16 @@ uint64_t Engine::scratch_bytes() const
     return scratch_offset_warps(3) * (uint64_t)PlanLimits().max_stream_multi * 3 * sizeof(double);
 }
 
+uint64_t Engine::arena_bytes(const Capacity& c) const { return carve(c, nullptr, nullptr); }
+
 phmm_status Engine::ensure_capacity(Slot& s, const Plan& plan, std::string& err)
 {
-    const Capacity need = need_of(plan, scratch_warps());
+    return reserve(s, need_of(plan, scratch_warps()), err);
+}
+
+phmm_status Engine::reserve(Slot& s, const Capacity& want, std::string& err)
+{
+    const Capacity need = Capacity::max_of(want, s.floor);
     if (s.dev && s.cap.covers(need)) return PHMM_OK;
     const Capacity nc = s.dev ? s.cap.grown_to(need) : need;
     const auto t0 = std::chrono::steady_clock::now();
@@ -856,6 +882,77 @@ phmm_status Engine::time_fp32_class(Slot& s, const Plan& plan, int cls, int reps
         return PHMM_ERR_DEVICE_STATUS;
     }
     *best_ms = best;
+    return PHMM_OK;
+}
+
+phmm_status Engine::profile_classes(Slot& s, const Plan& plan, float* class_ms, std::string& err)
+{
+    PHMM_CK(cudaSetDevice(dev_));
+    cudaStream_t m = s.main;
+    BatchView v{};
+    v.read_bases = s.d_rb;
+    v.read_q = s.d_rq;
+    v.read_i = s.d_ri;
+    v.read_d = s.d_rd;
+    v.read_c = s.d_rc;
+    v.read_off = s.d_read_off;
+    v.read_flags = s.d_read_flags;
+    v.hap_off = s.d_hap_off;
+    v.codes_inter = s.d_codes_inter;
+    v.codes_intra = s.d_codes_intra;
+    v.hap_flags = s.d_hap_flags;
+    v.regions = s.d_regions;
+    v.out = s.d_out;
+    v.pair_flags = s.d_pair_flags;
+    const uint64_t warps = scratch_warps();
+    const unsigned int scr_cols = s.cap.scratch_cols ? (unsigned int)(s.cap.scratch_cols / warps) : 0u;
+    std::vector<cudaEvent_t> ev(2 * kNumClasses, nullptr);
+    for (auto& e : ev) PHMM_CK(cudaEventCreate(&e));
+    struct Cleanup {
+        std::vector<cudaEvent_t>& ev;
+        ~Cleanup()
+        {
+            for (auto e : ev)
+                if (e) cudaEventDestroy(e);
+        }
+    } cleanup{ev};
+    PHMM_CK(cudaMemcpyAsync(s.d_desc, s.d_desc_pristine, kDescBytes, cudaMemcpyDeviceToDevice, m));
+    PHMM_CK(launch_prep(s.d_desc, s.d_hb, s.d_codes_inter, s.d_codes_intra, s.d_out, v.pair_flags, sms_, m));
+    const RegionApiView rv = region_view(s, d_jacobian_, log10_two_);
+    if (plan.region_api) PHMM_CK(launch_read_prep(rv, sms_, m));
+    bool ran[kNumClasses] = {};
+    for (int pass = 0; pass < 2; ++pass) {
+        const int precision = pass == 0 ? 32 : 64;
+        const int n_cls = pass == 0 ? kClasses32 : kClasses64;
+        const int slot0 = pass == 0 ? 0 : kClasses32;
+        for (int c = 0; c < n_cls; ++c) {
+            const uint32_t work = pass == 0 ? plan.classes[c].n_items : plan.classes[slot0 + c].rerun_cap;
+            if (work == 0) continue;
+            const bool multi = pass == 0 ? class32_multi(c) : c % 9 == 8;
+            const int region = pass == 0 ? 0 : (c / 9 == kInter ? 1 : 2);
+            PassControl pc;
+            pc.cd = s.d_classes + slot0 + c;
+            pc.cd64 = s.d_classes + kClasses32;
+            pc.items = s.d_items;
+            pc.rerun = s.d_rerun;
+            pc.status = s.d_status;
+            pc.scratch = multi ? (void*)((char*)s.d_scratch + scratch_offset_warps(region) * scr_cols * 24) : nullptr;
+            pc.scratch_cols = scr_cols;
+            PHMM_CK(cudaEventRecord(ev[2 * (slot0 + c)], m));
+            PHMM_CK(launch_fwd(precision, c, v, tf_, td_, pc, grid_for(precision, c, work), m));
+            PHMM_CK(cudaEventRecord(ev[2 * (slot0 + c) + 1], m));
+            ran[slot0 + c] = true;
+        }
+    }
+    if (plan.region_api) {
+        PHMM_CK(launch_post_region(rv, sms_, m));
+        if (!plan.events.empty()) PHMM_CK(launch_genotype(rv, sms_, m));
+    }
+    PHMM_CK(cudaStreamSynchronize(m));
+    for (int c = 0; c < kNumClasses; ++c) {
+        class_ms[c] = 0.f;
+        if (ran[c]) PHMM_CK(cudaEventElapsedTime(&class_ms[c], ev[2 * c], ev[2 * c + 1]));
+    }
     return PHMM_OK;
 }
 

@@ -23,6 +23,7 @@ struct Capacity {
     uint64_t events = 0, hap_allele = 0, allele_lk = 0, gl = 0;
     bool covers(const Capacity& o) const;
     Capacity grown_to(const Capacity& need) const;
+    static Capacity max_of(const Capacity& a, const Capacity& b);
 };
 
 // One device arena with everything a batch needs, plus its streams, events and captured graph.
@@ -33,6 +34,7 @@ struct Slot {
     char* pinned = nullptr;          // pinned host staging for the plan arrays and descriptors
     size_t pinned_bytes = 0;
     Capacity cap;
+    Capacity floor;                  // the arena is never sized below this (serving slots pre-size)
     // carved device pointers
     BatchDesc* d_desc = nullptr;
     char* d_desc_pristine = nullptr;  // the batch's descriptor block as uploaded, for replays
@@ -97,6 +99,8 @@ public:
     // restore = true resetting the descriptor from its pristine device copy first (replays).
     phmm_status upload(Slot& s, const Plan& plan, const phmm_batch& b, std::string& err,
                        const uint8_t* mapq = nullptr);
+    // Allocates the slot's arena for at least capacity c now (no-op if it already covers it).
+    phmm_status reserve(Slot& s, const Capacity& c, std::string& err);
     phmm_status run(Slot& s, const Plan& plan, bool want_flags, bool restore, std::string& err);
     phmm_status fp32_fma_peak(double* scalar_tflops, double* packed_tflops, std::string& err);
 
@@ -110,6 +114,9 @@ public:
         l.tiles = &t;
         return l;
     }
+    // Runs an uploaded plan once with every class alone on the slot's main stream, timing each
+    // launch with CUDA events (class_ms[kNumClasses], 0 where a class has no work).
+    phmm_status profile_classes(Slot& s, const Plan& plan, float* class_ms, std::string& err);
     // Measures the FP32 pass of one class alone on an uploaded plan: best of `reps` launches (ms).
     phmm_status time_fp32_class(Slot& s, const Plan& plan, int cls, int reps, float* best_ms, std::string& err);
     // Runs the tile-shape autotuner and installs its table (phmm_tune.cpp).
@@ -119,6 +126,7 @@ public:
     int num_sms() const { return sms_; }
     const phmm_config& config() const { return cfg_; }
     uint64_t scratch_bytes() const;  // device bytes of the stripe scratch rows (multi-stripe reads)
+    uint64_t arena_bytes(const Capacity& c) const;  // device bytes of an arena of capacity c
 
 private:
     Engine() = default;

@@ -132,11 +132,37 @@ void Server::worker(int idx)
     Slot* slot = nullptr;
     std::string err;
     const phmm_status mk = eng->make_slot(idx + 1, &slot, err);
+    // Pre-size the slot for a full batch (kMaxBatchCells of benchmark-shaped regions, about 700),
+    // when the budget allows: an arena that grows while other slots' batches run has to wait for
+    // them (freeing device or pinned memory synchronises the device) and capture its graph again.
+    Capacity floor;
+    floor.regions = 4096;
+    floor.reads = 256u << 10;
+    floor.haps = 64u << 10;
+    floor.read_bases = 48ull << 20;
+    floor.hap_bases = 16ull << 20;
+    floor.items = 256u << 10;
+    floor.rerun = floor.out = 4ull << 20;
+    floor.events = 64u << 10;
+    floor.hap_allele = 2ull << 20;
+    floor.allele_lk = 8ull << 20;
+    floor.gl = 1ull << 20;
+    const size_t in_floor = floor.hap_bases + 5 * floor.read_bases + floor.reads;
+    const size_t out_floor = floor.out * 9 + (floor.gl + floor.allele_lk) * 8 + floor.reads * 2;
+    if (slot && eng->arena_bytes(floor) + in_floor <= budget / kSlots) {
+        slot->floor = floor;
+        std::string rerr;
+        if (eng->reserve(*slot, floor, rerr) != PHMM_OK) slot->floor = Capacity();  // grow on demand instead
+    }
     std::vector<std::shared_ptr<Request>> batch;
     std::vector<uint32_t> nh, nr;
     std::vector<uint64_t> hoff, roff;
     std::vector<RegionApiParams> params;
     PinnedBuf in_buf, out_buf;
+    if (slot && slot->floor.read_bases) {
+        in_buf.reserve(in_floor);
+        out_buf.reserve(out_floor);
+    }
     for (;;) {
         batch.clear();
         uint64_t batch_bytes = 0, hap_total = 0, read_total = 0, out_total = 0, cells = 0;

@@ -436,6 +436,14 @@ class ResidentBatch:
         check(self._lib.phmm_resident_run(self._h, iterations, C.byref(st)))
         return st.as_dict()
 
+    def profile(self) -> dict:
+        """phmm_resident_profile: every kernel class alone, timed with CUDA events; returns
+        class_ms and class_cells (FP32 classes first, then FP64) as arrays."""
+        ms = np.zeros(_lib.FP32_CLASSES + _lib.FP64_CLASSES, np.float32)
+        cells = np.zeros(_lib.FP32_CLASSES + _lib.FP64_CLASSES, np.uint64)
+        check(self._lib.phmm_resident_profile(self._h, _ptr(ms), _ptr(cells)))
+        return {"class_ms": ms, "class_cells": cells}
+
     def results(self):
         out = np.empty(self.batch.out_size, np.float64)
         fl = np.empty(self.batch.out_size, np.uint8) if self.want_flags else None
