@@ -254,6 +254,22 @@ def underflow_stress(engine, n_regions: int = 100, sample: int = 2) -> dict:
                                       "sample_pairs": int(err.size)}}
 
 
+def wgs_mixture(engine, fraction: float = 0.05) -> dict:
+    """A seeded share of the WGS-like mixture (depth lognormal, median 60, sigma 0.5, clipped to
+    [5, 2000]; 150 bp reads (90%) or 250 bp; haplotypes geometric, mean 6, max 128, of 200-1,200 bp;
+    2% of regions from the underflow-stress regime): batched GCUPS end to end from pinned buffers."""
+    from rovaca_b200 import synth
+
+    pb = synth.make(4, scale=fraction, seed=4).pinned()
+    engine.compute(pb)
+    t = time.perf_counter()
+    _, _, st = engine.compute(pb)
+    el = time.perf_counter() - t
+    return {"regions": int(pb.n_regions), "cells": int(st["cells"]), "share_of_200k_regions": fraction,
+            "gcups_e2e": round(st["cells"] / el / 1e9, 1), "gcups_device": round(st["cells"] / st["device_ms"] / 1e6, 1),
+            "fp64_pairs": int(st["pairs_f64"]), "pairs": int(st["pairs"])}
+
+
 def genotyping_run(engine, n_regions: int = 400, check: int = 20) -> dict:
     """Region API with genotyping events on the GPU (read preparation, likelihoods, normalise and
     filter, allele marginalisation, diploid genotype likelihoods, calls): throughput through the
@@ -433,6 +449,7 @@ def run_ours(args, rank: int, world: int, dist) -> None:
         lat = [serving_latency(engine, batch, load, cap, args.serve_seconds, seed=rank)
                for load in (0.25, 0.5, 0.8, 0.95)]
         stress = underflow_stress(engine)
+        wgs = wgs_mixture(engine)
         geno = genotyping_run(engine)
 
         # roofline of the FP32 wavefront pass against the measured FP32 FMA peak
@@ -509,6 +526,7 @@ def run_ours(args, rank: int, world: int, dist) -> None:
             "latency": next(x for x in lat if x["load"] == 0.8),
             "latency_by_load": lat,
             "underflow_stress": stress,
+            "wgs_mixture": wgs,
             "genotyping": geno,
         }
     engine.close()
