@@ -101,17 +101,18 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def traffic_from_profiles() -> float | None:
-    """DRAM bytes per FP32-pass launch from the committed ncu summary (None if not captured)."""
-    p = ROOT / "profiles" / "fwd_f32_config1.md"
-    if not p.exists():
-        return None
-    for line in p.read_text().splitlines():
-        if line.strip().startswith("traffic_bytes_per_pass:"):
-            try:
-                return float(line.split(":", 1)[1].strip().split()[0])
-            except ValueError:
-                return None
+def traffic_from_profiles(kernel_class: int) -> float | None:
+    """DRAM bytes per launch of the dominant FP32 kernel from the committed ncu summary, when that
+    summary covers the same kernel class (None otherwise)."""
+    for p in sorted((ROOT / "profiles").glob("fwd_f32_*.md")):
+        cls, traffic = None, None
+        for line in p.read_text().splitlines():
+            if line.startswith("class:"):
+                cls = int(line.split(":", 1)[1])
+            if line.startswith("traffic_bytes_per_launch:"):
+                traffic = float(line.split(":", 1)[1])
+        if cls == kernel_class and traffic is not None:
+            return traffic
     return None
 
 
@@ -468,7 +469,7 @@ def run_ours(args, rank: int, world: int, dist) -> None:
         kh, multi = (shape + 1, False) if shape < 8 else (shape - 4, True)
         dom_name = (f"fwd_f32 class {dom}: {mode_names[dom // 13]}, {kh} row pairs per lane"
                     f"{', multi-stripe' if multi else ''}")
-        traffic = traffic_from_profiles()
+        traffic = traffic_from_profiles(dom)
 
         # CPU baseline: the reference's own PairHMM on all host cores, bounded sample
         cpu = None

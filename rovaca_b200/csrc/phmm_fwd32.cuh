@@ -58,8 +58,22 @@ __device__ __forceinline__ void run_pair2(const BatchView& b, const ProbTables<f
     }
 }
 
+// Resident warps per SM the compiler is asked to allow for the wide shapes (KH >= 6), whose natural
+// register count (170-230 per thread) leaves two warps per scheduler: each scheduler's sub-partition
+// holds 16K registers, so 168 registers per thread are the most that fit three warps.  A build-time
+// setting (1 leaves the compiler free).
+#ifndef PHMM_WIDE_MIN_WARPS
+#define PHMM_WIDE_MIN_WARPS 1
+#endif
+template <int KH>
+constexpr int min_blocks32()
+{
+    return KH >= 6 ? PHMM_WIDE_MIN_WARPS : 1;
+}
+
 template <int KH, int V, int PM, bool MULTI>
-__global__ void __launch_bounds__(kFwdBlock, 1) fwd_f32_kernel(BatchView b, ProbTables<float> tb, PassControl pc)
+__global__ void __launch_bounds__(kFwdBlock, min_blocks32<KH>()) fwd_f32_kernel(BatchView b, ProbTables<float> tb,
+                                                                                 PassControl pc)
 {
     const int lane = threadIdx.x & (kWarp - 1);
     const int group = lane / kLanesPerRead;
