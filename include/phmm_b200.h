@@ -172,8 +172,8 @@ PHMM_API phmm_status phmm_resident_run(phmm_resident* resident, int32_t iteratio
 /* Copies the latest results to the host (layout of phmm_compute_regions; flags may be NULL). */
 PHMM_API phmm_status phmm_resident_results(phmm_resident* resident, double* out, uint8_t* pair_flags);
 /* Runs the resident batch once with every kernel class alone (one after another on one stream,
- * CUDA events around each launch) for per-kernel timing: class_ms[57] (FP32 classes 0..38, then
- * FP64 classes; 0 for classes without work) and class_cells[57] (cells of the FP32 classes' work
+ * CUDA events around each launch) for per-kernel timing: class_ms[66] (FP32 classes 0..38, then
+ * FP64 classes; 0 for classes without work) and class_cells[66] (cells of the FP32 classes' work
  * items; 0 for FP64 classes, whose work is only known on the device).  The results equal those of
  * phmm_resident_run. */
 PHMM_API phmm_status phmm_resident_profile(phmm_resident* resident, float* class_ms, uint64_t* class_cells);
@@ -208,11 +208,12 @@ PHMM_API void phmm_host_normalize_filter(const double* lk_hap_read, uint32_t n_h
  *   shape: rows_per_lane KH (16 lanes per read hold 32 * KH rows) in one stripe (KH >= b), or
  *          multi_stripe with 4 <= KH < b, the read running as ceil(length / (32 * KH)) stripes.
  * FP32 kernel class = mode * 13 + (multi_stripe ? 4 + KH : KH - 1); FP64 recompute class =
- * ('N' ? 9 : 0) + (length > 256 ? 8 : b - 1).  Results do not depend on the shapes. */
+ * mode * 9 + (length > 256 ? 8 : b - 1), the mode of the FP32 class that ran the pair.  Results do
+ * not depend on the shapes. */
 #define PHMM_TILE_MODES 3
 #define PHMM_LEN_BUCKETS 24
 #define PHMM_FP32_CLASSES 39
-#define PHMM_FP64_CLASSES 18
+#define PHMM_FP64_CLASSES 27
 
 typedef struct phmm_tile_table {
     uint8_t rows_per_lane[PHMM_TILE_MODES][PHMM_LEN_BUCKETS];
@@ -250,7 +251,7 @@ PHMM_API phmm_status phmm_engine_autotune(phmm_engine* engine, phmm_tune_report*
  * (NULL: the default table):
  *   class_items[39]: work items per FP32 kernel class (numbering above); an item is two reads (one
  *     when a region has an odd count) of one shape against a haplotype run;
- *   class_pairs[18]: pairs per FP64 recompute class (the capacity reserved for pairs that
+ *   class_pairs[27]: pairs per FP64 recompute class (the capacity reserved for pairs that
  *     underflow in FP32);
  *   pairs, cells: totals of the batch.
  * Returns the same validation status phmm_compute_regions would. */

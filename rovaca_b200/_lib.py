@@ -52,7 +52,7 @@ class Stats(C.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
-TILE_MODES, LEN_BUCKETS, FP32_CLASSES, FP64_CLASSES = 3, 24, 39, 18
+TILE_MODES, LEN_BUCKETS, FP32_CLASSES, FP64_CLASSES = 3, 24, 39, 27
 
 
 class TileTable(C.Structure):

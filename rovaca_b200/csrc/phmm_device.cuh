@@ -88,42 +88,65 @@ __device__ __forceinline__ T shfl_up1(T v)
     return __shfl_up_sync(0xffffffffu, v, 1);
 }
 
+// Gap parameters: PM_ALL when a read's insertion, deletion and gap-continuation qualities are each
+// constant along it, PM_ROW otherwise.  In PM_ALL, mm, gapm, mx and my are held once per lane
+// instead of once per row (xx stays per row: pad rows need xx = 1), which frees registers.
+enum ParamMode : int { PM_ALL = 0, PM_ROW = 1 };
+
 // One lane's rows of the current stripe.
-template <typename T, int K>
+template <typename T, int K, int PM>
 struct LaneRows {
+    static constexpr int NR = PM == PM_ROW ? K : 1;
     T Mp[K], Ip[K], Dp[K];        // values at the previous column
-    T pa[K], pb[K], mm[K], gm[K], mx[K], xx[K], my[K];
+    T pa[K], pb[K], xx[K];
+    T mm[NR], gm[NR], mx[NR], my[NR];
     uint32_t rc[K];
     uint32_t padmask;             // bit k: slot k is a pad row
 };
 
-template <typename T, int K, int V>
-__device__ __forceinline__ void load_rows(LaneRows<T, K>& L, const BatchView& b, const ProbTables<T>& tb,
+template <typename T, int K, int V, int PM>
+__device__ __forceinline__ void load_rows(LaneRows<T, K, PM>& L, const BatchView& b, const ProbTables<T>& tb,
                                           uint64_t roff, int R, int first_padded_row, int pad, int lane)
 {
     L.padmask = 0;
+    if (PM == PM_ALL) {
+        // constant along the read: its first row gives them (pad rows ignore them)
+        const uint64_t o = roff;
+        const int iq = R > 0 ? b.read_i[o] & 127 : 0, dq = R > 0 ? b.read_d[o] & 127 : 0;
+        const int c = R > 0 ? b.read_c[o] & 127 : 0;
+        L.mm[0] = tb.mm[iq * 128 + dq];
+        L.gm[0] = tb.gapm[c];
+        L.mx[0] = tb.ph2pr[iq];
+        L.my[0] = tb.ph2pr[dq];
+    }
 #pragma unroll
     for (int k = 0; k < K; ++k) {
         const int i = first_padded_row + lane * K + k - pad;  // 0-based read position
+        const int r = PM == PM_ROW ? k : 0;
         if (i >= 0 && i < R) {
             const uint64_t o = roff + (uint64_t)i;
-            const int q = b.read_q[o] & 127, iq = b.read_i[o] & 127, dq = b.read_d[o] & 127, c = b.read_c[o] & 127;
+            const int q = b.read_q[o] & 127, c = b.read_c[o] & 127;
             L.pa[k] = tb.pmat[q];
             L.pb[k] = (V == kInter) ? tb.pmis_inter[q] : tb.pmis_intra[q];
-            L.mm[k] = tb.mm[iq * 128 + dq];
-            L.gm[k] = tb.gapm[c];
-            L.mx[k] = tb.ph2pr[iq];
             L.xx[k] = tb.ph2pr[c];
-            L.my[k] = tb.ph2pr[dq];
+            if (PM == PM_ROW) {
+                const int iq = b.read_i[o] & 127, dq = b.read_d[o] & 127;
+                L.mm[r] = tb.mm[iq * 128 + dq];
+                L.gm[r] = tb.gapm[c];
+                L.mx[r] = tb.ph2pr[iq];
+                L.my[r] = tb.ph2pr[dq];
+            }
             L.rc[k] = match_code(b.read_bases[o], V);
         } else {
             L.pa[k] = T(0);
             L.pb[k] = T(0);
-            L.mm[k] = T(0);
-            L.gm[k] = T(0);
-            L.mx[k] = T(0);
             L.xx[k] = T(1);
-            L.my[k] = T(0);
+            if (PM == PM_ROW) {
+                L.mm[r] = T(0);
+                L.gm[r] = T(0);
+                L.mx[r] = T(0);
+                L.my[r] = T(0);
+            }
             L.rc[k] = 0u;
             L.padmask |= 1u << k;
         }
@@ -131,23 +154,26 @@ __device__ __forceinline__ void load_rows(LaneRows<T, K>& L, const BatchView& b,
 }
 
 // Compute column p for all K rows of this lane.  (sM, sI, sD): the row above this lane's first
-// row at column p; (dM, dI, dD): the same row at column p-1.
-template <typename T, int K, int V>
-__device__ __forceinline__ void cells(LaneRows<T, K>& L, uint32_t hc, T sM, T sI, T dM, T dI, T dD)
+// row at column p; (dM, dI, dD): the same row at column p-1.  In PM_ALL pad rows share the lane's
+// gap parameters: their prior 0 keeps M = 0, their I stays 0 (the rows above are pad or boundary
+// rows with M = I = 0) and xx = 1 keeps D, so they still reproduce the boundary row.
+template <typename T, int K, int V, int PM>
+__device__ __forceinline__ void cells(LaneRows<T, K, PM>& L, uint32_t hc, T sM, T sI, T dM, T dI, T dD)
 {
     T diM = dM, diI = dI, diD = dD, upM = sM, upI = sI;
 #pragma unroll
     for (int k = 0; k < K; ++k) {
+        const int r = PM == PM_ROW ? k : 0;
         const T oM = L.Mp[k], oI = L.Ip[k], oD = L.Dp[k];
         const T prior = codes_match(hc, L.rc[k], V) ? L.pa[k] : L.pb[k];
         T s;
         if (V == kInter)
-            s = ftz(rfma(diD, L.gm[k], ftz(rfma(diM, L.mm[k], ftz(rmul(diI, L.gm[k]))))));
+            s = ftz(rfma(diD, L.gm[r], ftz(rfma(diM, L.mm[r], ftz(rmul(diI, L.gm[r]))))));
         else
-            s = ftz(rfma(diD, L.gm[k], ftz(rfma(diI, L.gm[k], ftz(rmul(diM, L.mm[k]))))));
+            s = ftz(rfma(diD, L.gm[r], ftz(rfma(diI, L.gm[r], ftz(rmul(diM, L.mm[r]))))));
         const T nM = ftz(rmul(s, prior));
-        const T nI = ftz(rfma(upI, L.xx[k], ftz(rmul(upM, L.mx[k]))));
-        const T nD = ftz(rfma(oD, L.xx[k], ftz(rmul(oM, L.my[k]))));
+        const T nI = ftz(rfma(upI, L.xx[k], ftz(rmul(upM, L.mx[r]))));
+        const T nD = ftz(rfma(oD, L.xx[k], ftz(rmul(oM, L.my[r]))));
         L.Mp[k] = nM;
         L.Ip[k] = nI;
         L.Dp[k] = nD;
@@ -171,8 +197,8 @@ struct SweepOut {
 //   FROM_SCR: the row above the stripe comes from scratch (stripe > 0), else the boundary row.
 //   TO_SCR:   the stripe's bottom row goes to scratch (not the last stripe), else it is summed.
 //   above_row0: the row above this lane's first slot is the boundary row 0 or a pad row.
-template <typename T, int K, int V, bool FROM_SCR, bool TO_SCR>
-__device__ void sweep(LaneRows<T, K>& L, const BatchView& b, const PassControl& pc, const SweepOut& so, uint32_t g_lo,
+template <typename T, int K, int V, int PM, bool FROM_SCR, bool TO_SCR>
+__device__ void sweep(LaneRows<T, K, PM>& L, const BatchView& b, const PassControl& pc, const SweepOut& so, uint32_t g_lo,
                       uint32_t g_hi, T* scr, int lane, bool above_row0)
 {
     const uint64_t s0 = b.hap_off[g_lo];
@@ -243,7 +269,7 @@ __device__ void sweep(LaneRows<T, K>& L, const BatchView& b, const PassControl& 
             }
         }
         const uint32_t hc = codes[p];
-        cells<T, K, V>(L, hc, sM, sI, dM, dI, dD);
+        cells<T, K, V, PM>(L, hc, sM, sI, dM, dI, dD);
         dM = sM;
         dI = sI;
         dD = sD;

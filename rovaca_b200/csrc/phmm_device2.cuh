@@ -29,7 +29,6 @@
 namespace phmm {
 
 constexpr int kLanesPerRead = 16;
-enum ParamMode : int { PM_ALL = 0, PM_ROW = 1 };
 
 __device__ __forceinline__ float2 f2(float x, float y) { return make_float2(x, y); }
 __device__ __forceinline__ float2 rmul2(float2 a, float2 b) { return __fmul2_rn(a, b); }

@@ -340,29 +340,29 @@ uint64_t Engine::scratch_warps() const
     // Each resident warp of a multi-stripe class owns a scratch row of 24 bytes per column: two
     // FP32 rows (one per read of the warp) or one FP64 row.  Classes that can run at the same time
     // need disjoint rows: the FP32 multi-stripe classes run one after another on a chained stream
-    // and share the first region; each FP64 multi-stripe class (inter, intra) has its own, since it
+    // and share the first region; each FP64 multi-stripe class (one per mode) has its own, since it
     // overlaps the FP32 pass.
-    return scratch_offset_warps(3);
+    return scratch_offset_warps(1 + kModes32);
 }
 
 uint64_t Engine::scratch_offset_warps(int region) const
 {
+    // region 0: FP32 multi-stripe classes; 1 + m: the FP64 multi-stripe class of mode m
     int occ32 = 1;
     for (int c = 0; c < kClasses32; ++c)
         if (class32_multi(c)) occ32 = std::max(occ32, occ_[0][c]);
-    const uint64_t w32 = (uint64_t)sms_ * occ32 * (kFwdBlock / kWarp);
-    const uint64_t w64i = (uint64_t)sms_ * occ_[1][class64(kInter, kMaxK, true)] * (kFwdBlock / kWarp);
-    const uint64_t w64n = (uint64_t)sms_ * occ_[1][class64(kIntra, kMaxK, true)] * (kFwdBlock / kWarp);
-    // region 0: FP32 multi-stripe classes; 1: FP64 inter multi-stripe; 2: FP64 intra multi-stripe
+    uint64_t at = (uint64_t)sms_ * occ32 * (kFwdBlock / kWarp);
     if (region == 0) return 0;
-    if (region == 1) return w32;
-    if (region == 2) return w32 + w64i;
-    return w32 + w64i + w64n;
+    for (int m = 0; m < kModes32; ++m) {
+        if (region == 1 + m) return at;
+        at += (uint64_t)sms_ * occ_[1][class64(m, kMaxK, true)] * (kFwdBlock / kWarp);
+    }
+    return at;
 }
 
 uint64_t Engine::scratch_bytes() const
 {
-    return scratch_offset_warps(3) * (uint64_t)PlanLimits().max_stream_multi * 3 * sizeof(double);
+    return scratch_warps() * (uint64_t)PlanLimits().max_stream_multi * 3 * sizeof(double);
 }
 
 uint64_t Engine::arena_bytes(const Capacity& c) const { return carve(c, nullptr, nullptr); }
@@ -457,23 +457,20 @@ RegionApiView region_view(const Slot& s, const double* jacobian, double log10_tw
     return rv;
 }
 
-// FP32 classes that can append reruns to FP64 class c64 under tile table t: the shapes of every
-// read-length bucket whose reads belong to c64, in each mode that can produce the class's variant
-// (a read without 'N' runs in the intra variant against haplotypes with 'N').
+// FP32 classes that can append reruns to FP64 class c64 under tile table t: the FP32 classes of the
+// same mode running the shapes of every read-length bucket whose reads belong to c64.  The intra
+// mode takes reads of every mode's table (a read without 'N' runs intra against haplotypes with 'N').
 void fp64_sources(const TileTable& t, int c64, bool src[kClasses32])
 {
     for (int c = 0; c < kClasses32; ++c) src[c] = false;
-    const int variant = c64 / 9;
+    const int mode = c64 / 9;
     for (int b = 1; b <= kLenBuckets; ++b) {
-        if (class64_for_len(variant, (uint64_t)b * kWarp) != c64) continue;
+        if (class64_for_len(mode, (uint64_t)b * kWarp) != c64) continue;
         for (int m = 0; m < kModes32; ++m) {
+            if (mode != 2 && m != mode) continue;
             const int kh = t.kh[m][b - 1];
             const bool multi = t.multi[m][b - 1] != 0;
-            if (variant == kInter) {
-                if (m < 2) src[class32(kInter, m, kh, multi)] = true;
-            } else {
-                src[class32(kIntra, 1, kh, multi)] = true;
-            }
+            src[mode * kShapes32 + shape32(kh, multi)] = true;
         }
     }
 }
@@ -536,7 +533,7 @@ phmm_status Engine::launch_pipeline(Slot& s, bool want_flags, const Plan* plan, 
             pc.rerun = s.d_rerun;
             pc.status = s.d_status;
             const bool multi = pass == 0 ? class32_multi(c) : c % 9 == 8;
-            const int region = pass == 0 ? 0 : (c / 9 == kInter ? 1 : 2);
+            const int region = pass == 0 ? 0 : 1 + c / 9;
             pc.scratch = multi ? (void*)((char*)s.d_scratch + scratch_offset_warps(region) * scr_cols * 24) : nullptr;
             pc.scratch_cols = scr_cols;
             cudaStream_t st = s.side[slot0 + c];
@@ -929,7 +926,7 @@ phmm_status Engine::profile_classes(Slot& s, const Plan& plan, float* class_ms, 
             const uint32_t work = pass == 0 ? plan.classes[c].n_items : plan.classes[slot0 + c].rerun_cap;
             if (work == 0) continue;
             const bool multi = pass == 0 ? class32_multi(c) : c % 9 == 8;
-            const int region = pass == 0 ? 0 : (c / 9 == kInter ? 1 : 2);
+            const int region = pass == 0 ? 0 : 1 + c / 9;
             PassControl pc;
             pc.cd = s.d_classes + slot0 + c;
             pc.cd64 = s.d_classes + kClasses32;

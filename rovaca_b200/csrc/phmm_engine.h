@@ -135,7 +135,8 @@ private:
     phmm_status capture_graph(Slot& s, bool want_flags, const TileTable& tiles, std::string& err);
     int grid_for(int precision, int cls, uint32_t work) const;
     uint64_t scratch_warps() const;
-    // First warp row of scratch region r (0 FP32 multi-stripe, 1 FP64 inter, 2 FP64 intra; 3: total).
+    // First warp row of scratch region r (0: FP32 multi-stripe classes, 1 + m: the FP64 multi-stripe
+    // class of mode m; 1 + kModes32: the total).
     uint64_t scratch_offset_warps(int region) const;
 
     phmm_config cfg_{};

@@ -36,9 +36,9 @@ __device__ __forceinline__ void run_pair2(const BatchView& b, const ProbTables<f
         if (lane == 0) atomicOr(pc.status, kStatusBadItem);
         return;
     }
-    // underflowed pairs go to the FP64 class of this read's length
+    // underflowed pairs go to the FP64 class of this mode and this read's length
     PassControl pr = pc;
-    pr.cd = pc.cd64 + class64_for_len(V, (uint64_t)R);
+    pr.cd = pc.cd64 + class64_for_len(mode32(V, PM), (uint64_t)R);
     const int pad = SR * S - R;
     if (!MULTI) {
         load_rows2<KH, V, PM>(L, b, tb, roff, R, 0, pad, l);
@@ -60,10 +60,11 @@ __device__ __forceinline__ void run_pair2(const BatchView& b, const ProbTables<f
 
 // Resident warps per SM the compiler is asked to allow for the wide shapes (KH >= 6), whose natural
 // register count (170-230 per thread) leaves two warps per scheduler: each scheduler's sub-partition
-// holds 16K registers, so 168 registers per thread are the most that fit three warps.  A build-time
-// setting (1 leaves the compiler free).
+// holds 16K registers, so 168 registers per thread are the most that fit three warps.  Measured on
+// B200 over the 2,000-region batch: 12 warps per SM (a few bytes of spills at KH 7-8) take the FP32
+// pass from 242 to 235 ms.  A build-time setting (1 leaves the compiler free).
 #ifndef PHMM_WIDE_MIN_WARPS
-#define PHMM_WIDE_MIN_WARPS 1
+#define PHMM_WIDE_MIN_WARPS 12
 #endif
 template <int KH>
 constexpr int min_blocks32()

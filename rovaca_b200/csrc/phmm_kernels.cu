@@ -54,11 +54,11 @@ __global__ void reset_outputs_kernel(const BatchDesc* __restrict__ desc, double*
 // ------------------------------------------------------------------------------------------
 // One read against a run of haplotypes [g_lo, g_hi).
 // ------------------------------------------------------------------------------------------
-template <typename T, int K, int V, bool MULTI>
+template <typename T, int K, int V, int PM, bool MULTI>
 __device__ __forceinline__ void run_read(const BatchView& b, const ProbTables<T>& tb, const PassControl& pc,
                                          const SweepOut& so, uint32_t g_lo, uint32_t g_hi, int lane, T* scr)
 {
-    LaneRows<T, K> L;
+    LaneRows<T, K, PM> L;
     const uint64_t roff = b.read_off[so.read];
     const int R = (int)(b.read_off[so.read + 1] - roff);
     const int Tcols = (int)(b.hap_off[g_hi] - b.hap_off[g_lo]);
@@ -70,21 +70,21 @@ __device__ __forceinline__ void run_read(const BatchView& b, const ProbTables<T>
     }
     if (!MULTI) {
         const int pad = kWarp * K - R;
-        load_rows<T, K, V>(L, b, tb, roff, R, 0, pad, lane);
-        sweep<T, K, V, false, false>(L, b, pc, so, g_lo, g_hi, scr, lane, lane * K <= pad);
+        load_rows<T, K, V, PM>(L, b, tb, roff, R, 0, pad, lane);
+        sweep<T, K, V, PM, false, false>(L, b, pc, so, g_lo, g_hi, scr, lane, lane * K <= pad);
     } else {
         constexpr int SR = kWarp * K;  // rows per stripe
         const int stripes = (R + SR - 1) / SR;
         const int pad = SR * stripes - R;
         for (int s = 0; s < stripes; ++s) {
-            load_rows<T, K, V>(L, b, tb, roff, R, s * SR, pad, lane);
+            load_rows<T, K, V, PM>(L, b, tb, roff, R, s * SR, pad, lane);
             const bool above_row0 = (s == 0) && (lane * K <= pad);
             if (s == 0)
-                sweep<T, K, V, false, true>(L, b, pc, so, g_lo, g_hi, scr, lane, above_row0);
+                sweep<T, K, V, PM, false, true>(L, b, pc, so, g_lo, g_hi, scr, lane, above_row0);
             else if (s == stripes - 1)
-                sweep<T, K, V, true, false>(L, b, pc, so, g_lo, g_hi, scr, lane, above_row0);
+                sweep<T, K, V, PM, true, false>(L, b, pc, so, g_lo, g_hi, scr, lane, above_row0);
             else
-                sweep<T, K, V, true, true>(L, b, pc, so, g_lo, g_hi, scr, lane, above_row0);
+                sweep<T, K, V, PM, true, true>(L, b, pc, so, g_lo, g_hi, scr, lane, above_row0);
             __syncwarp();  // lane 31's scratch row is read by lane 0 in the next stripe
         }
     }
@@ -94,8 +94,17 @@ __device__ __forceinline__ void run_read(const BatchView& b, const ProbTables<T>
 // FP64 pass for one class over the runs of underflowed pairs the FP32 pass appended, one run per
 // claim, streamed through the read like an FP32 work item.
 // ------------------------------------------------------------------------------------------
-template <int K, int V, bool MULTI>
-__global__ void __launch_bounds__(kFwdBlock, 1) fwd_f64_kernel(BatchView b, ProbTables<double> tb, PassControl pc)
+// FP64 kernels with constant gap parameters and 7-8 rows per lane fit three warps per scheduler when
+// held to 168 registers (no spills at 8 rows, 16 bytes for the multi-stripe one); the others keep
+// what they need.
+template <int K, int PM>
+constexpr int min_blocks64()
+{
+    return PM == PM_ALL && K >= 7 ? 12 : 1;
+}
+
+template <int K, int V, int PM, bool MULTI>
+__global__ void __launch_bounds__(kFwdBlock, min_blocks64<K, PM>()) fwd_f64_kernel(BatchView b, ProbTables<double> tb, PassControl pc)
 {
     const int lane = threadIdx.x & (kWarp - 1);
     const unsigned int warp_id = (blockIdx.x * blockDim.x + threadIdx.x) / kWarp;
@@ -112,7 +121,7 @@ __global__ void __launch_bounds__(kFwdBlock, 1) fwd_f64_kernel(BatchView b, Prob
         so.out_base = e.out_idx;
         so.out_stride = e.out_stride;
         so.read = e.read;
-        run_read<double, K, V, MULTI>(b, tb, pc, so, e.hap, e.hap + e.n_haps, lane, scr);
+        run_read<double, K, V, PM, MULTI>(b, tb, pc, so, e.hap, e.hap + e.n_haps, lane, scr);
     }
 }
 
@@ -165,12 +174,13 @@ cudaError_t launch_fma_peak(float* sink, int blocks, int iters, bool packed, cud
 // ------------------------------------------------------------------------------------------
 typedef void (*F64Kernel)(BatchView, ProbTables<double>, PassControl);
 
-#define PHMM_ROW64(V)                                                                                     \
-    fwd_f64_kernel<1, V, false>, fwd_f64_kernel<2, V, false>, fwd_f64_kernel<3, V, false>,                \
-        fwd_f64_kernel<4, V, false>, fwd_f64_kernel<5, V, false>, fwd_f64_kernel<6, V, false>,            \
-        fwd_f64_kernel<7, V, false>, fwd_f64_kernel<8, V, false>, fwd_f64_kernel<8, V, true>
+#define PHMM_ROW64(V, PM)                                                                                 \
+    fwd_f64_kernel<1, V, PM, false>, fwd_f64_kernel<2, V, PM, false>, fwd_f64_kernel<3, V, PM, false>,    \
+        fwd_f64_kernel<4, V, PM, false>, fwd_f64_kernel<5, V, PM, false>, fwd_f64_kernel<6, V, PM, false>, \
+        fwd_f64_kernel<7, V, PM, false>, fwd_f64_kernel<8, V, PM, false>, fwd_f64_kernel<8, V, PM, true>
 
-static const F64Kernel kF64[kClasses64] = {PHMM_ROW64(kInter), PHMM_ROW64(kIntra)};
+static const F64Kernel kF64[kClasses64] = {PHMM_ROW64(kInter, PM_ALL), PHMM_ROW64(kInter, PM_ROW),
+                                           PHMM_ROW64(kIntra, PM_ROW)};
 
 cudaError_t launch_prep(const BatchDesc* desc, const uint8_t* hap_bases, uint32_t* codes_inter, uint32_t* codes_intra,
                         double* out, uint8_t* flags, int num_sms, cudaStream_t st)

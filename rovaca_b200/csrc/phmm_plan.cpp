@@ -315,8 +315,9 @@ phmm_status build_plan(const phmm_batch& b, const PlanLimits& lim, Plan& plan, s
                     ++part.count[skey];
                     const uint32_t npairs = nreads * (uint32_t)(run.hi - run.lo);
                     // each read's pairs may go to the FP64 class of its own length
-                    part.rerun_cap[class64_for_len(it.variant, R0)] += run.hi - run.lo;
-                    if (r1 != kNoRead) part.rerun_cap[class64_for_len(it.variant, R1)] += run.hi - run.lo;
+                    const int m = mode32(it.variant, it.pmode);
+                    part.rerun_cap[class64_for_len(m, R0)] += run.hi - run.lo;
+                    if (r1 != kNoRead) part.rerun_cap[class64_for_len(m, R1)] += run.hi - run.lo;
                     part.pairs += npairs;
                     part.cells += (uint64_t)run.cols * rows;
                     if (multi) part.max_multi = std::max(part.max_multi, run.cols);

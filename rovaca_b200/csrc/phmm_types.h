@@ -49,14 +49,15 @@ PHMM_HD inline int class32_kh(int c)
     return s < kMaxK ? s + 1 : s - kMaxK + kMinMultiKH;
 }
 
-// FP64 recompute classes (scalar path, one read per warp): variant * 9 + (multi ? 8 : K - 1) with
+// FP64 recompute classes (scalar path, one read per warp): mode * 9 + (multi ? 8 : K - 1) with the
+// modes of the FP32 classes (constant gap qualities let a lane hold the gap parameters once) and
 // K = ceil(R / 32) rows per lane, multi for R > 256 (stripes of 256 rows).  A pair's FP64 class
-// depends only on its read length, whatever FP32 shape computed it.
-constexpr int kClasses64 = 18;
-PHMM_HD inline int class64(int variant, int k, bool multi) { return variant * 9 + (multi ? 8 : k - 1); }
-PHMM_HD inline int class64_for_len(int variant, uint64_t R)
+// follows the mode of the FP32 class that computed it and its read length, whatever FP32 shape ran.
+constexpr int kClasses64 = kModes32 * 9;
+PHMM_HD inline int class64(int mode, int k, bool multi) { return mode * 9 + (multi ? 8 : k - 1); }
+PHMM_HD inline int class64_for_len(int mode, uint64_t R)
 {
-    return R > (uint64_t)kWarp * kMaxK ? class64(variant, kMaxK, true) : class64(variant, len_bucket(R), false);
+    return R > (uint64_t)kWarp * kMaxK ? class64(mode, kMaxK, true) : class64(mode, len_bucket(R), false);
 }
 
 struct RegionDesc {               // 32 bytes

@@ -201,9 +201,10 @@ def class32(mode: int, kh: int, multi: bool = False) -> int:
     return mode * 13 + (4 + kh if multi else kh - 1)
 
 
-def class64(intra: bool, read_len: int) -> int:
-    """FP64 recompute class of a pair from its variant and read length."""
-    return (9 if intra else 0) + (8 if read_len > 256 else (read_len + 31) // 32 - 1)
+def class64(mode: int, read_len: int) -> int:
+    """FP64 recompute class of a pair from its mode (that of the FP32 class that ran it: 0 inter
+    constant gaps, 1 inter per-row, 2 intra) and its read length."""
+    return mode * 9 + (8 if read_len > 256 else (read_len + 31) // 32 - 1)
 
 
 class Engine:

@@ -68,8 +68,9 @@ def cls(variant, kh, multi=False, uniform=True):
     return class32(mode, kh, multi)
 
 
-def cls64(variant, kh, multi=False):
-    return variant * 9 + (8 if multi else kh - 1)
+def cls64(variant, kh, multi=False, uniform=True):
+    mode = 2 if variant else (0 if uniform else 1)
+    return mode * 9 + (8 if multi else kh - 1)
 
 
 def test_plan_rows_per_lane_follow_read_length():
@@ -99,8 +100,8 @@ def test_plan_routes_n_pairs_to_the_intra_variant():
     r = [h[5:60], h[10:40] + b"N" + h[41:70], h[:30]]
     s = plan_summary(PackedBatch.from_regions([_region([h, hn, h], r)]))
     # read with N: every pair intra; reads without N: the N haplotype alone is intra
-    assert s["class_pairs"][9:].sum() == 3 + 2
-    assert s["class_pairs"][:9].sum() == 2 * 2
+    assert s["class_pairs"][18:].sum() == 3 + 2
+    assert s["class_pairs"][:18].sum() == 2 * 2
     # each read without N streams [h] and [h] as two inter items split around the N haplotype
     assert s["class_items"][:26].sum() == 4
     assert s["class_items"][26:].sum() == 3
@@ -142,7 +143,7 @@ def test_tile_table_shapes_route_reads():
     assert s["class_items"][cls(0, 4, True)] == 1 and s["class_items"][cls(0, 5, True)] == 1
     assert s["class_items"][cls(0, 4)] == 1 and s["class_items"].sum() == 3
     assert np.array_equal(s["class_pairs"], d["class_pairs"])
-    assert s["class_pairs"][class64(False, 200)] == 4 and s["class_pairs"][class64(False, 240)] == 2
+    assert s["class_pairs"][class64(0, 200)] == 4 and s["class_pairs"][class64(0, 240)] == 2
     assert s["cells"] == d["cells"] and s["pairs"] == d["pairs"]
     for b, k, m in ((6, 7, 1), (6, 6, 0), (3, 3, 1)):  # multi needs 4 <= KH < bucket, single KH >= bucket
         kh2, mu2 = default_tiles().as_arrays()
