@@ -1,4 +1,6 @@
 """PairHMM oracle: test infrastructure that checks the CUDA engine (see oracle/oracle.py)."""
-from .oracle import FUSED, INTER, INTRA, UNFUSED, Oracle, Ref, build_oracle, build_ref, ref_available
+from .oracle import (FUSED, INTER, INTRA, UNFUSED, Oracle, Ref, SwOracle, SwRef, build_oracle, build_ref, build_ref_sw,
+                     cigar_string, ref_available)
 
-__all__ = ["Oracle", "Ref", "build_oracle", "build_ref", "ref_available", "INTER", "INTRA", "FUSED", "UNFUSED"]
+__all__ = ["Oracle", "Ref", "SwOracle", "SwRef", "build_oracle", "build_ref", "build_ref_sw", "cigar_string", "ref_available",
+           "INTER", "INTRA", "FUSED", "UNFUSED"]

@@ -19,6 +19,7 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 ORACLE_SRC = HERE / "phmm_oracle.c"
 ORACLE_SCHED_SRC = HERE / "phmm_oracle_sched.cpp"
+ORACLE_SW_SRC = HERE / "sw_oracle.c"
 ORACLE_LIB = HERE / "_build" / "libphmm_oracle.so"
 REF_LIB = HERE / "_ref" / "libphmm_ref.so"
 
@@ -29,15 +30,16 @@ UNFUSED, FUSED = 0, 1
 def build_oracle(force: bool = False) -> Path:
     """Compiles oracle/_build/libphmm_oracle.so (no FMA contraction beyond the explicit fma calls)."""
     ORACLE_LIB.parent.mkdir(exist_ok=True)
-    srcs = (ORACLE_SRC, ORACLE_SCHED_SRC)
+    srcs = (ORACLE_SRC, ORACLE_SCHED_SRC, ORACLE_SW_SRC)
     if force or not ORACLE_LIB.exists() or any(ORACLE_LIB.stat().st_mtime < s.stat().st_mtime for s in srcs):
         flags = ["-O2", "-ffp-contract=off", "-fno-fast-math", "-fPIC", "-Wall"]
         tmp = ORACLE_LIB.parent
         subprocess.run(["gcc", *flags, "-c", str(ORACLE_SRC), "-o", str(tmp / "phmm_oracle.o")], check=True)
+        subprocess.run(["gcc", *flags, "-c", str(ORACLE_SW_SRC), "-o", str(tmp / "sw_oracle.o")], check=True)
         subprocess.run(["g++", *flags, "-std=c++17", "-c", str(ORACLE_SCHED_SRC), "-o", str(tmp / "phmm_oracle_sched.o")],
                        check=True)
         subprocess.run(["g++", "-shared", "-o", str(ORACLE_LIB), str(tmp / "phmm_oracle.o"),
-                        str(tmp / "phmm_oracle_sched.o"), "-lm"], check=True)
+                        str(tmp / "phmm_oracle_sched.o"), str(tmp / "sw_oracle.o"), "-lm"], check=True)
     return ORACLE_LIB
 
 
@@ -51,6 +53,88 @@ def build_ref(reference_root: str = "/root/reference") -> Path | None:
         return REF_LIB
     subprocess.run(["bash", str(HERE / "build_ref.sh"), reference_root], check=True)
     return REF_LIB
+
+
+SW_REF_LIB = HERE / "_ref" / "libsw_ref.so"
+
+
+def build_ref_sw(reference_root: str = "/root/reference") -> Path | None:
+    """Builds oracle/_ref/libsw_ref.so (the reference's Smith-Waterman aligner) when the reference
+    sources are present; returns the library."""
+    if not Path(reference_root, "src/haplotypecaller/common/base/lib/ro_sw").is_dir():
+        return SW_REF_LIB if SW_REF_LIB.exists() else None
+    srcs = [HERE / "ref_sw_shim.c", HERE / "build_ref_sw.sh"]
+    if SW_REF_LIB.exists() and all(SW_REF_LIB.stat().st_mtime >= s.stat().st_mtime for s in srcs):
+        return SW_REF_LIB
+    subprocess.run(["bash", str(HERE / "build_ref_sw.sh"), reference_root], check=True)
+    return SW_REF_LIB
+
+
+class SwRef:
+    """The reference's Smith-Waterman aligner (oracle/_ref/libsw_ref.so), as HaplotypeCaller calls
+    it to realign a read to its best haplotype: seq1 = haplotype, seq2 = read."""
+
+    GENOTYPING = (10, -15, -30, -5)   # sw_parameters_genotype, lib/sw_avx/sw_avx.c:15
+    ASSEMBLY = (200, -150, -260, -11)  # sw_parameters_assemble, lib/sw_avx/sw_avx.c:14
+
+    def __init__(self, path: Path | str | None = None):
+        p = Path(path) if path else SW_REF_LIB
+        if not p.exists():
+            raise FileNotFoundError(f"{p} not built (oracle/build_ref_sw.sh)")
+        self.lib = C.CDLL(str(p))
+        self.lib.ref_sw_align.restype = C.c_int
+        self.lib.ref_sw_align.argtypes = [C.c_char_p, C.c_int, C.c_char_p, C.c_int, C.c_void_p, C.c_int,
+                                          C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                          C.POINTER(C.c_int32), C.c_void_p, C.c_int]
+        self.lib.ref_sw_uses_int32.restype = C.c_int
+        self.lib.ref_sw_uses_int32.argtypes = [C.c_int, C.c_int, C.c_int]
+
+    def align(self, hap: bytes, read: bytes, params=GENOTYPING, variant: int = 0):
+        """-> (score, alignment_offset, max_i, max_j, [cigar ops as (len << 4) | op])."""
+        prm = (C.c_int32 * 4)(*params)
+        cig = (C.c_uint32 * 4096)()
+        sc, off, mi, mj = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32()
+        n = self.lib.ref_sw_align(bytes(hap), len(hap), bytes(read), len(read), C.cast(prm, C.c_void_p), variant,
+                                  C.byref(sc), C.byref(off), C.byref(mi), C.byref(mj), C.cast(cig, C.c_void_p), 4096)
+        return sc.value, off.value, mi.value, mj.value, list(cig[:max(n, 0)])
+
+    def uses_int32(self, hap_len: int, read_len: int, match: int) -> bool:
+        return bool(self.lib.ref_sw_uses_int32(hap_len, read_len, match))
+
+
+class SwOracle:
+    """The C restatement of the reference's Smith-Waterman aligner (oracle/sw_oracle.c)."""
+
+    GENOTYPING = SwRef.GENOTYPING
+    ASSEMBLY = SwRef.ASSEMBLY
+
+    def __init__(self):
+        self.lib = C.CDLL(str(build_oracle()))
+        self.lib.sw_oracle_align.restype = C.c_int
+        self.lib.sw_oracle_align.argtypes = [C.c_char_p, C.c_int, C.c_char_p, C.c_int, C.c_void_p, C.c_int,
+                                             C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                             C.POINTER(C.c_int32), C.c_void_p, C.c_int]
+        self.lib.sw_oracle_uses_int32.restype = C.c_int
+        self.lib.sw_oracle_uses_int32.argtypes = [C.c_int, C.c_int, C.c_int]
+
+    def align(self, hap: bytes, read: bytes, params=GENOTYPING, variant: int = 0):
+        """-> (score, alignment_offset, max_i, max_j, [cigar ops as (len << 4) | op])."""
+        prm = (C.c_int32 * 4)(*params)
+        cig = (C.c_uint32 * 4096)()
+        sc, off, mi, mj = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32()
+        n = self.lib.sw_oracle_align(bytes(hap), len(hap), bytes(read), len(read), C.cast(prm, C.c_void_p), variant,
+                                     C.byref(sc), C.byref(off), C.byref(mi), C.byref(mj), C.cast(cig, C.c_void_p),
+                                     4096)
+        if n < 0:
+            raise MemoryError("sw_oracle_align: allocation failed")
+        return sc.value, off.value, mi.value, mj.value, list(cig[:n])
+
+    def uses_int32(self, hap_len: int, read_len: int, match: int) -> bool:
+        return bool(self.lib.sw_oracle_uses_int32(hap_len, read_len, match))
+
+
+def cigar_string(ops) -> str:
+    return "".join(f"{c >> 4}{'MIDNSHP=XB'[c & 15]}" for c in ops)
 
 
 def _b(x) -> bytes:

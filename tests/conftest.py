@@ -42,6 +42,18 @@ def golden_cases():
 
 
 @pytest.fixture(scope="session")
+def sw_golden():
+    return json.loads((GOLDEN / "sw_golden.json").read_text())["cases"]
+
+
+@pytest.fixture(scope="session")
+def sw_oracle():
+    from oracle import SwOracle
+
+    return SwOracle()
+
+
+@pytest.fixture(scope="session")
 def ref_regions():
     """{group: (PackedBatch, reference schedule_pairhmm log10 [hap][read] flat)} from the fixtures."""
     from rovaca_b200.pairhmm import PackedBatch
