@@ -341,6 +341,59 @@ typedef struct phmm_server_stats {
 
 PHMM_API phmm_status phmm_server_stats_get(phmm_engine* engine, phmm_server_stats* stats);
 
+/* ---- Smith-Waterman realignment of reads to their best haplotype ------------------------------
+ *
+ * Replaces the per-read aligner call of AlignmentUtils::create_read_aligned_to_ref
+ * (genotype/utils/alignment_utils.cpp:571-579: seq1 = haplotype, seq2 = read, then
+ * sw->avx_function(sw)) and of the assembler (apply/assemble/hc_assemble_cigar_cacl.c:417-428) with
+ * one batched call.  Each item's results are the fields that call leaves in the lib_sw_avx context
+ * (include/smithwaterman_common.h: score, max_i, max_j, alignment_offset, cigar, cigar_count), equal
+ * to the reference's bit for bit: the int16 / int32 kernel choice of ro_sw_avx512_run
+ * (lib/ro_sw/ro_sw.c:26-60), its recurrences, tie rules and trace-back (lib/ro_sw/sw_core_template.h,
+ * lib/ro_sw/sw_cigar.c).  Inputs whose longer sequence has 2048 bases or more are refused as the
+ * reference refuses them: alignment_offset 1, score 0, no CIGAR. */
+
+typedef struct phmm_sw_item {
+    uint64_t hap_offset;    /* byte offset of the haplotype (seq1) in hap_bases */
+    uint64_t read_offset;   /* byte offset of the read (seq2) in read_bases */
+    uint32_t hap_len;
+    uint32_t read_len;
+} phmm_sw_item;
+
+typedef struct phmm_sw_result {
+    int32_t score;
+    int32_t alignment_offset;   /* haplotype position of the first aligned read base */
+    int32_t max_i, max_j;       /* end cell of the alignment (haplotype, read) */
+    uint32_t cigar_count;       /* CIGAR ops of the alignment (at most 2047); the first
+                                   min(cigar_count, cigar_cap) are written */
+    uint32_t reserved;
+} phmm_sw_result;
+
+/* params = {match, mismatch, gap_open, gap_extend} (NULL: the genotyping parameters 10, -15, -30,
+ * -5 of lib/sw_avx/sw_avx.c:15; the assembler uses 200, -150, -260, -11).  variant: 0 = the
+ * reference's kernel choice, 1 = its int32 kernel, 2 = its int16 kernel.  cigars: n x cigar_cap
+ * BAM-encoded ops (length << 4 | op; M 0, I 1, D 2, S 4) in read order.  All pointers are host
+ * memory; the call copies in, runs on the engine's device and copies out before it returns. */
+PHMM_API phmm_status phmm_sw_align(phmm_engine* engine, const int32_t* params, int32_t variant, uint32_t n,
+                                   const phmm_sw_item* items, const uint8_t* hap_bases, uint64_t hap_bytes,
+                                   const uint8_t* read_bases, uint64_t read_bytes, phmm_sw_result* results,
+                                   uint32_t* cigars, uint32_t cigar_cap);
+
+/* Device-resident Smith-Waterman batch (no reference counterpart: it exists to time the kernels with
+ * the inputs already in HBM).  Created from host buffers, run `iterations` times back to back
+ * (ms_per_run: CUDA-event time per run on the aligner's stream; class_ms[13], optional: time of each
+ * kernel class in the last run), results read back on demand. */
+typedef struct phmm_sw_resident phmm_sw_resident;
+PHMM_API phmm_status phmm_sw_resident_create(phmm_engine* engine, const int32_t* params, int32_t variant,
+                                             uint32_t n, const phmm_sw_item* items, const uint8_t* hap_bases,
+                                             uint64_t hap_bytes, const uint8_t* read_bases, uint64_t read_bytes,
+                                             uint32_t cigar_cap, phmm_sw_resident** out);
+PHMM_API phmm_status phmm_sw_resident_run(phmm_sw_resident* resident, int32_t iterations, float* ms_per_run,
+                                          float* class_ms);
+PHMM_API phmm_status phmm_sw_resident_results(phmm_sw_resident* resident, phmm_sw_result* results,
+                                              uint32_t* cigars);
+PHMM_API phmm_status phmm_sw_resident_destroy(phmm_sw_resident* resident);
+
 #ifdef __cplusplus
 }
 #endif

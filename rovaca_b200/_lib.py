@@ -115,6 +115,17 @@ class ServerStats(C.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class SwItem(C.Structure):
+    """phmm_sw_item: one alignment (haplotype = seq1, read = seq2) as offsets into two base buffers."""
+    _fields_ = [("hap_offset", C.c_uint64), ("read_offset", C.c_uint64), ("hap_len", C.c_uint32),
+                ("read_len", C.c_uint32)]
+
+
+class SwResult(C.Structure):
+    _fields_ = [("score", C.c_int32), ("alignment_offset", C.c_int32), ("max_i", C.c_int32), ("max_j", C.c_int32),
+                ("cigar_count", C.c_uint32), ("reserved", C.c_uint32)]
+
+
 _lib = None
 
 
@@ -157,6 +168,11 @@ def load() -> C.CDLL:
         "phmm_wait": (I32, [P, U64, I64, C.POINTER(D), C.POINTER(D)]),
         "phmm_cancel": (I32, [P, U64]),
         "phmm_server_stats_get": (I32, [P, P]),
+        "phmm_sw_align": (I32, [P, P, I32, U32, P, P, U64, P, U64, P, P, U32]),
+        "phmm_sw_resident_create": (I32, [P, P, I32, U32, P, P, U64, P, U64, U32, C.POINTER(P)]),
+        "phmm_sw_resident_run": (I32, [P, I32, C.POINTER(C.c_float), P]),
+        "phmm_sw_resident_results": (I32, [P, P, P]),
+        "phmm_sw_resident_destroy": (I32, [P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -1,5 +1,6 @@
 // extern "C" entry points of include/phmm_b200.h.  No exception crosses this boundary: every
 // entry point catches, records the detail for phmm_last_error() and returns a status.
+#include <cstddef>
 #include <cstring>
 #include <exception>
 #include <new>
@@ -9,11 +10,16 @@
 #include "phmm_capi_internal.h"
 #include "phmm_engine.h"
 #include "phmm_plan.h"
+#include "phmm_sw.h"
 
 static_assert(sizeof(phmm_tile_table) == sizeof(phmm::TileTable), "tile table layouts differ");
 static_assert(PHMM_FP32_CLASSES == phmm::kClasses32 && PHMM_FP64_CLASSES == phmm::kClasses64 &&
                   PHMM_TILE_MODES == phmm::kModes32 && PHMM_LEN_BUCKETS == phmm::kLenBuckets,
               "class counts differ between the C ABI and the kernels");
+
+static_assert(sizeof(phmm_sw_item) == sizeof(phmm::SwItem) && offsetof(phmm_sw_item, hap_len) == offsetof(phmm::SwItem, hap_len) &&
+                  offsetof(phmm_sw_item, read_offset) == offsetof(phmm::SwItem, read_start),
+              "Smith-Waterman item layouts differ");
 
 namespace phmm {
 
@@ -332,6 +338,106 @@ phmm_status phmm_engine_autotune(phmm_engine* engine, phmm_tune_report* report)
     std::string err;
     phmm_status st = phmm::engine_of(engine)->autotune(report, err);
     return st == PHMM_OK ? PHMM_OK : set_error(st, err);
+    PHMM_GUARD_END
+}
+
+static phmm::SwParams sw_params(const int32_t* params)
+{
+    if (!params) return phmm::SwParams{10, -15, -30, -5};  // sw_parameters_genotype, lib/sw_avx/sw_avx.c:15
+    return phmm::SwParams{params[0], params[1], params[2], params[3]};
+}
+
+static phmm_status sw_get(phmm_engine* engine, phmm::SwAligner** a)
+{
+    std::string err;
+    phmm_status st = phmm::engine_of(engine)->sw_aligner(a, err);
+    return st == PHMM_OK ? PHMM_OK : set_error(st, err);
+}
+
+phmm_status phmm_sw_align(phmm_engine* engine, const int32_t* params, int32_t variant, uint32_t n,
+                          const phmm_sw_item* items, const uint8_t* hap_bases, uint64_t hap_bytes,
+                          const uint8_t* read_bases, uint64_t read_bytes, phmm_sw_result* results, uint32_t* cigars,
+                          uint32_t cigar_cap)
+{
+    PHMM_GUARD_BEGIN
+    phmm::clear_error();
+    if (!engine) return set_error(PHMM_ERR_NOT_INITIALIZED, "engine is null");
+    if (variant < 0 || variant > 2) return set_error(PHMM_ERR_INVALID_ARGUMENT, "variant must be 0, 1 or 2");
+    if (n == 0) return PHMM_OK;
+    if (!items || !results || (hap_bytes && !hap_bases) || (read_bytes && !read_bases) || (cigar_cap && !cigars))
+        return set_error(PHMM_ERR_INVALID_ARGUMENT, "null buffer");
+    phmm::SwAligner* a = nullptr;
+    phmm_status st = sw_get(engine, &a);
+    if (st != PHMM_OK) return st;
+    std::string err;
+    st = a->align(sw_params(params), variant, n, reinterpret_cast<const phmm::SwItem*>(items), hap_bases, hap_bytes,
+                  read_bases, read_bytes, results, cigars, cigar_cap, nullptr, err);
+    return st == PHMM_OK ? PHMM_OK : set_error(st, err);
+    PHMM_GUARD_END
+}
+
+struct phmm_sw_resident {
+    phmm::SwAligner* aligner = nullptr;
+    phmm::SwAligner::Resident* res = nullptr;
+};
+
+phmm_status phmm_sw_resident_create(phmm_engine* engine, const int32_t* params, int32_t variant, uint32_t n,
+                                    const phmm_sw_item* items, const uint8_t* hap_bases, uint64_t hap_bytes,
+                                    const uint8_t* read_bases, uint64_t read_bytes, uint32_t cigar_cap,
+                                    phmm_sw_resident** out)
+{
+    PHMM_GUARD_BEGIN
+    phmm::clear_error();
+    if (!out) return set_error(PHMM_ERR_INVALID_ARGUMENT, "out is null");
+    *out = nullptr;
+    if (!engine) return set_error(PHMM_ERR_NOT_INITIALIZED, "engine is null");
+    if (variant < 0 || variant > 2) return set_error(PHMM_ERR_INVALID_ARGUMENT, "variant must be 0, 1 or 2");
+    if ((n && !items) || (hap_bytes && !hap_bases) || (read_bytes && !read_bases))
+        return set_error(PHMM_ERR_INVALID_ARGUMENT, "null buffer");
+    phmm::SwAligner* a = nullptr;
+    phmm_status st = sw_get(engine, &a);
+    if (st != PHMM_OK) return st;
+    std::string err;
+    phmm::SwAligner::Resident* r = nullptr;
+    st = a->resident_create(sw_params(params), variant, n, reinterpret_cast<const phmm::SwItem*>(items), hap_bases,
+                            hap_bytes, read_bases, read_bytes, cigar_cap, &r, err);
+    if (st != PHMM_OK) return set_error(st, err);
+    *out = new phmm_sw_resident{a, r};
+    return PHMM_OK;
+    PHMM_GUARD_END
+}
+
+phmm_status phmm_sw_resident_run(phmm_sw_resident* resident, int32_t iterations, float* ms_per_run, float* class_ms)
+{
+    PHMM_GUARD_BEGIN
+    phmm::clear_error();
+    if (!resident) return set_error(PHMM_ERR_INVALID_ARGUMENT, "resident is null");
+    if (iterations < 0) return set_error(PHMM_ERR_INVALID_ARGUMENT, "iterations must be >= 0");
+    std::string err;
+    phmm_status st = resident->aligner->resident_run(resident->res, iterations, ms_per_run, class_ms, err);
+    return st == PHMM_OK ? PHMM_OK : set_error(st, err);
+    PHMM_GUARD_END
+}
+
+phmm_status phmm_sw_resident_results(phmm_sw_resident* resident, phmm_sw_result* results, uint32_t* cigars)
+{
+    PHMM_GUARD_BEGIN
+    phmm::clear_error();
+    if (!resident) return set_error(PHMM_ERR_INVALID_ARGUMENT, "resident is null");
+    std::string err;
+    phmm_status st = resident->aligner->resident_results(resident->res, results, cigars, err);
+    return st == PHMM_OK ? PHMM_OK : set_error(st, err);
+    PHMM_GUARD_END
+}
+
+phmm_status phmm_sw_resident_destroy(phmm_sw_resident* resident)
+{
+    PHMM_GUARD_BEGIN
+    phmm::clear_error();
+    if (!resident) return PHMM_OK;
+    resident->aligner->resident_destroy(resident->res);
+    delete resident;
+    return PHMM_OK;
     PHMM_GUARD_END
 }
 

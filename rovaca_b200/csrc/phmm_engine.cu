@@ -12,6 +12,7 @@
 // The arena only grows; all kernel arguments are arena pointers, so a graph captured for an arena
 // replays for every batch that fits it.
 #include "phmm_engine.h"
+#include "phmm_sw.h"
 
 #include <algorithm>
 #include <chrono>
@@ -288,8 +289,20 @@ phmm_status Engine::create(const phmm_config* cfg, Engine** out, std::string& er
 Engine::~Engine()
 {
     cudaSetDevice(dev_);
+    delete sw_;
     if (default_slot_) free_slot(default_slot_);
     if (d_tables_) cudaFree(d_tables_);
+}
+
+phmm_status Engine::sw_aligner(SwAligner** out, std::string& err)
+{
+    std::lock_guard<std::mutex> lk(sw_mu_);
+    if (!sw_) {
+        phmm_status st = SwAligner::create(dev_, &sw_, err);
+        if (st != PHMM_OK) return st;
+    }
+    *out = sw_;
+    return PHMM_OK;
 }
 
 phmm_status Engine::make_slot(int id, Slot** out, std::string& err)

@@ -16,6 +16,8 @@
 
 namespace phmm {
 
+class SwAligner;
+
 // Sizes an arena must hold.
 struct Capacity {
     uint64_t regions = 0, reads = 0, haps = 0, read_bases = 0, hap_bases = 0, items = 0, rerun = 0, out = 0;
@@ -121,6 +123,8 @@ public:
     phmm_status time_fp32_class(Slot& s, const Plan& plan, int cls, int reps, float* best_ms, std::string& err);
     // Runs the tile-shape autotuner and installs its table (phmm_tune.cpp).
     phmm_status autotune(phmm_tune_report* report, std::string& err);
+    // The engine's Smith-Waterman aligner (phmm_sw.cu), created on first use.
+    phmm_status sw_aligner(SwAligner** out, std::string& err);
 
     int device() const { return dev_; }
     int num_sms() const { return sms_; }
@@ -150,6 +154,8 @@ private:
     const double* d_jacobian_ = nullptr;  // genotyping Jacobian table (inside d_tables_)
     double log10_two_ = 0.0;
     Slot* default_slot_ = nullptr;
+    SwAligner* sw_ = nullptr;
+    std::mutex sw_mu_;
     std::mutex mu_;
     mutable std::mutex tiles_mu_;
     TileTable tiles_ = TileTable::defaults();

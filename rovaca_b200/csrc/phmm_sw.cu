@@ -1,0 +1,681 @@
+// Smith-Waterman realignment of reads to haplotypes on the GPU: the aligner HaplotypeCaller runs for
+// every read against its best haplotype (AssemblyBasedCallerUtils::realign_reads_to_their_best_haplotype,
+// genotype/utils/assembly_based_caller_utils.cpp:146-169 -> AlignmentUtils::create_read_aligned_to_ref,
+// alignment_utils.cpp:571-579, seq1 = haplotype, seq2 = read).
+//
+// Reference arithmetic (common/base/lib/ro_sw/sw_core_template.h:111-352, sw_cigar.c:22-171, ro_sw.c):
+//   E(i,j) = max(H(i,j-1) + open, E(i,j-1) + extend)   insertion; extension flag 4 unless open > ext
+//   F(i,j) = max(F(i-1,j) + extend, H(i-1,j) + open)   deletion;  extension flag 8 likewise
+//   H(i,j) = max(cutoff, H(i-1,j-1) + (s1[i] == s2[j] ? match : mismatch)), then E if E > H
+//            (state insertion 1), then F if F > H (state deletion 2)
+//   H(0,j) = H(i,0) = 0, E(i,0) = F(0,j) = low
+// in int16 with wrap-around adds (low -16384, cutoff -8192) or int32 (low INT32_MIN/2, cutoff -1e8) as
+// ro_sw_avx512_run chooses.  The best end cell is scanned over the last row and the last column in
+// the reference's anti-diagonal order with its two tie rules; the path is traced back through the
+// per-cell codes (soft clips at both ends, extension states), merged into runs and emitted as BAM
+// CIGAR ops in read order.  Results equal the reference build's bit for bit.
+//
+// Mapping: one warp per alignment.  A stripe of 32 x K read columns is spread over the lanes, K
+// consecutive columns per lane; the warp streams the haplotype rows as a wavefront (lane l works on
+// row t + 1 - l at step t), so that the left neighbour's H and E of the same row, and its H of the row
+// above (the diagonal), arrive by one shuffle each.  Reads longer than a stripe run stripe after
+// stripe, the right edge column of one stripe (H, E per row) feeding the next.  Each lane packs the
+// 4-bit codes of its K cells into ceil(K/8) words per row, stored to a per-warp scratch area in
+// HBM; the trace-back walks that area through bands of rows staged in shared memory.  The 16-bit
+// kernel is run in 32-bit arithmetic with the 16-bit constants whenever its adds cannot wrap
+// (sw_w16_cannot_wrap); otherwise one class emulates the wrap-around on every add.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <cstdint>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "phmm_sw.h"
+
+namespace phmm {
+
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kStIns = 1, kStDel = 2, kStInsExt = 4, kStDelExt = 8, kStClip = 9;
+
+struct SwView {
+    const SwItem* items;
+    const uint32_t* order;       // this class's item indices, most cells first
+    uint32_t n;
+    const uint8_t* hap;
+    const uint8_t* read;
+    SwParams prm;
+    int variant;
+    uint8_t* scratch;
+    uint64_t stride;             // scratch bytes per warp
+    unsigned int* claim;
+    phmm_sw_result* out;
+    uint32_t* cigar;
+    uint32_t cigar_cap;
+};
+
+template <bool WRAP>
+__device__ __forceinline__ int sadd(int a, int b)
+{
+    const int s = (int)((unsigned)a + (unsigned)b);
+    return WRAP ? (int)(short)s : s;
+}
+
+__device__ __forceinline__ uint32_t op_of(uint32_t run)
+{
+    const uint32_t st = run >> 16, len = run & 0xffffu;
+    const uint32_t op = st == 0 ? 0u : st == kStIns ? 1u : st == kStDel ? 2u : 4u;
+    return (len << 4) | op;
+}
+
+// Forward pass, end-cell selection and trace-back of one alignment.
+template <int K, bool WRAP>
+__device__ void sw_one(const SwView& v, uint32_t idx, int lane, uint8_t* scr, uint32_t* band)
+{
+    constexpr int NW = (K + 7) / 8;
+    constexpr int ROW = 32 * NW;                 // u32 words per stripe row
+    constexpr int BAND_ROWS = kSwBandWords / ROW;
+    constexpr int S = 32 * K;
+    const SwItem it = v.items[idx];
+    const int nrow = (int)it.hap_len, ncol = (int)it.read_len;
+    phmm_sw_result res{0, 0, 0, 0, 0, 0};
+    if (max(nrow, ncol) >= kSwMaxSeq) {
+        res.alignment_offset = 1;
+        if (lane == 0) v.out[idx] = res;
+        return;
+    }
+    const bool i32 = sw_uses_int32(v.variant, it.hap_len, it.read_len, v.prm.match);
+    const int match = i32 ? v.prm.match : (int)(short)v.prm.match;
+    const int mismatch = i32 ? v.prm.mismatch : (int)(short)v.prm.mismatch;
+    const int open = i32 ? v.prm.gap_open : (int)(short)v.prm.gap_open;
+    const int ext = i32 ? v.prm.gap_extend : (int)(short)v.prm.gap_extend;
+    const int low = i32 ? INT_MIN / 2 : -16384;
+    const int cutoff = i32 ? -100000000 : -8192;
+    int best = i32 ? INT_MIN : -32768;
+    int mi = 0, mj = 0;
+
+    const SwLayout L = sw_layout(it.hap_len, it.read_len, K);
+    uint32_t* bt = (uint32_t*)(scr + L.bt);
+    int* bh = (int*)(scr + L.bh);
+    int* be = (int*)(scr + L.be);
+    int* lrow = (int*)(scr + L.lrow);
+    int* lcol = (int*)(scr + L.lcol);
+    uint32_t* runs = (uint32_t*)(scr + L.runs);
+    const uint8_t* hap = v.hap + it.hap_start;
+    const uint8_t* rd = v.read + it.read_start;
+
+    if (nrow == 0 || ncol == 0) {
+        // only boundary cells: H = 0 on the last row (empty haplotype) or column (empty read); with
+        // both empty there is no candidate at all
+        if (nrow == 0 && ncol > 0) { best = 0; mj = 1; }
+        if (ncol == 0 && nrow > 0) { best = 0; mi = nrow; }
+    } else {
+        const int stripes = (ncol + S - 1) / S;
+        for (int s = 0; s < stripes; ++s) {
+            const int j0 = s * S;
+            const bool last = s == stripes - 1;
+            int rb[K], Hp[K], Fp[K];
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                const int j = j0 + lane * K + k + 1;
+                rb[k] = j <= ncol ? (int)rd[j - 1] : -1;
+                Hp[k] = 0;
+                Fp[k] = low;
+            }
+            const int jc = ncol - j0 - 1;          // stripe slot of column ncol (last stripe)
+            const bool holds_last_col = last && lane == jc / K;
+            const int kc = jc - (jc / K) * K;
+            int hb = 0, hnext = (int)hap[0];
+            int bnh = 0, bne = low;                // lane 0: left edge of the next row
+            if (s > 0 && lane == 0) { bnh = bh[1]; bne = be[1]; }
+            int hprev = 0;                         // H(i-1, left column) of this lane
+            int hout = 0, eout = low;              // H, E of this lane's last column, previous step
+            uint32_t* bts = bt + (uint64_t)s * nrow * ROW;
+            const int steps = nrow + 31;
+            for (int t = 0; t < steps; ++t) {
+                const int i = t + 1 - lane;
+                const bool act = i >= 1 && i <= nrow;
+                hb = __shfl_up_sync(kFull, hb, 1);
+                int hl = __shfl_up_sync(kFull, hout, 1);
+                int el = __shfl_up_sync(kFull, eout, 1);
+                if (lane == 0) {
+                    hb = hnext;
+                    hnext = t + 1 < nrow ? (int)hap[t + 1] : 0;
+                    hl = bnh;
+                    el = bne;
+                    if (s > 0 && t + 2 <= nrow) { bnh = bh[t + 2]; bne = be[t + 2]; }
+                }
+                int diag = hprev;
+                hprev = hl;
+                uint32_t code[NW];
+#pragma unroll
+                for (int w = 0; w < NW; ++w) code[w] = 0;
+                int hc = 0;
+#pragma unroll
+                for (int k = 0; k < K; ++k) {
+                    const int eo = sadd<WRAP>(hl, open), ee = sadd<WRAP>(el, ext);
+                    const int e = max(eo, ee);
+                    const int fe = sadd<WRAP>(Fp[k], ext), fo = sadd<WRAP>(Hp[k], open);
+                    const int f = max(fe, fo);
+                    int h = max(sadd<WRAP>(diag, hb == rb[k] ? match : mismatch), cutoff);
+                    uint32_t c = (eo > ee ? 0u : (uint32_t)kStInsExt) | (fo > fe ? 0u : (uint32_t)kStDelExt);
+                    if (e > h) { c |= kStIns; h = e; }
+                    if (f > h) { c = (c & ~3u) | kStDel; h = f; }
+                    diag = Hp[k];
+                    if (act) { Hp[k] = h; Fp[k] = f; }
+                    hl = h;
+                    el = e;
+                    code[k / 8] |= c << (4 * (k % 8));
+                    if (k == kc) hc = h;
+                }
+                hout = act ? hl : 0;               // a lane before its first row stands for row 0
+                eout = act ? el : low;
+                if (act) {
+                    uint32_t* row = bts + (uint64_t)(i - 1) * ROW + lane;
+#pragma unroll
+                    for (int w = 0; w < NW; ++w) row[w * 32] = code[w];
+                    if (i == nrow) {
+#pragma unroll
+                        for (int k = 0; k < K; ++k) {
+                            const int j = j0 + lane * K + k + 1;
+                            if (j <= ncol) lrow[j] = Hp[k];
+                        }
+                    }
+                    if (holds_last_col) lcol[i] = hc;
+                    if (!last && lane == 31) { bh[i] = hl; be[i] = el; }
+                }
+            }
+            __syncwarp();
+        }
+
+        // end cell: only candidates equal to the maximum matter, visited in the reference's order
+        // (anti-diagonal a ascending; the last-row cell (nrow, a - nrow) before the last-column cell
+        // (a - ncol, ncol)), sw_core_template.h:332-347
+        int smax = INT_MIN;
+        for (int j = 1 + lane; j <= ncol; j += 32) smax = max(smax, lrow[j]);
+        for (int i = 1 + lane; i <= nrow; i += 32) smax = max(smax, lcol[i]);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) smax = max(smax, __shfl_xor_sync(kFull, smax, o));
+        const int alo = min(nrow, ncol) + 1, ahi = nrow + ncol;
+        for (int a0 = alo; a0 <= ahi; a0 += 32) {
+            const int a = a0 + lane;
+            const bool rc = a <= ahi && a >= nrow + 1 && lrow[a - nrow] == smax;
+            const bool cc = a <= ahi && a >= ncol + 1 && lcol[a - ncol] == smax;
+            uint32_t mr = __ballot_sync(kFull, rc), mc = __ballot_sync(kFull, cc);
+            while (mr | mc) {
+                const int l = __ffs(mr | mc) - 1;
+                const int aa = a0 + l;
+                if ((mr >> l) & 1u) {
+                    const int ci = nrow, cj = aa - nrow;
+                    if (best < smax || abs(ci - cj) < abs(mi - mj)) { best = smax; mi = ci; mj = cj; }
+                }
+                if ((mc >> l) & 1u) {
+                    const int ci = aa - ncol, cj = ncol;
+                    if (best < smax || mj == ncol || abs(ci - cj) <= abs(mi - mj)) { best = smax; mi = ci; mj = cj; }
+                }
+                mr &= ~(1u << l);
+                mc &= ~(1u << l);
+            }
+        }
+    }
+
+    // trace-back (sw_cigar.c:36-146), uniform across the warp; runs merged as they come
+    int i = mi, j = mj;
+    int nr = 0, cst = -1, clen = 0;
+    auto push = [&](int st, int len) {
+        if (nr > 0 && cst == st) {
+            clen += len;
+        } else {
+            if (nr > 0 && lane == 0) runs[nr - 1] = ((uint32_t)cst << 16) | (uint32_t)clen;
+            cst = st;
+            clen = len;
+            ++nr;
+        }
+    };
+    if (j < ncol) push(kStClip, ncol - j);
+    int state = 0;
+    int bs = -1, br0 = 0, br1 = -1;
+    while (i > 0 && j > 0) {
+        const int s = (j - 1) / S, jj = (j - 1) - s * S, ln = jj / K, k = jj - ln * K;
+        if (s != bs || i - 1 < br0 || i - 1 > br1) {
+            bs = s;
+            br1 = i - 1;
+            br0 = max(0, br1 - BAND_ROWS + 1);
+            const uint32_t* src = bt + ((uint64_t)s * nrow + br0) * ROW;
+            const int words = (br1 - br0 + 1) * ROW;
+            __syncwarp();
+            for (int q = lane; q < words; q += 32) band[q] = src[q];
+            __syncwarp();
+        }
+        const uint32_t w = band[(i - 1 - br0) * ROW + (k >> 3) * 32 + ln];
+        const int b = (int)((w >> (4 * (k & 7))) & 15u);
+        if (state == kStInsExt) {
+            --j;
+            ++clen;
+            state = b & kStInsExt;
+        } else if (state == kStDelExt) {
+            --i;
+            ++clen;
+            state = b & kStDelExt;
+        } else if ((b & 3) == 0) {
+            --i;
+            --j;
+            push(0, 1);
+            state = 0;
+        } else if ((b & 3) == kStIns) {
+            --j;
+            push(kStIns, 1);
+            state = b & kStInsExt;
+        } else {
+            --i;
+            push(kStDel, 1);
+            state = b & kStDelExt;
+        }
+    }
+    if (j > 0) push(kStClip, j);
+    if (nr > 0 && lane == 0) runs[nr - 1] = ((uint32_t)cst << 16) | (uint32_t)clen;
+    __syncwarp();
+
+    // read order, at most kSwMaxSeq - 1 ops (sw_cigar.c:162-170)
+    const int count = min(nr, kSwMaxSeq - 1);
+    const int wr = min(count, (int)v.cigar_cap);
+    uint32_t* dst = v.cigar + (uint64_t)idx * v.cigar_cap;
+    for (int q = lane; q < wr; q += 32) dst[q] = op_of(runs[nr - 1 - q]);
+    res.score = best;
+    res.alignment_offset = i;
+    res.max_i = mi;
+    res.max_j = mj;
+    res.cigar_count = (uint32_t)count;
+    if (lane == 0) v.out[idx] = res;
+    __syncwarp();
+}
+
+template <int K, bool WRAP>
+__global__ void __launch_bounds__(32 * kSwBlockWarps) sw_kernel(SwView v)
+{
+    __shared__ uint32_t band[kSwBlockWarps][kSwBandWords];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    uint8_t* scr = v.scratch + ((uint64_t)blockIdx.x * kSwBlockWarps + wib) * v.stride;
+    for (;;) {
+        unsigned int q = 0;
+        if (lane == 0) q = atomicAdd(v.claim, 1u);
+        q = __shfl_sync(kFull, q, 0);
+        if (q >= v.n) break;
+        sw_one<K, WRAP>(v, v.order[q], lane, scr, band[wib]);
+    }
+}
+
+using SwKernel = void (*)(SwView);
+
+const SwKernel kSwKernels[kSwClasses] = {
+    sw_kernel<1, false>,  sw_kernel<2, false>,  sw_kernel<3, false>,  sw_kernel<4, false>, sw_kernel<5, false>,
+    sw_kernel<6, false>,  sw_kernel<8, false>,  sw_kernel<10, false>, sw_kernel<12, false>,
+    sw_kernel<16, false>, sw_kernel<20, false>, sw_kernel<24, false>, sw_kernel<24, true>,
+};
+
+}  // namespace
+
+int sw_class_of(const SwParams& prm, int variant, uint32_t nrow, uint32_t ncol)
+{
+    if (!sw_uses_int32(variant, nrow, ncol, prm.match) && ncol > 0 && nrow > 0 &&
+        std::max(nrow, ncol) < (uint32_t)kSwMaxSeq &&
+        !sw_w16_cannot_wrap((short)prm.match, (short)prm.mismatch, (short)prm.gap_open, (short)prm.gap_extend))
+        return kSwWrapClass;
+    const uint32_t k = std::max<uint32_t>(1, (ncol + 31) / 32);
+    for (int c = 0; c < kSwWrapClass; ++c)
+        if ((uint32_t)kSwK[c] >= k) return c;
+    return kSwWrapClass - 1;  // K = 24 stripes
+}
+
+struct SwAligner::Plan {
+    uint32_t n = 0;
+    std::vector<uint32_t> order;             // item indices grouped by class, most cells first
+    uint32_t begin[kSwClasses + 1] = {};
+    uint64_t stride[kSwClasses] = {};        // scratch bytes per warp of each class
+    int grid[kSwClasses] = {};
+    uint64_t scratch = 0;                    // bytes for the largest class launch
+    uint64_t cells = 0;
+};
+
+struct SwAligner::Resident {
+    SwParams prm{};
+    int variant = 0;
+    Plan plan;
+    uint32_t cigar_cap = 0;
+    void* arena = nullptr;
+    SwItem* items = nullptr;
+    uint32_t* order = nullptr;
+    uint8_t* hap = nullptr;
+    uint8_t* read = nullptr;
+    uint8_t* scratch = nullptr;
+    unsigned int* claim = nullptr;
+    phmm_sw_result* out = nullptr;
+    uint32_t* cigar = nullptr;
+};
+
+namespace {
+
+#define SW_CK(call)                                                                   \
+    do {                                                                              \
+        cudaError_t e_ = (call);                                                      \
+        if (e_ != cudaSuccess) {                                                      \
+            err = std::string(#call) + " failed: " + cudaGetErrorString(e_);          \
+            return PHMM_ERR_CUDA;                                                     \
+        }                                                                             \
+    } while (0)
+
+uint64_t a256(uint64_t x) { return (x + 255) & ~uint64_t(255); }
+
+// Scratch of one class launch is held under this bound by launching fewer resident warps.
+constexpr uint64_t kSwScratchCap = 6ull << 30;
+
+phmm_status check_items(uint32_t n, const SwItem* items, uint64_t hap_bytes, uint64_t read_bytes, std::string& err)
+{
+    for (uint32_t q = 0; q < n; ++q) {
+        const SwItem& it = items[q];
+        if (it.hap_start > hap_bytes || it.hap_len > hap_bytes - it.hap_start || it.read_start > read_bytes ||
+            it.read_len > read_bytes - it.read_start) {
+            err = "Smith-Waterman item " + std::to_string(q) + " lies outside its base buffers";
+            return PHMM_ERR_INVALID_ARGUMENT;
+        }
+    }
+    return PHMM_OK;
+}
+
+}  // namespace
+
+phmm_status SwAligner::create(int device, SwAligner** out, std::string& err)
+{
+    *out = nullptr;
+    SwAligner* a = new SwAligner();
+    a->dev_ = device;
+    auto fail = [&](phmm_status st) {
+        delete a;
+        return st;
+    };
+#define SW_CKC(call)                                                                  \
+    do {                                                                              \
+        cudaError_t e_ = (call);                                                      \
+        if (e_ != cudaSuccess) {                                                      \
+            err = std::string(#call) + " failed: " + cudaGetErrorString(e_);          \
+            return fail(PHMM_ERR_CUDA);                                               \
+        }                                                                             \
+    } while (0)
+    SW_CKC(cudaSetDevice(device));
+    SW_CKC(cudaDeviceGetAttribute(&a->sms_, cudaDevAttrMultiProcessorCount, device));
+    for (int c = 0; c < kSwClasses; ++c) {
+        int b = 0;
+        SW_CKC(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kSwKernels[c], 32 * kSwBlockWarps, 0));
+        a->occ_[c] = std::max(b, 1);
+    }
+    SW_CKC(cudaStreamCreateWithFlags(&a->stream_, cudaStreamNonBlocking));
+    SW_CKC(cudaEventCreate(&a->ev_[0]));
+    SW_CKC(cudaEventCreate(&a->ev_[1]));
+#undef SW_CKC
+    *out = a;
+    return PHMM_OK;
+}
+
+SwAligner::~SwAligner()
+{
+    cudaSetDevice(dev_);
+    if (arena_) cudaFree(arena_);
+    if (pinned_) cudaFreeHost(pinned_);
+    for (auto& e : ev_)
+        if (e) cudaEventDestroy(e);
+    if (stream_) cudaStreamDestroy(stream_);
+}
+
+void SwAligner::plan(const SwParams& prm, int variant, uint32_t n, const SwItem* items, Plan& p) const
+{
+    p.n = n;
+    std::vector<uint8_t> cls(n);
+    uint32_t counts[kSwClasses] = {};
+    for (uint32_t q = 0; q < n; ++q) {
+        cls[q] = (uint8_t)sw_class_of(prm, variant, items[q].hap_len, items[q].read_len);
+        ++counts[cls[q]];
+        p.cells += (uint64_t)items[q].hap_len * items[q].read_len;
+    }
+    p.begin[0] = 0;
+    for (int c = 0; c < kSwClasses; ++c) p.begin[c + 1] = p.begin[c] + counts[c];
+    p.order.assign(n, 0);
+    uint32_t fill[kSwClasses];
+    std::copy(p.begin, p.begin + kSwClasses, fill);
+    for (uint32_t q = 0; q < n; ++q) p.order[fill[cls[q]]++] = q;
+    p.scratch = 0;
+    for (int c = 0; c < kSwClasses; ++c) {
+        auto first = p.order.begin() + p.begin[c], lastp = p.order.begin() + p.begin[c + 1];
+        std::stable_sort(first, lastp, [&](uint32_t x, uint32_t y) {
+            return (uint64_t)items[x].hap_len * items[x].read_len > (uint64_t)items[y].hap_len * items[y].read_len;
+        });
+        uint64_t stride = 256;
+        for (auto it = first; it != lastp; ++it) {
+            const SwItem& x = items[*it];
+            if (std::max(x.hap_len, x.read_len) >= (uint32_t)kSwMaxSeq) continue;  // refused: no scratch
+            stride = std::max(stride, sw_layout(x.hap_len, x.read_len, kSwK[c]).total);
+        }
+        p.stride[c] = stride;
+        const uint32_t m = counts[c];
+        uint64_t g = std::min<uint64_t>((m + kSwBlockWarps - 1) / kSwBlockWarps, (uint64_t)occ_[c] * sms_);
+        g = std::min<uint64_t>(g, std::max<uint64_t>(1, kSwScratchCap / (kSwBlockWarps * stride)));
+        p.grid[c] = m == 0 ? 0 : (int)g;
+        p.scratch = std::max(p.scratch, (uint64_t)p.grid[c] * kSwBlockWarps * stride);
+    }
+}
+
+phmm_status SwAligner::launch(const Plan& p, const SwParams& prm, int variant, const void* d_items,
+                              const uint32_t* d_order, const uint8_t* d_hap, const uint8_t* d_read,
+                              uint8_t* d_scratch, unsigned int* d_claim, phmm_sw_result* d_out, uint32_t* d_cigar,
+                              uint32_t cigar_cap, cudaStream_t st, float* class_ms, std::string& err)
+{
+    SW_CK(cudaMemsetAsync(d_claim, 0, sizeof(unsigned int) * kSwClasses, st));
+    for (int c = 0; c < kSwClasses; ++c) {
+        if (class_ms) class_ms[c] = 0.f;
+        if (p.grid[c] == 0) continue;
+        SwView v{};
+        v.items = (const SwItem*)d_items;
+        v.order = d_order + p.begin[c];
+        v.n = p.begin[c + 1] - p.begin[c];
+        v.hap = d_hap;
+        v.read = d_read;
+        v.prm = prm;
+        v.variant = variant;
+        v.scratch = d_scratch;
+        v.stride = p.stride[c];
+        v.claim = d_claim + c;
+        v.out = d_out;
+        v.cigar = d_cigar;
+        v.cigar_cap = cigar_cap;
+        if (class_ms) SW_CK(cudaEventRecord(ev_[0], st));
+        kSwKernels[c]<<<p.grid[c], 32 * kSwBlockWarps, 0, st>>>(v);
+        SW_CK(cudaGetLastError());
+        if (class_ms) {
+            SW_CK(cudaEventRecord(ev_[1], st));
+            SW_CK(cudaEventSynchronize(ev_[1]));
+            SW_CK(cudaEventElapsedTime(&class_ms[c], ev_[0], ev_[1]));
+        }
+    }
+    return PHMM_OK;
+}
+
+phmm_status SwAligner::align(const SwParams& prm, int variant, uint32_t n, const SwItem* items, const uint8_t* hap,
+                             uint64_t hap_bytes, const uint8_t* read, uint64_t read_bytes, phmm_sw_result* out,
+                             uint32_t* cigar, uint32_t cigar_cap, float* device_ms, std::string& err)
+{
+    if (device_ms) *device_ms = 0.f;
+    if (n == 0) return PHMM_OK;
+    phmm_status cs = check_items(n, items, hap_bytes, read_bytes, err);
+    if (cs != PHMM_OK) return cs;
+    std::lock_guard<std::mutex> lk(mu_);
+    SW_CK(cudaSetDevice(dev_));
+    Plan p;
+    plan(prm, variant, n, items, p);
+    // arena: items | order | hap | read | claim | out | cigar | scratch
+    const uint64_t o_items = 0;
+    const uint64_t o_order = a256(o_items + sizeof(SwItem) * (uint64_t)n);
+    const uint64_t o_hap = a256(o_order + 4ull * n);
+    const uint64_t o_read = a256(o_hap + std::max<uint64_t>(hap_bytes, 1));
+    const uint64_t o_claim = a256(o_read + std::max<uint64_t>(read_bytes, 1));
+    const uint64_t o_out = a256(o_claim + 4ull * kSwClasses);
+    const uint64_t o_cigar = a256(o_out + sizeof(phmm_sw_result) * (uint64_t)n);
+    const uint64_t o_scr = a256(o_cigar + 4ull * n * cigar_cap);
+    const uint64_t need = o_scr + p.scratch;
+    if (need > arena_bytes_) {
+        if (arena_) {
+            SW_CK(cudaStreamSynchronize(stream_));
+            cudaFree(arena_);
+            arena_ = nullptr;
+            arena_bytes_ = 0;
+        }
+        const uint64_t sz = need + need / 4;
+        if (cudaMalloc(&arena_, sz) != cudaSuccess) {
+            cudaGetLastError();
+            err = "Smith-Waterman arena of " + std::to_string(sz) + " bytes could not be allocated";
+            return PHMM_ERR_OUT_OF_MEMORY;
+        }
+        arena_bytes_ = sz;
+    }
+    // inputs through pinned staging: items | order | hap | read; outputs back: out | cigar
+    const uint64_t in_bytes = o_claim, out_bytes = o_scr - o_out;
+    const uint64_t stage = std::max(in_bytes, out_bytes);
+    if (stage > pinned_bytes_) {
+        if (pinned_) cudaFreeHost(pinned_);
+        pinned_ = nullptr;
+        pinned_bytes_ = 0;
+        SW_CK(cudaMallocHost(&pinned_, stage + stage / 4));
+        pinned_bytes_ = stage + stage / 4;
+    }
+    uint8_t* h = (uint8_t*)pinned_;
+    uint8_t* d = (uint8_t*)arena_;
+    std::memcpy(h + o_items, items, sizeof(SwItem) * (size_t)n);
+    std::memcpy(h + o_order, p.order.data(), 4ull * n);
+    if (hap_bytes) std::memcpy(h + o_hap, hap, hap_bytes);
+    if (read_bytes) std::memcpy(h + o_read, read, read_bytes);
+    SW_CK(cudaMemcpyAsync(d, h, in_bytes, cudaMemcpyHostToDevice, stream_));
+    SW_CK(cudaEventRecord(ev_[0], stream_));
+    phmm_status st = launch(p, prm, variant, d + o_items, (const uint32_t*)(d + o_order), d + o_hap, d + o_read,
+                            d + o_scr, (unsigned int*)(d + o_claim), (phmm_sw_result*)(d + o_out),
+                            (uint32_t*)(d + o_cigar), cigar_cap, stream_, nullptr, err);
+    if (st != PHMM_OK) return st;
+    SW_CK(cudaEventRecord(ev_[1], stream_));
+    SW_CK(cudaMemcpyAsync(h, d + o_out, out_bytes, cudaMemcpyDeviceToHost, stream_));
+    SW_CK(cudaStreamSynchronize(stream_));
+    if (device_ms) SW_CK(cudaEventElapsedTime(device_ms, ev_[0], ev_[1]));
+    std::memcpy(out, h, sizeof(phmm_sw_result) * (size_t)n);
+    if (cigar && cigar_cap) std::memcpy(cigar, h + (o_cigar - o_out), 4ull * n * cigar_cap);
+    return PHMM_OK;
+}
+
+phmm_status SwAligner::resident_create(const SwParams& prm, int variant, uint32_t n, const SwItem* items,
+                                       const uint8_t* hap, uint64_t hap_bytes, const uint8_t* read,
+                                       uint64_t read_bytes, uint32_t cigar_cap, Resident** out, std::string& err)
+{
+    *out = nullptr;
+    phmm_status cs = check_items(n, items, hap_bytes, read_bytes, err);
+    if (cs != PHMM_OK) return cs;
+    std::lock_guard<std::mutex> lk(mu_);
+    SW_CK(cudaSetDevice(dev_));
+    Resident* r = new Resident();
+    r->prm = prm;
+    r->variant = variant;
+    r->cigar_cap = cigar_cap;
+    plan(prm, variant, n, items, r->plan);
+    const uint64_t o_items = 0;
+    const uint64_t o_order = a256(o_items + sizeof(SwItem) * (uint64_t)n);
+    const uint64_t o_hap = a256(o_order + 4ull * n);
+    const uint64_t o_read = a256(o_hap + std::max<uint64_t>(hap_bytes, 1));
+    const uint64_t o_claim = a256(o_read + std::max<uint64_t>(read_bytes, 1));
+    const uint64_t o_out = a256(o_claim + 4ull * kSwClasses);
+    const uint64_t o_cigar = a256(o_out + sizeof(phmm_sw_result) * (uint64_t)n);
+    const uint64_t o_scr = a256(o_cigar + 4ull * n * cigar_cap);
+    const uint64_t need = o_scr + r->plan.scratch;
+    if (cudaMalloc(&r->arena, need) != cudaSuccess) {
+        cudaGetLastError();
+        delete r;
+        err = "Smith-Waterman resident arena of " + std::to_string(need) + " bytes could not be allocated";
+        return PHMM_ERR_OUT_OF_MEMORY;
+    }
+    uint8_t* d = (uint8_t*)r->arena;
+    r->items = (SwItem*)(d + o_items);
+    r->order = (uint32_t*)(d + o_order);
+    r->hap = d + o_hap;
+    r->read = d + o_read;
+    r->claim = (unsigned int*)(d + o_claim);
+    r->out = (phmm_sw_result*)(d + o_out);
+    r->cigar = (uint32_t*)(d + o_cigar);
+    r->scratch = d + o_scr;
+    auto up = [&](void* dst, const void* src, uint64_t bytes) {
+        return bytes ? cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream_) : cudaSuccess;
+    };
+    cudaError_t e = up(r->items, items, sizeof(SwItem) * (uint64_t)n);
+    if (e == cudaSuccess) e = up(r->order, r->plan.order.data(), 4ull * n);
+    if (e == cudaSuccess) e = up(r->hap, hap, hap_bytes);
+    if (e == cudaSuccess) e = up(r->read, read, read_bytes);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+    if (e != cudaSuccess) {
+        err = std::string("Smith-Waterman resident upload failed: ") + cudaGetErrorString(e);
+        cudaFree(r->arena);
+        delete r;
+        return PHMM_ERR_CUDA;
+    }
+    *out = r;
+    return PHMM_OK;
+}
+
+phmm_status SwAligner::resident_run(Resident* r, int iterations, float* ms_per_run, float* class_ms, std::string& err)
+{
+    std::lock_guard<std::mutex> lk(mu_);
+    SW_CK(cudaSetDevice(dev_));
+    if (ms_per_run) *ms_per_run = 0.f;
+    if (iterations > 0) {
+        SW_CK(cudaEventRecord(ev_[0], stream_));
+        for (int it = 0; it < iterations; ++it) {
+            phmm_status st = launch(r->plan, r->prm, r->variant, r->items, r->order, r->hap, r->read, r->scratch,
+                                    r->claim, r->out, r->cigar, r->cigar_cap, stream_, nullptr, err);
+            if (st != PHMM_OK) return st;
+        }
+        SW_CK(cudaEventRecord(ev_[1], stream_));
+        SW_CK(cudaEventSynchronize(ev_[1]));
+        float ms = 0.f;
+        SW_CK(cudaEventElapsedTime(&ms, ev_[0], ev_[1]));
+        if (ms_per_run) *ms_per_run = ms / iterations;
+    }
+    if (class_ms) {
+        phmm_status st = launch(r->plan, r->prm, r->variant, r->items, r->order, r->hap, r->read, r->scratch,
+                                r->claim, r->out, r->cigar, r->cigar_cap, stream_, class_ms, err);
+        if (st != PHMM_OK) return st;
+        SW_CK(cudaStreamSynchronize(stream_));
+    }
+    return PHMM_OK;
+}
+
+phmm_status SwAligner::resident_results(Resident* r, phmm_sw_result* out, uint32_t* cigar, std::string& err)
+{
+    std::lock_guard<std::mutex> lk(mu_);
+    SW_CK(cudaSetDevice(dev_));
+    const uint32_t n = r->plan.n;
+    if (out && n) SW_CK(cudaMemcpyAsync(out, r->out, sizeof(phmm_sw_result) * (uint64_t)n, cudaMemcpyDeviceToHost, stream_));
+    if (cigar && n && r->cigar_cap)
+        SW_CK(cudaMemcpyAsync(cigar, r->cigar, 4ull * n * r->cigar_cap, cudaMemcpyDeviceToHost, stream_));
+    SW_CK(cudaStreamSynchronize(stream_));
+    return PHMM_OK;
+}
+
+void SwAligner::resident_destroy(Resident* r)
+{
+    if (!r) return;
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        cudaSetDevice(dev_);
+        cudaStreamSynchronize(stream_);
+        if (r->arena) cudaFree(r->arena);
+    }
+    delete r;
+}
+
+}  // namespace phmm

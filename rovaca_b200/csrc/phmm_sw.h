@@ -1,0 +1,133 @@
+// Smith-Waterman realignment of reads to haplotypes on the GPU (kernels and host side in phmm_sw.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/phmm_b200.h"
+
+namespace phmm {
+
+struct SwParams {
+    int32_t match, mismatch, gap_open, gap_extend;
+};
+
+// One alignment: seq1 = haplotype (rows), seq2 = read (columns); byte offsets into the base buffers.
+struct SwItem {
+    uint64_t hap_start, read_start;
+    uint32_t hap_len, read_len;
+};
+static_assert(sizeof(SwItem) == 24, "SwItem layout");
+
+// Reference limit: inputs whose longer sequence has kSwMaxSeq bases or more are refused with
+// alignment offset 1 (sw_core_template.h:354-361, MAX_SEQ_LEN of sw_avx.c:18).
+constexpr int kSwMaxSeq = 2048;
+constexpr int kSwBlockWarps = 4;
+constexpr int kSwBandWords = 1024;   // trace-back band in shared memory per warp (4 KB)
+constexpr int kSwClasses = 13;       // 12 stripe widths (kSwK) + the 16-bit wrap-around class
+constexpr int kSwWrapClass = 12;
+constexpr int kSwK[kSwClasses] = {1, 2, 3, 4, 5, 6, 8, 10, 12, 16, 20, 24, 24};
+
+// Per-warp scratch layout of one alignment (bytes, 256-aligned sections):
+//   bt    [stripes][nrow][32 * nw] u32: per cell a 4-bit code (state 1/2 | extension flags 4/8)
+//   bh/be [nrow + 1] i32: H and E of the stripe's right edge column, handed to the next stripe
+//   lrow  [ncol + 1] i32: H of the last row; lcol [nrow + 1] i32: H of the last column
+//   runs  [nrow + ncol + 4] u32: CIGAR runs in trace-back order
+struct SwLayout {
+    uint64_t bt, bh, be, lrow, lcol, runs, total;
+};
+
+__host__ __device__ inline uint64_t sw_align256(uint64_t x) { return (x + 255) & ~uint64_t(255); }
+
+__host__ __device__ inline SwLayout sw_layout(uint32_t nrow, uint32_t ncol, int K)
+{
+    const uint64_t nw = (uint64_t)(K + 7) / 8;
+    const uint64_t cols = 32ull * K;
+    const uint64_t stripes = ncol ? (ncol + cols - 1) / cols : 1;
+    SwLayout L;
+    L.bt = 0;
+    uint64_t o = sw_align256(stripes * nrow * 32ull * nw * 4ull);
+    L.bh = o;
+    o = sw_align256(o + 4ull * (nrow + 1));
+    L.be = o;
+    o = sw_align256(o + 4ull * (nrow + 1));
+    L.lrow = o;
+    o = sw_align256(o + 4ull * (ncol + 1));
+    L.lcol = o;
+    o = sw_align256(o + 4ull * (nrow + 1));
+    L.runs = o;
+    o = sw_align256(o + 4ull * (nrow + ncol + 4));
+    L.total = o;
+    return L;
+}
+
+// ro_sw_should_use_int32_avx512 (ro_sw.c:26-40): int32 for reads under 16 bases, match <= 0, or
+// min(length) x match above INT16_MAX; int16 otherwise.  variant: 0 as the reference, 1 int32, 2 int16.
+__host__ __device__ inline bool sw_uses_int32(int variant, uint32_t nrow, uint32_t ncol, int32_t match)
+{
+    if (variant == 1) return true;
+    if (variant == 2) return false;
+    if (ncol < 16 || match <= 0) return true;
+    const uint32_t m = nrow < ncol ? nrow : ncol;
+    return (long long)m * match > 32767;
+}
+
+// True when the 16-bit kernel's adds cannot wrap for these (16-bit) parameters, so that 32-bit
+// arithmetic with the 16-bit constants gives its results: scores stay within [cutoff + open + extend,
+// min(length) x match] (checked against [-32768, 32767] with the 16-bit low -16384 and cutoff -8192).
+__host__ __device__ inline bool sw_w16_cannot_wrap(int32_t match, int32_t mismatch, int32_t open, int32_t ext)
+{
+    return mismatch <= match && open <= 0 && ext <= 0 && mismatch >= -24576 && open + ext >= -24576 &&
+           ext >= -16384;
+}
+
+int sw_class_of(const SwParams& prm, int variant, uint32_t nrow, uint32_t ncol);
+
+// Device state of the aligner: a stream, a growable arena and pinned staging, owned by an engine.
+class SwAligner {
+public:
+    static phmm_status create(int device, SwAligner** out, std::string& err);
+    ~SwAligner();
+
+    // Host buffers in and out (copies inside), synchronous.  out[n]; cigar[n][cigar_cap].
+    phmm_status align(const SwParams& prm, int variant, uint32_t n, const SwItem* items, const uint8_t* hap,
+                      uint64_t hap_bytes, const uint8_t* read, uint64_t read_bytes, phmm_sw_result* out,
+                      uint32_t* cigar, uint32_t cigar_cap, float* device_ms, std::string& err);
+
+    // Resident batches: planned and uploaded once, run many times, results read back on demand.
+    struct Resident;
+    phmm_status resident_create(const SwParams& prm, int variant, uint32_t n, const SwItem* items,
+                                const uint8_t* hap, uint64_t hap_bytes, const uint8_t* read, uint64_t read_bytes,
+                                uint32_t cigar_cap, Resident** out, std::string& err);
+    phmm_status resident_run(Resident* r, int iterations, float* ms_per_run, float* class_ms, std::string& err);
+    phmm_status resident_results(Resident* r, phmm_sw_result* out, uint32_t* cigar, std::string& err);
+    void resident_destroy(Resident* r);
+
+    int device() const { return dev_; }
+
+private:
+    SwAligner() = default;
+    struct Plan;
+    void plan(const SwParams& prm, int variant, uint32_t n, const SwItem* items, Plan& p) const;
+    phmm_status launch(const Plan& p, const SwParams& prm, int variant, const void* d_items,
+                       const uint32_t* d_order, const uint8_t* d_hap, const uint8_t* d_read, uint8_t* d_scratch,
+                       unsigned int* d_claim, phmm_sw_result* d_out, uint32_t* d_cigar, uint32_t cigar_cap,
+                       cudaStream_t st, float* class_ms, std::string& err);
+
+    int dev_ = 0;
+    int sms_ = 0;
+    int occ_[kSwClasses] = {};
+    cudaStream_t stream_ = nullptr;
+    cudaEvent_t ev_[2] = {};
+    void* arena_ = nullptr;
+    size_t arena_bytes_ = 0;
+    void* pinned_ = nullptr;
+    size_t pinned_bytes_ = 0;
+    std::mutex mu_;
+};
+
+}  // namespace phmm

@@ -239,6 +239,19 @@ class Engine:
     def version() -> str:
         return _lib.load().phmm_version().decode()
 
+    def sw_align(self, batch, params=None, variant: int = 0, cigar_cap: int | None = None):
+        """Smith-Waterman realignment of a batch of (haplotype, read) pairs (rovaca_b200.sw)."""
+        from . import sw
+
+        return sw.align(self, batch, sw.GENOTYPING if params is None else params, variant,
+                        sw.MAX_CIGAR if cigar_cap is None else cigar_cap)
+
+    def sw_resident(self, batch, params=None, variant: int = 0, cigar_cap: int | None = None):
+        from . import sw
+
+        return sw.SwResident(self, batch, sw.GENOTYPING if params is None else params, variant,
+                             sw.MAX_CIGAR if cigar_cap is None else cigar_cap)
+
     # ---- batched -----------------------------------------------------------------------
     def compute(self, batch: PackedBatch, want_flags: bool = False, out: np.ndarray | None = None,
                 flags: np.ndarray | None = None):

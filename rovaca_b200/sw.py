@@ -1,0 +1,189 @@
+"""Smith-Waterman realignment of reads to haplotypes on the GPU (phmm_sw_align in include/phmm_b200.h).
+
+The reference aligns one read at a time through a ``lib_sw_avx`` context (seq1 = haplotype, seq2 =
+read, ``sw->avx_function(sw)``; genotype/utils/alignment_utils.cpp:571-579) and reads back score,
+alignment offset and CIGAR.  Here a batch of (haplotype, read) pairs goes to the device in one call and
+every pair's fields come back, equal to the reference's.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from typing import Sequence
+
+import numpy as np
+
+from . import _lib
+
+GENOTYPING = (10, -15, -30, -5)   # sw_parameters_genotype, lib/sw_avx/sw_avx.c:15
+ASSEMBLY = (200, -150, -260, -11)  # sw_parameters_assemble, lib/sw_avx/sw_avx.c:14
+MAX_CIGAR = 2047                   # the reference emits at most cigar_max_len - 1 ops (sw_cigar.c:164)
+CIGAR_OPS = "MIDNSHP=XB"
+
+SW_ITEM_DTYPE = np.dtype([("hap_offset", "<u8"), ("read_offset", "<u8"), ("hap_len", "<u4"), ("read_len", "<u4")])
+SW_RESULT_DTYPE = np.dtype([("score", "<i4"), ("alignment_offset", "<i4"), ("max_i", "<i4"), ("max_j", "<i4"),
+                            ("cigar_count", "<u4"), ("reserved", "<u4")])
+
+
+def cigar_string(ops) -> str:
+    return "".join(f"{int(c) >> 4}{CIGAR_OPS[int(c) & 15]}" for c in ops)
+
+
+def _bytes(x) -> bytes:
+    if isinstance(x, str):
+        return x.encode()
+    return bytes(x)
+
+
+@dataclass
+class SwBatch:
+    """Packed alignments: haplotype and read bases concatenated, one item per pair."""
+
+    hap_bases: np.ndarray   # uint8
+    read_bases: np.ndarray  # uint8
+    items: np.ndarray       # SW_ITEM_DTYPE
+
+    @property
+    def n(self) -> int:
+        return int(self.items.shape[0])
+
+    @property
+    def cells(self) -> int:
+        return int((self.items["hap_len"].astype(np.uint64) * self.items["read_len"].astype(np.uint64)).sum())
+
+    @classmethod
+    def from_pairs(cls, pairs: Sequence[tuple[bytes, bytes]]) -> "SwBatch":
+        """One item per (haplotype, read) pair; equal haplotypes given as the same object are stored once."""
+        haps, hap_at = [], {}
+        reads = []
+        items = np.zeros(len(pairs), SW_ITEM_DTYPE)
+        hoff = roff = 0
+        for q, (h, r) in enumerate(pairs):
+            key = id(h)
+            if key not in hap_at:
+                hb = _bytes(h)
+                hap_at[key] = (hoff, len(hb))
+                haps.append(hb)
+                hoff += len(hb)
+            items[q]["hap_offset"], items[q]["hap_len"] = hap_at[key]
+            rb = _bytes(r)
+            items[q]["read_offset"], items[q]["read_len"] = roff, len(rb)
+            reads.append(rb)
+            roff += len(rb)
+        return cls(np.frombuffer(b"".join(haps), np.uint8).copy(), np.frombuffer(b"".join(reads), np.uint8).copy(),
+                   items)
+
+    def pair(self, q: int) -> tuple[bytes, bytes]:
+        it = self.items[q]
+        h = self.hap_bases[int(it["hap_offset"]):int(it["hap_offset"]) + int(it["hap_len"])].tobytes()
+        r = self.read_bases[int(it["read_offset"]):int(it["read_offset"]) + int(it["read_len"])].tobytes()
+        return h, r
+
+
+def _params(params) -> C.Array:
+    p = tuple(int(x) for x in (params if params is not None else GENOTYPING))
+    if len(p) != 4:
+        raise ValueError("params = (match, mismatch, gap_open, gap_extend)")
+    return (C.c_int32 * 4)(*p)
+
+
+def _ptr(a: np.ndarray):
+    return C.c_void_p(a.ctypes.data) if a.size else None
+
+
+def _check_variant(variant: int) -> None:
+    if variant not in (0, 1, 2):
+        raise ValueError("variant must be 0 (the reference's choice), 1 (int32) or 2 (int16)")
+
+
+@dataclass
+class SwResults:
+    """Per alignment: score, alignment_offset, max_i, max_j, cigar_count (SW_RESULT_DTYPE) and the
+    CIGAR ops [n, cigar_cap] (BAM encoding, read order)."""
+
+    fields: np.ndarray
+    cigars: np.ndarray
+
+    def __len__(self) -> int:
+        return int(self.fields.shape[0])
+
+    def ops(self, q: int) -> list[int]:
+        n = min(int(self.fields[q]["cigar_count"]), self.cigars.shape[1])
+        return [int(x) for x in self.cigars[q, :n]]
+
+    def cigar(self, q: int) -> str:
+        return cigar_string(self.ops(q))
+
+    def tuple(self, q: int):
+        """(score, alignment_offset, max_i, max_j, ops): the oracle's result layout."""
+        f = self.fields[q]
+        return int(f["score"]), int(f["alignment_offset"]), int(f["max_i"]), int(f["max_j"]), self.ops(q)
+
+
+def align(engine, batch: SwBatch, params=GENOTYPING, variant: int = 0, cigar_cap: int = MAX_CIGAR) -> SwResults:
+    """Aligns every pair of the batch on the engine's device (host buffers in and out)."""
+    _check_variant(variant)
+    lib = _lib.load()
+    n = batch.n
+    fields = np.zeros(n, SW_RESULT_DTYPE)
+    cigars = np.zeros((n, cigar_cap), np.uint32)
+    if n:
+        _lib.check(lib.phmm_sw_align(engine._h, _params(params), variant, n, _ptr(batch.items),
+                                     _ptr(batch.hap_bases), batch.hap_bases.size, _ptr(batch.read_bases),
+                                     batch.read_bases.size, _ptr(fields), _ptr(cigars) if cigar_cap else None,
+                                     cigar_cap))
+    return SwResults(fields, cigars)
+
+
+class SwResident:
+    """A batch kept on the device: run it many times (device time per run), read results on demand."""
+
+    def __init__(self, engine, batch: SwBatch, params=GENOTYPING, variant: int = 0, cigar_cap: int = MAX_CIGAR):
+        _check_variant(variant)
+        self._lib = _lib.load()
+        self.engine = engine
+        self.n = batch.n
+        self.cells = batch.cells
+        self.cigar_cap = cigar_cap
+        h = C.c_void_p()
+        _lib.check(self._lib.phmm_sw_resident_create(engine._h, _params(params), variant, self.n, _ptr(batch.items),
+                                                     _ptr(batch.hap_bases), batch.hap_bases.size,
+                                                     _ptr(batch.read_bases), batch.read_bases.size, cigar_cap,
+                                                     C.byref(h)))
+        self._h = h
+
+    def run(self, iterations: int = 1) -> float:
+        """Runs the batch `iterations` times back to back; returns device ms per run."""
+        ms = C.c_float()
+        _lib.check(self._lib.phmm_sw_resident_run(self._h, iterations, C.byref(ms), None))
+        return float(ms.value)
+
+    def profile(self) -> np.ndarray:
+        """Device ms of each kernel class in one run (13 classes: stripe widths 1..24, then the 16-bit
+        wrap-around class)."""
+        cls = (C.c_float * 13)()
+        _lib.check(self._lib.phmm_sw_resident_run(self._h, 0, None, C.cast(cls, C.c_void_p)))
+        return np.array(cls[:], np.float32)
+
+    def results(self) -> SwResults:
+        fields = np.zeros(self.n, SW_RESULT_DTYPE)
+        cigars = np.zeros((self.n, self.cigar_cap), np.uint32)
+        _lib.check(self._lib.phmm_sw_resident_results(self._h, _ptr(fields), _ptr(cigars) if self.cigar_cap else None))
+        return SwResults(fields, cigars)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            self._lib.phmm_sw_resident_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

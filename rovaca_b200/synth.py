@@ -214,3 +214,28 @@ def genotyping_regions(n_regions: int, seed: int = 5, depth: int = 40, read_len:
         out.append({"haplotypes": [ACGT[h].tobytes() for h in haps], "reads": reads, "quals": quals,
                     "mapq": np.full(depth, 60, np.uint8), "events": events, "truth": truth})
     return out
+
+
+def sw_realignment(pb: PackedBatch, best_hap: np.ndarray | None = None):
+    """Every read of every region against one haplotype of its own region, as HaplotypeCaller
+    realigns reads to their best haplotype: best_hap[q] (index within the read's region) when given,
+    else haplotype q mod n_haps of the region.  Returns an ``sw.SwBatch`` over the batch's base buffers."""
+    from .sw import SW_ITEM_DTYPE, SwBatch
+
+    nh = pb.n_haps.astype(np.int64)
+    nr = pb.n_reads.astype(np.int64)
+    g = np.repeat(np.arange(len(nr)), nr)
+    first_read = np.concatenate([[0], np.cumsum(nr)[:-1]])
+    first_hap = np.concatenate([[0], np.cumsum(nh)[:-1]])
+    local = np.arange(int(nr.sum())) - first_read[g]
+    pick = local % nh[g] if best_hap is None else np.asarray(best_hap, np.int64)
+    h = first_hap[g] + pick
+    hap_off = pb.hap_off.astype(np.uint64)
+    read_off = pb.read_off.astype(np.uint64)
+    items = np.zeros(len(g), SW_ITEM_DTYPE)
+    items["hap_offset"] = hap_off[h]
+    items["hap_len"] = (hap_off[h + 1] - hap_off[h]).astype(np.uint32)
+    items["read_offset"] = read_off[:-1]
+    items["read_len"] = np.diff(read_off).astype(np.uint32)
+    return SwBatch(pb.hap_bases, pb.read_bases, items)
+
