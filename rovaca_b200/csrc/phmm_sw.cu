@@ -324,7 +324,8 @@ int sw_class_of(const SwParams& prm, int variant, uint32_t nrow, uint32_t ncol)
 {
     if (!sw_uses_int32(variant, nrow, ncol, prm.match) && ncol > 0 && nrow > 0 &&
         std::max(nrow, ncol) < (uint32_t)kSwMaxSeq &&
-        !sw_w16_cannot_wrap((short)prm.match, (short)prm.mismatch, (short)prm.gap_open, (short)prm.gap_extend))
+        !sw_w16_cannot_wrap((short)prm.match, (short)prm.mismatch, (short)prm.gap_open, (short)prm.gap_extend,
+                            std::min(nrow, ncol)))
         return kSwWrapClass;
     const uint32_t k = std::max<uint32_t>(1, (ncol + 31) / 32);
     for (int c = 0; c < kSwWrapClass; ++c)

@@ -76,13 +76,16 @@ __host__ __device__ inline bool sw_uses_int32(int variant, uint32_t nrow, uint32
     return (long long)m * match > 32767;
 }
 
-// True when the 16-bit kernel's adds cannot wrap for these (16-bit) parameters, so that 32-bit
-// arithmetic with the 16-bit constants gives its results: scores stay within [cutoff + open + extend,
-// min(length) x match] (checked against [-32768, 32767] with the 16-bit low -16384 and cutoff -8192).
-__host__ __device__ inline bool sw_w16_cannot_wrap(int32_t match, int32_t mismatch, int32_t open, int32_t ext)
+// True when the 16-bit kernel's adds cannot wrap for these (16-bit) parameters and the shorter
+// sequence's length, so that 32-bit arithmetic with the 16-bit constants gives its results: scores
+// stay within [cutoff + open + extend, min(length) x match] (checked against [-32768, 32767] with the
+// 16-bit low -16384 and cutoff -8192).  The reference's own kernel choice already bounds
+// min(length) x match; a forced 16-bit kernel does not.
+__host__ __device__ inline bool sw_w16_cannot_wrap(int32_t match, int32_t mismatch, int32_t open, int32_t ext,
+                                                   uint32_t min_len)
 {
     return mismatch <= match && open <= 0 && ext <= 0 && mismatch >= -24576 && open + ext >= -24576 &&
-           ext >= -16384;
+           ext >= -16384 && (match <= 0 || (long long)min_len * match <= 32767);
 }
 
 int sw_class_of(const SwParams& prm, int variant, uint32_t nrow, uint32_t ncol);
