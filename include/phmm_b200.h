@@ -364,25 +364,30 @@ typedef struct phmm_sw_result {
     int32_t score;
     int32_t alignment_offset;   /* haplotype position of the first aligned read base */
     int32_t max_i, max_j;       /* end cell of the alignment (haplotype, read) */
-    uint32_t cigar_count;       /* CIGAR ops of the alignment (at most 2047); the first
-                                   min(cigar_count, cigar_cap) are written */
-    uint32_t reserved;
+    uint32_t cigar_count;       /* CIGAR ops of the alignment (at most 2047) */
+    uint32_t cigar_offset;      /* its first op in `cigars`; min(cigar_count, cigar_cap) ops stored */
 } phmm_sw_result;
 
 /* params = {match, mismatch, gap_open, gap_extend} (NULL: the genotyping parameters 10, -15, -30,
  * -5 of lib/sw_avx/sw_avx.c:15; the assembler uses 200, -150, -260, -11).  variant: 0 = the
- * reference's kernel choice, 1 = its int32 kernel, 2 = its int16 kernel.  cigars: n x cigar_cap
- * BAM-encoded ops (length << 4 | op; M 0, I 1, D 2, S 4) in read order.  All pointers are host
- * memory; the call copies in, runs on the engine's device and copies out before it returns. */
+ * reference's kernel choice, 1 = its int32 kernel, 2 = its int16 kernel.
+ * CIGARs come back compact, in item order: item q's first min(cigar_count, cigar_cap) ops (BAM
+ * encoding, length << 4 | op with M 0, I 1, D 2, S 4; read order) at cigars[results[q].cigar_offset].
+ * cigar_cap bounds the ops stored per item (0: none; 2047 or more: all).  cigars holds
+ * cigar_capacity ops; *cigar_total (optional) receives the ops the batch needs.  If they exceed
+ * cigar_capacity the call returns PHMM_ERR_LIMIT_EXCEEDED with results filled and cigars untouched.
+ * All pointers are host memory; the call copies in, runs on the engine's device and copies out
+ * before it returns. */
 PHMM_API phmm_status phmm_sw_align(phmm_engine* engine, const int32_t* params, int32_t variant, uint32_t n,
                                    const phmm_sw_item* items, const uint8_t* hap_bases, uint64_t hap_bytes,
-                                   const uint8_t* read_bases, uint64_t read_bytes, phmm_sw_result* results,
-                                   uint32_t* cigars, uint32_t cigar_cap);
+                                   const uint8_t* read_bases, uint64_t read_bytes, uint32_t cigar_cap,
+                                   phmm_sw_result* results, uint32_t* cigars, uint64_t cigar_capacity,
+                                   uint64_t* cigar_total);
 
 /* Device-resident Smith-Waterman batch (no reference counterpart: it exists to time the kernels with
  * the inputs already in HBM).  Created from host buffers, run `iterations` times back to back
  * (ms_per_run: CUDA-event time per run on the aligner's stream; class_ms[13], optional: time of each
- * kernel class in the last run), results read back on demand. */
+ * kernel class in the last run), results read back on demand (the layout of phmm_sw_align). */
 typedef struct phmm_sw_resident phmm_sw_resident;
 PHMM_API phmm_status phmm_sw_resident_create(phmm_engine* engine, const int32_t* params, int32_t variant,
                                              uint32_t n, const phmm_sw_item* items, const uint8_t* hap_bases,
@@ -391,7 +396,7 @@ PHMM_API phmm_status phmm_sw_resident_create(phmm_engine* engine, const int32_t*
 PHMM_API phmm_status phmm_sw_resident_run(phmm_sw_resident* resident, int32_t iterations, float* ms_per_run,
                                           float* class_ms);
 PHMM_API phmm_status phmm_sw_resident_results(phmm_sw_resident* resident, phmm_sw_result* results,
-                                              uint32_t* cigars);
+                                              uint32_t* cigars, uint64_t cigar_capacity, uint64_t* cigar_total);
 PHMM_API phmm_status phmm_sw_resident_destroy(phmm_sw_resident* resident);
 
 #ifdef __cplusplus

@@ -13,6 +13,7 @@ LIB_PATH = Path(__file__).resolve().parent / "libphmm_b200.so"
 HEADER_PATH = Path(__file__).resolve().parent.parent / "include" / "phmm_b200.h"
 
 PHMM_OK = 0
+PHMM_ERR_LIMIT_EXCEEDED = 2
 STATUS_NAMES = {
     0: "PHMM_OK", 1: "PHMM_ERR_INVALID_ARGUMENT", 2: "PHMM_ERR_LIMIT_EXCEEDED", 3: "PHMM_ERR_OUT_OF_MEMORY",
     4: "PHMM_ERR_CUDA", 5: "PHMM_ERR_NOT_INITIALIZED", 6: "PHMM_ERR_TIMEOUT", 7: "PHMM_ERR_CANCELLED",
@@ -123,7 +124,7 @@ class SwItem(C.Structure):
 
 class SwResult(C.Structure):
     _fields_ = [("score", C.c_int32), ("alignment_offset", C.c_int32), ("max_i", C.c_int32), ("max_j", C.c_int32),
-                ("cigar_count", C.c_uint32), ("reserved", C.c_uint32)]
+                ("cigar_count", C.c_uint32), ("cigar_offset", C.c_uint32)]
 
 
 _lib = None
@@ -168,10 +169,10 @@ def load() -> C.CDLL:
         "phmm_wait": (I32, [P, U64, I64, C.POINTER(D), C.POINTER(D)]),
         "phmm_cancel": (I32, [P, U64]),
         "phmm_server_stats_get": (I32, [P, P]),
-        "phmm_sw_align": (I32, [P, P, I32, U32, P, P, U64, P, U64, P, P, U32]),
+        "phmm_sw_align": (I32, [P, P, I32, U32, P, P, U64, P, U64, U32, P, P, U64, C.POINTER(U64)]),
         "phmm_sw_resident_create": (I32, [P, P, I32, U32, P, P, U64, P, U64, U32, C.POINTER(P)]),
         "phmm_sw_resident_run": (I32, [P, I32, C.POINTER(C.c_float), P]),
-        "phmm_sw_resident_results": (I32, [P, P, P]),
+        "phmm_sw_resident_results": (I32, [P, P, P, U64, C.POINTER(U64)]),
         "phmm_sw_resident_destroy": (I32, [P]),
     }
     for name, (res, args) in sig.items():

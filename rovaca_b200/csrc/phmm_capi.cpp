@@ -17,7 +17,8 @@ static_assert(PHMM_FP32_CLASSES == phmm::kClasses32 && PHMM_FP64_CLASSES == phmm
                   PHMM_TILE_MODES == phmm::kModes32 && PHMM_LEN_BUCKETS == phmm::kLenBuckets,
               "class counts differ between the C ABI and the kernels");
 
-static_assert(sizeof(phmm_sw_item) == sizeof(phmm::SwItem) && offsetof(phmm_sw_item, hap_len) == offsetof(phmm::SwItem, hap_len) &&
+static_assert(sizeof(phmm_sw_item) == sizeof(phmm::SwItem) &&
+                  offsetof(phmm_sw_item, hap_len) == offsetof(phmm::SwItem, hap_len) &&
                   offsetof(phmm_sw_item, read_offset) == offsetof(phmm::SwItem, read_start),
               "Smith-Waterman item layouts differ");
 
@@ -356,22 +357,23 @@ static phmm_status sw_get(phmm_engine* engine, phmm::SwAligner** a)
 
 phmm_status phmm_sw_align(phmm_engine* engine, const int32_t* params, int32_t variant, uint32_t n,
                           const phmm_sw_item* items, const uint8_t* hap_bases, uint64_t hap_bytes,
-                          const uint8_t* read_bases, uint64_t read_bytes, phmm_sw_result* results, uint32_t* cigars,
-                          uint32_t cigar_cap)
+                          const uint8_t* read_bases, uint64_t read_bytes, uint32_t cigar_cap, phmm_sw_result* results,
+                          uint32_t* cigars, uint64_t cigar_capacity, uint64_t* cigar_total)
 {
     PHMM_GUARD_BEGIN
     phmm::clear_error();
+    if (cigar_total) *cigar_total = 0;
     if (!engine) return set_error(PHMM_ERR_NOT_INITIALIZED, "engine is null");
     if (variant < 0 || variant > 2) return set_error(PHMM_ERR_INVALID_ARGUMENT, "variant must be 0, 1 or 2");
     if (n == 0) return PHMM_OK;
-    if (!items || !results || (hap_bytes && !hap_bases) || (read_bytes && !read_bases) || (cigar_cap && !cigars))
+    if (!items || !results || (hap_bytes && !hap_bases) || (read_bytes && !read_bases) || (cigar_capacity && !cigars))
         return set_error(PHMM_ERR_INVALID_ARGUMENT, "null buffer");
     phmm::SwAligner* a = nullptr;
     phmm_status st = sw_get(engine, &a);
     if (st != PHMM_OK) return st;
     std::string err;
     st = a->align(sw_params(params), variant, n, reinterpret_cast<const phmm::SwItem*>(items), hap_bases, hap_bytes,
-                  read_bases, read_bytes, results, cigars, cigar_cap, nullptr, err);
+                  read_bases, read_bytes, cigar_cap, results, cigars, cigar_capacity, cigar_total, nullptr, err);
     return st == PHMM_OK ? PHMM_OK : set_error(st, err);
     PHMM_GUARD_END
 }
@@ -419,13 +421,17 @@ phmm_status phmm_sw_resident_run(phmm_sw_resident* resident, int32_t iterations,
     PHMM_GUARD_END
 }
 
-phmm_status phmm_sw_resident_results(phmm_sw_resident* resident, phmm_sw_result* results, uint32_t* cigars)
+phmm_status phmm_sw_resident_results(phmm_sw_resident* resident, phmm_sw_result* results, uint32_t* cigars,
+                                     uint64_t cigar_capacity, uint64_t* cigar_total)
 {
     PHMM_GUARD_BEGIN
     phmm::clear_error();
+    if (cigar_total) *cigar_total = 0;
     if (!resident) return set_error(PHMM_ERR_INVALID_ARGUMENT, "resident is null");
+    if (cigar_capacity && !cigars) return set_error(PHMM_ERR_INVALID_ARGUMENT, "null buffer");
     std::string err;
-    phmm_status st = resident->aligner->resident_results(resident->res, results, cigars, err);
+    phmm_status st = resident->aligner->resident_results(resident->res, results, cigars, cigar_capacity, cigar_total,
+                                                         err);
     return st == PHMM_OK ? PHMM_OK : set_error(st, err);
     PHMM_GUARD_END
 }

@@ -56,9 +56,13 @@ __device__ __forceinline__ double radd(double a, double b) { return __dadd_rn(a,
 
 // FP64 has no hardware flush-to-zero; the reference's MXCSR.FTZ flushes tiny double results, so
 // the FP64 path flushes explicitly.  Results below 2^-1022 only arise far below any likelihood
-// that survives the FP32 -> FP64 switch, so this only keeps the two paths identical.
+// that survives the FP32 -> FP64 switch, so this only keeps the two paths identical.  Every value
+// of the recurrence is >= 0 (probabilities times a positive scale), so a double is subnormal or
+// zero exactly when its high word is below 0x00100000 (biased exponent 0): an integer compare and
+// two selects, with no FP64-pipe instruction (a DSETP would take one of the pipe's slots per flush,
+// eight per cell).
 __device__ __forceinline__ float ftz(float x) { return x; }  // FP32: hardware FTZ (-ftz=true)
-__device__ __forceinline__ double ftz(double x) { return fabs(x) < 2.2250738585072014e-308 ? 0.0 * x : x; }
+__device__ __forceinline__ double ftz(double x) { return __double2hiint(x) < 0x00100000 ? 0.0 : x; }
 
 template <typename T>
 struct Scale;

@@ -55,7 +55,8 @@ struct SwView {
     uint64_t stride;             // scratch bytes per warp
     unsigned int* claim;
     phmm_sw_result* out;
-    uint32_t* cigar;
+    const uint64_t* slot_off;    // per item: its CIGAR slot in `ops` (min(cap, nrow + ncol) ops)
+    uint32_t* ops;
     uint32_t cigar_cap;
 };
 
@@ -284,7 +285,7 @@ __device__ void sw_one(const SwView& v, uint32_t idx, int lane, uint8_t* scr, ui
     // read order, at most kSwMaxSeq - 1 ops (sw_cigar.c:162-170)
     const int count = min(nr, kSwMaxSeq - 1);
     const int wr = min(count, (int)v.cigar_cap);
-    uint32_t* dst = v.cigar + (uint64_t)idx * v.cigar_cap;
+    uint32_t* dst = v.ops + v.slot_off[idx];
     for (int q = lane; q < wr; q += 32) dst[q] = op_of(runs[nr - 1 - q]);
     res.score = best;
     res.alignment_offset = i;
@@ -307,6 +308,75 @@ __global__ void __launch_bounds__(32 * kSwBlockWarps) sw_kernel(SwView v)
         q = __shfl_sync(kFull, q, 0);
         if (q >= v.n) break;
         sw_one<K, WRAP>(v, v.order[q], lane, scr, band[wib]);
+    }
+}
+
+// Exclusive scan of min(cigar_count, cap) over the items in order: each item's offset in the compact
+// CIGAR buffer, and the total.  One block; 4 items per thread per round.
+constexpr int kScanThreads = 1024, kScanItems = 4;
+
+__global__ void __launch_bounds__(kScanThreads) sw_scan_kernel(phmm_sw_result* out, uint32_t n, uint32_t cap,
+                                                               unsigned long long* total)
+{
+    __shared__ unsigned long long wsum[kScanThreads / 32];
+    __shared__ unsigned long long carry;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    if (tid == 0) carry = 0;
+    __syncthreads();
+    for (uint64_t base = 0; base < n; base += (uint64_t)kScanThreads * kScanItems) {
+        unsigned long long c[kScanItems], own = 0;
+#pragma unroll
+        for (int u = 0; u < kScanItems; ++u) {
+            const uint64_t q = base + (uint64_t)tid * kScanItems + u;
+            c[u] = q < n ? (unsigned long long)min(out[q].cigar_count, cap) : 0ull;
+            own += c[u];
+        }
+        unsigned long long x = own;  // inclusive scan over the warp
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long y = __shfl_up_sync(kFull, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) wsum[wid] = x;
+        __syncthreads();
+        if (wid == 0) {
+            unsigned long long w = wsum[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned long long y = __shfl_up_sync(kFull, w, o);
+                if (lane >= o) w += y;
+            }
+            wsum[lane] = w;
+        }
+        __syncthreads();
+        const unsigned long long chunk = wsum[kScanThreads / 32 - 1];
+        unsigned long long before = carry + (wid ? wsum[wid - 1] : 0ull) + (x - own);
+#pragma unroll
+        for (int u = 0; u < kScanItems; ++u) {
+            const uint64_t q = base + (uint64_t)tid * kScanItems + u;
+            if (q < n) out[q].cigar_offset = (uint32_t)before;
+            before += c[u];
+        }
+        __syncthreads();
+        if (tid == 0) carry += chunk;
+        __syncthreads();
+    }
+    if (tid == 0) *total = carry;
+}
+
+// Copies every item's CIGAR from its slot to its place in the compact buffer (one warp per item).
+__global__ void __launch_bounds__(256) sw_gather_kernel(const phmm_sw_result* __restrict__ out,
+                                                         const uint64_t* __restrict__ slot_off,
+                                                         const uint32_t* __restrict__ ops, uint32_t* __restrict__ compact,
+                                                         uint32_t n, uint32_t cap)
+{
+    const int lane = threadIdx.x & 31;
+    const uint64_t nwarps = (uint64_t)gridDim.x * (blockDim.x / 32);
+    for (uint64_t q = (uint64_t)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5); q < n; q += nwarps) {
+        const uint32_t cnt = min(out[q].cigar_count, cap);
+        const uint32_t* src = ops + slot_off[q];
+        uint32_t* dst = compact + out[q].cigar_offset;
+        for (uint32_t k = lane; k < cnt; k += 32) dst[k] = src[k];
     }
 }
 
@@ -335,7 +405,10 @@ int sw_class_of(const SwParams& prm, int variant, uint32_t nrow, uint32_t ncol)
 
 struct SwAligner::Plan {
     uint32_t n = 0;
+    uint32_t cigar_cap = 0;
     std::vector<uint32_t> order;             // item indices grouped by class, most cells first
+    std::vector<uint64_t> slot_off;          // per item: its CIGAR slot (ops) in the slot buffer
+    uint64_t slots = 0;                      // ops of all slots
     uint32_t begin[kSwClasses + 1] = {};
     uint64_t stride[kSwClasses] = {};        // scratch bytes per warp of each class
     int grid[kSwClasses] = {};
@@ -343,20 +416,38 @@ struct SwAligner::Plan {
     uint64_t cells = 0;
 };
 
+// Device arena of one batch: inputs (items, order, slot offsets, bases), then the outputs
+// (total, results), the CIGAR slots, the compact CIGAR buffer and the per-warp scratch.
+struct SwArenaLayout {
+    uint64_t items, order, slot_off, hap, read, claim, total, out, slots, compact, scratch, bytes;
+    uint64_t in_bytes() const { return claim; }                 // [0, claim): uploaded together
+    uint64_t head_bytes() const { return slots - total; }       // [total, slots): total + results
+
+    SwArenaLayout(uint32_t n, uint64_t hap_bytes, uint64_t read_bytes, uint64_t nslots, uint64_t scratch_bytes)
+    {
+        auto a = [](uint64_t x) { return (x + 255) & ~uint64_t(255); };
+        items = 0;
+        order = a(items + sizeof(SwItem) * (uint64_t)n);
+        slot_off = a(order + 4ull * n);
+        hap = a(slot_off + 8ull * n);
+        read = a(hap + std::max<uint64_t>(hap_bytes, 1));
+        claim = a(read + std::max<uint64_t>(read_bytes, 1));
+        total = a(claim + 4ull * kSwClasses);
+        out = total + 8;
+        slots = a(out + sizeof(phmm_sw_result) * (uint64_t)n);
+        compact = a(slots + 4ull * std::max<uint64_t>(nslots, 1));
+        scratch = a(compact + 4ull * std::max<uint64_t>(nslots, 1));
+        bytes = scratch + scratch_bytes;
+    }
+};
+
 struct SwAligner::Resident {
     SwParams prm{};
     int variant = 0;
     Plan plan;
-    uint32_t cigar_cap = 0;
     void* arena = nullptr;
-    SwItem* items = nullptr;
-    uint32_t* order = nullptr;
-    uint8_t* hap = nullptr;
-    uint8_t* read = nullptr;
-    uint8_t* scratch = nullptr;
-    unsigned int* claim = nullptr;
-    phmm_sw_result* out = nullptr;
-    uint32_t* cigar = nullptr;
+    uint8_t* d = nullptr;
+    SwArenaLayout lay{0, 0, 0, 0, 0};
 };
 
 namespace {
@@ -369,8 +460,6 @@ namespace {
             return PHMM_ERR_CUDA;                                                     \
         }                                                                             \
     } while (0)
-
-uint64_t a256(uint64_t x) { return (x + 255) & ~uint64_t(255); }
 
 // Scratch of one class launch is held under this bound by launching fewer resident warps.
 constexpr uint64_t kSwScratchCap = 6ull << 30;
@@ -432,15 +521,27 @@ SwAligner::~SwAligner()
     if (stream_) cudaStreamDestroy(stream_);
 }
 
-void SwAligner::plan(const SwParams& prm, int variant, uint32_t n, const SwItem* items, Plan& p) const
+phmm_status SwAligner::plan(const SwParams& prm, int variant, uint32_t n, const SwItem* items, uint32_t cigar_cap,
+                            Plan& p, std::string& err) const
 {
     p.n = n;
+    p.cigar_cap = std::min<uint32_t>(cigar_cap, kSwMaxSeq - 1);
     std::vector<uint8_t> cls(n);
     uint32_t counts[kSwClasses] = {};
+    p.slot_off.resize(n);
+    p.slots = 0;
     for (uint32_t q = 0; q < n; ++q) {
-        cls[q] = (uint8_t)sw_class_of(prm, variant, items[q].hap_len, items[q].read_len);
+        const SwItem& x = items[q];
+        cls[q] = (uint8_t)sw_class_of(prm, variant, x.hap_len, x.read_len);
         ++counts[cls[q]];
-        p.cells += (uint64_t)items[q].hap_len * items[q].read_len;
+        p.cells += (uint64_t)x.hap_len * x.read_len;
+        p.slot_off[q] = p.slots;
+        if (std::max(x.hap_len, x.read_len) < (uint32_t)kSwMaxSeq)  // runs <= rows + columns consumed
+            p.slots += std::min<uint64_t>(p.cigar_cap, (uint64_t)x.hap_len + x.read_len);
+    }
+    if (p.slots > 0xffffffffull) {
+        err = "Smith-Waterman batch needs more than 2^32 CIGAR ops of room: split it";
+        return PHMM_ERR_LIMIT_EXCEEDED;
     }
     p.begin[0] = 0;
     for (int c = 0; c < kSwClasses; ++c) p.begin[c + 1] = p.begin[c] + counts[c];
@@ -467,31 +568,34 @@ void SwAligner::plan(const SwParams& prm, int variant, uint32_t n, const SwItem*
         p.grid[c] = m == 0 ? 0 : (int)g;
         p.scratch = std::max(p.scratch, (uint64_t)p.grid[c] * kSwBlockWarps * stride);
     }
+    return PHMM_OK;
 }
 
-phmm_status SwAligner::launch(const Plan& p, const SwParams& prm, int variant, const void* d_items,
-                              const uint32_t* d_order, const uint8_t* d_hap, const uint8_t* d_read,
-                              uint8_t* d_scratch, unsigned int* d_claim, phmm_sw_result* d_out, uint32_t* d_cigar,
-                              uint32_t cigar_cap, cudaStream_t st, float* class_ms, std::string& err)
+phmm_status SwAligner::launch(const Plan& p, const SwParams& prm, int variant, uint8_t* d, const SwArenaLayout& L,
+                              float* class_ms, std::string& err)
 {
-    SW_CK(cudaMemsetAsync(d_claim, 0, sizeof(unsigned int) * kSwClasses, st));
+    cudaStream_t st = stream_;
+    unsigned int* claim = (unsigned int*)(d + L.claim);
+    phmm_sw_result* out = (phmm_sw_result*)(d + L.out);
+    SW_CK(cudaMemsetAsync(claim, 0, sizeof(unsigned int) * kSwClasses, st));
     for (int c = 0; c < kSwClasses; ++c) {
         if (class_ms) class_ms[c] = 0.f;
         if (p.grid[c] == 0) continue;
         SwView v{};
-        v.items = (const SwItem*)d_items;
-        v.order = d_order + p.begin[c];
+        v.items = (const SwItem*)(d + L.items);
+        v.order = (const uint32_t*)(d + L.order) + p.begin[c];
         v.n = p.begin[c + 1] - p.begin[c];
-        v.hap = d_hap;
-        v.read = d_read;
+        v.hap = d + L.hap;
+        v.read = d + L.read;
         v.prm = prm;
         v.variant = variant;
-        v.scratch = d_scratch;
+        v.scratch = d + L.scratch;
         v.stride = p.stride[c];
-        v.claim = d_claim + c;
-        v.out = d_out;
-        v.cigar = d_cigar;
-        v.cigar_cap = cigar_cap;
+        v.claim = claim + c;
+        v.out = out;
+        v.slot_off = (const uint64_t*)(d + L.slot_off);
+        v.ops = (uint32_t*)(d + L.slots);
+        v.cigar_cap = p.cigar_cap;
         if (class_ms) SW_CK(cudaEventRecord(ev_[0], st));
         kSwKernels[c]<<<p.grid[c], 32 * kSwBlockWarps, 0, st>>>(v);
         SW_CK(cudaGetLastError());
@@ -501,39 +605,80 @@ phmm_status SwAligner::launch(const Plan& p, const SwParams& prm, int variant, c
             SW_CK(cudaEventElapsedTime(&class_ms[c], ev_[0], ev_[1]));
         }
     }
+    sw_scan_kernel<<<1, kScanThreads, 0, st>>>(out, p.n, p.cigar_cap, (unsigned long long*)(d + L.total));
+    SW_CK(cudaGetLastError());
+    const int gblocks = (int)std::max<uint64_t>(1, std::min<uint64_t>((p.n + 7) / 8, (uint64_t)sms_ * 8));
+    sw_gather_kernel<<<gblocks, 256, 0, st>>>(out, (const uint64_t*)(d + L.slot_off), (const uint32_t*)(d + L.slots),
+                                              (uint32_t*)(d + L.compact), p.n, p.cigar_cap);
+    SW_CK(cudaGetLastError());
+    return PHMM_OK;
+}
+
+phmm_status SwAligner::ensure_pinned(uint64_t bytes, std::string& err)
+{
+    if (bytes <= pinned_bytes_) return PHMM_OK;
+    if (pinned_) {
+        SW_CK(cudaStreamSynchronize(stream_));
+        cudaFreeHost(pinned_);
+    }
+    pinned_ = nullptr;
+    pinned_bytes_ = 0;
+    SW_CK(cudaMallocHost(&pinned_, bytes + bytes / 4));
+    pinned_bytes_ = bytes + bytes / 4;
+    return PHMM_OK;
+}
+
+// Results and the compact CIGARs of an arena that has run, to host memory (synchronous).
+phmm_status SwAligner::read_back(uint8_t* d, const SwArenaLayout& L, uint32_t n, phmm_sw_result* out,
+                                 uint32_t* cigars, uint64_t capacity, uint64_t* total, std::string& err)
+{
+    phmm_status st = ensure_pinned(L.head_bytes(), err);
+    if (st != PHMM_OK) return st;
+    uint8_t* h = (uint8_t*)pinned_;
+    SW_CK(cudaMemcpyAsync(h, d + L.total, L.head_bytes(), cudaMemcpyDeviceToHost, stream_));
+    SW_CK(cudaStreamSynchronize(stream_));
+    uint64_t tot = 0;
+    std::memcpy(&tot, h, 8);
+    if (out) std::memcpy(out, h + (L.out - L.total), sizeof(phmm_sw_result) * (size_t)n);
+    if (total) *total = tot;
+    if (!cigars || tot == 0) return PHMM_OK;
+    if (tot > capacity) {
+        err = "the batch's CIGARs need " + std::to_string(tot) + " ops, the buffer holds " + std::to_string(capacity);
+        return PHMM_ERR_LIMIT_EXCEEDED;
+    }
+    st = ensure_pinned(4 * tot, err);
+    if (st != PHMM_OK) return st;
+    h = (uint8_t*)pinned_;
+    SW_CK(cudaMemcpyAsync(h, d + L.compact, 4 * tot, cudaMemcpyDeviceToHost, stream_));
+    SW_CK(cudaStreamSynchronize(stream_));
+    std::memcpy(cigars, h, 4 * tot);
     return PHMM_OK;
 }
 
 phmm_status SwAligner::align(const SwParams& prm, int variant, uint32_t n, const SwItem* items, const uint8_t* hap,
-                             uint64_t hap_bytes, const uint8_t* read, uint64_t read_bytes, phmm_sw_result* out,
-                             uint32_t* cigar, uint32_t cigar_cap, float* device_ms, std::string& err)
+                             uint64_t hap_bytes, const uint8_t* read, uint64_t read_bytes, uint32_t cigar_cap,
+                             phmm_sw_result* out, uint32_t* cigars, uint64_t cigar_capacity, uint64_t* cigar_total,
+                             float* device_ms, std::string& err)
 {
     if (device_ms) *device_ms = 0.f;
+    if (cigar_total) *cigar_total = 0;
     if (n == 0) return PHMM_OK;
-    phmm_status cs = check_items(n, items, hap_bytes, read_bytes, err);
-    if (cs != PHMM_OK) return cs;
+    phmm_status st = check_items(n, items, hap_bytes, read_bytes, err);
+    if (st != PHMM_OK) return st;
     std::lock_guard<std::mutex> lk(mu_);
     SW_CK(cudaSetDevice(dev_));
     Plan p;
-    plan(prm, variant, n, items, p);
-    // arena: items | order | hap | read | claim | out | cigar | scratch
-    const uint64_t o_items = 0;
-    const uint64_t o_order = a256(o_items + sizeof(SwItem) * (uint64_t)n);
-    const uint64_t o_hap = a256(o_order + 4ull * n);
-    const uint64_t o_read = a256(o_hap + std::max<uint64_t>(hap_bytes, 1));
-    const uint64_t o_claim = a256(o_read + std::max<uint64_t>(read_bytes, 1));
-    const uint64_t o_out = a256(o_claim + 4ull * kSwClasses);
-    const uint64_t o_cigar = a256(o_out + sizeof(phmm_sw_result) * (uint64_t)n);
-    const uint64_t o_scr = a256(o_cigar + 4ull * n * cigar_cap);
-    const uint64_t need = o_scr + p.scratch;
-    if (need > arena_bytes_) {
+    st = plan(prm, variant, n, items, cigar_cap, p, err);
+    if (st != PHMM_OK) return st;
+    const SwArenaLayout L(n, hap_bytes, read_bytes, p.slots, p.scratch);
+    if (L.bytes > arena_bytes_) {
         if (arena_) {
             SW_CK(cudaStreamSynchronize(stream_));
             cudaFree(arena_);
             arena_ = nullptr;
             arena_bytes_ = 0;
         }
-        const uint64_t sz = need + need / 4;
+        const uint64_t sz = L.bytes + L.bytes / 4;
         if (cudaMalloc(&arena_, sz) != cudaSuccess) {
             cudaGetLastError();
             err = "Smith-Waterman arena of " + std::to_string(sz) + " bytes could not be allocated";
@@ -541,35 +686,24 @@ phmm_status SwAligner::align(const SwParams& prm, int variant, uint32_t n, const
         }
         arena_bytes_ = sz;
     }
-    // inputs through pinned staging: items | order | hap | read; outputs back: out | cigar
-    const uint64_t in_bytes = o_claim, out_bytes = o_scr - o_out;
-    const uint64_t stage = std::max(in_bytes, out_bytes);
-    if (stage > pinned_bytes_) {
-        if (pinned_) cudaFreeHost(pinned_);
-        pinned_ = nullptr;
-        pinned_bytes_ = 0;
-        SW_CK(cudaMallocHost(&pinned_, stage + stage / 4));
-        pinned_bytes_ = stage + stage / 4;
-    }
+    // inputs through pinned staging in one copy: items | order | slot offsets | haplotypes | reads
+    st = ensure_pinned(L.in_bytes(), err);
+    if (st != PHMM_OK) return st;
     uint8_t* h = (uint8_t*)pinned_;
     uint8_t* d = (uint8_t*)arena_;
-    std::memcpy(h + o_items, items, sizeof(SwItem) * (size_t)n);
-    std::memcpy(h + o_order, p.order.data(), 4ull * n);
-    if (hap_bytes) std::memcpy(h + o_hap, hap, hap_bytes);
-    if (read_bytes) std::memcpy(h + o_read, read, read_bytes);
-    SW_CK(cudaMemcpyAsync(d, h, in_bytes, cudaMemcpyHostToDevice, stream_));
+    std::memcpy(h + L.items, items, sizeof(SwItem) * (size_t)n);
+    std::memcpy(h + L.order, p.order.data(), 4ull * n);
+    std::memcpy(h + L.slot_off, p.slot_off.data(), 8ull * n);
+    if (hap_bytes) std::memcpy(h + L.hap, hap, hap_bytes);
+    if (read_bytes) std::memcpy(h + L.read, read, read_bytes);
+    SW_CK(cudaMemcpyAsync(d, h, L.in_bytes(), cudaMemcpyHostToDevice, stream_));
     SW_CK(cudaEventRecord(ev_[0], stream_));
-    phmm_status st = launch(p, prm, variant, d + o_items, (const uint32_t*)(d + o_order), d + o_hap, d + o_read,
-                            d + o_scr, (unsigned int*)(d + o_claim), (phmm_sw_result*)(d + o_out),
-                            (uint32_t*)(d + o_cigar), cigar_cap, stream_, nullptr, err);
+    st = launch(p, prm, variant, d, L, nullptr, err);
     if (st != PHMM_OK) return st;
     SW_CK(cudaEventRecord(ev_[1], stream_));
-    SW_CK(cudaMemcpyAsync(h, d + o_out, out_bytes, cudaMemcpyDeviceToHost, stream_));
-    SW_CK(cudaStreamSynchronize(stream_));
-    if (device_ms) SW_CK(cudaEventElapsedTime(device_ms, ev_[0], ev_[1]));
-    std::memcpy(out, h, sizeof(phmm_sw_result) * (size_t)n);
-    if (cigar && cigar_cap) std::memcpy(cigar, h + (o_cigar - o_out), 4ull * n * cigar_cap);
-    return PHMM_OK;
+    st = read_back(d, L, n, out, cigars, cigar_capacity, cigar_total, err);
+    if (device_ms) cudaEventElapsedTime(device_ms, ev_[0], ev_[1]);
+    return st;
 }
 
 phmm_status SwAligner::resident_create(const SwParams& prm, int variant, uint32_t n, const SwItem* items,
@@ -577,46 +711,36 @@ phmm_status SwAligner::resident_create(const SwParams& prm, int variant, uint32_
                                        uint64_t read_bytes, uint32_t cigar_cap, Resident** out, std::string& err)
 {
     *out = nullptr;
-    phmm_status cs = check_items(n, items, hap_bytes, read_bytes, err);
-    if (cs != PHMM_OK) return cs;
+    phmm_status st = check_items(n, items, hap_bytes, read_bytes, err);
+    if (st != PHMM_OK) return st;
     std::lock_guard<std::mutex> lk(mu_);
     SW_CK(cudaSetDevice(dev_));
     Resident* r = new Resident();
     r->prm = prm;
     r->variant = variant;
-    r->cigar_cap = cigar_cap;
-    plan(prm, variant, n, items, r->plan);
-    const uint64_t o_items = 0;
-    const uint64_t o_order = a256(o_items + sizeof(SwItem) * (uint64_t)n);
-    const uint64_t o_hap = a256(o_order + 4ull * n);
-    const uint64_t o_read = a256(o_hap + std::max<uint64_t>(hap_bytes, 1));
-    const uint64_t o_claim = a256(o_read + std::max<uint64_t>(read_bytes, 1));
-    const uint64_t o_out = a256(o_claim + 4ull * kSwClasses);
-    const uint64_t o_cigar = a256(o_out + sizeof(phmm_sw_result) * (uint64_t)n);
-    const uint64_t o_scr = a256(o_cigar + 4ull * n * cigar_cap);
-    const uint64_t need = o_scr + r->plan.scratch;
-    if (cudaMalloc(&r->arena, need) != cudaSuccess) {
+    st = plan(prm, variant, n, items, cigar_cap, r->plan, err);
+    if (st != PHMM_OK) {
+        delete r;
+        return st;
+    }
+    r->lay = SwArenaLayout(n, hap_bytes, read_bytes, r->plan.slots, r->plan.scratch);
+    if (cudaMalloc(&r->arena, r->lay.bytes) != cudaSuccess) {
         cudaGetLastError();
         delete r;
-        err = "Smith-Waterman resident arena of " + std::to_string(need) + " bytes could not be allocated";
+        err = "Smith-Waterman resident arena of " + std::to_string(r->lay.bytes) + " bytes could not be allocated";
         return PHMM_ERR_OUT_OF_MEMORY;
     }
-    uint8_t* d = (uint8_t*)r->arena;
-    r->items = (SwItem*)(d + o_items);
-    r->order = (uint32_t*)(d + o_order);
-    r->hap = d + o_hap;
-    r->read = d + o_read;
-    r->claim = (unsigned int*)(d + o_claim);
-    r->out = (phmm_sw_result*)(d + o_out);
-    r->cigar = (uint32_t*)(d + o_cigar);
-    r->scratch = d + o_scr;
-    auto up = [&](void* dst, const void* src, uint64_t bytes) {
-        return bytes ? cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream_) : cudaSuccess;
+    r->d = (uint8_t*)r->arena;
+    auto up = [&](uint64_t off, const void* src, uint64_t bytes) {
+        return bytes ? cudaMemcpyAsync(r->d + off, src, bytes, cudaMemcpyHostToDevice, stream_) : cudaSuccess;
     };
-    cudaError_t e = up(r->items, items, sizeof(SwItem) * (uint64_t)n);
-    if (e == cudaSuccess) e = up(r->order, r->plan.order.data(), 4ull * n);
-    if (e == cudaSuccess) e = up(r->hap, hap, hap_bytes);
-    if (e == cudaSuccess) e = up(r->read, read, read_bytes);
+    const SwArenaLayout& L = r->lay;
+    cudaError_t e = up(L.items, items, sizeof(SwItem) * (uint64_t)n);
+    if (e == cudaSuccess) e = up(L.order, r->plan.order.data(), 4ull * n);
+    if (e == cudaSuccess) e = up(L.slot_off, r->plan.slot_off.data(), 8ull * n);
+    if (e == cudaSuccess) e = up(L.hap, hap, hap_bytes);
+    if (e == cudaSuccess) e = up(L.read, read, read_bytes);
+    if (e == cudaSuccess) e = cudaMemsetAsync(r->d + L.total, 0, L.head_bytes(), stream_);
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
     if (e != cudaSuccess) {
         err = std::string("Smith-Waterman resident upload failed: ") + cudaGetErrorString(e);
@@ -633,11 +757,11 @@ phmm_status SwAligner::resident_run(Resident* r, int iterations, float* ms_per_r
     std::lock_guard<std::mutex> lk(mu_);
     SW_CK(cudaSetDevice(dev_));
     if (ms_per_run) *ms_per_run = 0.f;
+    if (r->plan.n == 0) return PHMM_OK;
     if (iterations > 0) {
         SW_CK(cudaEventRecord(ev_[0], stream_));
         for (int it = 0; it < iterations; ++it) {
-            phmm_status st = launch(r->plan, r->prm, r->variant, r->items, r->order, r->hap, r->read, r->scratch,
-                                    r->claim, r->out, r->cigar, r->cigar_cap, stream_, nullptr, err);
+            phmm_status st = launch(r->plan, r->prm, r->variant, r->d, r->lay, nullptr, err);
             if (st != PHMM_OK) return st;
         }
         SW_CK(cudaEventRecord(ev_[1], stream_));
@@ -647,24 +771,21 @@ phmm_status SwAligner::resident_run(Resident* r, int iterations, float* ms_per_r
         if (ms_per_run) *ms_per_run = ms / iterations;
     }
     if (class_ms) {
-        phmm_status st = launch(r->plan, r->prm, r->variant, r->items, r->order, r->hap, r->read, r->scratch,
-                                r->claim, r->out, r->cigar, r->cigar_cap, stream_, class_ms, err);
+        phmm_status st = launch(r->plan, r->prm, r->variant, r->d, r->lay, class_ms, err);
         if (st != PHMM_OK) return st;
         SW_CK(cudaStreamSynchronize(stream_));
     }
     return PHMM_OK;
 }
 
-phmm_status SwAligner::resident_results(Resident* r, phmm_sw_result* out, uint32_t* cigar, std::string& err)
+phmm_status SwAligner::resident_results(Resident* r, phmm_sw_result* out, uint32_t* cigars, uint64_t capacity,
+                                        uint64_t* total, std::string& err)
 {
     std::lock_guard<std::mutex> lk(mu_);
     SW_CK(cudaSetDevice(dev_));
-    const uint32_t n = r->plan.n;
-    if (out && n) SW_CK(cudaMemcpyAsync(out, r->out, sizeof(phmm_sw_result) * (uint64_t)n, cudaMemcpyDeviceToHost, stream_));
-    if (cigar && n && r->cigar_cap)
-        SW_CK(cudaMemcpyAsync(cigar, r->cigar, 4ull * n * r->cigar_cap, cudaMemcpyDeviceToHost, stream_));
-    SW_CK(cudaStreamSynchronize(stream_));
-    return PHMM_OK;
+    if (total) *total = 0;
+    if (r->plan.n == 0) return PHMM_OK;
+    return read_back(r->d, r->lay, r->plan.n, out, cigars, capacity, total, err);
 }
 
 void SwAligner::resident_destroy(Resident* r)

@@ -90,16 +90,19 @@ __host__ __device__ inline bool sw_w16_cannot_wrap(int32_t match, int32_t mismat
 
 int sw_class_of(const SwParams& prm, int variant, uint32_t nrow, uint32_t ncol);
 
+struct SwArenaLayout;
+
 // Device state of the aligner: a stream, a growable arena and pinned staging, owned by an engine.
 class SwAligner {
 public:
     static phmm_status create(int device, SwAligner** out, std::string& err);
     ~SwAligner();
 
-    // Host buffers in and out (copies inside), synchronous.  out[n]; cigar[n][cigar_cap].
+    // Host buffers in and out (copies inside), synchronous.  out[n]; compact CIGARs (phmm_sw_align).
     phmm_status align(const SwParams& prm, int variant, uint32_t n, const SwItem* items, const uint8_t* hap,
-                      uint64_t hap_bytes, const uint8_t* read, uint64_t read_bytes, phmm_sw_result* out,
-                      uint32_t* cigar, uint32_t cigar_cap, float* device_ms, std::string& err);
+                      uint64_t hap_bytes, const uint8_t* read, uint64_t read_bytes, uint32_t cigar_cap,
+                      phmm_sw_result* out, uint32_t* cigars, uint64_t cigar_capacity, uint64_t* cigar_total,
+                      float* device_ms, std::string& err);
 
     // Resident batches: planned and uploaded once, run many times, results read back on demand.
     struct Resident;
@@ -107,7 +110,8 @@ public:
                                 const uint8_t* hap, uint64_t hap_bytes, const uint8_t* read, uint64_t read_bytes,
                                 uint32_t cigar_cap, Resident** out, std::string& err);
     phmm_status resident_run(Resident* r, int iterations, float* ms_per_run, float* class_ms, std::string& err);
-    phmm_status resident_results(Resident* r, phmm_sw_result* out, uint32_t* cigar, std::string& err);
+    phmm_status resident_results(Resident* r, phmm_sw_result* out, uint32_t* cigars, uint64_t capacity,
+                                 uint64_t* total, std::string& err);
     void resident_destroy(Resident* r);
 
     int device() const { return dev_; }
@@ -115,11 +119,13 @@ public:
 private:
     SwAligner() = default;
     struct Plan;
-    void plan(const SwParams& prm, int variant, uint32_t n, const SwItem* items, Plan& p) const;
-    phmm_status launch(const Plan& p, const SwParams& prm, int variant, const void* d_items,
-                       const uint32_t* d_order, const uint8_t* d_hap, const uint8_t* d_read, uint8_t* d_scratch,
-                       unsigned int* d_claim, phmm_sw_result* d_out, uint32_t* d_cigar, uint32_t cigar_cap,
-                       cudaStream_t st, float* class_ms, std::string& err);
+    phmm_status plan(const SwParams& prm, int variant, uint32_t n, const SwItem* items, uint32_t cigar_cap, Plan& p,
+                     std::string& err) const;
+    phmm_status launch(const Plan& p, const SwParams& prm, int variant, uint8_t* d, const SwArenaLayout& L,
+                       float* class_ms, std::string& err);
+    phmm_status ensure_pinned(uint64_t bytes, std::string& err);
+    phmm_status read_back(uint8_t* d, const SwArenaLayout& L, uint32_t n, phmm_sw_result* out, uint32_t* cigars,
+                          uint64_t capacity, uint64_t* total, std::string& err);
 
     int dev_ = 0;
     int sms_ = 0;

@@ -239,12 +239,12 @@ class Engine:
     def version() -> str:
         return _lib.load().phmm_version().decode()
 
-    def sw_align(self, batch, params=None, variant: int = 0, cigar_cap: int | None = None):
+    def sw_align(self, batch, params=None, variant: int = 0, cigar_cap: int | None = None, **kw):
         """Smith-Waterman realignment of a batch of (haplotype, read) pairs (rovaca_b200.sw)."""
         from . import sw
 
         return sw.align(self, batch, sw.GENOTYPING if params is None else params, variant,
-                        sw.MAX_CIGAR if cigar_cap is None else cigar_cap)
+                        sw.MAX_CIGAR if cigar_cap is None else cigar_cap, **kw)
 
     def sw_resident(self, batch, params=None, variant: int = 0, cigar_cap: int | None = None):
         from . import sw

@@ -22,7 +22,7 @@ CIGAR_OPS = "MIDNSHP=XB"
 
 SW_ITEM_DTYPE = np.dtype([("hap_offset", "<u8"), ("read_offset", "<u8"), ("hap_len", "<u4"), ("read_len", "<u4")])
 SW_RESULT_DTYPE = np.dtype([("score", "<i4"), ("alignment_offset", "<i4"), ("max_i", "<i4"), ("max_j", "<i4"),
-                            ("cigar_count", "<u4"), ("reserved", "<u4")])
+                            ("cigar_count", "<u4"), ("cigar_offset", "<u4")])
 
 
 def cigar_string(ops) -> str:
@@ -98,18 +98,21 @@ def _check_variant(variant: int) -> None:
 
 @dataclass
 class SwResults:
-    """Per alignment: score, alignment_offset, max_i, max_j, cigar_count (SW_RESULT_DTYPE) and the
-    CIGAR ops [n, cigar_cap] (BAM encoding, read order)."""
+    """Per alignment: score, alignment_offset, max_i, max_j, cigar_count, cigar_offset
+    (SW_RESULT_DTYPE) and the compact CIGAR ops (BAM encoding, read order): alignment q's first
+    min(cigar_count, cigar_cap) ops at cigars[cigar_offset:]."""
 
     fields: np.ndarray
     cigars: np.ndarray
+    cigar_cap: int
 
     def __len__(self) -> int:
         return int(self.fields.shape[0])
 
     def ops(self, q: int) -> list[int]:
-        n = min(int(self.fields[q]["cigar_count"]), self.cigars.shape[1])
-        return [int(x) for x in self.cigars[q, :n]]
+        f = self.fields[q]
+        o, n = int(f["cigar_offset"]), min(int(f["cigar_count"]), self.cigar_cap)
+        return [int(x) for x in self.cigars[o:o + n]]
 
     def cigar(self, q: int) -> str:
         return cigar_string(self.ops(q))
@@ -120,19 +123,36 @@ class SwResults:
         return int(f["score"]), int(f["alignment_offset"]), int(f["max_i"]), int(f["max_j"]), self.ops(q)
 
 
-def align(engine, batch: SwBatch, params=GENOTYPING, variant: int = 0, cigar_cap: int = MAX_CIGAR) -> SwResults:
-    """Aligns every pair of the batch on the engine's device (host buffers in and out)."""
+def _capacity(batch: SwBatch, cigar_cap: int) -> int:
+    """Ops the compact CIGAR buffer needs at most: min(cap, haplotype + read length) per alignment."""
+    ln = batch.items["hap_len"].astype(np.int64) + batch.items["read_len"].astype(np.int64)
+    return int(np.minimum(ln, min(cigar_cap, MAX_CIGAR)).sum())
+
+
+def align(engine, batch: SwBatch, params=GENOTYPING, variant: int = 0, cigar_cap: int = MAX_CIGAR,
+          ops_per_alignment: int = 32) -> SwResults:
+    """Aligns every pair of the batch on the engine's device (host buffers in and out).  The CIGAR
+    buffer starts at ops_per_alignment ops per pair (or the most the batch can need, if smaller);
+    a batch that needs more is aligned again with the size the first call reported."""
     _check_variant(variant)
     lib = _lib.load()
     n = batch.n
     fields = np.zeros(n, SW_RESULT_DTYPE)
-    cigars = np.zeros((n, cigar_cap), np.uint32)
-    if n:
-        _lib.check(lib.phmm_sw_align(engine._h, _params(params), variant, n, _ptr(batch.items),
-                                     _ptr(batch.hap_bases), batch.hap_bases.size, _ptr(batch.read_bases),
-                                     batch.read_bases.size, _ptr(fields), _ptr(cigars) if cigar_cap else None,
-                                     cigar_cap))
-    return SwResults(fields, cigars)
+    size = min(_capacity(batch, cigar_cap), n * ops_per_alignment)
+    total = C.c_uint64()
+    for _ in range(2):
+        cigars = np.empty(max(size, 1), np.uint32)
+        if not n:
+            break
+        st = lib.phmm_sw_align(engine._h, _params(params), variant, n, _ptr(batch.items), _ptr(batch.hap_bases),
+                               batch.hap_bases.size, _ptr(batch.read_bases), batch.read_bases.size, cigar_cap,
+                               _ptr(fields), _ptr(cigars), cigars.size, C.byref(total))
+        if st == _lib.PHMM_ERR_LIMIT_EXCEEDED and total.value > size:
+            size = total.value
+            continue
+        _lib.check(st)
+        break
+    return SwResults(fields, cigars[:total.value], cigar_cap)
 
 
 class SwResident:
@@ -167,9 +187,12 @@ class SwResident:
 
     def results(self) -> SwResults:
         fields = np.zeros(self.n, SW_RESULT_DTYPE)
-        cigars = np.zeros((self.n, self.cigar_cap), np.uint32)
-        _lib.check(self._lib.phmm_sw_resident_results(self._h, _ptr(fields), _ptr(cigars) if self.cigar_cap else None))
-        return SwResults(fields, cigars)
+        total = C.c_uint64()
+        _lib.check(self._lib.phmm_sw_resident_results(self._h, _ptr(fields), None, 0, C.byref(total)))
+        cigars = np.empty(max(total.value, 1), np.uint32)
+        _lib.check(self._lib.phmm_sw_resident_results(self._h, _ptr(fields), _ptr(cigars), cigars.size,
+                                                      C.byref(total)))
+        return SwResults(fields, cigars[:total.value], self.cigar_cap)
 
     def close(self) -> None:
         if getattr(self, "_h", None) and self._h.value:

@@ -126,18 +126,49 @@ def test_empty_and_tiny_inputs(engine, sw_oracle):
     _check(engine, sw_oracle, pairs, sw.ASSEMBLY)
 
 
+def _core(fields):
+    return fields[["score", "alignment_offset", "max_i", "max_j", "cigar_count"]]
+
+
 def test_cigar_capacity_and_counts(engine, sw_oracle):
-    """With a smaller CIGAR capacity the first ops are written and cigar_count stays the full count."""
+    """With a smaller per-alignment capacity the first ops are stored and cigar_count stays the full
+    count; the compact buffer holds the alignments in item order."""
     rng = random.Random(61)
     pairs = _realign_pairs(rng, 300)
     batch = sw.SwBatch.from_pairs(pairs)
     full = engine.sw_align(batch)
     capped = engine.sw_align(batch, cigar_cap=2)
-    assert np.array_equal(full.fields, capped.fields)
+    assert np.array_equal(_core(full.fields), _core(capped.fields))
     for q in range(len(pairs)):
-        assert list(capped.cigars[q, :min(2, int(full.fields[q]["cigar_count"]))]) == full.ops(q)[:2]
+        assert capped.ops(q) == full.ops(q)[:2]
+    offs = full.fields["cigar_offset"].astype(np.int64)
+    assert offs[0] == 0 and np.array_equal(np.diff(offs), full.fields["cigar_count"][:-1].astype(np.int64))
+    assert full.cigars.size == int(full.fields["cigar_count"].sum())
     none = engine.sw_align(batch, cigar_cap=0)
-    assert np.array_equal(full.fields, none.fields)
+    assert np.array_equal(_core(full.fields), _core(none.fields)) and none.cigars.size == 0
+
+
+def test_small_cigar_buffer_is_reported_and_retried(engine):
+    """A CIGAR buffer smaller than the batch needs: PHMM_ERR_LIMIT_EXCEEDED with the needed size and
+    the results filled (C ABI); the Python call retries once with that size."""
+    import ctypes as C
+
+    from rovaca_b200 import _lib
+
+    rng = random.Random(62)
+    batch = sw.SwBatch.from_pairs(_realign_pairs(rng, 200, read_len=(100, 250)))
+    want = engine.sw_align(batch)
+    again = engine.sw_align(batch, ops_per_alignment=1)
+    assert np.array_equal(again.fields, want.fields) and np.array_equal(again.cigars, want.cigars)
+    lib = _lib.load()
+    fields = np.zeros(batch.n, sw.SW_RESULT_DTYPE)
+    small = np.zeros(4, np.uint32)
+    total = C.c_uint64()
+    st = lib.phmm_sw_align(engine._h, None, 0, batch.n, batch.items.ctypes.data, batch.hap_bases.ctypes.data,
+                           batch.hap_bases.size, batch.read_bases.ctypes.data, batch.read_bases.size, 2047,
+                           fields.ctypes.data, small.ctypes.data, small.size, C.byref(total))
+    assert st == _lib.PHMM_ERR_LIMIT_EXCEEDED and total.value == want.cigars.size
+    assert np.array_equal(fields, want.fields) and not small.any()
 
 
 def test_cigar_consumes_the_read_and_the_haplotype_span(engine):
