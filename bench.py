@@ -12,6 +12,8 @@ every read x haplotype pair and the FP64 recompute of the pairs whose FP32 sum f
   latency    p50/p99 region latency of the serving loop under Poisson arrivals at 80% of capacity
   roofline   the FP32 wavefront pass: 12 FLOP per cell against the device's measured FP32 FMA peak
   cpu_baseline  the reference's own AVX PairHMM (compiled from its sources) on all host cores
+  smith_waterman  realignment of every read of the batch to a haplotype of its region on the GPU
+             (resident and end to end), checked against the oracle; the reference's aligner on the host
 
 Multi-GPU: one process per GPU (torchrun); every rank runs its own 2,000 regions (regions are
 independent: weak scaling, no collective on the data path); value = all ranks' cells / max time.
@@ -333,6 +335,64 @@ def genotyping_run(engine, n_regions: int = 400, check: int = 20) -> dict:
             "form": "phmm_submit_region with events, genotype likelihoods only back to the host (PCR CONSERVATIVE, Q18)"}
 
 
+def smith_waterman_run(engine, batch, steps: int, warmup: int, cpu: bool) -> dict:
+    """Smith-Waterman realignment of every read of the batch against a haplotype of its own region
+    (the aligner HaplotypeCaller runs per read after genotyping; genotyping parameters, the
+    reference's int16/int32 choice): cell updates per second with the batch resident in HBM, end to
+    end through phmm_sw_align from host buffers, results checked against the oracle on a sample, and
+    the reference's own aligner on the host cores for a bounded sample."""
+    from oracle import SwOracle, SwRef, build_ref_sw
+    from rovaca_b200 import sw, synth
+
+    b = synth.sw_realignment(batch)
+    with engine.sw_resident(b) as rs:
+        rs.run(warmup)
+        ms = rs.run(steps)
+        cls = rs.profile()
+        res = rs.results()
+    engine.sw_align(b)
+    t = time.perf_counter()
+    e2e_res = engine.sw_align(b)
+    e2e_s = time.perf_counter() - t
+    same = bool(np.array_equal(e2e_res.fields, res.fields) and np.array_equal(e2e_res.cigars, res.cigars))
+    orc = SwOracle()
+    rng = np.random.default_rng(7)
+    sample = rng.choice(b.n, min(2000, b.n), replace=False)
+    mism = sum(res.tuple(int(q)) != orc.align(*b.pair(int(q))) for q in sample)
+    # bytes of 4-bit cell codes written per run (the per-warp scratch the trace-back reads)
+    k_of = np.array(sw.CLASS_K[:-1])
+    rl = b.items["read_len"].astype(np.int64)
+    hl = b.items["hap_len"].astype(np.int64)
+    kk = k_of[np.minimum(np.searchsorted(k_of, np.maximum((rl + 31) // 32, 1)), len(k_of) - 1)]
+    stripes = np.maximum((rl + 32 * kk - 1) // (32 * kk), 1)
+    code_bytes = int((stripes * hl * 128 * ((kk + 7) // 8)).sum())
+    out = {"alignments": b.n, "cells": b.cells, "gcups_device": round(b.cells / ms / 1e6, 1),
+           "ms_per_run": round(ms, 3), "gcups_e2e": round(b.cells / e2e_s / 1e9, 1),
+           "e2e_ms": round(e2e_s * 1e3, 3), "e2e_equal_resident": same,
+           "h2d_bytes": int(b.items.nbytes + b.hap_bases.size + b.read_bases.size + 12 * b.n),
+           "d2h_bytes": int(24 * b.n + 4 * res.cigars.size),
+           "class_ms": {str(k): round(float(v), 3) for k, v in zip(list(k_of) + ["wrap"], cls) if v > 0},
+           "oracle_sample": int(len(sample)), "oracle_mismatches": int(mism),
+           "cell_code_bytes_per_run": code_bytes,
+           "cell_code_gbs": round(code_bytes / (ms / 1e3) / 1e9, 1),
+           "workload": "every read of the 2,000-region batch against haplotype (read index mod haplotypes) of "
+                       "its region; genotyping parameters (10, -15, -30, -5)"}
+    if cpu and build_ref_sw() is not None:
+        ref = SwRef()
+        pairs = [b.pair(int(q)) for q in sample]
+        cells = sum(len(h) * len(r) for h, r in pairs)
+        th = os.cpu_count() or 1
+        t = time.perf_counter()
+        with ThreadPoolExecutor(th) as ex:
+            outs = list(ex.map(lambda pr: ref.align(pr[0], pr[1]), pairs))
+        dt = time.perf_counter() - t
+        out["cpu_baseline"] = {"value": round(cells / dt / 1e9, 2), "unit": "GCUPS", "cores": th, "kind": "reference",
+                               "sample": f"{len(pairs)} alignments of the batch ({dt:.2f} s), the reference's "
+                                         "ro_sw aligner compiled from its sources, one alignment per task",
+                               "mismatches_vs_gpu": int(sum(o != res.tuple(int(q)) for o, q in zip(outs, sample)))}
+    return out
+
+
 def run_resident_only(args) -> None:
     """Profiling mode: only the device-resident replay (the launches the ncu summaries cover)."""
     import torch
@@ -349,6 +409,23 @@ def run_resident_only(args) -> None:
                       "ms_per_step": st["device_ms"] / args.steps, "fp32_pass_ms": st["fp32_ms"],
                       "fp64_pass_ms": st["fp64_ms"], "gcups": batch.cells() * args.steps / st["device_ms"] / 1e6,
                       "kernel_launches": st["kernel_launches"]}), flush=True)
+
+
+def run_sw_only(args) -> None:
+    """Profiling mode: the resident Smith-Waterman realignment of the reads of 500 regions of the
+    benchmark's shape (about 125,000 alignments), warm-up and timed runs only."""
+    import torch
+
+    from rovaca_b200 import Engine, synth
+
+    torch.cuda.set_device(0)
+    b = synth.sw_realignment(synth.config1(n_regions=500, seed=1))
+    with Engine(device=0, autotune=False) as engine:
+        with engine.sw_resident(b) as rs:
+            rs.run(args.warmup)
+            ms = rs.run(args.steps)
+    print(json.dumps({"mode": "sw", "alignments": b.n, "cells": b.cells, "steps": args.steps, "ms_per_run": ms,
+                      "gcups": b.cells / ms / 1e6}), flush=True)
 
 
 def run_ours(args, rank: int, world: int, dist) -> None:
@@ -453,6 +530,7 @@ def run_ours(args, rank: int, world: int, dist) -> None:
         stress = underflow_stress(engine)
         wgs = wgs_mixture(engine)
         geno = genotyping_run(engine)
+        swr = smith_waterman_run(engine, batch, args.steps, args.warmup, world == 1)
 
         # roofline of the FP32 wavefront pass against the measured FP32 FMA peak
         peak_scalar, peak_packed = engine.fp32_fma_peak()
@@ -530,6 +608,7 @@ def run_ours(args, rank: int, world: int, dist) -> None:
             "underflow_stress": stress,
             "wgs_mixture": wgs,
             "genotyping": geno,
+            "smith_waterman": swr,
         }
     engine.close()
     if line is not None:
@@ -545,8 +624,9 @@ def main() -> None:
     ap.add_argument("--serve-seconds", type=float, default=6.0)
     ap.add_argument("--no-autotune", action="store_true",
                     help="default tile shapes (profiling runs: no calibration launches before the batch)")
-    ap.add_argument("--only", choices=["all", "resident"], default="all",
-                    help="resident: only the device-resident replay (for profiling)")
+    ap.add_argument("--only", choices=["all", "resident", "sw"], default="all",
+                    help="resident: only the device-resident replay (for profiling); sw: only the resident "
+                         "Smith-Waterman realignment of a 500-region batch's reads (for profiling)")
     ap.add_argument("--no-graph", action="store_true", help="direct launches instead of CUDA-graph replay")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -566,6 +646,8 @@ def main() -> None:
     try:
         if args.only == "resident":
             run_resident_only(args)
+        elif args.only == "sw":
+            run_sw_only(args)
         elif args.impl == "reference":
             run_reference(args, rank, world)
         else:

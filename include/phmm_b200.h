@@ -386,8 +386,9 @@ PHMM_API phmm_status phmm_sw_align(phmm_engine* engine, const int32_t* params, i
 
 /* Device-resident Smith-Waterman batch (no reference counterpart: it exists to time the kernels with
  * the inputs already in HBM).  Created from host buffers, run `iterations` times back to back
- * (ms_per_run: CUDA-event time per run on the aligner's stream; class_ms[13], optional: time of each
- * kernel class in the last run), results read back on demand (the layout of phmm_sw_align). */
+ * (ms_per_run: CUDA-event time per run on the aligner's stream; class_ms[14], optional: time of each
+ * kernel class in one more run: stripe widths 1-8, 10, 12, 16, 20, 24 read columns per lane, then the
+ * 16-bit wrap-around class), results read back on demand (the layout of phmm_sw_align). */
 typedef struct phmm_sw_resident phmm_sw_resident;
 PHMM_API phmm_status phmm_sw_resident_create(phmm_engine* engine, const int32_t* params, int32_t variant,
                                              uint32_t n, const phmm_sw_item* items, const uint8_t* hap_bases,

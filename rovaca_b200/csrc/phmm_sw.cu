@@ -32,6 +32,7 @@
 #include <cstring>
 #include <numeric>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "phmm_sw.h"
@@ -138,9 +139,12 @@ __device__ void sw_one(const SwView& v, uint32_t idx, int lane, uint8_t* scr, ui
             int hout = 0, eout = low;              // H, E of this lane's last column, previous step
             uint32_t* bts = bt + (uint64_t)s * nrow * ROW;
             const int steps = nrow + 31;
-            for (int t = 0; t < steps; ++t) {
+            // one wavefront step; FULL: every lane is on a real row (steps 31 .. nrow - 1), so the
+            // activity tests drop out of the cell loop
+            auto step = [&](int t, auto full) {
+                constexpr bool FULL = decltype(full)::value;
                 const int i = t + 1 - lane;
-                const bool act = i >= 1 && i <= nrow;
+                const bool act = FULL || (i >= 1 && i <= nrow);
                 hb = __shfl_up_sync(kFull, hb, 1);
                 int hl = __shfl_up_sync(kFull, hout, 1);
                 int el = __shfl_up_sync(kFull, eout, 1);
@@ -190,7 +194,11 @@ __device__ void sw_one(const SwView& v, uint32_t idx, int lane, uint8_t* scr, ui
                     if (holds_last_col) lcol[i] = hc;
                     if (!last && lane == 31) { bh[i] = hl; be[i] = el; }
                 }
-            }
+            };
+            int t = 0;
+            for (; t < min(31, steps); ++t) step(t, std::false_type{});
+            for (; t < nrow; ++t) step(t, std::true_type{});
+            for (; t < steps; ++t) step(t, std::false_type{});
             __syncwarp();
         }
 
@@ -383,8 +391,8 @@ __global__ void __launch_bounds__(256) sw_gather_kernel(const phmm_sw_result* __
 using SwKernel = void (*)(SwView);
 
 const SwKernel kSwKernels[kSwClasses] = {
-    sw_kernel<1, false>,  sw_kernel<2, false>,  sw_kernel<3, false>,  sw_kernel<4, false>, sw_kernel<5, false>,
-    sw_kernel<6, false>,  sw_kernel<8, false>,  sw_kernel<10, false>, sw_kernel<12, false>,
+    sw_kernel<1, false>,  sw_kernel<2, false>,  sw_kernel<3, false>,  sw_kernel<4, false>,  sw_kernel<5, false>,
+    sw_kernel<6, false>,  sw_kernel<7, false>,  sw_kernel<8, false>,  sw_kernel<10, false>, sw_kernel<12, false>,
     sw_kernel<16, false>, sw_kernel<20, false>, sw_kernel<24, false>, sw_kernel<24, true>,
 };
 

@@ -28,9 +28,9 @@ static_assert(sizeof(SwItem) == 24, "SwItem layout");
 constexpr int kSwMaxSeq = 2048;
 constexpr int kSwBlockWarps = 4;
 constexpr int kSwBandWords = 1024;   // trace-back band in shared memory per warp (4 KB)
-constexpr int kSwClasses = 13;       // 12 stripe widths (kSwK) + the 16-bit wrap-around class
-constexpr int kSwWrapClass = 12;
-constexpr int kSwK[kSwClasses] = {1, 2, 3, 4, 5, 6, 8, 10, 12, 16, 20, 24, 24};
+constexpr int kSwClasses = 14;       // 13 stripe widths (kSwK) + the 16-bit wrap-around class
+constexpr int kSwWrapClass = 13;
+constexpr int kSwK[kSwClasses] = {1, 2, 3, 4, 5, 6, 7, 8, 10, 12, 16, 20, 24, 24};
 
 // Per-warp scratch layout of one alignment (bytes, 256-aligned sections):
 //   bt    [stripes][nrow][32 * nw] u32: per cell a 4-bit code (state 1/2 | extension flags 4/8)

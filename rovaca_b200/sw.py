@@ -19,6 +19,9 @@ GENOTYPING = (10, -15, -30, -5)   # sw_parameters_genotype, lib/sw_avx/sw_avx.c:
 ASSEMBLY = (200, -150, -260, -11)  # sw_parameters_assemble, lib/sw_avx/sw_avx.c:14
 MAX_CIGAR = 2047                   # the reference emits at most cigar_max_len - 1 ops (sw_cigar.c:164)
 CIGAR_OPS = "MIDNSHP=XB"
+# read columns per lane of the kernel classes (phmm_sw.h kSwK); the last class is the 16-bit
+# wrap-around class for parameters whose int16 adds can wrap
+CLASS_K = (1, 2, 3, 4, 5, 6, 7, 8, 10, 12, 16, 20, 24, 24)
 
 SW_ITEM_DTYPE = np.dtype([("hap_offset", "<u8"), ("read_offset", "<u8"), ("hap_len", "<u4"), ("read_len", "<u4")])
 SW_RESULT_DTYPE = np.dtype([("score", "<i4"), ("alignment_offset", "<i4"), ("max_i", "<i4"), ("max_j", "<i4"),
@@ -179,9 +182,9 @@ class SwResident:
         return float(ms.value)
 
     def profile(self) -> np.ndarray:
-        """Device ms of each kernel class in one run (13 classes: stripe widths 1..24, then the 16-bit
-        wrap-around class)."""
-        cls = (C.c_float * 13)()
+        """Device ms of each kernel class in one run (CLASS_K: read columns per lane of the 14 classes;
+        the last is the 16-bit wrap-around class)."""
+        cls = (C.c_float * len(CLASS_K))()
         _lib.check(self._lib.phmm_sw_resident_run(self._h, 0, None, C.cast(cls, C.c_void_p)))
         return np.array(cls[:], np.float32)
 
