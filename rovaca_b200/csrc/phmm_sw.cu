@@ -61,11 +61,13 @@ struct SwView {
     uint32_t cigar_cap;
 };
 
+// Score add: two's-complement 32-bit, wrapped to 16 bits in the wrap-around class when the
+// alignment runs the int16 kernel (w16; an int32 alignment in that class adds in 32 bits).
 template <bool WRAP>
-__device__ __forceinline__ int sadd(int a, int b)
+__device__ __forceinline__ int sadd(int a, int b, bool w16)
 {
     const int s = (int)((unsigned)a + (unsigned)b);
-    return WRAP ? (int)(short)s : s;
+    return (WRAP && w16) ? (int)(short)s : s;
 }
 
 __device__ __forceinline__ uint32_t op_of(uint32_t run)
@@ -92,6 +94,7 @@ __device__ void sw_one(const SwView& v, uint32_t idx, int lane, uint8_t* scr, ui
         return;
     }
     const bool i32 = sw_uses_int32(v.variant, it.hap_len, it.read_len, v.prm.match);
+    const bool w16 = !i32;
     const int match = i32 ? v.prm.match : (int)(short)v.prm.match;
     const int mismatch = i32 ? v.prm.mismatch : (int)(short)v.prm.mismatch;
     const int open = i32 ? v.prm.gap_open : (int)(short)v.prm.gap_open;
@@ -163,11 +166,11 @@ __device__ void sw_one(const SwView& v, uint32_t idx, int lane, uint8_t* scr, ui
                 int hc = 0;
 #pragma unroll
                 for (int k = 0; k < K; ++k) {
-                    const int eo = sadd<WRAP>(hl, open), ee = sadd<WRAP>(el, ext);
+                    const int eo = sadd<WRAP>(hl, open, w16), ee = sadd<WRAP>(el, ext, w16);
                     const int e = max(eo, ee);
-                    const int fe = sadd<WRAP>(Fp[k], ext), fo = sadd<WRAP>(Hp[k], open);
+                    const int fe = sadd<WRAP>(Fp[k], ext, w16), fo = sadd<WRAP>(Hp[k], open, w16);
                     const int f = max(fe, fo);
-                    int h = max(sadd<WRAP>(diag, hb == rb[k] ? match : mismatch), cutoff);
+                    int h = max(sadd<WRAP>(diag, hb == rb[k] ? match : mismatch, w16), cutoff);
                     uint32_t c = (eo > ee ? 0u : (uint32_t)kStInsExt) | (fo > fe ? 0u : (uint32_t)kStDelExt);
                     if (e > h) { c |= kStIns; h = e; }
                     if (f > h) { c = (c & ~3u) | kStDel; h = f; }
