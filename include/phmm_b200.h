@@ -309,6 +309,38 @@ typedef struct phmm_region_events {
 PHMM_API phmm_status phmm_submit_region(phmm_engine* engine, const phmm_region_input* region,
                                         const phmm_region_events* events, double* out, uint8_t* keep,
                                         uint32_t* n_kept, phmm_ticket* ticket);
+/* Realignment of a region's kept reads to their best haplotypes on the GPU, on the bases already
+ * uploaded for the likelihoods (AssemblyBasedCallerUtils::realign_reads_to_their_best_haplotype,
+ * genotype/utils/assembly_based_caller_utils.cpp:146-169):
+ *   best haplotype of each kept read = AlleleLikelihoods::search_best_allele over the normalised,
+ *     filtered likelihoods, ties among haplotypes within 0.2 log10 of the best broken by hap_priority
+ *     (genotype/allele_likelihoods.hpp:589-658; HaplotypeCaller's priority is (is_reference ? 1 : 0)
+ *     + 1 - cigar elements, assembly_based_caller_utils.cpp:150-155);
+ *   Smith-Waterman of the read without its soft clips (clip_left / clip_right bases removed at each
+ *     end, ReadClipper::hard_clip_soft_clipped_bases) against that haplotype with the genotyping
+ *     parameters, as AlignmentUtils::create_read_aligned_to_ref calls it (alignment_utils.cpp:571-579).
+ * Outputs are per read in the region's read order: best_hap -1 and a zero result for dropped reads;
+ * sw[r].cigar_offset indexes `cigars`, which receives the region's CIGAR ops in read order.  When
+ * they exceed cigar_capacity the request completes with PHMM_ERR_LIMIT_EXCEEDED, *cigar_total set
+ * and everything but cigars filled. */
+typedef struct phmm_region_realign {
+    const double* hap_priority;  /* [n_haps] */
+    const uint16_t* clip_left;   /* [n_reads] or NULL (none) */
+    const uint16_t* clip_right;  /* [n_reads] or NULL (none) */
+    int32_t* best_hap;           /* out [n_reads] */
+    struct phmm_sw_result* sw;   /* out [n_reads] (phmm_sw_result, declared with phmm_sw_align) */
+    uint32_t* cigars;            /* out [cigar_capacity] */
+    uint64_t cigar_capacity;
+    uint64_t* cigar_total;       /* out, optional: ops the region's CIGARs need */
+} phmm_region_realign;
+
+/* phmm_submit_region with the realignment of the region's kept reads after the likelihoods (and the
+ * genotyping, when events are given), in the same batch on the device (no reference counterpart as
+ * one call: it joins call_pairhmm and the realignment that follows it per region). */
+PHMM_API phmm_status phmm_submit_region_realign(phmm_engine* engine, const phmm_region_input* region,
+                                                const phmm_region_events* events,
+                                                const phmm_region_realign* realign, double* out, uint8_t* keep,
+                                                uint32_t* n_kept, phmm_ticket* ticket);
 /* *done = 1 once the request's results are in out (or it failed / was cancelled). */
 PHMM_API phmm_status phmm_poll(phmm_engine* engine, phmm_ticket ticket, int32_t* done);
 /* Blocks up to timeout_us (negative = forever).  Once the request is done it returns the request's

@@ -14,6 +14,12 @@ Restates, for one sample and ploidy 2, what HaplotypeCaller does after call_pair
   * approximate_log10sum(a, b) = max + table[round((max - min) * 1e4)] below a difference of 8, the
     Jacobian table log10(1 + 10^(-k/1e4))   src/haplotypecaller/common/utils/math_utils.cpp:280-290,
                                               math_utils.h:209-242
+  * best haplotype of a read for the realignment: search_best_allele with can_be_reference and
+    priorities -- the running maximum and runner-up over the haplotypes (strict >), then, when the
+    runner-up is within 0.2 (log10) of the best, the haplotypes within 0.2 of it ranked by priority
+    (strict >)                                src/haplotypecaller/genotype/allele_likelihoods.hpp:589-658
+    HaplotypeCaller's priority: (is_reference ? 1 : 0) + 1 - cigar elements
+                                              src/haplotypecaller/genotype/utils/assembly_based_caller_utils.cpp:150-155
 The reference's own unit test (genotype/test/genotype_likelihood_calculator_unit_test.cpp:86-130)
 defines GL as sum_r [log10sum_c(lk(r, a_c) + log10(count_c)) - log10(2)] and accepts 1e-4; the
 tests here hold this restatement to that definition.
@@ -120,3 +126,33 @@ def genotype_region(lk_hr: np.ndarray, read_len, events):
         gl = genotype_likelihoods(alk)
         res.append((gl, best_genotype(gl), alk))
     return res, norm, keep
+
+
+INFORMATIVE_LOG10 = 0.2  # s_log_10_informative_threshold, allele_likelihoods.hpp:27
+
+
+def search_best_allele(values, priorities) -> int:
+    """Index of the best allele (haplotype) for one read's likelihoods, ties within the informative
+    threshold broken by priority."""
+    M = len(values)
+    best, second = 0, 0
+    bl, sl = float(values[0]), -math.inf
+    for a in range(1, M):
+        c = float(values[a])
+        if c > bl:
+            second, best, sl, bl = best, a, bl, c
+        elif c > sl:
+            second, sl = a, c
+    if bl - sl < INFORMATIVE_LOG10:
+        bp, sp = float(priorities[best]), float(priorities[second])
+        for a in range(M):
+            c = float(values[a])
+            if a == best or bl - c > INFORMATIVE_LOG10:
+                continue
+            cp = float(priorities[a])
+            if cp > bp:
+                second, best, sp, bp = best, a, bp, cp
+            elif cp > sp:
+                second, sp = a, cp
+    return best
+

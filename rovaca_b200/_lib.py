@@ -116,6 +116,13 @@ class ServerStats(C.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class RegionRealign(C.Structure):
+    """phmm_region_realign: realignment of a region's kept reads to their best haplotypes."""
+    _fields_ = [("hap_priority", C.c_void_p), ("clip_left", C.c_void_p), ("clip_right", C.c_void_p),
+                ("best_hap", C.c_void_p), ("sw", C.c_void_p), ("cigars", C.c_void_p), ("cigar_capacity", C.c_uint64),
+                ("cigar_total", C.c_void_p)]
+
+
 class SwItem(C.Structure):
     """phmm_sw_item: one alignment (haplotype = seq1, read = seq2) as offsets into two base buffers."""
     _fields_ = [("hap_offset", C.c_uint64), ("read_offset", C.c_uint64), ("hap_len", C.c_uint32),
@@ -169,6 +176,7 @@ def load() -> C.CDLL:
         "phmm_wait": (I32, [P, U64, I64, C.POINTER(D), C.POINTER(D)]),
         "phmm_cancel": (I32, [P, U64]),
         "phmm_server_stats_get": (I32, [P, P]),
+        "phmm_submit_region_realign": (I32, [P, P, P, P, P, P, C.POINTER(U32), C.POINTER(U64)]),
         "phmm_sw_align": (I32, [P, P, I32, U32, P, P, U64, P, U64, U32, P, P, U64, C.POINTER(U64)]),
         "phmm_sw_resident_create": (I32, [P, P, I32, U32, P, P, U64, P, U64, U32, C.POINTER(P)]),
         "phmm_sw_resident_run": (I32, [P, I32, C.POINTER(C.c_float), P]),

@@ -294,6 +294,122 @@ Engine::~Engine()
     if (d_tables_) cudaFree(d_tables_);
 }
 
+namespace {
+
+// Grows a device or pinned buffer of a slot (only between batches of that slot: the slot's stream
+// is idle when its serving worker calls these).
+phmm_status grow_device(char*& p, size_t& bytes, size_t need, std::string& err)
+{
+    if (need <= bytes) return PHMM_OK;
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+    const size_t want = std::max(need, need / 2 * 3);
+    if (cudaMalloc(&p, want) != cudaSuccess) {
+        cudaGetLastError();
+        err = "realignment arena of " + std::to_string(want) + " bytes could not be allocated";
+        return PHMM_ERR_OUT_OF_MEMORY;
+    }
+    bytes = want;
+    return PHMM_OK;
+}
+
+phmm_status grow_pinned(char*& p, size_t& bytes, size_t need, std::string& err)
+{
+    if (need <= bytes) return PHMM_OK;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    bytes = 0;
+    const size_t want = std::max(need, need / 2 * 3);
+    if (cudaMallocHost(&p, want) != cudaSuccess) {
+        cudaGetLastError();
+        err = "pinned realignment staging of " + std::to_string(want) + " bytes could not be allocated";
+        return PHMM_ERR_OUT_OF_MEMORY;
+    }
+    bytes = want;
+    return PHMM_OK;
+}
+
+}  // namespace
+
+phmm_status Engine::realign_enqueue(Slot& s, RealignBatch& rb, std::string& err)
+{
+    if (rb.plan.n == 0) return PHMM_OK;
+    rb.layout();
+    // growing frees the old buffers, which waits for the device: only this slot's work is queued
+    // before the wait, and arenas stop growing once they cover the slot's largest batch
+    if (rb.bytes > s.rdev_bytes) PHMM_CK(cudaStreamSynchronize(s.main));
+    phmm_status st = grow_device(s.rdev, s.rdev_bytes, rb.bytes, err);
+    if (st != PHMM_OK) return st;
+    st = grow_pinned(s.rpin, s.rpin_bytes, std::max(rb.upload_bytes(), rb.head_bytes()), err);
+    if (st != PHMM_OK) return st;
+    char* h = s.rpin;
+    char* d = s.rdev;
+    std::memcpy(h + rb.o_rr, rb.regions.data(), sizeof(RealignRegion) * rb.regions.size());
+    std::memcpy(h + rb.o_prio, rb.prio.data(), 8 * rb.prio.size());
+    std::memcpy(h + rb.o_clip, rb.clip.data(), 2 * rb.clip.size());
+    std::memcpy(h + rb.o_order, rb.plan.order.data(), 4ull * rb.plan.n);
+    std::memcpy(h + rb.o_slot, rb.plan.slot_off.data(), 8ull * rb.plan.n);
+    PHMM_CK(cudaMemcpyAsync(d, h, rb.upload_bytes(), cudaMemcpyHostToDevice, s.main));
+    RealignView v{};
+    v.regions = s.d_regions;
+    v.hap_off = s.d_hap_off;
+    v.read_off = s.d_read_off;
+    v.norm = s.d_out2;
+    v.keep = s.d_keep;
+    v.rr = (const RealignRegion*)(d + rb.o_rr);
+    v.n_rr = (uint32_t)rb.regions.size();
+    v.prio = (const double*)(d + rb.o_prio);
+    v.clip = (const uint16_t*)(d + rb.o_clip);
+    v.items = (SwItem*)(d + rb.o_items);
+    v.best = (int32_t*)(d + rb.o_best);
+    PHMM_CK(launch_realign_items(v, sms_ * 4, s.main));
+    SwDeviceBufs b;
+    b.items = v.items;
+    b.order = (const uint32_t*)(d + rb.o_order);
+    b.slot_off = (const uint64_t*)(d + rb.o_slot);
+    b.hap = s.d_hb;
+    b.read = s.d_rb;
+    b.claim = (unsigned int*)(d + rb.o_claim);
+    b.total = (unsigned long long*)(d + rb.o_total);
+    b.out = (phmm_sw_result*)(d + rb.o_out);
+    b.slots = (uint32_t*)(d + rb.o_slots);
+    b.compact = (uint32_t*)(d + rb.o_compact);
+    b.scratch = (uint8_t*)(d + rb.o_scratch);
+    const SwParams prm{10, -15, -30, -5};  // sw_parameters_genotype, lib/sw_avx/sw_avx.c:15
+    st = sw_launch(rb.plan, prm, 0, b, s.main, nullptr, nullptr, nullptr, err);
+    if (st != PHMM_OK) return st;
+    s.launches += 1 + 2;
+    for (int c = 0; c < kSwClasses; ++c) s.launches += rb.plan.grid[c] ? 1 : 0;
+    // total, results and best haplotypes come back with the rest of the batch's outputs
+    PHMM_CK(cudaMemcpyAsync(h, d + rb.o_total, rb.head_bytes(), cudaMemcpyDeviceToHost, s.main));
+    return PHMM_OK;
+}
+
+phmm_status Engine::realign_finish(Slot& s, RealignBatch& rb, std::string& err)
+{
+    const uint32_t n = rb.plan.n;
+    rb.res.assign(n, phmm_sw_result{});
+    rb.best.assign(n, -1);
+    rb.total = 0;
+    rb.cigars.clear();
+    if (n == 0) return PHMM_OK;
+    PHMM_CK(cudaStreamSynchronize(s.main));
+    const char* h = s.rpin;
+    std::memcpy(&rb.total, h, 8);
+    std::memcpy(rb.res.data(), h + (rb.o_out - rb.o_total), sizeof(phmm_sw_result) * n);
+    std::memcpy(rb.best.data(), h + (rb.o_best - rb.o_total), 4ull * n);
+    rb.cigars.resize(rb.total);
+    if (rb.total) {
+        phmm_status st = grow_pinned(s.rpin, s.rpin_bytes, 4 * rb.total, err);
+        if (st != PHMM_OK) return st;
+        PHMM_CK(cudaMemcpyAsync(s.rpin, s.rdev + rb.o_compact, 4 * rb.total, cudaMemcpyDeviceToHost, s.main));
+        PHMM_CK(cudaStreamSynchronize(s.main));
+        std::memcpy(rb.cigars.data(), s.rpin, 4 * rb.total);
+    }
+    return PHMM_OK;
+}
+
 phmm_status Engine::sw_aligner(SwAligner** out, std::string& err)
 {
     std::lock_guard<std::mutex> lk(sw_mu_);
@@ -338,6 +454,8 @@ void Engine::free_slot(Slot* s)
     if (s->graph) cudaGraphExecDestroy(s->graph);
     if (s->dev) cudaFree(s->dev);
     if (s->pinned) cudaFreeHost(s->pinned);
+    if (s->rdev) cudaFree(s->rdev);
+    if (s->rpin) cudaFreeHost(s->rpin);
     for (int c = 0; c < kNumClasses; ++c) {
         if (s->side[c]) cudaStreamDestroy(s->side[c]);
         if (s->ev_side[c]) cudaEventDestroy(s->ev_side[c]);

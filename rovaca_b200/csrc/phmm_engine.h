@@ -17,6 +17,7 @@
 namespace phmm {
 
 class SwAligner;
+struct RealignBatch;
 
 // Sizes an arena must hold.
 struct Capacity {
@@ -74,6 +75,11 @@ struct Slot {
     uint64_t arena_grows = 0;        // arena (re)allocations
     uint64_t graph_captures = 0;
     double setup_ms = 0.0;           // wall time spent growing the arena and capturing graphs
+    // realignment of region-API reads to their best haplotypes (grown on demand)
+    char* rdev = nullptr;
+    size_t rdev_bytes = 0;
+    char* rpin = nullptr;
+    size_t rpin_bytes = 0;
 };
 
 class Engine {
@@ -123,6 +129,12 @@ public:
     phmm_status time_fp32_class(Slot& s, const Plan& plan, int cls, int reps, float* best_ms, std::string& err);
     // Runs the tile-shape autotuner and installs its table (phmm_tune.cpp).
     phmm_status autotune(phmm_tune_report* report, std::string& err);
+    // Realignment of a batch's kept region-API reads to their best haplotypes, on the slot's main
+    // stream after the pipeline enqueue() launched (best haplotypes, Smith-Waterman, CIGAR
+    // compaction; results and CIGAR sizes copied back before finish() returns); realign_finish()
+    // after finish() fetches the CIGARs into rb.
+    phmm_status realign_enqueue(Slot& s, RealignBatch& rb, std::string& err);
+    phmm_status realign_finish(Slot& s, RealignBatch& rb, std::string& err);
     // The engine's Smith-Waterman aligner (phmm_sw.cu), created on first use.
     phmm_status sw_aligner(SwAligner** out, std::string& err);
 

@@ -33,7 +33,8 @@ phmm_status server_submit(phmm_engine* engine, const phmm_batch& b, double* out,
 phmm_status server_wait(phmm_engine* engine, phmm_ticket ticket, int64_t timeout_us, bool release, double* queued_us,
                         double* total_us, std::string& err);
 phmm_status server_submit_region(phmm_engine* engine, const phmm_region_input& in, const phmm_region_events* events,
-                                 double* out, uint8_t* keep, uint32_t* n_kept, phmm_ticket* ticket, std::string& err);
+                                 double* out, uint8_t* keep, uint32_t* n_kept, phmm_ticket* ticket, std::string& err,
+                                 const phmm_region_realign* realign = nullptr);
 
 namespace {
 

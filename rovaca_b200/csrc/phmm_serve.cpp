@@ -26,6 +26,7 @@
 #include "../../include/phmm_b200.h"
 #include "phmm_capi_internal.h"
 #include "phmm_engine.h"
+#include "phmm_sw.h"
 #include "phmm_plan.h"
 
 namespace phmm {
@@ -66,6 +67,18 @@ struct Request {
     int32_t* best = nullptr;
     double* allele_lk = nullptr;
     uint64_t gl_n = 0, allele_lk_n = 0;
+    // realignment of the kept reads to their best haplotypes (region API)
+    bool realign = false;
+    std::vector<double> prio;            // [n_haps]
+    std::vector<uint16_t> clip;          // [n_reads][2]
+    uint32_t max_hap = 0;                // longest haplotype
+    int32_t* best_hap = nullptr;
+    phmm_sw_result* sw = nullptr;
+    uint32_t* cigars = nullptr;
+    uint64_t cigar_capacity = 0;
+    uint64_t* cigar_total = nullptr;
+    phmm_status own_status = PHMM_OK;    // a failure of this request alone (its CIGAR buffer)
+    std::string own_error;
     uint64_t out_n = 0;
     uint64_t cells = 0;
     uint64_t bytes = 0;  // device footprint estimate for admission
@@ -124,6 +137,34 @@ uint64_t footprint(uint64_t read_bases, uint64_t hap_bases, uint64_t pairs, uint
 double ms_between(Clock::time_point a, Clock::time_point b)
 {
     return std::chrono::duration<double, std::milli>(b - a).count();
+}
+
+// A realigning request's share of the batch's realignment: its reads' best haplotypes and
+// alignments (a zero result for dropped reads) and its CIGAR ops, offsets rebased to its buffer.
+void scatter_realign(Request& r, const RealignBatch& rb, size_t region)
+{
+    size_t k = 0;
+    while (k < rb.regions.size() && rb.regions[k].region != region) ++k;
+    if (k == rb.regions.size()) return;
+    const uint32_t i0 = rb.regions[k].item_begin, n = r.n_reads;
+    const uint64_t first = n ? rb.res[i0].cigar_offset : 0;
+    const uint64_t end = n == 0 ? first : (i0 + n < rb.plan.n) ? rb.res[i0 + n].cigar_offset : rb.total;
+    const uint64_t ops = end - first;
+    if (r.cigar_total) *r.cigar_total = ops;
+    for (uint32_t q = 0; q < n; ++q) {
+        r.best_hap[q] = rb.best[i0 + q];
+        phmm_sw_result x = rb.res[i0 + q];
+        if (rb.best[i0 + q] < 0) x = phmm_sw_result{};
+        else x.cigar_offset = (uint32_t)(x.cigar_offset - first);
+        r.sw[q] = x;
+    }
+    if (ops > r.cigar_capacity) {
+        r.own_status = PHMM_ERR_LIMIT_EXCEEDED;
+        r.own_error = "realign: the region's CIGARs need " + std::to_string(ops) + " ops, the buffer holds " +
+                      std::to_string(r.cigar_capacity);
+        return;
+    }
+    if (ops) std::memcpy(r.cigars, rb.cigars.data() + first, 4 * ops);
 }
 
 void Server::worker(int idx)
@@ -295,6 +336,30 @@ void Server::worker(int idx)
                 plan.allele_lk_total = alk_o;
             }
             if (st == PHMM_OK) st = eng->enqueue(*slot, plan, b, want_flags, berr, api ? mq : nullptr);
+            // realignment of the kept reads of the requests that asked for it, after the pipeline
+            RealignBatch rb;
+            if (st == PHMM_OK && api) {
+                uint32_t item = 0;
+                for (size_t i = 0; i < batch.size(); ++i) {
+                    auto& r = batch[i];
+                    if (!r->realign) continue;
+                    rb.regions.push_back(RealignRegion{(uint32_t)i, item, (uint64_t)rb.prio.size()});
+                    rb.prio.insert(rb.prio.end(), r->prio.begin(), r->prio.end());
+                    rb.clip.insert(rb.clip.end(), r->clip.begin(), r->clip.end());
+                    for (uint32_t k = 0; k < r->n_reads; ++k) {
+                        const uint64_t len = r->read_off[k + 1] - r->read_off[k];
+                        rb.nrow.push_back(r->max_hap);
+                        rb.ncol.push_back((uint32_t)(len - r->clip[2 * k] - r->clip[2 * k + 1]));
+                    }
+                    item += r->n_reads;
+                }
+                if (item) {
+                    const SwParams prm{10, -15, -30, -5};  // sw_parameters_genotype, lib/sw_avx/sw_avx.c:15
+                    st = sw_plan(eng->device(), prm, 0, item, rb.nrow.data(), rb.ncol.data(), kSwMaxSeq - 1, rb.plan,
+                                 berr);
+                    if (st == PHMM_OK) st = eng->realign_enqueue(*slot, rb, berr);
+                }
+            }
             double* out = (double*)out_buf.p;
             uint8_t* flags = want_flags ? (uint8_t*)(out + out_total) : nullptr;
             double* gl = out + out_total;
@@ -308,6 +373,7 @@ void Server::worker(int idx)
             if (st == PHMM_OK)
                 st = eng->finish(*slot, plan, (!api || want_out) ? out : nullptr, flags, &ps, berr, keep, kept_n,
                                  n_events ? gl : nullptr, n_events ? best : nullptr, want_alk ? alk : nullptr);
+            if (st == PHMM_OK && rb.plan.n) st = eng->realign_finish(*slot, rb, berr);
             device_ms = ps.device_ms;
             wait_ms = ms_between(t_fin, Clock::now());
             if (st == PHMM_OK) {
@@ -320,6 +386,7 @@ void Server::worker(int idx)
                         if (r->n_reads) std::memcpy(r->keep, keep + ko, r->n_reads);
                         *r->n_kept = kept_n[i];
                     }
+                    if (r->realign) scatter_realign(*r, rb, i);
                     if (!r->n_alleles.empty()) {
                         std::memcpy(r->gl, gl + go, r->gl_n * sizeof(double));
                         std::memcpy(r->best, best + eo, r->n_alleles.size() * sizeof(int32_t));
@@ -337,8 +404,8 @@ void Server::worker(int idx)
             std::lock_guard<std::mutex> lk(mu);
             const auto now = Clock::now();
             for (auto& r : batch) {
-                r->status = st;
-                r->error = st == PHMM_OK ? std::string() : berr;
+                r->status = st != PHMM_OK ? st : r->own_status;
+                r->error = st != PHMM_OK ? berr : r->own_error;
                 r->state = ReqState::Done;
                 r->t_done = now;
                 std::vector<uint8_t>().swap(r->data);  // inputs are no longer needed
@@ -488,7 +555,8 @@ phmm_status server_submit(phmm_engine* engine, const phmm_batch& b, double* out,
 // Submits one region with call_pairhmm semantics: raw base qualities and MAPQ are copied, the
 // device prepares the reads and post-processes the likelihoods.
 phmm_status server_submit_region(phmm_engine* engine, const phmm_region_input& in, const phmm_region_events* events,
-                                 double* out, uint8_t* keep, uint32_t* n_kept, phmm_ticket* ticket, std::string& err)
+                                 double* out, uint8_t* keep, uint32_t* n_kept, phmm_ticket* ticket, std::string& err,
+                                 const phmm_region_realign* realign)
 {
     if (!in.hap_off || !in.read_off || (in.n_reads && (!in.mapq || !keep)) || !n_kept) {
         err = "null argument";
@@ -566,6 +634,35 @@ phmm_status server_submit_region(phmm_engine* engine, const phmm_region_input& i
         std::memcpy(r->data.data() + sc.hap_bases + sc.read_bases, in.read_qual + sc.read_base0, sc.read_bases);
     }
     r->mapq.assign(in.mapq, in.mapq + sc.n_reads);
+    if (realign) {
+        if ((sc.n_haps && !realign->hap_priority) || (sc.n_reads && (!realign->best_hap || !realign->sw)) ||
+            (realign->cigar_capacity && !realign->cigars)) {
+            err = "realign: hap_priority, best_hap and sw are required (cigars when cigar_capacity > 0)";
+            return PHMM_ERR_INVALID_ARGUMENT;
+        }
+        r->realign = true;
+        if (sc.n_haps) r->prio.assign(realign->hap_priority, realign->hap_priority + sc.n_haps);
+        r->clip.assign(2ull * sc.n_reads, 0);
+        for (uint32_t k = 0; k < sc.n_reads; ++k) {
+            const uint64_t len = r->read_off[k + 1] - r->read_off[k];
+            const uint32_t cl = realign->clip_left ? realign->clip_left[k] : 0;
+            const uint32_t cr = realign->clip_right ? realign->clip_right[k] : 0;
+            if (cl + cr > len) {
+                err = "realign: read " + std::to_string(k) + " clips " + std::to_string(cl) + " + " +
+                      std::to_string(cr) + " bases of " + std::to_string(len);
+                return PHMM_ERR_INVALID_ARGUMENT;
+            }
+            r->clip[2 * k] = (uint16_t)cl;
+            r->clip[2 * k + 1] = (uint16_t)cr;
+        }
+        for (uint32_t h = 0; h < sc.n_haps; ++h)
+            r->max_hap = std::max<uint32_t>(r->max_hap, (uint32_t)(r->hap_off[h + 1] - r->hap_off[h]));
+        r->best_hap = realign->best_hap;
+        r->sw = realign->sw;
+        r->cigars = realign->cigars;
+        r->cigar_capacity = realign->cigar_capacity;
+        r->cigar_total = realign->cigar_total;
+    }
     r->out = out;
     r->keep = keep;
     r->n_kept = n_kept;
@@ -573,6 +670,10 @@ phmm_status server_submit_region(phmm_engine* engine, const phmm_region_input& i
     r->cells = sc.cells;
     r->bytes = footprint(sc.read_bases, sc.hap_bases, sc.out_total, sc.n_reads, sc.n_haps) + sc.out_total * 8 +
                sc.n_reads * 2 + r->hap_allele.size() + (r->gl_n + r->allele_lk_n) * 8 + n_events * 36;
+    if (r->realign)  // items, results and two CIGAR slots per read, and its share of the scratch
+        r->bytes += sc.n_reads * (96 + 8ull * std::min<uint64_t>(kSwMaxSeq - 1, r->max_hap + (sc.read_bases /
+                                                                        std::max<uint32_t>(sc.n_reads, 1) + 1)))
+                    + sc.read_bases * (r->max_hap / 2 + 64) + 4096;
     for (uint32_t k = 0; k < sc.n_reads; ++k)
         if (r->read_off[k + 1] - r->read_off[k] > (uint64_t)kWarp * kMaxK) {
             r->bytes += engine_of(engine)->scratch_bytes();
@@ -640,7 +741,26 @@ phmm_status phmm_submit_region(phmm_engine* engine, const phmm_region_input* reg
         if (!engine) return set_error(PHMM_ERR_NOT_INITIALIZED, "engine is null");
         if (!region || !ticket) return set_error(PHMM_ERR_INVALID_ARGUMENT, "region or ticket is null");
         std::string err;
-        phmm_status st = phmm::server_submit_region(engine, *region, events, out, keep, n_kept, ticket, err);
+        phmm_status st = phmm::server_submit_region(engine, *region, events, out, keep, n_kept, ticket, err, nullptr);
+        return st == PHMM_OK ? PHMM_OK : set_error(st, err);
+    } catch (const std::bad_alloc&) {
+        return set_error(PHMM_ERR_OUT_OF_MEMORY, "host allocation failed");
+    } catch (const std::exception& ex) {
+        return set_error(PHMM_ERR_INTERNAL, ex.what());
+    }
+}
+
+phmm_status phmm_submit_region_realign(phmm_engine* engine, const phmm_region_input* region,
+                                       const phmm_region_events* events, const phmm_region_realign* realign,
+                                       double* out, uint8_t* keep, uint32_t* n_kept, phmm_ticket* ticket)
+{
+    try {
+        phmm::clear_error();
+        if (!engine) return set_error(PHMM_ERR_NOT_INITIALIZED, "engine is null");
+        if (!region || !ticket) return set_error(PHMM_ERR_INVALID_ARGUMENT, "region or ticket is null");
+        std::string err;
+        phmm_status st =
+            phmm::server_submit_region(engine, *region, events, out, keep, n_kept, ticket, err, realign);
         return st == PHMM_OK ? PHMM_OK : set_error(st, err);
     } catch (const std::bad_alloc&) {
         return set_error(PHMM_ERR_OUT_OF_MEMORY, "host allocation failed");

@@ -30,12 +30,14 @@
 #include <climits>
 #include <cstdint>
 #include <cstring>
+#include <mutex>
 #include <numeric>
 #include <string>
 #include <type_traits>
 #include <vector>
 
 #include "phmm_sw.h"
+#include "phmm_types.h"
 
 namespace phmm {
 
@@ -391,6 +393,100 @@ __global__ void __launch_bounds__(256) sw_gather_kernel(const phmm_sw_result* __
     }
 }
 
+// AlleleLikelihoods::search_best_allele with can_be_reference and priorities
+// (genotype/allele_likelihoods.hpp:589-658): the most likely haplotype of one read (column `col` of
+// a [hap][read] block with row stride `stride`); when the runner-up is within the log10 informative
+// threshold (0.2, allele_likelihoods.hpp:27), the haplotypes within that threshold of the best are
+// ranked by priority instead.
+__device__ int search_best_haplotype(const double* v, uint64_t stride, uint32_t col, uint32_t M, const double* pr)
+{
+    const double thr = 0.2;
+    int best = 0, second = 0;
+    double lb = v[col], sl = -__longlong_as_double(0x7ff0000000000000ll);
+    for (uint32_t a = 1; a < M; ++a) {
+        const double c = v[(uint64_t)a * stride + col];
+        if (c > lb) {
+            second = best;
+            best = (int)a;
+            sl = lb;
+            lb = c;
+        } else if (c > sl) {
+            second = (int)a;
+            sl = c;
+        }
+    }
+    if (lb - sl < thr) {
+        double bp = pr[best], sp = pr[second];
+        for (uint32_t a = 0; a < M; ++a) {
+            const double c = v[(uint64_t)a * stride + col];
+            if ((int)a == best || lb - c > thr) continue;
+            const double cp = pr[a];
+            if (cp > bp) {
+                second = best;
+                best = (int)a;
+                sp = bp;
+                bp = cp;
+            } else if (cp > sp) {
+                second = (int)a;
+                sp = cp;
+            }
+        }
+    }
+    return best;
+}
+
+constexpr int kRealignThreads = 256;
+
+// One block per realigned region: each kept read's column in the normalised block (a block scan of
+// the kept flags, as the post-processing placed them), its best haplotype and its alignment item.
+__global__ void __launch_bounds__(kRealignThreads) realign_items_kernel(RealignView v)
+{
+    __shared__ uint32_t warp_sums[kRealignThreads / 32];
+    __shared__ uint32_t base_kept;
+    for (uint32_t k = blockIdx.x; k < v.n_rr; k += gridDim.x) {
+        const RealignRegion rr = v.rr[k];
+        const RegionDesc rg = v.regions[rr.region];
+        const uint32_t M = rg.n_haps, N = rg.n_reads;
+        const double* norm = v.norm + rg.out_off;
+        if (threadIdx.x == 0) base_kept = 0;
+        __syncthreads();
+        for (uint32_t r0 = 0; r0 < N; r0 += blockDim.x) {
+            const uint32_t r = r0 + threadIdx.x;
+            const bool keep = r < N && v.keep[rg.read_begin + r] != 0;
+            const unsigned int ballot = __ballot_sync(kFull, keep);
+            const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+            if (lane == 0) warp_sums[w] = __popc(ballot);
+            __syncthreads();
+            uint32_t col = base_kept;
+            for (int q = 0; q < w; ++q) col += warp_sums[q];
+            col += __popc(ballot & ((1u << lane) - 1u));
+            if (r < N) {
+                SwItem it{};
+                int b = -1;
+                if (keep && M > 0) {
+                    b = search_best_haplotype(norm, N, col, M, v.prio + rr.prio_off);
+                    const uint64_t h0 = v.hap_off[rg.hap_begin + b], h1 = v.hap_off[rg.hap_begin + b + 1];
+                    const uint64_t q0 = v.read_off[rg.read_begin + r], q1 = v.read_off[rg.read_begin + r + 1];
+                    const uint32_t cl = v.clip[2ull * (rr.item_begin + r)], cr = v.clip[2ull * (rr.item_begin + r) + 1];
+                    it.hap_start = h0;
+                    it.hap_len = (uint32_t)(h1 - h0);
+                    it.read_start = q0 + cl;
+                    it.read_len = (uint32_t)(q1 - q0) - cl - cr;  // clips checked against the length at submit
+                }
+                v.items[rr.item_begin + r] = it;
+                v.best[rr.item_begin + r] = b;
+            }
+            __syncthreads();
+            if (threadIdx.x == blockDim.x - 1) {
+                uint32_t total = 0;
+                for (int q = 0; q < (int)(blockDim.x >> 5); ++q) total += warp_sums[q];
+                base_kept += total;
+            }
+            __syncthreads();
+        }
+    }
+}
+
 using SwKernel = void (*)(SwView);
 
 const SwKernel kSwKernels[kSwClasses] = {
@@ -414,20 +510,7 @@ int sw_class_of(const SwParams& prm, int variant, uint32_t nrow, uint32_t ncol)
     return kSwWrapClass - 1;  // K = 24 stripes
 }
 
-struct SwAligner::Plan {
-    uint32_t n = 0;
-    uint32_t cigar_cap = 0;
-    std::vector<uint32_t> order;             // item indices grouped by class, most cells first
-    std::vector<uint64_t> slot_off;          // per item: its CIGAR slot (ops) in the slot buffer
-    uint64_t slots = 0;                      // ops of all slots
-    uint32_t begin[kSwClasses + 1] = {};
-    uint64_t stride[kSwClasses] = {};        // scratch bytes per warp of each class
-    int grid[kSwClasses] = {};
-    uint64_t scratch = 0;                    // bytes for the largest class launch
-    uint64_t cells = 0;
-};
-
-// Device arena of one batch: inputs (items, order, slot offsets, bases), then the outputs
+// Device arena of one aligner batch: inputs (items, order, slot offsets, bases), then the outputs
 // (total, results), the CIGAR slots, the compact CIGAR buffer and the per-warp scratch.
 struct SwArenaLayout {
     uint64_t items, order, slot_off, hap, read, claim, total, out, slots, compact, scratch, bytes;
@@ -450,12 +533,29 @@ struct SwArenaLayout {
         scratch = a(compact + 4ull * std::max<uint64_t>(nslots, 1));
         bytes = scratch + scratch_bytes;
     }
+
+    SwDeviceBufs bufs(uint8_t* d) const
+    {
+        SwDeviceBufs b;
+        b.items = (const SwItem*)(d + items);
+        b.order = (const uint32_t*)(d + order);
+        b.slot_off = (const uint64_t*)(d + slot_off);
+        b.hap = d + hap;
+        b.read = d + read;
+        b.claim = (unsigned int*)(d + claim);
+        b.total = (unsigned long long*)(d + total);
+        b.out = (phmm_sw_result*)(d + out);
+        b.slots = (uint32_t*)(d + slots);
+        b.compact = (uint32_t*)(d + compact);
+        b.scratch = d + scratch;
+        return b;
+    }
 };
 
 struct SwAligner::Resident {
     SwParams prm{};
     int variant = 0;
-    Plan plan;
+    SwPlan plan;
     void* arena = nullptr;
     uint8_t* d = nullptr;
     SwArenaLayout lay{0, 0, 0, 0, 0};
@@ -488,7 +588,159 @@ phmm_status check_items(uint32_t n, const SwItem* items, uint64_t hap_bytes, uin
     return PHMM_OK;
 }
 
+// Multiprocessors and resident blocks per multiprocessor of each kernel class, per device (once).
+struct SwDeviceInfo {
+    bool ready = false;
+    int sms = 0;
+    int occ[kSwClasses] = {};
+};
+std::mutex g_info_mu;
+SwDeviceInfo g_info[64];
+
+phmm_status device_info(int device, SwDeviceInfo& out, std::string& err)
+{
+    if (device < 0 || device >= 64) {
+        err = "device ordinal out of range";
+        return PHMM_ERR_NO_DEVICE;
+    }
+    std::lock_guard<std::mutex> lk(g_info_mu);
+    SwDeviceInfo& di = g_info[device];
+    if (!di.ready) {
+        int cur = 0;
+        SW_CK(cudaGetDevice(&cur));
+        SW_CK(cudaSetDevice(device));
+        SW_CK(cudaDeviceGetAttribute(&di.sms, cudaDevAttrMultiProcessorCount, device));
+        for (int c = 0; c < kSwClasses; ++c) {
+            int b = 0;
+            SW_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kSwKernels[c], 32 * kSwBlockWarps, 0));
+            di.occ[c] = std::max(b, 1);
+        }
+        SW_CK(cudaSetDevice(cur));
+        di.ready = true;
+    }
+    out = di;
+    return PHMM_OK;
+}
+
 }  // namespace
+
+phmm_status sw_plan(int device, const SwParams& prm, int variant, uint32_t n, const uint32_t* nrow,
+                    const uint32_t* ncol, uint32_t cigar_cap, SwPlan& p, std::string& err)
+{
+    SwDeviceInfo di;
+    phmm_status st = device_info(device, di, err);
+    if (st != PHMM_OK) return st;
+    p = SwPlan();
+    p.n = n;
+    p.cigar_cap = std::min<uint32_t>(cigar_cap, kSwMaxSeq - 1);
+    std::vector<uint8_t> cls(n);
+    uint32_t counts[kSwClasses] = {};
+    p.slot_off.resize(n);
+    for (uint32_t q = 0; q < n; ++q) {
+        cls[q] = (uint8_t)sw_class_of(prm, variant, nrow[q], ncol[q]);
+        ++counts[cls[q]];
+        p.cells += (uint64_t)nrow[q] * ncol[q];
+        p.slot_off[q] = p.slots;
+        if (std::max(nrow[q], ncol[q]) < (uint32_t)kSwMaxSeq)  // runs <= rows + columns consumed
+            p.slots += std::min<uint64_t>(p.cigar_cap, (uint64_t)nrow[q] + ncol[q]);
+    }
+    if (p.slots > 0xffffffffull) {
+        err = "Smith-Waterman batch needs more than 2^32 CIGAR ops of room: split it";
+        return PHMM_ERR_LIMIT_EXCEEDED;
+    }
+    p.begin[0] = 0;
+    for (int c = 0; c < kSwClasses; ++c) p.begin[c + 1] = p.begin[c] + counts[c];
+    p.order.assign(n, 0);
+    uint32_t fill[kSwClasses];
+    std::copy(p.begin, p.begin + kSwClasses, fill);
+    for (uint32_t q = 0; q < n; ++q) p.order[fill[cls[q]]++] = q;
+    p.scratch = 0;
+    for (int c = 0; c < kSwClasses; ++c) {
+        auto first = p.order.begin() + p.begin[c], lastp = p.order.begin() + p.begin[c + 1];
+        std::stable_sort(first, lastp, [&](uint32_t x, uint32_t y) {
+            return (uint64_t)nrow[x] * ncol[x] > (uint64_t)nrow[y] * ncol[y];
+        });
+        uint64_t stride = 256;
+        for (auto it = first; it != lastp; ++it) {
+            if (std::max(nrow[*it], ncol[*it]) >= (uint32_t)kSwMaxSeq) continue;  // refused: no scratch
+            stride = std::max(stride, sw_layout(nrow[*it], ncol[*it], kSwK[c]).total);
+        }
+        p.stride[c] = stride;
+        const uint32_t m = counts[c];
+        uint64_t g = std::min<uint64_t>((m + kSwBlockWarps - 1) / kSwBlockWarps, (uint64_t)di.occ[c] * di.sms);
+        g = std::min<uint64_t>(g, std::max<uint64_t>(1, kSwScratchCap / (kSwBlockWarps * stride)));
+        p.grid[c] = m == 0 ? 0 : (int)g;
+        p.scratch = std::max(p.scratch, (uint64_t)p.grid[c] * kSwBlockWarps * stride);
+    }
+    p.gather_blocks = (int)std::max<uint64_t>(1, std::min<uint64_t>((n + 7) / 8, (uint64_t)di.sms * 8));
+    return PHMM_OK;
+}
+
+phmm_status sw_launch(const SwPlan& p, const SwParams& prm, int variant, const SwDeviceBufs& b, cudaStream_t st,
+                      cudaEvent_t ev0, cudaEvent_t ev1, float* class_ms, std::string& err)
+{
+    if (p.n == 0) return PHMM_OK;
+    SW_CK(cudaMemsetAsync(b.claim, 0, sizeof(unsigned int) * kSwClasses, st));
+    for (int c = 0; c < kSwClasses; ++c) {
+        if (class_ms) class_ms[c] = 0.f;
+        if (p.grid[c] == 0) continue;
+        SwView v{};
+        v.items = b.items;
+        v.order = b.order + p.begin[c];
+        v.n = p.begin[c + 1] - p.begin[c];
+        v.hap = b.hap;
+        v.read = b.read;
+        v.prm = prm;
+        v.variant = variant;
+        v.scratch = b.scratch;
+        v.stride = p.stride[c];
+        v.claim = b.claim + c;
+        v.out = b.out;
+        v.slot_off = b.slot_off;
+        v.ops = b.slots;
+        v.cigar_cap = p.cigar_cap;
+        if (class_ms) SW_CK(cudaEventRecord(ev0, st));
+        kSwKernels[c]<<<p.grid[c], 32 * kSwBlockWarps, 0, st>>>(v);
+        SW_CK(cudaGetLastError());
+        if (class_ms) {
+            SW_CK(cudaEventRecord(ev1, st));
+            SW_CK(cudaEventSynchronize(ev1));
+            SW_CK(cudaEventElapsedTime(&class_ms[c], ev0, ev1));
+        }
+    }
+    sw_scan_kernel<<<1, kScanThreads, 0, st>>>(b.out, p.n, p.cigar_cap, b.total);
+    SW_CK(cudaGetLastError());
+    sw_gather_kernel<<<p.gather_blocks, 256, 0, st>>>(b.out, b.slot_off, b.slots, b.compact, p.n, p.cigar_cap);
+    SW_CK(cudaGetLastError());
+    return PHMM_OK;
+}
+
+cudaError_t launch_realign_items(const RealignView& v, int blocks, cudaStream_t st)
+{
+    if (v.n_rr == 0) return cudaSuccess;
+    realign_items_kernel<<<std::max(1, std::min<int>(blocks, (int)v.n_rr)), kRealignThreads, 0, st>>>(v);
+    return cudaGetLastError();
+}
+
+void RealignBatch::layout()
+{
+    auto a = [](uint64_t x) { return (x + 255) & ~uint64_t(255); };
+    const uint64_t n = plan.n;
+    o_rr = 0;
+    o_prio = a(o_rr + sizeof(RealignRegion) * regions.size());
+    o_clip = a(o_prio + 8ull * prio.size());
+    o_order = a(o_clip + 2ull * clip.size());
+    o_slot = a(o_order + 4ull * n);
+    o_items = a(o_slot + 8ull * n);
+    o_claim = a(o_items + sizeof(SwItem) * n);
+    o_total = a(o_claim + 4ull * kSwClasses);
+    o_out = o_total + 8;
+    o_best = o_out + sizeof(phmm_sw_result) * n;
+    o_slots = a(o_best + 4ull * n);
+    o_compact = a(o_slots + 4ull * std::max<uint64_t>(plan.slots, 1));
+    o_scratch = a(o_compact + 4ull * std::max<uint64_t>(plan.slots, 1));
+    bytes = o_scratch + plan.scratch;
+}
 
 phmm_status SwAligner::create(int device, SwAligner** out, std::string& err)
 {
@@ -508,12 +760,6 @@ phmm_status SwAligner::create(int device, SwAligner** out, std::string& err)
         }                                                                             \
     } while (0)
     SW_CKC(cudaSetDevice(device));
-    SW_CKC(cudaDeviceGetAttribute(&a->sms_, cudaDevAttrMultiProcessorCount, device));
-    for (int c = 0; c < kSwClasses; ++c) {
-        int b = 0;
-        SW_CKC(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kSwKernels[c], 32 * kSwBlockWarps, 0));
-        a->occ_[c] = std::max(b, 1);
-    }
     SW_CKC(cudaStreamCreateWithFlags(&a->stream_, cudaStreamNonBlocking));
     SW_CKC(cudaEventCreate(&a->ev_[0]));
     SW_CKC(cudaEventCreate(&a->ev_[1]));
@@ -533,96 +779,14 @@ SwAligner::~SwAligner()
 }
 
 phmm_status SwAligner::plan(const SwParams& prm, int variant, uint32_t n, const SwItem* items, uint32_t cigar_cap,
-                            Plan& p, std::string& err) const
+                            SwPlan& p, std::string& err) const
 {
-    p.n = n;
-    p.cigar_cap = std::min<uint32_t>(cigar_cap, kSwMaxSeq - 1);
-    std::vector<uint8_t> cls(n);
-    uint32_t counts[kSwClasses] = {};
-    p.slot_off.resize(n);
-    p.slots = 0;
+    std::vector<uint32_t> nrow(n), ncol(n);
     for (uint32_t q = 0; q < n; ++q) {
-        const SwItem& x = items[q];
-        cls[q] = (uint8_t)sw_class_of(prm, variant, x.hap_len, x.read_len);
-        ++counts[cls[q]];
-        p.cells += (uint64_t)x.hap_len * x.read_len;
-        p.slot_off[q] = p.slots;
-        if (std::max(x.hap_len, x.read_len) < (uint32_t)kSwMaxSeq)  // runs <= rows + columns consumed
-            p.slots += std::min<uint64_t>(p.cigar_cap, (uint64_t)x.hap_len + x.read_len);
+        nrow[q] = items[q].hap_len;
+        ncol[q] = items[q].read_len;
     }
-    if (p.slots > 0xffffffffull) {
-        err = "Smith-Waterman batch needs more than 2^32 CIGAR ops of room: split it";
-        return PHMM_ERR_LIMIT_EXCEEDED;
-    }
-    p.begin[0] = 0;
-    for (int c = 0; c < kSwClasses; ++c) p.begin[c + 1] = p.begin[c] + counts[c];
-    p.order.assign(n, 0);
-    uint32_t fill[kSwClasses];
-    std::copy(p.begin, p.begin + kSwClasses, fill);
-    for (uint32_t q = 0; q < n; ++q) p.order[fill[cls[q]]++] = q;
-    p.scratch = 0;
-    for (int c = 0; c < kSwClasses; ++c) {
-        auto first = p.order.begin() + p.begin[c], lastp = p.order.begin() + p.begin[c + 1];
-        std::stable_sort(first, lastp, [&](uint32_t x, uint32_t y) {
-            return (uint64_t)items[x].hap_len * items[x].read_len > (uint64_t)items[y].hap_len * items[y].read_len;
-        });
-        uint64_t stride = 256;
-        for (auto it = first; it != lastp; ++it) {
-            const SwItem& x = items[*it];
-            if (std::max(x.hap_len, x.read_len) >= (uint32_t)kSwMaxSeq) continue;  // refused: no scratch
-            stride = std::max(stride, sw_layout(x.hap_len, x.read_len, kSwK[c]).total);
-        }
-        p.stride[c] = stride;
-        const uint32_t m = counts[c];
-        uint64_t g = std::min<uint64_t>((m + kSwBlockWarps - 1) / kSwBlockWarps, (uint64_t)occ_[c] * sms_);
-        g = std::min<uint64_t>(g, std::max<uint64_t>(1, kSwScratchCap / (kSwBlockWarps * stride)));
-        p.grid[c] = m == 0 ? 0 : (int)g;
-        p.scratch = std::max(p.scratch, (uint64_t)p.grid[c] * kSwBlockWarps * stride);
-    }
-    return PHMM_OK;
-}
-
-phmm_status SwAligner::launch(const Plan& p, const SwParams& prm, int variant, uint8_t* d, const SwArenaLayout& L,
-                              float* class_ms, std::string& err)
-{
-    cudaStream_t st = stream_;
-    unsigned int* claim = (unsigned int*)(d + L.claim);
-    phmm_sw_result* out = (phmm_sw_result*)(d + L.out);
-    SW_CK(cudaMemsetAsync(claim, 0, sizeof(unsigned int) * kSwClasses, st));
-    for (int c = 0; c < kSwClasses; ++c) {
-        if (class_ms) class_ms[c] = 0.f;
-        if (p.grid[c] == 0) continue;
-        SwView v{};
-        v.items = (const SwItem*)(d + L.items);
-        v.order = (const uint32_t*)(d + L.order) + p.begin[c];
-        v.n = p.begin[c + 1] - p.begin[c];
-        v.hap = d + L.hap;
-        v.read = d + L.read;
-        v.prm = prm;
-        v.variant = variant;
-        v.scratch = d + L.scratch;
-        v.stride = p.stride[c];
-        v.claim = claim + c;
-        v.out = out;
-        v.slot_off = (const uint64_t*)(d + L.slot_off);
-        v.ops = (uint32_t*)(d + L.slots);
-        v.cigar_cap = p.cigar_cap;
-        if (class_ms) SW_CK(cudaEventRecord(ev_[0], st));
-        kSwKernels[c]<<<p.grid[c], 32 * kSwBlockWarps, 0, st>>>(v);
-        SW_CK(cudaGetLastError());
-        if (class_ms) {
-            SW_CK(cudaEventRecord(ev_[1], st));
-            SW_CK(cudaEventSynchronize(ev_[1]));
-            SW_CK(cudaEventElapsedTime(&class_ms[c], ev_[0], ev_[1]));
-        }
-    }
-    sw_scan_kernel<<<1, kScanThreads, 0, st>>>(out, p.n, p.cigar_cap, (unsigned long long*)(d + L.total));
-    SW_CK(cudaGetLastError());
-    const int gblocks = (int)std::max<uint64_t>(1, std::min<uint64_t>((p.n + 7) / 8, (uint64_t)sms_ * 8));
-    sw_gather_kernel<<<gblocks, 256, 0, st>>>(out, (const uint64_t*)(d + L.slot_off), (const uint32_t*)(d + L.slots),
-                                              (uint32_t*)(d + L.compact), p.n, p.cigar_cap);
-    SW_CK(cudaGetLastError());
-    return PHMM_OK;
+    return sw_plan(dev_, prm, variant, n, nrow.data(), ncol.data(), cigar_cap, p, err);
 }
 
 phmm_status SwAligner::ensure_pinned(uint64_t bytes, std::string& err)
@@ -678,7 +842,7 @@ phmm_status SwAligner::align(const SwParams& prm, int variant, uint32_t n, const
     if (st != PHMM_OK) return st;
     std::lock_guard<std::mutex> lk(mu_);
     SW_CK(cudaSetDevice(dev_));
-    Plan p;
+    SwPlan p;
     st = plan(prm, variant, n, items, cigar_cap, p, err);
     if (st != PHMM_OK) return st;
     const SwArenaLayout L(n, hap_bytes, read_bytes, p.slots, p.scratch);
@@ -709,7 +873,7 @@ phmm_status SwAligner::align(const SwParams& prm, int variant, uint32_t n, const
     if (read_bytes) std::memcpy(h + L.read, read, read_bytes);
     SW_CK(cudaMemcpyAsync(d, h, L.in_bytes(), cudaMemcpyHostToDevice, stream_));
     SW_CK(cudaEventRecord(ev_[0], stream_));
-    st = launch(p, prm, variant, d, L, nullptr, err);
+    st = sw_launch(p, prm, variant, L.bufs(d), stream_, ev_[0], ev_[1], nullptr, err);
     if (st != PHMM_OK) return st;
     SW_CK(cudaEventRecord(ev_[1], stream_));
     st = read_back(d, L, n, out, cigars, cigar_capacity, cigar_total, err);
@@ -737,8 +901,8 @@ phmm_status SwAligner::resident_create(const SwParams& prm, int variant, uint32_
     r->lay = SwArenaLayout(n, hap_bytes, read_bytes, r->plan.slots, r->plan.scratch);
     if (cudaMalloc(&r->arena, r->lay.bytes) != cudaSuccess) {
         cudaGetLastError();
-        delete r;
         err = "Smith-Waterman resident arena of " + std::to_string(r->lay.bytes) + " bytes could not be allocated";
+        delete r;
         return PHMM_ERR_OUT_OF_MEMORY;
     }
     r->d = (uint8_t*)r->arena;
@@ -769,10 +933,11 @@ phmm_status SwAligner::resident_run(Resident* r, int iterations, float* ms_per_r
     SW_CK(cudaSetDevice(dev_));
     if (ms_per_run) *ms_per_run = 0.f;
     if (r->plan.n == 0) return PHMM_OK;
+    const SwDeviceBufs b = r->lay.bufs(r->d);
     if (iterations > 0) {
         SW_CK(cudaEventRecord(ev_[0], stream_));
         for (int it = 0; it < iterations; ++it) {
-            phmm_status st = launch(r->plan, r->prm, r->variant, r->d, r->lay, nullptr, err);
+            phmm_status st = sw_launch(r->plan, r->prm, r->variant, b, stream_, nullptr, nullptr, nullptr, err);
             if (st != PHMM_OK) return st;
         }
         SW_CK(cudaEventRecord(ev_[1], stream_));
@@ -782,7 +947,7 @@ phmm_status SwAligner::resident_run(Resident* r, int iterations, float* ms_per_r
         if (ms_per_run) *ms_per_run = ms / iterations;
     }
     if (class_ms) {
-        phmm_status st = launch(r->plan, r->prm, r->variant, r->d, r->lay, class_ms, err);
+        phmm_status st = sw_launch(r->plan, r->prm, r->variant, b, stream_, ev_[0], ev_[1], class_ms, err);
         if (st != PHMM_OK) return st;
         SW_CK(cudaStreamSynchronize(stream_));
     }

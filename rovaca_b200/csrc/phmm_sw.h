@@ -90,7 +90,98 @@ __host__ __device__ inline bool sw_w16_cannot_wrap(int32_t match, int32_t mismat
 
 int sw_class_of(const SwParams& prm, int variant, uint32_t nrow, uint32_t ncol);
 
+// Host plan of one batch of alignments: kernel class of each (by read columns, or the wrap-around
+// class), alignments grouped by class most cells first, CIGAR slots, grids and scratch.
+struct SwPlan {
+    uint32_t n = 0;
+    uint32_t cigar_cap = 0;
+    std::vector<uint32_t> order;             // item indices grouped by class, most cells first
+    std::vector<uint64_t> slot_off;          // per item: its CIGAR slot (ops) in the slot buffer
+    uint64_t slots = 0;                      // ops of all slots
+    uint32_t begin[kSwClasses + 1] = {};
+    uint64_t stride[kSwClasses] = {};        // scratch bytes per warp of each class
+    int grid[kSwClasses] = {};
+    int gather_blocks = 1;
+    uint64_t scratch = 0;                    // bytes for the largest class launch
+    uint64_t cells = 0;
+};
+
+// Device buffers of one batch (see SwPlan for their sizes: n items, n results, `slots` ops twice,
+// `scratch` bytes, kSwClasses claim counters).
+struct SwDeviceBufs {
+    const SwItem* items = nullptr;
+    const uint32_t* order = nullptr;
+    const uint64_t* slot_off = nullptr;
+    const uint8_t* hap = nullptr;            // base of the items' haplotype offsets
+    const uint8_t* read = nullptr;           // base of the items' read offsets
+    unsigned int* claim = nullptr;
+    unsigned long long* total = nullptr;     // out: CIGAR ops of the batch
+    phmm_sw_result* out = nullptr;
+    uint32_t* slots = nullptr;
+    uint32_t* compact = nullptr;
+    uint8_t* scratch = nullptr;
+};
+
+// Plans n alignments on `device` from their rows (haplotype lengths, or upper bounds of them) and
+// columns (read lengths).
+phmm_status sw_plan(int device, const SwParams& prm, int variant, uint32_t n, const uint32_t* nrow,
+                    const uint32_t* ncol, uint32_t cigar_cap, SwPlan& p, std::string& err);
+// Launches a planned batch on stream st: the class kernels, the CIGAR offset scan and the gather.
+// class_ms (optional, kSwClasses): every class timed alone with ev0/ev1 (synchronising).
+phmm_status sw_launch(const SwPlan& p, const SwParams& prm, int variant, const SwDeviceBufs& b, cudaStream_t st,
+                      cudaEvent_t ev0, cudaEvent_t ev1, float* class_ms, std::string& err);
+
 struct SwArenaLayout;
+
+// ---- realignment of region-API regions' kept reads to their best haplotypes (device side) ----
+
+struct RegionDesc;
+
+// A region-API region of the batch whose kept reads are realigned.
+struct RealignRegion {           // 16 bytes
+    uint32_t region;             // index in the batch
+    uint32_t item_begin;         // its first Smith-Waterman item (one per read, in read order)
+    uint64_t prio_off;           // its haplotypes' tie-break priorities
+};
+
+struct RealignView {
+    const RegionDesc* regions;
+    const uint64_t* hap_off;     // batch haplotype offsets into the haplotype bases
+    const uint64_t* read_off;    // batch read offsets into the read bases
+    const double* norm;          // normalised likelihoods: region blocks at out_off, kept reads first
+    const uint8_t* keep;         // [batch reads]
+    const RealignRegion* rr;
+    uint32_t n_rr;
+    const double* prio;
+    const uint16_t* clip;        // [items][2]: bases dropped at the read's start and end
+    SwItem* items;               // out: the read against its best haplotype
+    int32_t* best;               // out: best haplotype (index in the region), -1 for dropped reads
+};
+
+// Fills the items and best haplotypes of every realigned region (one block per region).
+cudaError_t launch_realign_items(const RealignView& v, int blocks, cudaStream_t st);
+
+// Host side of one batch's realignment: the regions, their inputs, the plan, the device layout in
+// the slot's realignment arena, and (after it ran) the results per item.
+struct RealignBatch {
+    std::vector<RealignRegion> regions;
+    std::vector<double> prio;
+    std::vector<uint16_t> clip;              // 2 per item
+    std::vector<uint32_t> nrow, ncol;        // per item: the region's longest haplotype, the clipped read
+    SwPlan plan;
+    // device layout (bytes): [rr | prio | clip | order | slot_off] uploaded, then the items,
+    // claim counters, [total | results | best] read back, CIGAR slots, compact CIGARs, scratch
+    uint64_t o_rr = 0, o_prio = 0, o_clip = 0, o_order = 0, o_slot = 0, o_items = 0, o_claim = 0, o_total = 0,
+             o_out = 0, o_best = 0, o_slots = 0, o_compact = 0, o_scratch = 0, bytes = 0;
+    uint64_t upload_bytes() const { return o_items; }
+    uint64_t head_bytes() const { return o_slots - o_total; }
+    void layout();
+    // results (realign_finish)
+    uint64_t total = 0;
+    std::vector<phmm_sw_result> res;
+    std::vector<int32_t> best;
+    std::vector<uint32_t> cigars;
+};
 
 // Device state of the aligner: a stream, a growable arena and pinned staging, owned by an engine.
 class SwAligner {
@@ -118,18 +209,13 @@ public:
 
 private:
     SwAligner() = default;
-    struct Plan;
-    phmm_status plan(const SwParams& prm, int variant, uint32_t n, const SwItem* items, uint32_t cigar_cap, Plan& p,
-                     std::string& err) const;
-    phmm_status launch(const Plan& p, const SwParams& prm, int variant, uint8_t* d, const SwArenaLayout& L,
-                       float* class_ms, std::string& err);
+    phmm_status plan(const SwParams& prm, int variant, uint32_t n, const SwItem* items, uint32_t cigar_cap,
+                     SwPlan& p, std::string& err) const;
     phmm_status ensure_pinned(uint64_t bytes, std::string& err);
     phmm_status read_back(uint8_t* d, const SwArenaLayout& L, uint32_t n, phmm_sw_result* out, uint32_t* cigars,
                           uint64_t capacity, uint64_t* total, std::string& err);
 
     int dev_ = 0;
-    int sms_ = 0;
-    int occ_[kSwClasses] = {};
     cudaStream_t stream_ = nullptr;
     cudaEvent_t ev_[2] = {};
     void* arena_ = nullptr;

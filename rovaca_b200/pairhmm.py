@@ -339,13 +339,16 @@ class Engine:
     # ---- region API ----------------------------------------------------------------------
     def submit_region(self, haplotypes, reads, base_quals, mapq, min_quality_threshold: int = 18,
                       pcr_option: str | int = "CONSERVATIVE", events=None, want_matrix: bool = True,
-                      want_allele_lk: bool = False) -> "RegionTicket":
+                      want_allele_lk: bool = False, realign=None) -> "RegionTicket":
         """phmm_submit_region: queues one region with call_pairhmm semantics (read preparation and
         post-processing on the GPU).  events: optional list of (n_alleles, allele of each haplotype,
-        -1 for none) to genotype on the GPU.  RegionTicket.wait() returns (matrix or None, keep mask)
-        and RegionTicket.genotypes() the per-event results."""
+        -1 for none) to genotype on the GPU.  realign: optional dict with "priority" (one per
+        haplotype) and optional "clip_left" / "clip_right" (one per read) to realign the kept reads
+        to their best haplotypes on the GPU (phmm_submit_region_realign).  RegionTicket.wait() returns
+        (matrix or None, keep mask), RegionTicket.genotypes() the per-event results and
+        RegionTicket.realignment() the best haplotypes and alignments."""
         return RegionTicket(self, haplotypes, reads, base_quals, mapq, min_quality_threshold, pcr_option, events,
-                            want_matrix, want_allele_lk)
+                            want_matrix, want_allele_lk, realign)
 
     def call_region(self, haplotypes, reads, base_quals, mapq, min_quality_threshold: int = 18,
                     pcr_option: str | int = "CONSERVATIVE"):
@@ -373,7 +376,7 @@ class RegionTicket:
     """A region submitted with phmm_submit_region; keeps its buffers alive until wait()."""
 
     def __init__(self, engine: Engine, haplotypes, reads, base_quals, mapq, min_quality_threshold, pcr_option,
-                 events=None, want_matrix: bool = True, want_allele_lk: bool = False):
+                 events=None, want_matrix: bool = True, want_allele_lk: bool = False, realign=None):
         pcr = PCR_MODELS[pcr_option] if isinstance(pcr_option, str) else int(pcr_option)
         hs = [_u8(h) for h in haplotypes]
         rs = [_u8(r) for r in reads]
@@ -409,9 +412,44 @@ class RegionTicket:
             ev_ptr = C.byref(self.events)
         self._engine = engine
         t = C.c_uint64()
-        check(engine._lib.phmm_submit_region(engine._h, C.byref(inp), ev_ptr, _ptr(self.out), _ptr(self.keep),
-                                             C.byref(self.n_kept), C.byref(t)))
+        self.realign = None
+        if realign is not None:
+            from . import sw
+
+            prio = np.ascontiguousarray(np.asarray(realign["priority"], np.float64).reshape(-1))
+            zeros = np.zeros(self.n_reads, np.uint16)
+            cl = np.ascontiguousarray(np.asarray(realign.get("clip_left", zeros), np.uint16).reshape(-1))
+            cr = np.ascontiguousarray(np.asarray(realign.get("clip_right", zeros), np.uint16).reshape(-1))
+            if prio.size != self.n_haps or cl.size != self.n_reads or cr.size != self.n_reads:
+                raise ValueError("realign: one priority per haplotype and one clip per read")
+            lens = np.array([len(r) for r in rs], np.int64)
+            cap = int(np.minimum(lens - cl - cr + max((len(h) for h in hs), default=0), sw.MAX_CIGAR).sum())
+            cap = int(realign.get("cigar_capacity", cap))
+            self.best_hap = np.empty(max(self.n_reads, 1), np.int32)
+            self.sw_res = np.zeros(max(self.n_reads, 1), sw.SW_RESULT_DTYPE)
+            self.cigars = np.empty(max(cap, 1), np.uint32)
+            self.cigar_total = C.c_uint64()
+            self._keepalive += [prio, cl, cr]
+            self.realign = _lib.RegionRealign(prio.ctypes.data, cl.ctypes.data, cr.ctypes.data,
+                                              self.best_hap.ctypes.data, self.sw_res.ctypes.data,
+                                              self.cigars.ctypes.data, self.cigars.size,
+                                              C.cast(C.byref(self.cigar_total), C.c_void_p))
+            check(engine._lib.phmm_submit_region_realign(engine._h, C.byref(inp), ev_ptr, C.byref(self.realign),
+                                                         _ptr(self.out), _ptr(self.keep), C.byref(self.n_kept),
+                                                         C.byref(t)))
+        else:
+            check(engine._lib.phmm_submit_region(engine._h, C.byref(inp), ev_ptr, _ptr(self.out), _ptr(self.keep),
+                                                 C.byref(self.n_kept), C.byref(t)))
         self.ticket = t.value
+
+    def realignment(self):
+        """(best haplotype per read, -1 for dropped reads; sw.SwResults of each read against it) after
+        wait()."""
+        from . import sw
+
+        n = self.n_reads
+        return self.best_hap[:n].copy(), sw.SwResults(self.sw_res[:n].copy(),
+                                                     self.cigars[:self.cigar_total.value].copy(), sw.MAX_CIGAR)
 
     def wait(self):
         """Blocks until done; returns (matrix [n_haps][n_reads] with kept reads first or None, keep mask)."""

@@ -59,3 +59,34 @@ def test_marginalisation_takes_the_best_haplotype_and_skips_nan():
     alk = G.marginalize(norm, 2, [0, 0, 1], 3)
     assert alk[0].tolist() == [-1.0, -3.0] and alk[1].tolist() == [-0.5, -4.0]
     assert alk[2].tolist() == [-math.inf, -math.inf]
+
+
+def test_best_haplotype_follows_reference_unit_test_rule():
+    """With the reference-allele priority (1 for the reference, 0 otherwise) the best allele is the
+    most likely one unless the reference is within 0.2 of it, then the reference
+    (allele_likelihoods_unit_test.cpp:106-163, testBestAlleles)."""
+    import random
+
+    from oracle.genotype import search_best_allele
+
+    rng = random.Random(3)
+    for _ in range(3000):
+        M = rng.randint(1, 8)
+        vals = [round(-rng.random() * 3, rng.choice([1, 2, 6])) for _ in range(M)]
+        ref = rng.randrange(M)
+        prio = [1.0 if a == ref else 0.0 for a in range(M)]
+        best_idx, best_lk = -1, float("-inf")
+        for a, v in enumerate(vals):
+            if v > best_lk:
+                best_idx, best_lk = a, v
+        override = ref != best_idx and best_lk - vals[ref] < 0.2
+        assert search_best_allele(vals, prio) == (ref if override else best_idx), (vals, ref)
+
+
+def test_best_haplotype_priorities_break_ties():
+    from oracle.genotype import search_best_allele
+
+    assert search_best_allele([-1.0, -1.1, -5.0], [0, 2, 9]) == 1      # -5 is outside the threshold
+    assert search_best_allele([-1.0, -1.5], [0, 9]) == 0               # not within 0.2: likelihood wins
+    assert search_best_allele([-1.0, -1.0, -1.0], [3, 1, 3]) == 0      # equal priorities keep the first
+    assert search_best_allele([-2.0], [0]) == 0
