@@ -39,6 +39,12 @@
 #include "phmm_sw.h"
 #include "phmm_types.h"
 
+// 1: the cell update of the 32-bit classes through the dynamic-programming max instructions
+// (__vibmax_s32, __viaddmax_s32); 0: plain compares and selects.  Both give the same results.
+#ifndef PHMM_SW_DPX
+#define PHMM_SW_DPX 0
+#endif
+
 namespace phmm {
 
 namespace {
@@ -168,14 +174,32 @@ __device__ void sw_one(const SwView& v, uint32_t idx, int lane, uint8_t* scr, ui
                 int hc = 0;
 #pragma unroll
                 for (int k = 0; k < K; ++k) {
-                    const int eo = sadd<WRAP>(hl, open, w16), ee = sadd<WRAP>(el, ext, w16);
-                    const int e = max(eo, ee);
-                    const int fe = sadd<WRAP>(Fp[k], ext, w16), fo = sadd<WRAP>(Hp[k], open, w16);
-                    const int f = max(fe, fo);
-                    int h = max(sadd<WRAP>(diag, hb == rb[k] ? match : mismatch, w16), cutoff);
-                    uint32_t c = (eo > ee ? 0u : (uint32_t)kStInsExt) | (fo > fe ? 0u : (uint32_t)kStDelExt);
-                    if (e > h) { c |= kStIns; h = e; }
-                    if (f > h) { c = (c & ~3u) | kStDel; h = f; }
+                    int e, f, h;
+                    uint32_t c;
+#if PHMM_SW_DPX
+                    if (!WRAP) {
+                        // the same comparisons through the dynamic-programming max instructions:
+                        // __vibmax_s32(a, b, &p) = max(a, b) with p = (a >= b)
+                        bool pe, pf, ph_e, ph_f;
+                        e = __vibmax_s32(el + ext, hl + open, &pe);        // pe: extension (not open > ext)
+                        f = __vibmax_s32(Fp[k] + ext, Hp[k] + open, &pf);  // pf: extension
+                        h = __viaddmax_s32(diag, hb == rb[k] ? match : mismatch, cutoff);
+                        h = __vibmax_s32(h, e, &ph_e);                     // !ph_e: E strictly greater
+                        h = __vibmax_s32(h, f, &ph_f);                     // !ph_f: F strictly greater
+                        c = (pe ? (uint32_t)kStInsExt : 0u) | (pf ? (uint32_t)kStDelExt : 0u) |
+                            (!ph_f ? (uint32_t)kStDel : (!ph_e ? (uint32_t)kStIns : 0u));
+                    } else
+#endif
+                    {
+                        const int eo = sadd<WRAP>(hl, open, w16), ee = sadd<WRAP>(el, ext, w16);
+                        e = max(eo, ee);
+                        const int fe = sadd<WRAP>(Fp[k], ext, w16), fo = sadd<WRAP>(Hp[k], open, w16);
+                        f = max(fe, fo);
+                        h = max(sadd<WRAP>(diag, hb == rb[k] ? match : mismatch, w16), cutoff);
+                        c = (eo > ee ? 0u : (uint32_t)kStInsExt) | (fo > fe ? 0u : (uint32_t)kStDelExt);
+                        if (e > h) { c |= kStIns; h = e; }
+                        if (f > h) { c = (c & ~3u) | kStDel; h = f; }
+                    }
                     diag = Hp[k];
                     if (act) { Hp[k] = h; Fp[k] = f; }
                     hl = h;
