@@ -39,10 +39,11 @@
 #include "phmm_sw.h"
 #include "phmm_types.h"
 
-// 1: the cell update of the 32-bit classes through the dynamic-programming max instructions
-// (__vibmax_s32, __viaddmax_s32); 0: plain compares and selects.  Both give the same results.
-#ifndef PHMM_SW_DPX
-#define PHMM_SW_DPX 0
+// 1: the 32-bit classes add scores with integer multiply-adds by a unit factor the compiler cannot
+// see (the FMA pipe), leaving the ALU pipe the maxima, compares and selects; 0: plain adds.  Both
+// give the same results.
+#ifndef PHMM_SW_IMAD
+#define PHMM_SW_IMAD 1
 #endif
 
 namespace phmm {
@@ -67,13 +68,15 @@ struct SwView {
     const uint64_t* slot_off;    // per item: its CIGAR slot in `ops` (min(cap, nrow + ncol) ops)
     uint32_t* ops;
     uint32_t cigar_cap;
+    int one;                     // 1 (a value the compiler cannot fold, see PHMM_SW_IMAD)
 };
 
 // Score add: two's-complement 32-bit, wrapped to 16 bits in the wrap-around class when the
 // alignment runs the int16 kernel (w16; an int32 alignment in that class adds in 32 bits).
 template <bool WRAP>
-__device__ __forceinline__ int sadd(int a, int b, bool w16)
+__device__ __forceinline__ int sadd(int a, int b, bool w16, int one)
 {
+    if (!WRAP && PHMM_SW_IMAD) return (int)((unsigned)a * (unsigned)one + (unsigned)b);
     const int s = (int)((unsigned)a + (unsigned)b);
     return (WRAP && w16) ? (int)(short)s : s;
 }
@@ -86,7 +89,23 @@ __device__ __forceinline__ uint32_t op_of(uint32_t run)
 }
 
 // Forward pass, end-cell selection and trace-back of one alignment.
-template <int K, bool WRAP>
+// Whether max(cutoff, H(i-1,j-1) + s) can change any cell of an alignment.  E(i,j) >= open + (j-1) x
+// min(extend, 0) for every cell (E(i,1) >= H(i,0) + open, then each step adds at most -extend), and
+// wherever E > cutoff the cutoff changes neither H nor the state (E then wins over a diagonal term
+// below the cutoff with or without it).  So an alignment whose read is short enough for
+// open + (ncol - 1) x min(extend, 0) > cutoff runs without it.  Only for classes without 16-bit
+// wrap-around, where these bounds are exact integer bounds.
+__device__ __forceinline__ bool sw_cutoff_can_bind(const SwView& v, const SwItem& it)
+{
+    const bool i32 = sw_uses_int32(v.variant, it.hap_len, it.read_len, v.prm.match);
+    const long long open = i32 ? v.prm.gap_open : (short)v.prm.gap_open;
+    const long long ext = i32 ? v.prm.gap_extend : (short)v.prm.gap_extend;
+    const long long cutoff = i32 ? -100000000 : -8192;
+    const long long ncol = it.read_len;
+    return !(open + (ncol > 0 ? ncol - 1 : 0) * (ext < 0 ? ext : 0) > cutoff);
+}
+
+template <int K, bool WRAP, bool CUT>
 __device__ void sw_one(const SwView& v, uint32_t idx, int lane, uint8_t* scr, uint32_t* band)
 {
     constexpr int NW = (K + 7) / 8;
@@ -103,6 +122,7 @@ __device__ void sw_one(const SwView& v, uint32_t idx, int lane, uint8_t* scr, ui
     }
     const bool i32 = sw_uses_int32(v.variant, it.hap_len, it.read_len, v.prm.match);
     const bool w16 = !i32;
+    const int one = v.one;
     const int match = i32 ? v.prm.match : (int)(short)v.prm.match;
     const int mismatch = i32 ? v.prm.mismatch : (int)(short)v.prm.mismatch;
     const int open = i32 ? v.prm.gap_open : (int)(short)v.prm.gap_open;
@@ -174,37 +194,20 @@ __device__ void sw_one(const SwView& v, uint32_t idx, int lane, uint8_t* scr, ui
                 int hc = 0;
 #pragma unroll
                 for (int k = 0; k < K; ++k) {
-                    int e, f, h;
-                    uint32_t c;
-#if PHMM_SW_DPX
-                    if (!WRAP) {
-                        // the same comparisons through the dynamic-programming max instructions:
-                        // __vibmax_s32(a, b, &p) = max(a, b) with p = (a >= b)
-                        bool pe, pf, ph_e, ph_f;
-                        e = __vibmax_s32(el + ext, hl + open, &pe);        // pe: extension (not open > ext)
-                        f = __vibmax_s32(Fp[k] + ext, Hp[k] + open, &pf);  // pf: extension
-                        h = __viaddmax_s32(diag, hb == rb[k] ? match : mismatch, cutoff);
-                        h = __vibmax_s32(h, e, &ph_e);                     // !ph_e: E strictly greater
-                        h = __vibmax_s32(h, f, &ph_f);                     // !ph_f: F strictly greater
-                        c = (pe ? (uint32_t)kStInsExt : 0u) | (pf ? (uint32_t)kStDelExt : 0u) |
-                            (!ph_f ? (uint32_t)kStDel : (!ph_e ? (uint32_t)kStIns : 0u));
-                    } else
-#endif
-                    {
-                        const int eo = sadd<WRAP>(hl, open, w16), ee = sadd<WRAP>(el, ext, w16);
-                        e = max(eo, ee);
-                        const int fe = sadd<WRAP>(Fp[k], ext, w16), fo = sadd<WRAP>(Hp[k], open, w16);
-                        f = max(fe, fo);
-                        h = max(sadd<WRAP>(diag, hb == rb[k] ? match : mismatch, w16), cutoff);
-                        c = (eo > ee ? 0u : (uint32_t)kStInsExt) | (fo > fe ? 0u : (uint32_t)kStDelExt);
-                        if (e > h) { c |= kStIns; h = e; }
-                        if (f > h) { c = (c & ~3u) | kStDel; h = f; }
-                    }
+                    const int eo = sadd<WRAP>(hl, open, w16, one), ee = sadd<WRAP>(el, ext, w16, one);
+                    const int e = max(eo, ee);
+                    const int fe = sadd<WRAP>(Fp[k], ext, w16, one), fo = sadd<WRAP>(Hp[k], open, w16, one);
+                    const int f = max(fe, fo);
+                    int h = sadd<WRAP>(diag, hb == rb[k] ? match : mismatch, w16, one);
+                    if (CUT) h = max(h, cutoff);
+                    uint32_t c = (eo > ee ? 0u : (uint32_t)kStInsExt) | (fo > fe ? 0u : (uint32_t)kStDelExt);
+                    if (e > h) { c |= kStIns; h = e; }
+                    if (f > h) { c = (c & ~3u) | kStDel; h = f; }
                     diag = Hp[k];
                     if (act) { Hp[k] = h; Fp[k] = f; }
                     hl = h;
                     el = e;
-                    code[k / 8] |= c << (4 * (k % 8));
+                    code[k / 8] = (k % 8 == 0) ? c : (uint32_t)sadd<WRAP>((int)(c << (4 * (k % 8))), (int)code[k / 8], false, one);
                     if (k == kc) hc = h;
                 }
                 hout = act ? hl : 0;               // a lane before its first row stands for row 0
@@ -333,8 +336,16 @@ __device__ void sw_one(const SwView& v, uint32_t idx, int lane, uint8_t* scr, ui
     __syncwarp();
 }
 
+// Resident blocks per SM the register allocation must allow: 5 for up to 6 columns per lane (102
+// registers), 4 up to 12 (128), 3 beyond (170).
+template <int K>
+constexpr int sw_min_blocks()
+{
+    return K <= 6 ? 5 : K <= 12 ? 4 : 3;
+}
+
 template <int K, bool WRAP>
-__global__ void __launch_bounds__(32 * kSwBlockWarps) sw_kernel(SwView v)
+__global__ void __launch_bounds__(32 * kSwBlockWarps, sw_min_blocks<K>()) sw_kernel(SwView v)
 {
     __shared__ uint32_t band[kSwBlockWarps][kSwBandWords];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -344,7 +355,11 @@ __global__ void __launch_bounds__(32 * kSwBlockWarps) sw_kernel(SwView v)
         if (lane == 0) q = atomicAdd(v.claim, 1u);
         q = __shfl_sync(kFull, q, 0);
         if (q >= v.n) break;
-        sw_one<K, WRAP>(v, v.order[q], lane, scr, band[wib]);
+        const uint32_t idx = v.order[q];
+        if (WRAP || sw_cutoff_can_bind(v, v.items[idx]))
+            sw_one<K, WRAP, true>(v, idx, lane, scr, band[wib]);
+        else
+            sw_one<K, WRAP, false>(v, idx, lane, scr, band[wib]);
     }
 }
 
@@ -723,6 +738,7 @@ phmm_status sw_launch(const SwPlan& p, const SwParams& prm, int variant, const S
         v.slot_off = b.slot_off;
         v.ops = b.slots;
         v.cigar_cap = p.cigar_cap;
+        v.one = 1;
         if (class_ms) SW_CK(cudaEventRecord(ev0, st));
         kSwKernels[c]<<<p.grid[c], 32 * kSwBlockWarps, 0, st>>>(v);
         SW_CK(cudaGetLastError());
