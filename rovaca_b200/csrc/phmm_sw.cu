@@ -39,13 +39,6 @@
 #include "phmm_sw.h"
 #include "phmm_types.h"
 
-// 1: the 32-bit classes add scores with integer multiply-adds by a unit factor the compiler cannot
-// see (the FMA pipe), leaving the ALU pipe the maxima, compares and selects; 0: plain adds.  Both
-// give the same results.
-#ifndef PHMM_SW_IMAD
-#define PHMM_SW_IMAD 1
-#endif
-
 namespace phmm {
 
 namespace {
@@ -68,15 +61,13 @@ struct SwView {
     const uint64_t* slot_off;    // per item: its CIGAR slot in `ops` (min(cap, nrow + ncol) ops)
     uint32_t* ops;
     uint32_t cigar_cap;
-    int one;                     // 1 (a value the compiler cannot fold, see PHMM_SW_IMAD)
 };
 
 // Score add: two's-complement 32-bit, wrapped to 16 bits in the wrap-around class when the
 // alignment runs the int16 kernel (w16; an int32 alignment in that class adds in 32 bits).
 template <bool WRAP>
-__device__ __forceinline__ int sadd(int a, int b, bool w16, int one)
+__device__ __forceinline__ int sadd(int a, int b, bool w16)
 {
-    if (!WRAP && PHMM_SW_IMAD) return (int)((unsigned)a * (unsigned)one + (unsigned)b);
     const int s = (int)((unsigned)a + (unsigned)b);
     return (WRAP && w16) ? (int)(short)s : s;
 }
@@ -122,7 +113,6 @@ __device__ void sw_one(const SwView& v, uint32_t idx, int lane, uint8_t* scr, ui
     }
     const bool i32 = sw_uses_int32(v.variant, it.hap_len, it.read_len, v.prm.match);
     const bool w16 = !i32;
-    const int one = v.one;
     const int match = i32 ? v.prm.match : (int)(short)v.prm.match;
     const int mismatch = i32 ? v.prm.mismatch : (int)(short)v.prm.mismatch;
     const int open = i32 ? v.prm.gap_open : (int)(short)v.prm.gap_open;
@@ -194,11 +184,11 @@ __device__ void sw_one(const SwView& v, uint32_t idx, int lane, uint8_t* scr, ui
                 int hc = 0;
 #pragma unroll
                 for (int k = 0; k < K; ++k) {
-                    const int eo = sadd<WRAP>(hl, open, w16, one), ee = sadd<WRAP>(el, ext, w16, one);
+                    const int eo = sadd<WRAP>(hl, open, w16), ee = sadd<WRAP>(el, ext, w16);
                     const int e = max(eo, ee);
-                    const int fe = sadd<WRAP>(Fp[k], ext, w16, one), fo = sadd<WRAP>(Hp[k], open, w16, one);
+                    const int fe = sadd<WRAP>(Fp[k], ext, w16), fo = sadd<WRAP>(Hp[k], open, w16);
                     const int f = max(fe, fo);
-                    int h = sadd<WRAP>(diag, hb == rb[k] ? match : mismatch, w16, one);
+                    int h = sadd<WRAP>(diag, hb == rb[k] ? match : mismatch, w16);
                     if (CUT) h = max(h, cutoff);
                     uint32_t c = (eo > ee ? 0u : (uint32_t)kStInsExt) | (fo > fe ? 0u : (uint32_t)kStDelExt);
                     if (e > h) { c |= kStIns; h = e; }
@@ -207,7 +197,7 @@ __device__ void sw_one(const SwView& v, uint32_t idx, int lane, uint8_t* scr, ui
                     if (act) { Hp[k] = h; Fp[k] = f; }
                     hl = h;
                     el = e;
-                    code[k / 8] = (k % 8 == 0) ? c : (uint32_t)sadd<WRAP>((int)(c << (4 * (k % 8))), (int)code[k / 8], false, one);
+                    code[k / 8] |= c << (4 * (k % 8));
                     if (k == kc) hc = h;
                 }
                 hout = act ? hl : 0;               // a lane before its first row stands for row 0
@@ -738,7 +728,6 @@ phmm_status sw_launch(const SwPlan& p, const SwParams& prm, int variant, const S
         v.slot_off = b.slot_off;
         v.ops = b.slots;
         v.cigar_cap = p.cigar_cap;
-        v.one = 1;
         if (class_ms) SW_CK(cudaEventRecord(ev0, st));
         kSwKernels[c]<<<p.grid[c], 32 * kSwBlockWarps, 0, st>>>(v);
         SW_CK(cudaGetLastError());
