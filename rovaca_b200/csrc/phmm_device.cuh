@@ -161,9 +161,12 @@ __device__ __forceinline__ void load_rows(LaneRows<T, K, PM>& L, const BatchView
 // row at column p; (dM, dI, dD): the same row at column p-1.  In PM_ALL pad rows share the lane's
 // gap parameters: their prior 0 keeps M = 0, their I stays 0 (the rows above are pad or boundary
 // rows with M = I = 0) and xx = 1 keeps D, so they still reproduce the boundary row.
-template <typename T, int K, int V, int PM>
+// FLUSH: flush every result below 2^-1022 to zero (FP64 steps whose inputs may be that small); the
+// FP32 path flushes in hardware either way.
+template <typename T, int K, int V, int PM, bool FLUSH = true>
 __device__ __forceinline__ void cells(LaneRows<T, K, PM>& L, uint32_t hc, T sM, T sI, T dM, T dI, T dD)
 {
+    auto fz = [](T x) { return FLUSH ? ftz(x) : x; };
     T diM = dM, diI = dI, diD = dD, upM = sM, upI = sI;
 #pragma unroll
     for (int k = 0; k < K; ++k) {
@@ -172,12 +175,12 @@ __device__ __forceinline__ void cells(LaneRows<T, K, PM>& L, uint32_t hc, T sM, 
         const T prior = codes_match(hc, L.rc[k], V) ? L.pa[k] : L.pb[k];
         T s;
         if (V == kInter)
-            s = ftz(rfma(diD, L.gm[r], ftz(rfma(diM, L.mm[r], ftz(rmul(diI, L.gm[r]))))));
+            s = fz(rfma(diD, L.gm[r], fz(rfma(diM, L.mm[r], fz(rmul(diI, L.gm[r]))))));
         else
-            s = ftz(rfma(diD, L.gm[r], ftz(rfma(diI, L.gm[r], ftz(rmul(diM, L.mm[r]))))));
-        const T nM = ftz(rmul(s, prior));
-        const T nI = ftz(rfma(upI, L.xx[k], ftz(rmul(upM, L.mx[r]))));
-        const T nD = ftz(rfma(oD, L.xx[k], ftz(rmul(oM, L.my[r]))));
+            s = fz(rfma(diD, L.gm[r], fz(rfma(diI, L.gm[r], fz(rmul(diM, L.mm[r]))))));
+        const T nM = fz(rmul(s, prior));
+        const T nI = fz(rfma(upI, L.xx[k], fz(rmul(upM, L.mx[r]))));
+        const T nD = fz(rfma(oD, L.xx[k], fz(rmul(oM, L.my[r]))));
         L.Mp[k] = nM;
         L.Ip[k] = nI;
         L.Dp[k] = nD;
@@ -187,6 +190,40 @@ __device__ __forceinline__ void cells(LaneRows<T, K, PM>& L, uint32_t hc, T sM, 
         upM = nM;
         upI = nI;
     }
+}
+
+// Smallest value every nonzero input of an FP64 step must reach for no result of that step to fall
+// below 2^-1022, so that the step may skip the flushes and still give the flushed results.  Every
+// nonzero probability of the tables is at least 2^-44 (the smallest, ph2pr(127) / 3, is 6.6e-14), all
+// values are >= 0, and a sum of non-negative terms is at least its largest term; the longest chain
+// of products in one step is the insertion recurrence down the lane's K rows (I(a) >= I(a-1) xx,
+// after M(a-1) = s prior and the product M mx), so every nonzero result is >= input x 2^(-44 (K+1)).
+// Expressed as the high word of that double (biased exponent 1023 - 1022 + 44 (K + 1)).
+#ifndef PHMM_F64_VOTE
+#define PHMM_F64_VOTE 1  // 0: every FP64 step flushes (no vote)
+#endif
+
+template <int K>
+__device__ __forceinline__ uint32_t flush_free_hi()
+{
+    return (uint32_t)(1 + 44 * (K + 1)) << 20;
+}
+
+// Whether every nonzero input of the lane's next step reaches flush_free_hi<K>(): its rows and the
+// diagonal values (dM, dI, dD) it holds; the values from the row above are the neighbour lane's rows,
+// checked by that lane.  Flushed values are 0 or normal, so a zero high word means the value is 0.
+template <int K, int PM>
+__device__ __forceinline__ bool rows_flush_free(const LaneRows<double, K, PM>& L, double dM, double dI, double dD)
+{
+    uint32_t m = min(min((uint32_t)__double2hiint(dM) - 1u, (uint32_t)__double2hiint(dI) - 1u),
+                     (uint32_t)__double2hiint(dD) - 1u);
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        m = min(m, (uint32_t)__double2hiint(L.Mp[k]) - 1u);
+        m = min(m, (uint32_t)__double2hiint(L.Ip[k]) - 1u);
+        m = min(m, (uint32_t)__double2hiint(L.Dp[k]) - 1u);
+    }
+    return m >= flush_free_hi<K>() - 1u;
 }
 
 struct SweepOut {
@@ -218,6 +255,7 @@ __device__ void sweep(LaneRows<T, K, PM>& L, const BatchView& b, const PassContr
     T D0 = T(0);
     T sumM = T(0), sumI = T(0);
     T dM = T(0), dI = T(0), dD = T(0);
+    bool flush_free = false;  // FP64: the current step's inputs are all 0 or above the bound
 
     const int steps = Tcols + kWarp;  // lane 31 reaches column Tcols (the end) at step Tcols + 31
 
@@ -225,7 +263,8 @@ __device__ void sweep(LaneRows<T, K, PM>& L, const BatchView& b, const PassContr
     auto boundary = [&]() {
         if (started) {
             if (!TO_SCR && lane == kWarp - 1) {
-                const T tot = ftz(radd(sumM, sumI));
+                // sums of flushed non-negative values are 0 or normal: no flush needed
+                const T tot = radd(sumM, sumI);
                 const uint64_t oi = so.out_base + (uint64_t)(cur - g_lo) * so.out_stride;
                 so.out[oi] = log10((double)tot) - Scale<T>::log10_initial();
             }
@@ -273,7 +312,13 @@ __device__ void sweep(LaneRows<T, K, PM>& L, const BatchView& b, const PassContr
             }
         }
         const uint32_t hc = codes[p];
-        cells<T, K, V, PM>(L, hc, sM, sI, dM, dI, dD);
+        // FP64: the flushes can only change a step whose inputs hold a value below the bound; the
+        // warp votes after every step (the scratch row read by stripes after the first is not checked)
+        constexpr bool kVote = PHMM_F64_VOTE && sizeof(T) == 8 && !FROM_SCR;
+        if (kVote && flush_free)
+            cells<T, K, V, PM, false>(L, hc, sM, sI, dM, dI, dD);
+        else
+            cells<T, K, V, PM, true>(L, hc, sM, sI, dM, dI, dD);
         dM = sM;
         dI = sI;
         dD = sD;
@@ -284,9 +329,10 @@ __device__ void sweep(LaneRows<T, K, PM>& L, const BatchView& b, const PassContr
                 scr[3 * p + 2] = L.Dp[K - 1];
             }
         } else {
-            sumM = ftz(radd(sumM, L.Mp[K - 1]));
-            sumI = ftz(radd(sumI, L.Ip[K - 1]));
+            sumM = radd(sumM, L.Mp[K - 1]);
+            sumI = radd(sumI, L.Ip[K - 1]);
         }
+        if constexpr (kVote) flush_free = __all_sync(0xffffffffu, rows_flush_free(L, dM, dI, dD));
     };
 
     for (int t0 = 0; t0 < steps; t0 += kChunkScalar) {
