@@ -737,14 +737,39 @@ phmm_status Engine::capture_graph(Slot& s, bool want_flags, const TileTable& til
     return PHMM_OK;
 }
 
-phmm_status Engine::upload(Slot& s, const Plan& plan, const phmm_batch& b, std::string& err, const uint8_t* mapq)
+bool Engine::upload_raw(Slot& s, const BatchScan& sc, const phmm_batch& b)
+{
+    if (!s.dev || sc.read_bases > s.cap.read_bases || sc.hap_bases > s.cap.hap_bases) return false;
+    cudaStream_t m = s.main;
+    const uint64_t rb = sc.read_bases;
+    cudaError_t e = cudaSuccess;
+    if (rb) {
+        e = cudaMemcpyAsync(s.d_rb, b.read_bases + sc.read_base0, rb, cudaMemcpyHostToDevice, m);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(s.d_rq, b.read_qual + sc.read_base0, rb, cudaMemcpyHostToDevice, m);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(s.d_ri, b.read_ins + sc.read_base0, rb, cudaMemcpyHostToDevice, m);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(s.d_rd, b.read_del + sc.read_base0, rb, cudaMemcpyHostToDevice, m);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(s.d_rc, b.read_gcp + sc.read_base0, rb, cudaMemcpyHostToDevice, m);
+    }
+    if (e == cudaSuccess && sc.hap_bases)
+        e = cudaMemcpyAsync(s.d_hb, b.hap_bases + sc.hap_base0, sc.hap_bases, cudaMemcpyHostToDevice, m);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return false;  // upload() copies them again
+    }
+    return true;
+}
+
+phmm_status Engine::upload(Slot& s, const Plan& plan, const phmm_batch& b, std::string& err, const uint8_t* mapq,
+                           bool raw_sent)
 {
     if (plan.region_api && plan.n_reads && !mapq) {
         err = "region-API batch without MAPQ";
         return PHMM_ERR_INVALID_ARGUMENT;
     }
+    const uint64_t grows = s.arena_grows;
     phmm_status st = ensure_capacity(s, plan, err);
     if (st != PHMM_OK) return st;
+    if (s.arena_grows != grows) raw_sent = false;  // a new arena: copies into the old one are gone
     PHMM_CK(cudaSetDevice(dev_));
     // stage descriptors + plan arrays in pinned memory, then copy
     char* p = s.pinned;
@@ -790,7 +815,7 @@ phmm_status Engine::upload(Slot& s, const Plan& plan, const phmm_batch& b, std::
         PHMM_CK(cudaMemcpyAsync(s.d_hap_flags, h_hap_flags, plan.hap_flags.size(), cudaMemcpyHostToDevice, m));
     if (!plan.items.empty())
         PHMM_CK(cudaMemcpyAsync(s.d_items, h_items, plan.items.size() * sizeof(WorkItem), cudaMemcpyHostToDevice, m));
-    const uint64_t rb = plan.read_bases;
+    const uint64_t rb = raw_sent ? 0 : plan.read_bases;
     if (rb) {
         PHMM_CK(cudaMemcpyAsync(s.d_rb, b.read_bases + plan.read_base0, rb, cudaMemcpyHostToDevice, m));
         PHMM_CK(cudaMemcpyAsync(s.d_rq, b.read_qual + plan.read_base0, rb, cudaMemcpyHostToDevice, m));
@@ -800,7 +825,7 @@ phmm_status Engine::upload(Slot& s, const Plan& plan, const phmm_batch& b, std::
             PHMM_CK(cudaMemcpyAsync(s.d_rc, b.read_gcp + plan.read_base0, rb, cudaMemcpyHostToDevice, m));
         }
     }
-    if (plan.hap_bases)
+    if (plan.hap_bases && !raw_sent)
         PHMM_CK(cudaMemcpyAsync(s.d_hb, b.hap_bases + plan.hap_base0, plan.hap_bases, cudaMemcpyHostToDevice, m));
 
     if (plan.region_api && plan.n_reads)
@@ -832,9 +857,9 @@ phmm_status Engine::run(Slot& s, const Plan& plan, bool want_flags, bool restore
 }
 
 phmm_status Engine::enqueue(Slot& s, const Plan& plan, const phmm_batch& b, bool want_flags, std::string& err,
-                            const uint8_t* mapq)
+                            const uint8_t* mapq, bool raw_sent)
 {
-    phmm_status st = upload(s, plan, b, err, mapq);
+    phmm_status st = upload(s, plan, b, err, mapq, raw_sent);
     if (st != PHMM_OK) return st;
     return run(s, plan, want_flags, false, err);
 }
@@ -934,13 +959,22 @@ phmm_status Engine::compute(const phmm_batch& b, double* out, uint8_t* pair_flag
     std::lock_guard<std::mutex> lk(mu_);
     Plan plan;
     const TileTable t = tiles();
-    phmm_status st = build_plan(b, limits_with(t), plan, err);
+    // validate, then let the bases and qualities travel while the host plans the batch
+    BatchScan sc;
+    phmm_status st = scan_batch(b, limits_with(t), sc, err);
     if (st != PHMM_OK) return st;
-    if (plan.out_total && !out) {
+    PHMM_CK(cudaSetDevice(dev_));
+    const bool raw_sent = b.n_regions > 0 && upload_raw(*default_slot_, sc, b);
+    st = build_plan(b, limits_with(t), plan, err);
+    if (st == PHMM_OK && plan.out_total && !out) {
         err = "out is null";
-        return PHMM_ERR_INVALID_ARGUMENT;
+        st = PHMM_ERR_INVALID_ARGUMENT;
     }
-    st = enqueue(*default_slot_, plan, b, pair_flags != nullptr, err);
+    if (st != PHMM_OK) {
+        if (raw_sent) cudaStreamSynchronize(default_slot_->main);  // the copies read the caller's buffers
+        return st;
+    }
+    st = enqueue(*default_slot_, plan, b, pair_flags != nullptr, err, nullptr, raw_sent);
     if (st != PHMM_OK) return st;
     st = finish(*default_slot_, plan, out, pair_flags, stats, err);
     if (stats) stats->host_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();

@@ -94,8 +94,10 @@ public:
     phmm_status make_slot(int id, Slot** out, std::string& err);
     void free_slot(Slot* s);
     // mapq: MAPQ per read, region-API plans only (their raw qualities are prepared on the device).
+    // raw_sent: the batch's bases and qualities were already copied to this arena (upload_raw) and it
+    // has not grown since; they are not copied again.
     phmm_status enqueue(Slot& s, const Plan& plan, const phmm_batch& b, bool want_flags, std::string& err,
-                        const uint8_t* mapq = nullptr);
+                        const uint8_t* mapq = nullptr, bool raw_sent = false);
     // Region-API plans: out receives the normalised matrices (kept reads first), keep the kept flag
     // of every read and n_kept the kept reads of every region.
     // Genotyping outputs (plans with events): gl [gl_total], best [events], allele_lk (optional).
@@ -106,7 +108,10 @@ public:
     // Upload only (descriptor, plan arrays, reads, haplotypes); then run the device pipeline, with
     // restore = true resetting the descriptor from its pristine device copy first (replays).
     phmm_status upload(Slot& s, const Plan& plan, const phmm_batch& b, std::string& err,
-                       const uint8_t* mapq = nullptr);
+                       const uint8_t* mapq = nullptr, bool raw_sent = false);
+    // Copies a validated batch's bases and qualities into the slot's arena when it already holds
+    // them (returns false, copying nothing, otherwise): the copies then overlap the host planning.
+    bool upload_raw(Slot& s, const BatchScan& sc, const phmm_batch& b);
     // Allocates the slot's arena for at least capacity c now (no-op if it already covers it).
     phmm_status reserve(Slot& s, const Capacity& c, std::string& err);
     phmm_status run(Slot& s, const Plan& plan, bool want_flags, bool restore, std::string& err);
