@@ -97,10 +97,13 @@ __device__ __forceinline__ void run_read(const BatchView& b, const ProbTables<T>
 // FP64 kernels with constant gap parameters and 7-8 rows per lane fit three warps per scheduler when
 // held to 168 registers (no spills at 8 rows, 16 bytes for the multi-stripe one); the others keep
 // what they need.
+#ifndef PHMM_F64_MIN_WARPS
+#define PHMM_F64_MIN_WARPS 12
+#endif
 template <int K, int PM>
 constexpr int min_blocks64()
 {
-    return PM == PM_ALL && K >= 7 ? 12 : 1;
+    return PM == PM_ALL && K >= 7 ? PHMM_F64_MIN_WARPS : 1;
 }
 
 template <int K, int V, int PM, bool MULTI>
