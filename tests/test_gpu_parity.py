@@ -81,6 +81,33 @@ def test_region_result_independent_of_batch(engine):
         assert np.array_equal(back[roffs[r]:roffs[r + 1]], full[offs[g]:offs[g + 1]], equal_nan=True)
 
 
+def test_bases_sent_early_then_arena_grows(oracle):
+    """phmm_compute_regions copies bases and qualities while it plans when the arena already holds
+    them; a batch with fewer bases but more pairs then grows the arena after those copies, which are
+    made again: results equal the oracle's either way, also with a fresh engine at each size."""
+    from rovaca_b200 import Engine, Region
+    from rovaca_b200.pairhmm import PackedBatch
+
+    rng = np.random.default_rng(8)
+    bases = lambda n: bytes(rng.choice(np.frombuffer(b"ACGT", np.uint8), n))
+    qual = lambda n: bytes(rng.integers(10, 41, n, dtype=np.uint8))
+    haps = [bases(300) for _ in range(30)]
+
+    def batch(n_reads, length):
+        reads = [bases(length) for _ in range(n_reads)]
+        gap = [bytes([45]) * length] * n_reads
+        return PackedBatch.from_regions([Region(haps, reads, [qual(length) for _ in reads], gap, gap,
+                                                [bytes([10]) * length] * n_reads)])
+
+    many_bases = batch(40, 250)   # 10,000 read bases, 1,200 pairs
+    many_pairs = batch(200, 30)   # 6,000 read bases (they fit), 6,000 pairs (the arena grows)
+    with Engine(device=0, autotune=False) as eng:
+        for pb in (many_bases, many_pairs, many_bases, many_pairs):
+            got, _, _ = eng.compute(pb)
+            want, _ = oracle.batch(pb)
+            assert np.max(np.abs(got - want)) <= EXACT
+
+
 def test_underflow_stress_region(engine, oracle):
     """Config-2 regime: most pairs fall below 1e-28 in FP32 and are recomputed in FP64."""
     pb = synth.config2(2, seed=21)
