@@ -138,6 +138,33 @@ def reference_gcups(batch, regions, threads: int) -> tuple[float, float]:
     return cells / dt / 1e9, dt
 
 
+# ---- ranks --------------------------------------------------------------------------------------
+
+def shard_seed(rank: int) -> int:
+    """Each rank computes its own 2,000-region batch of the benchmark's shape (regions are
+    independent: weak scaling, no data exchanged between ranks)."""
+    return 1 + rank
+
+
+def rank_reduce(dist, x: float, op: str = "max", device: str = "cpu") -> float:
+    """Max or sum of a per-rank number over all ranks (identity with one process).  Every rank calls
+    it the same number of times in the same order."""
+    if dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def weak_scaling_value(dist, cells_per_step: float, steps: int, device_ms: float, device: str = "cpu") -> tuple:
+    """(GCUPS of the whole job, ms per step): all ranks' cells over the slowest rank's device time."""
+    dev_ms = rank_reduce(dist, device_ms, "max", device)
+    total = rank_reduce(dist, float(cells_per_step), "sum", device) * steps
+    return total / (dev_ms / 1e3) / 1e9, dev_ms / steps
+
+
 def run_reference(args, rank: int, world: int) -> None:
     if rank != 0:
         return
@@ -435,9 +462,10 @@ def run_ours(args, rank: int, world: int, dist) -> None:
 
     device = int(os.environ.get("LOCAL_RANK", 0))
     torch.cuda.set_device(device)
-    batch = synth.config1(seed=1 + rank)
+    batch = synth.config1(seed=shard_seed(rank))
     cells = batch.cells()
     engine = Engine(device=device, use_cuda_graph=not args.no_graph)
+    dev = f"cuda:{device}"
 
     def barrier():
         if dist is not None:
@@ -445,18 +473,7 @@ def run_ours(args, rank: int, world: int, dist) -> None:
         torch.cuda.synchronize()
 
     def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{device}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    def sum_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{device}")
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        return float(t.item())
+        return rank_reduce(dist, x, "max", dev)
 
     # device-resident batched throughput
     res = engine.resident(batch, want_flags=True)
@@ -465,10 +482,8 @@ def run_ours(args, rank: int, world: int, dist) -> None:
     with ClockSampler(device) as clk:
         st = res.run(args.steps)
         barrier()
-    dev_ms = max_over_ranks(st["device_ms"])
-    ms_per_step = dev_ms / args.steps
-    total_cells = sum_over_ranks(float(cells)) * args.steps
-    value = total_cells / (dev_ms / 1e3) / 1e9
+    value, ms_per_step = weak_scaling_value(dist, float(cells), args.steps, st["device_ms"], dev)
+    total_cells = value * ms_per_step * args.steps * 1e6
     fp32_pass_ms = max_over_ranks(st["fp32_ms"])
     out, flags = res.results()
     # every kernel class alone, after the timed region (CUDA events around each launch)
