@@ -21,10 +21,6 @@
 #include "phmm_regionk.h"
 #include "phmm_tables.h"
 
-#ifndef PHMM_STREAM_PRIORITY
-#define PHMM_STREAM_PRIORITY 1  // 0: all class streams at the default priority
-#endif
-
 namespace phmm {
 
 #define PHMM_CK(call)                                                                    \
@@ -433,25 +429,7 @@ phmm_status Engine::make_slot(int id, Slot** out, std::string& err)
     s->id = id;
     auto cleanup = [&]() { free_slot(s); };
     cudaError_t e = cudaStreamCreateWithFlags(&s->main, cudaStreamNonBlocking);
-    // Class streams by priority: FP64 classes first (once their FP32 sources are done they take the
-    // SMs that free up), then FP32 classes of longer reads, whose FP64 reruns go to the longer FP64
-    // classes: those sources finish early and their reruns overlap the rest of the FP32 pass.
-    int least = 0, greatest = 0;
-    if (e == cudaSuccess) e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
-    for (int c = 0; c < kNumClasses && e == cudaSuccess; ++c) {
-        int prio = least;
-        if (PHMM_STREAM_PRIORITY && greatest < least) {
-            const int levels = least - greatest;  // e.g. 5: priorities 0 (least) .. -5
-            if (c >= kClasses32) {
-                prio = greatest;
-            } else {
-                const int shape = c % kShapes32;  // 0..7 single stripes of KH 1..8, 8..12 multi-stripe
-                const int rank = shape >= 8 ? 4 : std::max(0, shape - 4);  // KH 1-5: 0, 6: 1, 7: 2, 8: 3, multi: 4
-                prio = least - std::min(levels - 1, rank);
-            }
-        }
-        e = cudaStreamCreateWithPriority(&s->side[c], cudaStreamNonBlocking, prio);
-    }
+    for (int c = 0; c < kNumClasses && e == cudaSuccess; ++c) e = cudaStreamCreateWithFlags(&s->side[c], cudaStreamNonBlocking);
     for (int c = 0; c < kNumClasses && e == cudaSuccess; ++c) e = cudaEventCreateWithFlags(&s->ev_side[c], cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreate(&s->ev_t0);
