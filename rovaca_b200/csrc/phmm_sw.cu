@@ -33,6 +33,7 @@
 #include <mutex>
 #include <numeric>
 #include <string>
+#include <thread>
 #include <type_traits>
 #include <vector>
 
@@ -604,6 +605,27 @@ namespace {
 // Scratch of one class launch is held under this bound by launching fewer resident warps.
 constexpr uint64_t kSwScratchCap = 6ull << 30;
 
+// Copy into the pinned staging buffer; large copies are split over host threads (one thread copies
+// at a fraction of the memory bandwidth, and the bases of a genome-scale batch are ~100 MB).
+void staged_copy(void* dst, const void* src, size_t bytes)
+{
+    constexpr size_t kPerThread = 8u << 20;
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const unsigned nt = (unsigned)std::min<size_t>({hw, 8u, bytes / kPerThread});
+    if (nt <= 1) {
+        std::memcpy(dst, src, bytes);
+        return;
+    }
+    const size_t part = (bytes + nt - 1) / nt;
+    std::vector<std::thread> pool;
+    for (unsigned t = 1; t < nt; ++t) {
+        const size_t o = (size_t)t * part;
+        if (o < bytes) pool.emplace_back([=] { std::memcpy((char*)dst + o, (const char*)src + o, std::min(part, bytes - o)); });
+    }
+    std::memcpy(dst, src, std::min(part, bytes));
+    for (auto& th : pool) th.join();
+}
+
 phmm_status check_items(uint32_t n, const SwItem* items, uint64_t hap_bytes, uint64_t read_bytes, std::string& err)
 {
     for (uint32_t q = 0; q < n; ++q) {
@@ -895,11 +917,11 @@ phmm_status SwAligner::align(const SwParams& prm, int variant, uint32_t n, const
     if (st != PHMM_OK) return st;
     uint8_t* h = (uint8_t*)pinned_;
     uint8_t* d = (uint8_t*)arena_;
-    std::memcpy(h + L.items, items, sizeof(SwItem) * (size_t)n);
+    staged_copy(h + L.items, items, sizeof(SwItem) * (size_t)n);
     std::memcpy(h + L.order, p.order.data(), 4ull * n);
     std::memcpy(h + L.slot_off, p.slot_off.data(), 8ull * n);
-    if (hap_bytes) std::memcpy(h + L.hap, hap, hap_bytes);
-    if (read_bytes) std::memcpy(h + L.read, read, read_bytes);
+    if (hap_bytes) staged_copy(h + L.hap, hap, hap_bytes);
+    if (read_bytes) staged_copy(h + L.read, read, read_bytes);
     SW_CK(cudaMemcpyAsync(d, h, L.in_bytes(), cudaMemcpyHostToDevice, stream_));
     SW_CK(cudaEventRecord(ev_[0], stream_));
     st = sw_launch(p, prm, variant, L.bufs(d), stream_, ev_[0], ev_[1], nullptr, err);
