@@ -161,10 +161,6 @@ __device__ __forceinline__ void load_rows(LaneRows<T, K, PM>& L, const BatchView
 // row at column p; (dM, dI, dD): the same row at column p-1.  In PM_ALL pad rows share the lane's
 // gap parameters: their prior 0 keeps M = 0, their I stays 0 (the rows above are pad or boundary
 // rows with M = I = 0) and xx = 1 keeps D, so they still reproduce the boundary row.
-#ifndef PHMM_SCALAR_PHASED
-#define PHMM_SCALAR_PHASED 0  // 1: a step's independent work first, then the insertion chain
-#endif
-
 // FLUSH: flush every result below 2^-1022 to zero (FP64 steps whose inputs may be that small); the
 // FP32 path flushes in hardware either way.
 template <typename T, int K, int V, int PM, bool FLUSH = true>
@@ -172,36 +168,6 @@ __device__ __forceinline__ void cells(LaneRows<T, K, PM>& L, uint32_t hc, T sM, 
 {
     auto fz = [](T x) { return FLUSH ? ftz(x) : x; };
     T diM = dM, diI = dI, diD = dD, upM = sM, upI = sI;
-#if PHMM_SCALAR_PHASED
-    // every row's M, D and M x mx first (they depend on the previous column only), then the
-    // insertion recurrence down the rows; the same operations and roundings as the loop below
-    T t[K];
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-        const int r = PM == PM_ROW ? k : 0;
-        const T oM = L.Mp[k], oI = L.Ip[k], oD = L.Dp[k];
-        const T prior = codes_match(hc, L.rc[k], V) ? L.pa[k] : L.pb[k];
-        T s;
-        if (V == kInter)
-            s = fz(rfma(diD, L.gm[r], fz(rfma(diM, L.mm[r], fz(rmul(diI, L.gm[r]))))));
-        else
-            s = fz(rfma(diD, L.gm[r], fz(rfma(diI, L.gm[r], fz(rmul(diM, L.mm[r]))))));
-        const T nM = fz(rmul(s, prior));
-        t[k] = fz(rmul(upM, L.mx[r]));
-        L.Dp[k] = fz(rfma(oD, L.xx[k], fz(rmul(oM, L.my[r]))));
-        L.Mp[k] = nM;
-        diM = oM;
-        diI = oI;
-        diD = oD;
-        upM = nM;
-    }
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-        upI = fz(rfma(upI, L.xx[k], t[k]));
-        L.Ip[k] = upI;
-    }
-    return;
-#endif
 #pragma unroll
     for (int k = 0; k < K; ++k) {
         const int r = PM == PM_ROW ? k : 0;

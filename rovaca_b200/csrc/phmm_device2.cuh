@@ -30,10 +30,6 @@ namespace phmm {
 
 constexpr int kLanesPerRead = 16;
 
-#ifndef PHMM_F32_PHASED
-#define PHMM_F32_PHASED 0  // 1: a step's independent work first, then the insertion chain
-#endif
-
 __device__ __forceinline__ float2 f2(float x, float y) { return make_float2(x, y); }
 __device__ __forceinline__ float2 rmul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
 __device__ __forceinline__ float2 rfma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
@@ -124,37 +120,6 @@ template <int KH, int V, int PM>
 __device__ __forceinline__ void cells2(LaneRows2<KH, PM>& L, uint32_t hcA, uint32_t hcB, float2 upM, float2 upI,
                                        float2 dgM, float2 dgI, float2 dgD)
 {
-#if PHMM_F32_PHASED
-    // M and D of every row depend only on the previous column, and so does the product M x mx that
-    // feeds the next row's insertion: all of them first, then the insertion recurrence down the rows
-    // (the only chain within a step).  The operations and their roundings are those of the loop below.
-    float2 t[KH];
-#pragma unroll
-    for (int a = 0; a < KH; ++a) {
-        const int r = PM == PM_ROW ? a : 0;
-        const float2 oM = L.Mp[a], oI = L.Ip[a], oD = L.Dp[a];
-        const float2 prior = f2(codes_match(hcA, L.rcA[a], V) ? L.pa[a].x : L.pb[a].x,
-                                codes_match(hcB, L.rcB[a], V) ? L.pa[a].y : L.pb[a].y);
-        float2 s;
-        if (V == kInter)
-            s = rfma2(dgD, L.gm[r], rfma2(dgM, L.mm[r], rmul2(dgI, L.gm[r])));
-        else
-            s = rfma2(dgD, L.gm[r], rfma2(dgI, L.gm[r], rmul2(dgM, L.mm[r])));
-        const float2 nM = rmul2(s, prior);
-        t[a] = rmul2(upM, L.mx[r]);  // row a's insertion term: M of the row above x mx
-        L.Dp[a] = rfma2(oD, L.xx[a], rmul2(oM, L.my[r]));
-        L.Mp[a] = nM;
-        dgM = oM;
-        dgI = oI;
-        dgD = oD;
-        upM = nM;
-    }
-#pragma unroll
-    for (int a = 0; a < KH; ++a) {
-        upI = rfma2(upI, L.xx[a], t[a]);
-        L.Ip[a] = upI;
-    }
-#else
 #pragma unroll
     for (int a = 0; a < KH; ++a) {
         const int r = PM == PM_ROW ? a : 0;
@@ -178,7 +143,6 @@ __device__ __forceinline__ void cells2(LaneRows2<KH, PM>& L, uint32_t hcA, uint3
         upM = nM;
         upI = nI;
     }
-#endif
 }
 
 // Sweep one stripe of both reads of the warp over the column stream of haplotypes [g_lo, g_hi).
