@@ -701,16 +701,21 @@ phmm_status sw_plan(int device, const SwParams& prm, int variant, uint32_t n, co
     }
     p.begin[0] = 0;
     for (int c = 0; c < kSwClasses; ++c) p.begin[c + 1] = p.begin[c] + counts[c];
+    // one counting sort: by class, then most cells first in buckets of 4096 cells (the claim order
+    // only balances the persistent warps' load, so buckets are as good as an exact order)
+    constexpr uint32_t kBuckets = 1024;
+    auto key = [&](uint32_t q) {
+        const uint64_t b = std::min<uint64_t>(kBuckets - 1, ((uint64_t)nrow[q] * ncol[q]) >> 12);
+        return (uint32_t)cls[q] * kBuckets + (kBuckets - 1 - (uint32_t)b);
+    };
+    std::vector<uint32_t> start((size_t)kSwClasses * kBuckets + 1, 0);
+    for (uint32_t q = 0; q < n; ++q) ++start[key(q) + 1];
+    for (size_t k = 1; k < start.size(); ++k) start[k] += start[k - 1];
     p.order.assign(n, 0);
-    uint32_t fill[kSwClasses];
-    std::copy(p.begin, p.begin + kSwClasses, fill);
-    for (uint32_t q = 0; q < n; ++q) p.order[fill[cls[q]]++] = q;
+    for (uint32_t q = 0; q < n; ++q) p.order[start[key(q)]++] = q;
     p.scratch = 0;
     for (int c = 0; c < kSwClasses; ++c) {
         auto first = p.order.begin() + p.begin[c], lastp = p.order.begin() + p.begin[c + 1];
-        std::stable_sort(first, lastp, [&](uint32_t x, uint32_t y) {
-            return (uint64_t)nrow[x] * ncol[x] > (uint64_t)nrow[y] * ncol[y];
-        });
         uint64_t stride = 256;
         for (auto it = first; it != lastp; ++it) {
             if (std::max(nrow[*it], ncol[*it]) >= (uint32_t)kSwMaxSeq) continue;  // refused: no scratch
