@@ -87,3 +87,23 @@ def test_random_pairs_bit_exact_against_reference_build(oracle, ref):
         got = ref.inter(clean[g:g + w], raw=True)
         want = [oracle.raw_f32(*p, kernel=INTER) for p in clean[g:g + w]]
         assert np.array_equal(np.float32(got), np.float32(want))
+
+
+def test_table_probabilities_bound_used_by_flush_free_fp64_steps(oracle):
+    """The FP64 pass skips its flushes in steps whose inputs are all 0 or at least
+    2^(-1022 + 44 (K + 1)); that bound rests on every nonzero probability the cell update multiplies
+    by being at least 2^-44 (and none negative).  Checked over the whole tables."""
+    import ctypes as C
+
+    lib = oracle.lib
+    lib.oracle_ph2pr_f64.restype = C.c_double
+    lib.oracle_ph2pr_f64.argtypes = [C.c_int]
+    lib.oracle_mm_f64.restype = C.c_double
+    lib.oracle_mm_f64.argtypes = [C.c_int, C.c_int]
+    vals = []
+    for q in range(128):
+        d = lib.oracle_ph2pr_f64(q)
+        vals += [d, d / 3.0, 1.0 - d]                  # gap and base-quality terms, mismatch, match, gapm
+    vals += [lib.oracle_mm_f64(i, j) for i in range(128) for j in range(128)]
+    assert min(vals) >= 0.0
+    assert min(v for v in vals if v > 0.0) >= 2.0 ** -44
