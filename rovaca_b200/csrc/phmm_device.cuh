@@ -203,10 +203,14 @@ __device__ __forceinline__ void cells(LaneRows<T, K, PM>& L, uint32_t hc, T sM, 
 #define PHMM_F64_VOTE 1  // 0: every FP64 step flushes (no vote)
 #endif
 
-template <int K>
+#ifndef PHMM_F64_VOTE_EVERY
+#define PHMM_F64_VOTE_EVERY 1  // steps per vote: the bound then covers that many steps
+#endif
+
+template <int K, int STEPS = PHMM_F64_VOTE_EVERY>
 __device__ __forceinline__ uint32_t flush_free_hi()
 {
-    return (uint32_t)(1 + 44 * (K + 1)) << 20;
+    return (uint32_t)(1 + 44 * STEPS * (K + 1)) << 20;
 }
 
 // Whether every nonzero input of the lane's next step reaches flush_free_hi<K>(): its rows and the
@@ -332,7 +336,9 @@ __device__ void sweep(LaneRows<T, K, PM>& L, const BatchView& b, const PassContr
             sumM = radd(sumM, L.Mp[K - 1]);
             sumI = radd(sumI, L.Ip[K - 1]);
         }
-        if constexpr (kVote) flush_free = __all_sync(0xffffffffu, rows_flush_free(L, dM, dI, dD));
+        if constexpr (kVote)
+            if (PHMM_F64_VOTE_EVERY == 1 || t % PHMM_F64_VOTE_EVERY == PHMM_F64_VOTE_EVERY - 1)
+                flush_free = __all_sync(0xffffffffu, rows_flush_free(L, dM, dI, dD));
     };
 
     for (int t0 = 0; t0 < steps; t0 += kChunkScalar) {
