@@ -203,8 +203,12 @@ __device__ __forceinline__ void cells(LaneRows<T, K, PM>& L, uint32_t hc, T sM, 
 #define PHMM_F64_VOTE 1  // 0: every FP64 step flushes (no vote)
 #endif
 
+// Steps per vote: the bound then covers that many steps (an input of the second step is at least
+// the first step's inputs x 2^(-44 (K+1))).  Measured on B200: 2 cut the FP64 pass of the
+// underflow-stress shape from 56 to 50 ms against 1; 3 gained nothing more, and at 4 the bound
+// (2^562 for K = 8) is above most values, so nearly every step flushes.
 #ifndef PHMM_F64_VOTE_EVERY
-#define PHMM_F64_VOTE_EVERY 1  // steps per vote: the bound then covers that many steps
+#define PHMM_F64_VOTE_EVERY 2
 #endif
 
 template <int K, int STEPS = PHMM_F64_VOTE_EVERY>
@@ -317,7 +321,8 @@ __device__ void sweep(LaneRows<T, K, PM>& L, const BatchView& b, const PassContr
         }
         const uint32_t hc = codes[p];
         // FP64: the flushes can only change a step whose inputs hold a value below the bound; the
-        // warp votes after every step (the scratch row read by stripes after the first is not checked)
+        // warp votes every PHMM_F64_VOTE_EVERY steps (the scratch row read by stripes after the first
+        // is not checked)
         constexpr bool kVote = PHMM_F64_VOTE && sizeof(T) == 8 && !FROM_SCR;
         if (kVote && flush_free)
             cells<T, K, V, PM, false>(L, hc, sM, sI, dM, dI, dD);
