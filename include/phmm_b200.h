@@ -205,7 +205,7 @@ PHMM_API void phmm_host_normalize_filter(const double* lk_hap_read, uint32_t n_h
  *   mode 0: pairs without 'N' whose read has constant insertion/deletion/gap qualities,
  *   mode 1: other pairs without 'N', mode 2: pairs with 'N';
  *   bucket b = ceil(read length / 32), 1..24;
- *   shape: rows_per_lane KH (16 lanes per read hold 32 * KH rows) in one stripe (KH >= b), or
+ *   shape: rows_per_lane KH (32 lanes hold 32 * KH rows of each read) in one stripe (KH >= b), or
  *          multi_stripe with 4 <= KH < b, the read running as ceil(length / (32 * KH)) stripes.
  * FP32 kernel class = mode * 13 + (multi_stripe ? 4 + KH : KH - 1); FP64 recompute class =
  * mode * 9 + (length > 256 ? 8 : b - 1), the mode of the FP32 class that ran the pair.  Results do

@@ -319,7 +319,7 @@ __device__ void sweep(LaneRows<T, K, PM>& L, const BatchView& b, const PassContr
                 sD = D0;
             }
         }
-        const uint32_t hc = codes[p];
+        const uint32_t hc = codes[p] & kCodeMatchMask;
         // FP64: the flushes can only change a step whose inputs hold a value below the bound; the
         // warp votes every PHMM_F64_VOTE_EVERY steps (the scratch row read by stripes after the first
         // is not checked)

@@ -1,20 +1,26 @@
-// FP32 wavefront with packed FP32 arithmetic (sm_100a __ffma2_rn / __fmul2_rn).
+// FP32 wavefront with packed FP32 arithmetic (sm_100a __ffma2_rn / __fmul2_rn / __fadd2_rn).
 //
 // Arithmetic per cell is exactly the reference's (see phmm_device.cuh for the operation order and
 // the reference lines); a packed instruction applies it to two cells with the same per-component
 // rounding as the scalar intrinsics, so results stay bit-identical.
 //
-// Mapping.  16 lanes per read, two reads per warp (lanes 0-15 and 16-31), both streaming the same
-// run of haplotype columns.  Lane l of a group holds 2*KH rows of its read as two halves of KH rows
-// that behave as two "virtual lanes" v = 2l (half A) and v = 2l + 1 (half B): virtual lane v works
-// on stream column p = t - v at step t, so half B runs one column behind half A.  Row a of half A and
-// row a of half B are then independent within a step (half B's top row reads half A's bottom row of
-// the previous step), so each pair of rows is one float2: the M, I and D updates of both halves are
-// single packed instructions and the I recurrence down the rows runs for both halves at once.
-// Virtual lane 31 (lane 15, half B) holds the read's last row; rows are padded at the top and pad
-// rows reproduce the boundary row exactly (prior 0 keeps M = 0, I stays 0 because the rows above
-// have M = I = 0, and xx = 1 keeps D = C/H).  Reads longer than 256 rows run as stripes linked
-// through a per-group scratch row, as in the scalar path.
+// Mapping.  A warp sweeps two reads of one region, X in the .x components and Y in the .y
+// components, through the same run of haplotype columns.  Lane l holds rows l*KH .. l*KH+KH-1 of
+// both reads' stripes and works on stream column p = t - l at step t, so the two components of every
+// float2 meet the same haplotype base: one packed instruction updates row a of X and row a of Y.
+// The three values of a lane's bottom rows go to lane l+1 by shuffle; lane 31 holds both reads'
+// last rows and sums them per haplotype.  Rows are padded at the top, each read by its own count,
+// and pad rows reproduce the boundary row exactly (prior 0 keeps M = 0, I stays 0 because the rows
+// above have M = I = 0, and xx = 1 keeps D = C/H).  Reads longer than one stripe run as stripes
+// linked through a per-warp scratch row of float2 values.
+//
+// Match prior.  A cell's prior depends only on its read row and the class of its haplotype base, and
+// a lane's rows are fixed for a stripe, so each lane tabulates its rows' priors for the five base
+// classes (kTabClasses; the class rides in the haplotype code word) in shared memory once per
+// stripe.  A step then loads the priors of two row pairs with one 128-bit shared-memory load at its
+// column's class, where a compare and a select per cell would otherwise take the integer pipe.
+// Inter reads with bytes outside A/C/G/T can equal a haplotype byte of class 4; a warp holding such
+// a row runs every step on the checked path, which corrects the class-4 priors by comparing bytes.
 //
 // Gap parameters: PM_ALL when a read's insertion, deletion and gap-continuation qualities are each
 // constant along it (the region API without a PCR model, and the benchmark data), PM_ROW otherwise.
@@ -28,23 +34,49 @@
 
 namespace phmm {
 
-constexpr int kLanesPerRead = 16;
-
 __device__ __forceinline__ float2 f2(float x, float y) { return make_float2(x, y); }
 __device__ __forceinline__ float2 rmul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
 __device__ __forceinline__ float2 rfma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 radd2(float2 a, float2 b) { return __fadd2_rn(a, b); }
 
-__device__ __forceinline__ float shfl_up16(float v) { return __shfl_up_sync(0xffffffffu, v, 1, kLanesPerRead); }
-__device__ __forceinline__ int shfl_idx(int v, int src) { return __shfl_sync(0xffffffffu, v, src); }
+__device__ __forceinline__ float2 shfl_up2(float2 v)
+{
+    return f2(__shfl_up_sync(0xffffffffu, v.x, 1), __shfl_up_sync(0xffffffffu, v.y, 1));
+}
+
+// Prior table of one warp: [class][quad][lane] float4, a quad holding the (X, Y) priors of two row
+// pairs.  A class plane spans tab_quads 512-byte quads; the code word's class field (class <<
+// kTabShift, a multiple of 2 KB) becomes the plane offset by a right shift of tab_shift.
+template <int KH>
+__host__ __device__ constexpr int tab_quads()
+{
+    return KH > 4 ? 4 : KH > 2 ? 2 : 1;
+}
+template <int KH>
+__host__ __device__ constexpr int tab_shift()
+{
+    return KH > 4 ? 0 : KH > 2 ? 1 : 2;
+}
+template <int KH>
+__host__ __device__ constexpr int tab_floats4()
+{
+    return kTabClasses * tab_quads<KH>() * kWarp;
+}
 
 template <int KH, int PM>
 struct LaneRows2 {
     static constexpr int NR = PM == PM_ROW ? KH : 1;
-    float2 Mp[KH], Ip[KH], Dp[KH];  // (half A, half B) values at each half's previous column
-    float2 pa[KH], pb[KH], xx[KH];
-    uint32_t rcA[KH], rcB[KH];
+    float2 Mp[KH], Ip[KH], Dp[KH];  // (X, Y) values at the previous column
+    float2 xx[KH];
     float2 mm[NR], gm[NR], mx[NR], my[NR];
-    uint32_t padA, padB;            // bit a: row a of the half is a pad row
+    uint32_t padX, padY;            // bit a: row a of the read is a pad row
+};
+
+// The two reads of a work item (Y may be absent: R = 0, every row a pad row).
+struct ReadPair {
+    uint64_t roff[2];
+    int R[2];
+    int pad[2];                     // pad rows above each read (all stripes together)
 };
 
 struct RowParams {
@@ -79,238 +111,298 @@ __device__ __forceinline__ RowParams row_params(const BatchView& b, const ProbTa
     return r;
 }
 
-// Loads this lane's rows of the stripe starting at padded row `first` (`pad` rows precede row 1).
-template <int KH, int V, int PM>
-__device__ __forceinline__ void load_rows2(LaneRows2<KH, PM>& L, const BatchView& b, const ProbTables<float>& tb,
-                                           uint64_t roff, int R, int first, int pad, int l)
+template <int V>
+__device__ __forceinline__ float class_prior(const RowParams& r, uint32_t cls)
 {
-    L.padA = 0;
-    L.padB = 0;
-    if (PM == PM_ALL) {
-        // constant along the read: any real row gives them (pad rows ignore them)
-        const RowParams r0 = row_params<V>(b, tb, roff, R, R > 0 ? 0 : -1);
-        L.mm[0] = f2(r0.mm, r0.mm);
-        L.gm[0] = f2(r0.gm, r0.gm);
-        L.mx[0] = f2(r0.mx, r0.mx);
-        L.my[0] = f2(r0.my, r0.my);
-    }
-#pragma unroll
-    for (int a = 0; a < KH; ++a) {
-        const RowParams A = row_params<V>(b, tb, roff, R, first + (2 * l) * KH + a - pad);
-        const RowParams B = row_params<V>(b, tb, roff, R, first + (2 * l + 1) * KH + a - pad);
-        L.pa[a] = f2(A.pa, B.pa);
-        L.pb[a] = f2(A.pb, B.pb);
-        L.xx[a] = f2(A.xx, B.xx);
-        L.rcA[a] = A.rc;
-        L.rcB[a] = B.rc;
-        if (PM == PM_ROW) {
-            L.mm[a] = f2(A.mm, B.mm);
-            L.gm[a] = f2(A.gm, B.gm);
-            L.mx[a] = f2(A.mx, B.mx);
-            L.my[a] = f2(A.my, B.my);
-        }
-        L.padA |= (A.pad ? 1u : 0u) << a;
-        L.padB |= (B.pad ? 1u : 0u) << a;
-    }
+    return class_matches(cls, r.rc, V) ? r.pa : r.pb;  // pad rows: pa = pb = 0
 }
 
-// All 2*KH rows of the lane for one step.  (upM, upI): row above each half's first row at that
-// half's column; (dgM, dgI, dgD): the same rows one column to the left.
+// Loads this lane's rows of the stripe starting at padded row `first` and writes their prior table.
+// Returns true when one of the lane's rows is an inter row with a byte outside A/C/G/T.
 template <int KH, int V, int PM>
-__device__ __forceinline__ void cells2(LaneRows2<KH, PM>& L, uint32_t hcA, uint32_t hcB, float2 upM, float2 upI,
+__device__ __forceinline__ bool load_rows2(LaneRows2<KH, PM>& L, float4* tab, const BatchView& b,
+                                           const ProbTables<float>& tb, const ReadPair& rp, int first, int lane)
+{
+    constexpr int QJ = tab_quads<KH>();
+    L.padX = 0;
+    L.padY = 0;
+    if (PM == PM_ALL) {
+        // constant along the read: any real row gives them (pad rows ignore them)
+        const RowParams x0 = row_params<V>(b, tb, rp.roff[0], rp.R[0], rp.R[0] > 0 ? 0 : -1);
+        const RowParams y0 = row_params<V>(b, tb, rp.roff[1], rp.R[1], rp.R[1] > 0 ? 0 : -1);
+        L.mm[0] = f2(x0.mm, y0.mm);
+        L.gm[0] = f2(x0.gm, y0.gm);
+        L.mx[0] = f2(x0.mx, y0.mx);
+        L.my[0] = f2(x0.my, y0.my);
+    }
+    bool exotic = false;
+    float2* t2 = reinterpret_cast<float2*>(tab);
+#pragma unroll
+    for (int a = 0; a < KH; ++a) {
+        const int row = first + lane * KH + a;
+        const RowParams X = row_params<V>(b, tb, rp.roff[0], rp.R[0], row - rp.pad[0]);
+        const RowParams Y = row_params<V>(b, tb, rp.roff[1], rp.R[1], row - rp.pad[1]);
+        L.xx[a] = f2(X.xx, Y.xx);
+        if (PM == PM_ROW) {
+            L.mm[a] = f2(X.mm, Y.mm);
+            L.gm[a] = f2(X.gm, Y.gm);
+            L.mx[a] = f2(X.mx, Y.mx);
+            L.my[a] = f2(X.my, Y.my);
+        }
+        L.padX |= (X.pad ? 1u : 0u) << a;
+        L.padY |= (Y.pad ? 1u : 0u) << a;
+        if (V == kInter)
+            exotic |= (!X.pad && base_class((uint8_t)X.rc) == 4u) || (!Y.pad && base_class((uint8_t)Y.rc) == 4u);
+#pragma unroll
+        for (int c = 0; c < kTabClasses; ++c)
+            t2[((c * QJ + a / 2) * kWarp + lane) * 2 + (a & 1)] =
+                f2(class_prior<V>(X, (uint32_t)c), class_prior<V>(Y, (uint32_t)c));
+    }
+    if (KH & 1) {
+#pragma unroll
+        for (int c = 0; c < kTabClasses; ++c) t2[((c * QJ + KH / 2) * kWarp + lane) * 2 + 1] = f2(0.f, 0.f);
+    }
+    return exotic;
+}
+
+// Load the next step's priors during the current step (build-time setting): shortens the step of
+// a warp that runs alone on its scheduler, at the cost of KH register pairs.  Measured on B200 with
+// 12 warps per SM for KH >= 4: one region per call 140 instead of 124 GCUPS on the device, the
+// 2,000-region batch 2279 instead of 2361 GCUPS; off by default, the batch being the target.
+#ifndef PHMM_PRIOR_PREFETCH
+#define PHMM_PRIOR_PREFETCH 0
+#endif
+
+template <int V, int PM, int KH>
+__device__ __forceinline__ float2 diag_sum(const LaneRows2<KH, PM>& L, int r, float2 dgM, float2 dgI, float2 dgD)
+{
+    if (V == kInter) return rfma2(dgD, L.gm[r], rfma2(dgM, L.mm[r], rmul2(dgI, L.gm[r])));
+    return rfma2(dgD, L.gm[r], rfma2(dgI, L.gm[r], rmul2(dgM, L.mm[r])));
+}
+
+// All KH row pairs of the lane for one step.  (upM, upI): the row above the lane's first row at this
+// column; (dgM, dgI, dgD): the same row one column to the left; pr: the rows' priors.
+// Order: row a+1's diagonal sum first (it reads row a's old values), then row a's D, M and I, so
+// every old value is dead before its row's new value is written and each row's state keeps its
+// registers from step to step.  Measured on B200 over the 2,000-region benchmark batch: 1.7% faster
+// than updating M, I and D of a row together, with the same results.
+template <int KH, int V, int PM>
+__device__ __forceinline__ void cells2(LaneRows2<KH, PM>& L, const float2 (&pr)[KH], float2 upM, float2 upI,
                                        float2 dgM, float2 dgI, float2 dgD)
 {
+    float2 s = diag_sum<V, PM>(L, 0, dgM, dgI, dgD);
 #pragma unroll
     for (int a = 0; a < KH; ++a) {
         const int r = PM == PM_ROW ? a : 0;
         const float2 oM = L.Mp[a], oI = L.Ip[a], oD = L.Dp[a];
-        const float2 prior = f2(codes_match(hcA, L.rcA[a], V) ? L.pa[a].x : L.pb[a].x,
-                                codes_match(hcB, L.rcB[a], V) ? L.pa[a].y : L.pb[a].y);
-        float2 s;
-        if (V == kInter)
-            s = rfma2(dgD, L.gm[r], rfma2(dgM, L.mm[r], rmul2(dgI, L.gm[r])));
-        else
-            s = rfma2(dgD, L.gm[r], rfma2(dgI, L.gm[r], rmul2(dgM, L.mm[r])));
-        const float2 nM = rmul2(s, prior);
+        float2 sn = s;
+        if (a + 1 < KH) sn = diag_sum<V, PM>(L, PM == PM_ROW ? a + 1 : 0, oM, oI, oD);
+        L.Dp[a] = rfma2(oD, L.xx[a], rmul2(oM, L.my[r]));
+        const float2 nM = rmul2(s, pr[a]);
         const float2 nI = rfma2(upI, L.xx[a], rmul2(upM, L.mx[r]));
-        const float2 nD = rfma2(oD, L.xx[a], rmul2(oM, L.my[r]));
         L.Mp[a] = nM;
         L.Ip[a] = nI;
-        L.Dp[a] = nD;
-        dgM = oM;
-        dgI = oI;
-        dgD = oD;
         upM = nM;
         upI = nI;
+        s = sn;
     }
 }
 
-// Sweep one stripe of both reads of the warp over the column stream of haplotypes [g_lo, g_hi).
-//   FROM_SCR: the row above virtual lane 0 comes from the group's scratch row (stripe > 0).
-//   TO_SCR:   virtual lane 31's bottom row goes to the scratch row (not the last stripe).
-// so.read is this group's read (UINT32_MAX: no read; the group computes pad rows only and writes
-// nothing).  aboveA / aboveB: the row above half A's / half B's first row is row 0 or a pad row.
+// Output side of a sweep: the two reads' likelihood columns and FP64 rerun lists.
+struct SweepOut2 {
+    double* out;
+    uint8_t* pair_flags;
+    uint64_t out_base[2];           // output index of the stream's first haplotype, per read
+    uint32_t out_stride;            // output index step between consecutive haplotypes
+    uint32_t read[2];               // global read indices (kNoRead: none)
+    ClassDesc* cd64[2];             // FP64 class of each read (its rerun segment)
+};
+
+// Sweep one stripe of both reads over the column stream of haplotypes [g_lo, g_hi).
+//   FROM_SCR: the row above lane 0 comes from the warp's scratch row (stripe > 0).
+//   TO_SCR:   lane 31's bottom rows go to the scratch row (not the last stripe).
+// first: the stripe's first padded row.  aboveX / aboveY: the row above the lane's first row is
+// row 0 or a pad row, per read.  exotic: the warp holds an inter row with a byte outside A/C/G/T
+// (every step runs the checked path).
 template <int KH, int V, int PM, bool FROM_SCR, bool TO_SCR>
-__device__ void sweep2(LaneRows2<KH, PM>& L, const BatchView& b, const PassControl& pc, const SweepOut& so,
-                       uint32_t g_lo, uint32_t g_hi, float* scr, int lane, bool aboveA)
+__device__ void sweep2(LaneRows2<KH, PM>& L, const float4* tab, const BatchView& b, const ProbTables<float>& tb,
+                       const PassControl& pc, const SweepOut2& so, const ReadPair& rp, int first, uint32_t g_lo,
+                       uint32_t g_hi, float2* scr, int lane, bool aboveX, bool aboveY, bool exotic)
 {
-    const int l = lane & (kLanesPerRead - 1);
-    const bool writer = (l == kLanesPerRead - 1) && so.read != 0xffffffffu;
+    constexpr int QJ = tab_quads<KH>();
     const uint64_t s0 = b.hap_off[g_lo];
     const int Tcols = (int)(b.hap_off[g_hi] - s0);
     const uint32_t* codes = (V == kInter ? b.codes_inter : b.codes_intra) + kCodePad + s0;
+    const char* tab_lane = reinterpret_cast<const char*>(tab) + lane * (int)sizeof(float4);
     const float C = Scale<float>::initial();
+    const bool writer = lane == kWarp - 1;
 
-    // cursors of the two virtual lanes (B trails A by one column)
-    uint32_t curA = g_lo, curB = g_lo;
-    int nbA = 0, nbB = 0;
-    bool startedB = false;
-    float D0A = 0.f, D0B = 0.f;
-    float sumM = 0.f, sumI = 0.f;
-    float dM = 0.f, dI = 0.f, dD = 0.f;  // row above half A's top row, one column left (from the shuffle)
-    float eM = 0.f, eI = 0.f, eD = 0.f;  // half A's bottom row two columns left: half B's diagonal
-    uint32_t hcPrev = 0u;
+    // Per-lane stream cursor: cur = haplotype being processed, nb = stream column of the next
+    // boundary (first column of the next haplotype, or the end of the stream).
+    uint32_t cur = g_lo;
+    int nb = 0;
+    bool started = false;
+    float D0 = 0.f;
+    float2 sumM = f2(0.f, 0.f), sumI = f2(0.f, 0.f);
+    float2 dM = f2(0.f, 0.f), dI = f2(0.f, 0.f), dD = f2(0.f, 0.f);
 
-    const int steps = Tcols + 2 * kLanesPerRead;
+    const int steps = Tcols + kWarp;  // lane 31 reaches column Tcols (the end) at step Tcols + 31
 
-    auto boundaryA = [&]() {
-        if (curA < g_hi) {
-            const int H = (int)(b.hap_off[curA + 1] - b.hap_off[curA]);
-            nbA += H;
-            D0A = C / (float)H;
-#pragma unroll
-            for (int a = 0; a < KH; ++a) {
-                L.Mp[a].x = 0.f;
-                L.Ip[a].x = 0.f;
-                L.Dp[a].x = ((L.padA >> a) & 1u) ? D0A : 0.f;
-            }
-            dM = 0.f;
-            dI = 0.f;
-            dD = aboveA ? D0A : 0.f;
-            ++curA;
-        } else {
-            nbA = 0x7fffffff;
-        }
-    };
-    // Writer lane: the open run of consecutive underflowed haplotypes (first haplotype, its output).
-    uint32_t run_lo = 0xffffffffu;
-    uint64_t run_oi = 0;
-    auto close_run = [&](uint32_t end) {
-        if (run_lo == 0xffffffffu) return;
-        const unsigned int slot = atomicAdd(&pc.cd->rerun_count, 1u);
-        if (slot < pc.cd->rerun_cap) {
+    // Writer lane: per read, the open run of consecutive underflowed haplotypes (first haplotype,
+    // its output index).
+    uint32_t run_lo[2] = {0xffffffffu, 0xffffffffu};
+    uint64_t run_oi[2] = {0, 0};
+    auto close_run = [&](int k, uint32_t end) {
+        if (run_lo[k] == 0xffffffffu) return;
+        ClassDesc* cd = so.cd64[k];
+        const unsigned int slot = atomicAdd(&cd->rerun_count, 1u);
+        if (slot < cd->rerun_cap) {
             RerunEntry e;
-            e.out_idx = run_oi;
-            e.read = so.read;
-            e.hap = run_lo;
-            e.n_haps = end - run_lo;
+            e.out_idx = run_oi[k];
+            e.read = so.read[k];
+            e.hap = run_lo[k];
+            e.n_haps = end - run_lo[k];
             e.out_stride = so.out_stride;
-            pc.rerun[pc.cd->rerun_off + slot] = e;
-            atomicAdd(&pc.cd->rerun_pairs, end - run_lo);
+            pc.rerun[cd->rerun_off + slot] = e;
+            atomicAdd(&cd->rerun_pairs, end - run_lo[k]);
         } else {
             atomicOr(pc.status, kStatusRerunOverflow);
         }
-        run_lo = 0xffffffffu;
+        run_lo[k] = 0xffffffffu;
     };
-    auto boundaryB = [&]() {
-        if (startedB) {
-            if (writer && !TO_SCR) {
-                const float tot = radd(sumM, sumI);
-                const uint64_t oi = so.out_base + (uint64_t)(curB - g_lo) * so.out_stride;
-                so.out[oi] = log10((double)tot) - Scale<float>::log10_initial();
-                const bool under = (double)tot < (double)1e-28f;
-                if (under) {
-                    if (run_lo == 0xffffffffu) {
-                        run_lo = curB;
-                        run_oi = oi;
-                    }
-                } else {
-                    close_run(curB);
-                }
-                if (curB + 1 == g_hi) close_run(g_hi);
-                if (so.pair_flags) so.pair_flags[oi] = under ? 1 : 0;
+    auto emit = [&](int k, float tot) {
+        if (so.read[k] == kNoRead) return;
+        const uint64_t oi = so.out_base[k] + (uint64_t)(cur - g_lo) * so.out_stride;
+        so.out[oi] = log10((double)tot) - Scale<float>::log10_initial();
+        const bool under = (double)tot < (double)1e-28f;
+        if (under) {
+            if (run_lo[k] == 0xffffffffu) {
+                run_lo[k] = cur;
+                run_oi[k] = oi;
             }
-            ++curB;
+        } else {
+            close_run(k, cur);
         }
-        startedB = true;
-        if (curB < g_hi) {
-            const int H = (int)(b.hap_off[curB + 1] - b.hap_off[curB]);
-            nbB += H;
-            D0B = C / (float)H;
+        if (cur + 1 == g_hi) close_run(k, g_hi);
+        if (so.pair_flags) so.pair_flags[oi] = under ? 1 : 0;
+    };
+
+    // Run by a lane whose column p has reached nb, after the step's shuffles.
+    auto boundary = [&]() {
+        if (started) {
+            if (!TO_SCR && writer) {
+                // sums of flushed non-negative values are 0 or normal: no flush needed
+                emit(0, __fadd_rn(sumM.x, sumI.x));
+                emit(1, __fadd_rn(sumM.y, sumI.y));
+            }
+            ++cur;
+        }
+        started = true;
+        if (cur < g_hi) {
+            const int H = (int)(b.hap_off[cur + 1] - b.hap_off[cur]);
+            nb += H;
+            D0 = C / (float)H;
+            // Left edge of the new haplotype: column 0 is zero in every real row; pad rows stand
+            // for the boundary row 0, whose D is C/H in every column.
 #pragma unroll
             for (int a = 0; a < KH; ++a) {
-                L.Mp[a].y = 0.f;
-                L.Ip[a].y = 0.f;
-                L.Dp[a].y = ((L.padB >> a) & 1u) ? D0B : 0.f;
+                L.Mp[a] = f2(0.f, 0.f);
+                L.Ip[a] = f2(0.f, 0.f);
+                L.Dp[a] = f2(((L.padX >> a) & 1u) ? D0 : 0.f, ((L.padY >> a) & 1u) ? D0 : 0.f);
             }
-            // half B's diagonal at its first column is half A's bottom row at column -1: half A
-            // reset it one step earlier, so eM/eI/eD already hold the boundary values.
-            sumM = 0.f;
-            sumI = 0.f;
+            dM = f2(0.f, 0.f);
+            dI = f2(0.f, 0.f);
+            dD = f2(aboveX ? D0 : 0.f, aboveY ? D0 : 0.f);
+            sumM = f2(0.f, 0.f);
+            sumI = f2(0.f, 0.f);
         } else {
-            nbB = 0x7fffffff;
+            nb = 0x7fffffff;
         }
     };
 
-    auto step = [&](int t, bool check) {
-        const int pA = t - 2 * l;
-        const int pB = pA - 1;
-        // Half B's up input is half A's bottom row at B's column, computed in the previous step.
-        // It is read before half A's boundary reset: when A starts a new haplotype at this step,
-        // B is still on the last column of the previous one.
-        const float aM = L.Mp[KH - 1].x, aI = L.Ip[KH - 1].x;
-        float sM = shfl_up16(L.Mp[KH - 1].y);
-        float sI = shfl_up16(L.Ip[KH - 1].y);
-        float sD = shfl_up16(L.Dp[KH - 1].y);
-        if (check) {
-            if (pA == nbA) boundaryA();
-            if (pB == nbB) boundaryB();
-        }
-        if (l == 0) {
-            if (FROM_SCR) {
-                const bool ok = pA >= 0 && pA < Tcols;
-                sM = ok ? scr[3 * pA + 0] : 0.f;
-                sI = ok ? scr[3 * pA + 1] : 0.f;
-                sD = ok ? scr[3 * pA + 2] : 0.f;
-            } else {
-                sM = 0.f;
-                sI = 0.f;
-                sD = D0A;
+    // The priors of a column: its code word's class selects the plane of the lane's table.
+    auto load_priors = [&](int p, float2(&dst)[KH]) -> uint32_t {
+        // p lies in [-31, Tcols + 32]: the guard words around the stream cover it
+        const uint32_t w = codes[p];
+        const char* tp = tab_lane + ((w & kTabMask) >> tab_shift<KH>());
+#pragma unroll
+        for (int j = 0; j < QJ; ++j) {
+            if (2 * j < KH) {
+                const float4 q = *reinterpret_cast<const float4*>(tp + j * kWarp * (int)sizeof(float4));
+                dst[2 * j] = f2(q.x, q.y);
+                if (2 * j + 1 < KH) dst[2 * j + 1] = f2(q.z, q.w);
             }
         }
-        const uint32_t hcA = codes[pA];
-        const uint32_t hcB = hcPrev;
-        hcPrev = hcA;
-        // half B's inputs: half A's bottom row at B's column and one column to the left.  The value
-        // kept for B's next diagonal is taken after A's reset: if A started a haplotype here, B
-        // starts it one step later and its diagonal there is the boundary value.
-        const float2 upM = f2(sM, aM);
-        const float2 upI = f2(sI, aI);
-        const float2 dgM = f2(dM, eM), dgI = f2(dI, eI), dgD = f2(dD, eD);
-        eM = L.Mp[KH - 1].x;
-        eI = L.Ip[KH - 1].x;
-        eD = L.Dp[KH - 1].x;
-        dM = sM;
-        dI = sI;
-        dD = sD;
-        cells2<KH, V, PM>(L, hcA, hcB, upM, upI, dgM, dgI, dgD);
+        return w;
+    };
+#if PHMM_PRIOR_PREFETCH
+    float2 prn[KH];
+    uint32_t wn = load_priors(-lane, prn);
+#endif
+
+    auto step = [&](int t, bool check) {
+        const int p = t - lane;
+        float2 uM = shfl_up2(L.Mp[KH - 1]);
+        float2 uI = shfl_up2(L.Ip[KH - 1]);
+        float2 uD = shfl_up2(L.Dp[KH - 1]);
+        if (check && p == nb) boundary();
+        if (lane == 0) {
+            if (FROM_SCR) {
+                const bool ok = p >= 0 && p < Tcols;
+                uM = ok ? scr[3 * p + 0] : f2(0.f, 0.f);
+                uI = ok ? scr[3 * p + 1] : f2(0.f, 0.f);
+                uD = ok ? scr[3 * p + 2] : f2(0.f, 0.f);
+            } else {
+                uM = f2(0.f, 0.f);
+                uI = f2(0.f, 0.f);
+                uD = f2(D0, D0);
+            }
+        }
+        float2 pr[KH];
+#if PHMM_PRIOR_PREFETCH
+        const uint32_t w = wn;
+#pragma unroll
+        for (int a = 0; a < KH; ++a) pr[a] = prn[a];
+        wn = load_priors(p + 1, prn);
+#else
+        const uint32_t w = load_priors(p, pr);
+#endif
+        if (V == kInter && check && exotic && (w & kTabMask) == (4u << kTabShift)) {
+            // class 4 holds the mismatch prior for every row; a row whose byte equals this
+            // haplotype byte takes the match prior (the raw byte compare of the inter variant)
+            const uint32_t hb = w & kCodeMatchMask;
+#pragma unroll
+            for (int a = 0; a < KH; ++a) {
+                const int row = first + lane * KH + a;
+                const int iX = row - rp.pad[0], iY = row - rp.pad[1];
+                if (iX >= 0 && iX < rp.R[0] && b.read_bases[rp.roff[0] + iX] == hb)
+                    pr[a].x = tb.pmat[b.read_q[rp.roff[0] + iX] & 127];
+                if (iY >= 0 && iY < rp.R[1] && b.read_bases[rp.roff[1] + iY] == hb)
+                    pr[a].y = tb.pmat[b.read_q[rp.roff[1] + iY] & 127];
+            }
+        }
+        cells2<KH, V, PM>(L, pr, uM, uI, dM, dI, dD);
+        dM = uM;
+        dI = uI;
+        dD = uD;
         if (TO_SCR) {
-            if (l == kLanesPerRead - 1 && pB >= 0 && pB < Tcols) {
-                scr[3 * pB + 0] = L.Mp[KH - 1].y;
-                scr[3 * pB + 1] = L.Ip[KH - 1].y;
-                scr[3 * pB + 2] = L.Dp[KH - 1].y;
+            if (writer && p >= 0 && p < Tcols) {
+                scr[3 * p + 0] = L.Mp[KH - 1];
+                scr[3 * p + 1] = L.Ip[KH - 1];
+                scr[3 * p + 2] = L.Dp[KH - 1];
             }
         } else {
-            sumM = radd(sumM, L.Mp[KH - 1].y);
-            sumI = radd(sumI, L.Ip[KH - 1].y);
+            sumM = radd2(sumM, L.Mp[KH - 1]);
+            sumI = radd2(sumI, L.Ip[KH - 1]);
         }
     };
 
     for (int t0 = 0; t0 < steps; t0 += kChunk) {
-        // Virtual lanes cover columns [t0-31, t0+kChunk-1] in this chunk; virtual lane 31 (lane 15,
-        // half B) trails, so its next boundary is the first one at or after t0-31.
-        const int nbLast = shfl_idx(nbB, kLanesPerRead - 1);
-        if (nbLast >= t0 + kChunk && t0 + kChunk <= steps) {
+        // Lanes cover stream columns [t0-31, t0+kChunk-1] in this chunk.  Lane 31 trails, so its
+        // next boundary is the first boundary at or after t0-31: past the chunk means no lane meets
+        // a boundary and the chunk needs no per-step check.
+        const int nb31 = __shfl_sync(0xffffffffu, nb, kWarp - 1);
+        if (!exotic && nb31 >= t0 + kChunk && t0 + kChunk <= steps) {
 #pragma unroll
             for (int u = 0; u < kChunk; ++u) step(t0 + u, false);
         } else {

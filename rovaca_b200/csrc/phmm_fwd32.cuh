@@ -11,90 +11,103 @@
 
 namespace phmm {
 
-// Two reads per warp (one per 16-lane group) against a run of haplotypes.  The stripe holds
-// 32 * KH rows; MULTI runs `stripes` of them top to bottom, linked through the group's scratch row.
+// Two reads per warp (X and Y, the two components of every float2) against a run of haplotypes.
+// The stripe holds 32 * KH rows; MULTI runs `stripes` of them top to bottom, linked through the
+// warp's scratch row.
 template <int KH, int V, int PM, bool MULTI>
 __device__ __forceinline__ void run_pair2(const BatchView& b, const ProbTables<float>& tb, const PassControl& pc,
-                                          const SweepOut& so, uint32_t g_lo, uint32_t g_hi, int lane, int stripes,
-                                          float* scr)
+                                          const SweepOut2& so, uint32_t g_lo, uint32_t g_hi, int lane, int stripes,
+                                          float2* scr, float4* tab)
 {
-    constexpr int SR = 2 * kLanesPerRead * KH;  // rows per stripe (32 virtual lanes x KH)
-    const int l = lane & (kLanesPerRead - 1);
+    constexpr int SR = kWarp * KH;  // rows per stripe
     LaneRows2<KH, PM> L;
-    uint64_t roff = 0;
-    int R = 0;
-    if (so.read != kNoRead) {
-        roff = b.read_off[so.read];
-        R = (int)(b.read_off[so.read + 1] - roff);
-    }
+    ReadPair rp;
+    bool bad = false;
     const int S = MULTI ? stripes : 1;
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        rp.roff[k] = 0;
+        rp.R[k] = 0;
+        if (so.read[k] != kNoRead) {
+            rp.roff[k] = b.read_off[so.read[k]];
+            rp.R[k] = (int)(b.read_off[so.read[k] + 1] - rp.roff[k]);
+            bad |= rp.R[k] <= 0;
+        }
+        bad |= rp.R[k] > SR * S;
+        rp.pad[k] = SR * S - rp.R[k];
+    }
     const int Tcols = (int)(b.hap_off[g_hi] - b.hap_off[g_lo]);
-    // Both groups run the sweep together (full-warp shuffles), so a planning error in either skips
-    // the item for both; its pairs stay NaN and the status word reports it.
-    const bool bad = (so.read != kNoRead && R <= 0) || R > SR * S || (MULTI && (S < 2 || Tcols > (int)pc.scratch_cols));
-    if (__any_sync(0xffffffffu, bad)) {
+    // A planning error skips the item; its pairs stay NaN and the status word reports it.
+    bad |= so.read[0] == kNoRead || (MULTI && (S < 2 || Tcols > (int)pc.scratch_cols));
+    if (bad) {
         if (lane == 0) atomicOr(pc.status, kStatusBadItem);
         return;
     }
-    // underflowed pairs go to the FP64 class of this mode and this read's length
-    PassControl pr = pc;
-    pr.cd = pc.cd64 + class64_for_len(mode32(V, PM), (uint64_t)R);
-    const int pad = SR * S - R;
+    const bool aboveX = lane * KH <= rp.pad[0], aboveY = lane * KH <= rp.pad[1];
     if (!MULTI) {
-        load_rows2<KH, V, PM>(L, b, tb, roff, R, 0, pad, l);
-        sweep2<KH, V, PM, false, false>(L, b, pr, so, g_lo, g_hi, scr, lane, 2 * l * KH <= pad);
+        const bool exotic = __any_sync(0xffffffffu, load_rows2<KH, V, PM>(L, tab, b, tb, rp, 0, lane));
+        sweep2<KH, V, PM, false, false>(L, tab, b, tb, pc, so, rp, 0, g_lo, g_hi, scr, lane, aboveX, aboveY, exotic);
     } else {
         for (int s = 0; s < S; ++s) {
-            load_rows2<KH, V, PM>(L, b, tb, roff, R, s * SR, pad, l);
-            const bool aboveA = (s == 0) && (2 * l * KH <= pad);
+            const bool exotic = __any_sync(0xffffffffu, load_rows2<KH, V, PM>(L, tab, b, tb, rp, s * SR, lane));
+            const bool aX = s == 0 && aboveX, aY = s == 0 && aboveY;
             if (s == 0)
-                sweep2<KH, V, PM, false, true>(L, b, pr, so, g_lo, g_hi, scr, lane, aboveA);
+                sweep2<KH, V, PM, false, true>(L, tab, b, tb, pc, so, rp, 0, g_lo, g_hi, scr, lane, aX, aY, exotic);
             else if (s == S - 1)
-                sweep2<KH, V, PM, true, false>(L, b, pr, so, g_lo, g_hi, scr, lane, aboveA);
+                sweep2<KH, V, PM, true, false>(L, tab, b, tb, pc, so, rp, s * SR, g_lo, g_hi, scr, lane, aX, aY,
+                                               exotic);
             else
-                sweep2<KH, V, PM, true, true>(L, b, pr, so, g_lo, g_hi, scr, lane, aboveA);
-            __syncwarp();  // lane 15's scratch row is read by lane 0 of the group in the next stripe
+                sweep2<KH, V, PM, true, true>(L, tab, b, tb, pc, so, rp, s * SR, g_lo, g_hi, scr, lane, aX, aY,
+                                              exotic);
+            __syncwarp();  // lane 31's scratch row is read by lane 0 in the next stripe
         }
     }
 }
 
-// Resident warps per SM the compiler is asked to allow for the wide shapes (KH >= 6), whose natural
-// register count (170-230 per thread) leaves two warps per scheduler: each scheduler's sub-partition
-// holds 16K registers, so 168 registers per thread are the most that fit three warps.  Measured on
-// B200 over the 2,000-region batch: 12 warps per SM (a few bytes of spills at KH 7-8) take the FP32
-// pass from 242 to 235 ms.  A build-time setting (1 leaves the compiler free).
-#ifndef PHMM_WIDE_MIN_WARPS
-#define PHMM_WIDE_MIN_WARPS 12
+// Resident warps per SM the compiler is asked to allow, one byte per KH (KH = 1 in the low byte).
+// Each scheduler's sub-partition holds 16K registers: 168 registers per thread fit three warps, 128
+// fit four; left free, the compiler spends registers on loading the priors of a whole chunk of
+// steps early.  A build-time setting (1 leaves the compiler free).
+#ifndef PHMM_F32_MIN_WARPS
+#define PHMM_F32_MIN_WARPS 0x10101010100c0101ull
 #endif
 template <int KH>
-constexpr int min_blocks32()
+__host__ __device__ constexpr int min_blocks32()
 {
-    return KH >= 6 ? PHMM_WIDE_MIN_WARPS : 1;
+    return (int)(((unsigned long long)(PHMM_F32_MIN_WARPS) >> (8 * (KH - 1))) & 0xffu);
 }
 
 template <int KH, int V, int PM, bool MULTI>
 __global__ void __launch_bounds__(kFwdBlock, min_blocks32<KH>()) fwd_f32_kernel(BatchView b, ProbTables<float> tb,
                                                                                  PassControl pc)
 {
+    __shared__ float4 tab[tab_floats4<KH>()];
     const int lane = threadIdx.x & (kWarp - 1);
-    const int group = lane / kLanesPerRead;
     const unsigned int warp_id = (blockIdx.x * blockDim.x + threadIdx.x) / kWarp;
-    float* scr = MULTI ? (float*)pc.scratch + ((size_t)warp_id * 2 + group) * pc.scratch_cols * 3 : nullptr;
+    float2* scr = MULTI ? (float2*)pc.scratch + (size_t)warp_id * pc.scratch_cols * 3 : nullptr;
     const unsigned int n = pc.cd->n_items;
     const WorkItem* items = pc.items + pc.cd->item_off;
+    const int mode = mode32(V, PM);
     for (;;) {
         const unsigned int idx = claim(&pc.cd->claim32, lane);
         if (idx >= n) break;
         const WorkItem it = items[idx];
         const RegionDesc rg = b.regions[it.region];
-        SweepOut so;
+        SweepOut2 so;
         so.out = b.out;
         so.pair_flags = b.pair_flags;
-        so.read = it.read[group];
-        so.out_base = rg.out_off + (uint64_t)it.hap_lo * rg.n_reads + (so.read - rg.read_begin);
         so.out_stride = rg.n_reads;
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            so.read[k] = it.read[k];
+            const uint32_t r = it.read[k] == kNoRead ? rg.read_begin : it.read[k];
+            so.out_base[k] = rg.out_off + (uint64_t)it.hap_lo * rg.n_reads + (r - rg.read_begin);
+            // underflowed pairs go to the FP64 class of this mode and the read's length
+            const uint64_t R = it.read[k] == kNoRead ? 1 : b.read_off[r + 1] - b.read_off[r];
+            so.cd64[k] = pc.cd64 + class64_for_len(mode, R);
+        }
         run_pair2<KH, V, PM, MULTI>(b, tb, pc, so, rg.hap_begin + it.hap_lo, rg.hap_begin + it.hap_hi, lane,
-                                    it.stripes, scr);
+                                    it.stripes, scr, tab);
     }
 }
 

@@ -24,8 +24,8 @@ __global__ void prep_codes_kernel(const BatchDesc* __restrict__ desc, const uint
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
         const uint8_t b = hap_bases[i];
-        codes_inter[kCodePad + i] = match_code(b, kInter);
-        codes_intra[kCodePad + i] = match_code(b, kIntra);
+        codes_inter[kCodePad + i] = hap_code(b, kInter);
+        codes_intra[kCodePad + i] = hap_code(b, kIntra);
     }
     // guard codes on both sides of the stream: match nothing
     if (blockIdx.x == 0 && threadIdx.x < kCodePad) {

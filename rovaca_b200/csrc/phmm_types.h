@@ -27,7 +27,7 @@ enum Variant : int { kInter = 0, kIntra = 1 };
 constexpr int kLenBuckets = 24;
 PHMM_HD inline int len_bucket(uint64_t R) { return (int)((R + kWarp - 1) / kWarp); }
 
-// FP32 kernel classes (packed path: 16 lanes per read, two reads per warp).  A class is a mode
+// FP32 kernel classes (packed path: two reads per warp, one per float2 component).  A class is a mode
 //   0: inter, gap qualities constant along the read;  1: inter, per-row;  2: intra (pairs with 'N')
 // and a tile shape: KH row pairs per lane in one stripe of 32*KH rows (KH = 1..8), or stripes of
 // 32*KH rows linked through per-warp scratch rows (KH = 4..8).  Which shape a read-length bucket
@@ -72,7 +72,7 @@ struct RegionDesc {               // 32 bytes
 };
 constexpr uint32_t kRegionApi = 1u;
 
-// FP32 work item: two reads of one region (one per 16-lane group; read[1] may be kNoRead) against a
+// FP32 work item: two reads of one region (the two float2 components; read[1] may be kNoRead) against a
 // run of the region's haplotypes.
 constexpr uint32_t kNoRead = 0xffffffffu;
 struct WorkItem {                 // 20 bytes
@@ -219,6 +219,34 @@ PHMM_HD inline uint32_t match_code(uint8_t b, int variant)
 PHMM_HD inline bool codes_match(uint32_t hc, uint32_t rc, int variant)
 {
     return variant == kInter ? hc == rc : (hc & rc) != 0u;
+}
+
+// Haplotype code words of the code streams: the match code in bits 0-7 (kCodeMatchMask; the intra
+// code of N is 0xF there, which matches every read code as 0xffffffff does) and the base's prior
+// class in bits 11-13 for the packed FP32 kernels' prior tables: A, C, G, T are classes 0-3; class 4
+// is N in the intra variant and every other byte in the inter variant; letters in A's intra class
+// are class 0 there.  Guard words (0) are class 0 and match nothing.
+constexpr uint32_t kCodeMatchMask = 0xffu;
+constexpr int kTabShift = 11;
+constexpr uint32_t kTabMask = 7u << kTabShift;
+constexpr int kTabClasses = 5;
+PHMM_HD inline uint32_t base_class(uint8_t b)
+{
+    return b == 'A' ? 0u : b == 'C' ? 1u : b == 'G' ? 2u : b == 'T' ? 3u : 4u;
+}
+PHMM_HD inline uint32_t hap_code(uint8_t b, int variant)
+{
+    if (variant == kInter) return (uint32_t)b | (base_class(b) << kTabShift);
+    const uint32_t c = base_class(b);
+    if (c < 4u) return match_code(b, kIntra) | (c << kTabShift);
+    return b == 'N' ? (0xfu | (4u << kTabShift)) : 1u;  // other letters: A's class
+}
+// The match code that a prior class stands for when a read row is tested against it (class 4 of
+// the inter variant stands for a byte outside A/C/G/T: it matches no A/C/G/T row).
+PHMM_HD inline bool class_matches(uint32_t cls, uint32_t rc, int variant)
+{
+    if (variant == kInter) return cls < 4u && rc == (cls == 0u ? 'A' : cls == 1u ? 'C' : cls == 2u ? 'G' : 'T');
+    return ((cls < 4u ? 1u << cls : 0xfu) & rc) != 0u;
 }
 
 }  // namespace phmm
