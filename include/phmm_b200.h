@@ -69,7 +69,10 @@ typedef struct phmm_config {
                                   process; later engines reuse its table); 0: default shapes */
     int32_t reserved0;
     uint64_t hbm_budget_bytes; /* serving-loop admission budget for resident region data; 0 = 40 GiB */
-    uint64_t reserved1;
+    uint64_t chunk_cells;      /* phmm_compute_regions runs a batch of at least this many cells as a
+                                  pipeline of region chunks on two device slots, planning and
+                                  uploading each chunk while the previous one runs (same results);
+                                  0 = 4e10, UINT64_MAX = never */
 } phmm_config;
 
 /* A batch of independent active regions in flat, concatenated arrays (host memory). */

@@ -33,7 +33,7 @@ class PhmmError(RuntimeError):
 
 class Config(C.Structure):
     _fields_ = [("device", C.c_int32), ("use_cuda_graph", C.c_int32), ("autotune", C.c_int32),
-                ("reserved0", C.c_int32), ("hbm_budget_bytes", C.c_uint64), ("reserved1", C.c_uint64)]
+                ("reserved0", C.c_int32), ("hbm_budget_bytes", C.c_uint64), ("chunk_cells", C.c_uint64)]
 
 
 class Batch(C.Structure):

@@ -37,6 +37,9 @@ namespace {
 size_t align_up(size_t x, size_t a = 256) { return (x + a - 1) / a * a; }
 
 constexpr size_t kDescBytes = sizeof(BatchDesc) + sizeof(ClassDesc) * kNumClasses + 4 * sizeof(unsigned int);
+// Default phmm_config.chunk_cells: a batch of this many cells keeps the device busy for about 17 ms,
+// several times what planning and uploading its first chunk take.
+constexpr uint64_t kDefaultChunkCells = 40000000000ull;
 
 // Carves the arena for capacity c starting at base (nullptr: only measure).  Returns the size.
 size_t carve(const Capacity& c, char* base, Slot* s)
@@ -291,6 +294,8 @@ Engine::~Engine()
     cudaSetDevice(dev_);
     delete sw_;
     if (default_slot_) free_slot(default_slot_);
+    if (chunk_slot_) free_slot(chunk_slot_);
+    if (ev_span_) cudaEventDestroy(ev_span_);
     if (d_tables_) cudaFree(d_tables_);
 }
 
@@ -953,6 +958,141 @@ phmm_status Engine::fp32_fma_peak(double* scalar_tflops, double* packed_tflops, 
     return PHMM_OK;
 }
 
+namespace {
+
+// Regions [r0, r1) of a synchronous batch that run as one chunk, with their first haplotype, first
+// read and first likelihood in the whole batch.
+struct ChunkRange {
+    uint32_t r0, r1;
+    uint64_t hap0, read0, out0;
+};
+
+// Cuts a validated batch at region boundaries near these cumulative shares of its cells: a small
+// first chunk gets the device going after little planning and uploading, and the rest is planned
+// and uploaded while it runs.  Measured on B200 over the 2,000-region benchmark batch end to end:
+// one cut at 15% 2278 GCUPS, one pipeline 2213; cuts at 10% and 55% 2238 and at 12.5%, 42% and 71%
+// 2237, their extra chunk tails adding 7-8 ms of device time.
+std::vector<ChunkRange> split_chunks(const phmm_batch& b, uint64_t total_cells)
+{
+    static const double kEnds[] = {0.15};
+    constexpr int kCuts = (int)(sizeof(kEnds) / sizeof(kEnds[0]));
+    std::vector<ChunkRange> ch;
+    ChunkRange cur{0, 0, 0, 0, 0};
+    uint64_t h = 0, r = 0, o = 0, cells = 0;
+    int next = 0;
+    for (uint32_t g = 0; g < b.n_regions; ++g) {
+        const uint32_t nh = b.n_haps[g], nr = b.n_reads[g];
+        cells += (b.hap_off[h + nh] - b.hap_off[h]) * (b.read_off[r + nr] - b.read_off[r]);
+        h += nh;
+        r += nr;
+        o += (uint64_t)nh * nr;
+        cur.r1 = g + 1;
+        if (next < kCuts && (double)cells >= kEnds[next] * (double)total_cells && g + 1 < b.n_regions) {
+            ch.push_back(cur);
+            cur = ChunkRange{g + 1, g + 1, h, r, o};
+            while (next < kCuts && (double)cells >= kEnds[next] * (double)total_cells) ++next;
+        }
+    }
+    if (cur.r1 > cur.r0) ch.push_back(cur);
+    return ch;
+}
+
+phmm_batch chunk_view(const phmm_batch& b, const ChunkRange& c)
+{
+    phmm_batch v = b;  // offsets stay absolute: the planner and the uploads start at hap_off[0] / read_off[0]
+    v.n_regions = c.r1 - c.r0;
+    v.n_haps = b.n_haps + c.r0;
+    v.n_reads = b.n_reads + c.r0;
+    v.hap_off = b.hap_off + c.hap0;
+    v.read_off = b.read_off + c.read0;
+    return v;
+}
+
+}  // namespace
+
+phmm_status Engine::compute_chunked(const phmm_batch& b, const BatchScan& sc, double* out, uint8_t* pair_flags,
+                                    phmm_stats* stats, std::string& err, bool* ran)
+{
+    *ran = false;
+    const std::vector<ChunkRange> ch = split_chunks(b, sc.cells);
+    if (ch.size() < 2) return PHMM_OK;
+    *ran = true;
+    phmm_status st = PHMM_OK;
+    if (!chunk_slot_) {
+        st = make_slot(1, &chunk_slot_, err);
+        if (st != PHMM_OK) return st;
+    }
+    if (!ev_span_) PHMM_CK(cudaEventCreate(&ev_span_));
+    Slot* slots[2] = {default_slot_, chunk_slot_};
+    Plan plans[2];
+    int pending[2] = {-1, -1};  // chunk in flight on each slot
+    const TileTable t = tiles();
+    phmm_stats acc{};
+    float span_ms = 0.f;
+    // Reads a slot's chunk back (waiting for it) and adds its statistics.
+    auto retire = [&](int j) -> phmm_status {
+        const ChunkRange& c = ch[pending[j]];
+        phmm_stats cs{};
+        const phmm_status r = finish(*slots[j], plans[j], out ? out + c.out0 : nullptr,
+                                     pair_flags ? pair_flags + c.out0 : nullptr, &cs, err);
+        pending[j] = -1;
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, ev_span_, slots[j]->ev_t2) == cudaSuccess) span_ms = std::max(span_ms, ms);
+        acc.regions += cs.regions;
+        acc.pairs += cs.pairs;
+        acc.cells += cs.cells;
+        acc.pairs_f64 += cs.pairs_f64;
+        acc.work_items += cs.work_items;
+        acc.kernel_launches += cs.kernel_launches;
+        acc.h2d_bytes += cs.h2d_bytes;
+        acc.d2h_bytes += cs.d2h_bytes;
+        acc.fp32_ms += cs.fp32_ms;
+        acc.fp64_ms += cs.fp64_ms;
+        return r;
+    };
+    for (size_t k = 0; k < ch.size() && st == PHMM_OK; ++k) {
+        const int j = (int)(k & 1);
+        Slot& s = *slots[j];
+        if (pending[j] >= 0) {
+            st = retire(j);
+            if (st != PHMM_OK) break;
+        }
+        const phmm_batch v = chunk_view(b, ch[k]);
+        BatchScan vs;
+        st = scan_batch(v, limits_with(t), vs, err);
+        if (st != PHMM_OK) break;
+        const bool raw_sent = upload_raw(s, vs, v);
+        st = build_plan(v, limits_with(t), plans[j], err);
+        if (st == PHMM_OK) st = upload(s, plans[j], v, err, nullptr, raw_sent);
+        if (st == PHMM_OK && k == 0 && cudaEventRecord(ev_span_, s.main) != cudaSuccess) {
+            err = "event record failed";
+            st = PHMM_ERR_CUDA;
+        }
+        if (st == PHMM_OK) st = run(s, plans[j], pair_flags != nullptr, false, err);
+        if (st != PHMM_OK) {
+            cudaStreamSynchronize(s.main);  // copies already queued read the caller's buffers
+            break;
+        }
+        pending[j] = (int)k;
+    }
+    // the older chunk first
+    const int first = (pending[0] >= 0 && (pending[1] < 0 || pending[0] < pending[1])) ? 0 : 1;
+    for (int j : {first, 1 - first}) {
+        if (pending[j] < 0) continue;
+        if (st == PHMM_OK) {
+            st = retire(j);
+        } else {
+            cudaStreamSynchronize(slots[j]->main);
+            pending[j] = -1;
+        }
+    }
+    if (st == PHMM_OK && stats) {
+        acc.device_ms = span_ms;
+        *stats = acc;
+    }
+    return st;
+}
+
 phmm_status Engine::compute(const phmm_batch& b, double* out, uint8_t* pair_flags, phmm_stats* stats, std::string& err)
 {
     const auto t0 = std::chrono::steady_clock::now();
@@ -964,6 +1104,20 @@ phmm_status Engine::compute(const phmm_batch& b, double* out, uint8_t* pair_flag
     phmm_status st = scan_batch(b, limits_with(t), sc, err);
     if (st != PHMM_OK) return st;
     PHMM_CK(cudaSetDevice(dev_));
+    const uint64_t chunk_cells = cfg_.chunk_cells ? cfg_.chunk_cells : kDefaultChunkCells;
+    if (sc.cells >= chunk_cells && b.n_regions >= 2) {
+        if (sc.out_total && !out) {
+            err = "out is null";
+            return PHMM_ERR_INVALID_ARGUMENT;
+        }
+        bool ran = false;
+        st = compute_chunked(b, sc, out, pair_flags, stats, err, &ran);
+        if (ran) {
+            if (stats) stats->host_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+            return st;
+        }
+        if (st != PHMM_OK) return st;
+    }
     const bool raw_sent = b.n_regions > 0 && upload_raw(*default_slot_, sc, b);
     st = build_plan(b, limits_with(t), plan, err);
     if (st == PHMM_OK && plan.out_total && !out) {

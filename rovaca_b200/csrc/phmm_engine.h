@@ -159,6 +159,11 @@ private:
     // First warp row of scratch region r (0: FP32 multi-stripe classes, 1 + m: the FP64 multi-stripe
     // class of mode m; 1 + kModes32: the total).
     uint64_t scratch_offset_warps(int region) const;
+    // compute() of a batch of at least cfg_.chunk_cells cells: region chunks alternating between the
+    // default slot and chunk_slot_, each planned and uploaded while the previous one runs.  *ran is
+    // false when the batch does not split (the caller then runs it as one pipeline).
+    phmm_status compute_chunked(const phmm_batch& b, const BatchScan& sc, double* out, uint8_t* pair_flags,
+                                phmm_stats* stats, std::string& err, bool* ran);
 
     phmm_config cfg_{};
     int dev_ = 0;
@@ -171,6 +176,8 @@ private:
     const double* d_jacobian_ = nullptr;  // genotyping Jacobian table (inside d_tables_)
     double log10_two_ = 0.0;
     Slot* default_slot_ = nullptr;
+    Slot* chunk_slot_ = nullptr;          // second slot of the chunked synchronous path (made on first use)
+    cudaEvent_t ev_span_ = nullptr;       // start of a chunked call's device pipeline
     SwAligner* sw_ = nullptr;
     std::mutex sw_mu_;
     std::mutex mu_;

@@ -211,9 +211,11 @@ class Engine:
     """One engine per CUDA device (phmm_engine_create)."""
 
     def __init__(self, device: int = 0, use_cuda_graph: bool = True, autotune: bool = True,
-                 hbm_budget_bytes: int = 0):
+                 hbm_budget_bytes: int = 0, chunk_cells: int = 0):
+        """chunk_cells: compute() runs batches of at least this many cells as a pipeline of region
+        chunks (0: the library default, 2**64 - 1: never)."""
         self._lib = _lib.load()
-        cfg = _lib.Config(device, int(use_cuda_graph), int(autotune), 0, hbm_budget_bytes, 0)
+        cfg = _lib.Config(device, int(use_cuda_graph), int(autotune), 0, hbm_budget_bytes, chunk_cells)
         h = C.c_void_p()
         check(self._lib.phmm_engine_create(C.byref(cfg), C.byref(h)))
         self._h = h

@@ -182,6 +182,38 @@ def test_random_lengths_all_classes(engine, oracle):
     assert np.array_equal(flags.astype(bool), used)
 
 
+def test_chunked_compute_equals_one_pipeline(oracle):
+    """phmm_compute_regions run as a pipeline of region chunks on two device slots (chunk_cells
+    forced down) gives the likelihoods, flags and counts of one pipeline, again when a second call
+    reuses both slots; a smaller batch afterwards and an invalid region in a later chunk behave as
+    without chunks (the whole batch is validated before anything is launched)."""
+    from rovaca_b200 import Engine
+
+    pb = synth.config1(40, seed=9)
+    with Engine(device=0, autotune=False, chunk_cells=2**64 - 1) as one:
+        want, wflags, ws = one.compute(pb, want_flags=True)
+    offs = pb.out_offsets()
+    with Engine(device=0, autotune=False, chunk_cells=1) as eng:
+        for _ in range(2):
+            got, flags, st = eng.compute(pb, want_flags=True)
+            assert np.array_equal(got, want, equal_nan=True) and np.array_equal(flags, wflags)
+            for k in ("regions", "pairs", "cells", "pairs_f64", "work_items", "h2d_bytes", "d2h_bytes"):
+                assert st[k] == ws[k], k
+            assert st["device_ms"] > 0 and st["kernel_launches"] > ws["kernel_launches"]
+        got3, _, _ = eng.compute(pb.subset([3, 4, 5]))
+        assert np.array_equal(got3, want[offs[3]:offs[6]], equal_nan=True)
+        bad = Region([b"A" * 1537], [b"ACGT"], [b"\x1e" * 4], [b"-" * 4], [b"-" * 4], [b"\x0a" * 4])
+        with pytest.raises(PhmmError) as e:
+            eng.compute(PackedBatch.from_regions([pb.region(g) for g in range(6)] + [bad]))
+        assert e.value.name == "PHMM_ERR_LIMIT_EXCEEDED"
+        again, _, _ = eng.compute(pb)
+        assert np.array_equal(again, want, equal_nan=True)
+    sample = [0, 17, 39]
+    ref, used = oracle.batch(pb.subset(sample))
+    got_s = np.concatenate([want[offs[g]:offs[g + 1]] for g in sample])
+    assert np.max(np.abs(got_s - ref)) <= EXACT
+
+
 def test_bytes_outside_acgtn(engine, oracle):
     """Lower-case and IUPAC letters: pairs without 'N' compare raw bytes (so 'a' and 'E', or 'R' and
     'R', are told apart or matched exactly as bytes), pairs with 'N' use the reference's base classes."""
