@@ -267,7 +267,7 @@ def underflow_stress(engine, n_regions: int = 100, sample: int = 2) -> dict:
     from rovaca_b200 import synth
 
     pb = synth.config2(n_regions, seed=2)
-    engine.compute(pb)  # warm-up
+    engine.compute(pb, want_flags=True)  # warm-up in the measured form (arena sizes, captured graphs)
     out, flags, st = engine.compute(pb, want_flags=True)
     orc = Oracle()
     sub = pb.subset(list(range(sample)))

@@ -843,16 +843,22 @@ phmm_status Engine::upload(Slot& s, const Plan& plan, const phmm_batch& b, std::
     return PHMM_OK;
 }
 
+phmm_status Engine::ensure_graph(Slot& s, const Plan& plan, bool want_flags, std::string& err)
+{
+    if (cfg_.use_cuda_graph &&
+        (!s.graph || s.graph_flags != want_flags || std::memcmp(&s.graph_tiles, &plan.tiles, sizeof(TileTable)) != 0))
+        return capture_graph(s, want_flags, plan.tiles, err);
+    return PHMM_OK;
+}
+
 phmm_status Engine::run(Slot& s, const Plan& plan, bool want_flags, bool restore, std::string& err)
 {
     phmm_status st = PHMM_OK;
     cudaStream_t m = s.main;
     if (restore) PHMM_CK(cudaMemcpyAsync(s.d_desc, s.d_desc_pristine, kDescBytes, cudaMemcpyDeviceToDevice, m));
     if (cfg_.use_cuda_graph) {
-        if (!s.graph || s.graph_flags != want_flags || std::memcmp(&s.graph_tiles, &plan.tiles, sizeof(TileTable)) != 0) {
-            st = capture_graph(s, want_flags, plan.tiles, err);
-            if (st != PHMM_OK) return st;
-        }
+        st = ensure_graph(s, plan, want_flags, err);
+        if (st != PHMM_OK) return st;
         PHMM_CK(cudaGraphLaunch(s.graph, m));
     } else {
         st = launch_pipeline(s, want_flags, &plan, plan.tiles, err);
@@ -1064,6 +1070,9 @@ phmm_status Engine::compute_chunked(const phmm_batch& b, const BatchScan& sc, do
         const bool raw_sent = upload_raw(s, vs, v);
         st = build_plan(v, limits_with(t), plans[j], err);
         if (st == PHMM_OK) st = upload(s, plans[j], v, err, nullptr, raw_sent);
+        // the span starts where the first chunk's pipeline starts: after a graph capture, which
+        // runs on the host while the device waits
+        if (st == PHMM_OK && k == 0) st = ensure_graph(s, plans[j], pair_flags != nullptr, err);
         if (st == PHMM_OK && k == 0 && cudaEventRecord(ev_span_, s.main) != cudaSuccess) {
             err = "event record failed";
             st = PHMM_ERR_CUDA;

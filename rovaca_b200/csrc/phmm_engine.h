@@ -115,6 +115,9 @@ public:
     // Allocates the slot's arena for at least capacity c now (no-op if it already covers it).
     phmm_status reserve(Slot& s, const Capacity& c, std::string& err);
     phmm_status run(Slot& s, const Plan& plan, bool want_flags, bool restore, std::string& err);
+    // Captures the slot's pipeline graph again if the graph is missing or was captured for other
+    // flags or tiles (no-op without graphs).
+    phmm_status ensure_graph(Slot& s, const Plan& plan, bool want_flags, std::string& err);
     phmm_status fp32_fma_peak(double* scalar_tflops, double* packed_tflops, std::string& err);
 
     // FP32 tile shapes used for new plans (thread-safe copy / replace).
