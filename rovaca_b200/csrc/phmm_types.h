@@ -225,7 +225,8 @@ PHMM_HD inline bool codes_match(uint32_t hc, uint32_t rc, int variant)
 // code of N is 0xF there, which matches every read code as 0xffffffff does) and the base's prior
 // class in bits 11-13 for the packed FP32 kernels' prior tables: A, C, G, T are classes 0-3; class 4
 // is N in the intra variant and every other byte in the inter variant; letters in A's intra class
-// are class 0 there.  Guard words (0) are class 0 and match nothing.
+// are class 0 there.  Guard words (0) are class 0: the cells computed at guard columns lie outside
+// every haplotype and are discarded.
 constexpr uint32_t kCodeMatchMask = 0xffu;
 constexpr int kTabShift = 11;
 constexpr uint32_t kTabMask = 7u << kTabShift;
