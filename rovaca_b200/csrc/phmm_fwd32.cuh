@@ -64,21 +64,32 @@ __device__ __forceinline__ void run_pair2(const BatchView& b, const ProbTables<f
     }
 }
 
-// Resident warps per SM the compiler is asked to allow, one byte per KH (KH = 1 in the low byte).
-// Each scheduler's sub-partition holds 16K registers: 168 registers per thread fit three warps, 128
-// fit four; left free, the compiler spends registers on loading the priors of a whole chunk of
-// steps early.  A build-time setting (1 leaves the compiler free).
+// Resident warps per SM the compiler is asked to allow, one byte per KH (KH = 1 in the low byte):
+// PHMM_F32_MIN_WARPS for mode 0 (inter, constant gap qualities), PHMM_F32_MIN_WARPS_OTHER for modes 1
+// and 2, whose per-row gap parameters or intra arithmetic need more registers.  Each scheduler's
+// sub-partition holds 16K registers: 168 registers per thread fit three warps, 128 fit four; left
+// free, the compiler spends registers on loading the priors of a whole chunk of steps early.  Build-
+// time settings (1 leaves the compiler free).  Measured on B200: mode 0 runs the 2,000-region batch
+// 1.5% faster with 16 warps per SM than with 12 for KH >= 4; modes 1 and 2 spill at 128 registers
+// and run a batch of per-row gap qualities and N reads (300 regions) at 2090 GCUPS with 12 warps per
+// SM against 1614 with 16.
 #ifndef PHMM_F32_MIN_WARPS
 #define PHMM_F32_MIN_WARPS 0x10101010100c0101ull
 #endif
-template <int KH>
+#ifndef PHMM_F32_MIN_WARPS_OTHER
+#define PHMM_F32_MIN_WARPS_OTHER 0x0c0c0c0c0c0c0101ull
+#endif
+template <int KH, int V, int PM>
 __host__ __device__ constexpr int min_blocks32()
 {
-    return (int)(((unsigned long long)(PHMM_F32_MIN_WARPS) >> (8 * (KH - 1))) & 0xffu);
+    return (int)((((V == kInter && PM == PM_ALL) ? (unsigned long long)(PHMM_F32_MIN_WARPS)
+                                                 : (unsigned long long)(PHMM_F32_MIN_WARPS_OTHER)) >>
+                  (8 * (KH - 1))) &
+                 0xffu);
 }
 
 template <int KH, int V, int PM, bool MULTI>
-__global__ void __launch_bounds__(kFwdBlock, min_blocks32<KH>()) fwd_f32_kernel(BatchView b, ProbTables<float> tb,
+__global__ void __launch_bounds__(kFwdBlock, min_blocks32<KH, V, PM>()) fwd_f32_kernel(BatchView b, ProbTables<float> tb,
                                                                                  PassControl pc)
 {
     __shared__ float4 tab[tab_floats4<KH>()];
