@@ -1022,13 +1022,22 @@ phmm_status Engine::compute_chunked(const phmm_batch& b, const BatchScan& sc, do
     *ran = false;
     const std::vector<ChunkRange> ch = split_chunks(b, sc.cells);
     if (ch.size() < 2) return PHMM_OK;
-    *ran = true;
     phmm_status st = PHMM_OK;
     if (!chunk_slot_) {
-        st = make_slot(1, &chunk_slot_, err);
-        if (st != PHMM_OK) return st;
+        // without a second slot (device memory short) the batch runs as one pipeline
+        std::string slot_err;
+        if (make_slot(1, &chunk_slot_, slot_err) != PHMM_OK) {
+            chunk_slot_ = nullptr;
+            cudaGetLastError();
+            return PHMM_OK;
+        }
     }
-    if (!ev_span_) PHMM_CK(cudaEventCreate(&ev_span_));
+    if (!ev_span_ && cudaEventCreate(&ev_span_) != cudaSuccess) {
+        ev_span_ = nullptr;
+        cudaGetLastError();
+        return PHMM_OK;
+    }
+    *ran = true;
     Slot* slots[2] = {default_slot_, chunk_slot_};
     Plan plans[2];
     int pending[2] = {-1, -1};  // chunk in flight on each slot
@@ -1057,8 +1066,7 @@ phmm_status Engine::compute_chunked(const phmm_batch& b, const BatchScan& sc, do
         return r;
     };
     for (size_t k = 0; k < ch.size() && st == PHMM_OK; ++k) {
-        const int j = (int)(k & 1);
-        Slot& s = *slots[j];
+        int j = (int)(k & 1);
         if (pending[j] >= 0) {
             st = retire(j);
             if (st != PHMM_OK) break;
@@ -1067,9 +1075,22 @@ phmm_status Engine::compute_chunked(const phmm_batch& b, const BatchScan& sc, do
         BatchScan vs;
         st = scan_batch(v, limits_with(t), vs, err);
         if (st != PHMM_OK) break;
-        const bool raw_sent = upload_raw(s, vs, v);
+        const bool raw_sent = upload_raw(*slots[j], vs, v);
         st = build_plan(v, limits_with(t), plans[j], err);
-        if (st == PHMM_OK) st = upload(s, plans[j], v, err, nullptr, raw_sent);
+        if (st == PHMM_OK) st = upload(*slots[j], plans[j], v, err, nullptr, raw_sent);
+        if (st == PHMM_ERR_OUT_OF_MEMORY && j == 1) {
+            // the second slot cannot grow for this chunk: run it on the first slot once that is free
+            cudaStreamSynchronize(slots[1]->main);
+            cudaGetLastError();
+            err.clear();
+            st = PHMM_OK;
+            if (pending[0] >= 0) st = retire(0);
+            if (st != PHMM_OK) break;
+            j = 0;
+            plans[0] = std::move(plans[1]);
+            st = upload(*slots[0], plans[0], v, err, nullptr, false);
+        }
+        Slot& s = *slots[j];
         // the span starts where the first chunk's pipeline starts: after a graph capture, which
         // runs on the host while the device waits
         if (st == PHMM_OK && k == 0) st = ensure_graph(s, plans[j], pair_flags != nullptr, err);
