@@ -28,6 +28,38 @@ def test_library_exports_every_declared_symbol():
         assert hasattr(lib, n), n
 
 
+def test_ctypes_mirrors_match_the_c_header_layout(tmp_path):
+    """Every public struct of include/phmm_b200.h has the size and the field offsets (in declaration
+    order) of its ctypes mirror in rovaca_b200/_lib.py: tests/native/abi_layout.c prints them as
+    the C compiler lays them out."""
+    import shutil
+    import subprocess
+    from pathlib import Path
+
+    cc = shutil.which("gcc")
+    if cc is None:
+        pytest.skip("gcc not available")
+    exe = tmp_path / "abi_layout"
+    src = Path(__file__).resolve().parent / "native" / "abi_layout.c"
+    subprocess.run([cc, "-std=c11", "-Wall", "-Wextra", "-Werror", str(src), "-o", str(exe)], check=True)
+    sizes, fields = {}, {}
+    for line in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.splitlines():
+        kind, name, value = line.split()
+        if kind == "struct":
+            sizes[name] = int(value)
+        else:
+            fields.setdefault(name.split(".")[0], []).append(int(value))
+    mirrors = {"phmm_config": _lib.Config, "phmm_batch": _lib.Batch, "phmm_stats": _lib.Stats,
+               "phmm_tile_table": _lib.TileTable, "phmm_tune_entry": _lib.TuneEntry,
+               "phmm_tune_report": _lib.TuneReport, "phmm_region_input": _lib.RegionInput,
+               "phmm_region_events": _lib.RegionEvents, "phmm_region_realign": _lib.RegionRealign,
+               "phmm_server_stats": _lib.ServerStats, "phmm_sw_item": _lib.SwItem, "phmm_sw_result": _lib.SwResult}
+    assert set(mirrors) == set(sizes)
+    for name, cls in mirrors.items():
+        assert C.sizeof(cls) == sizes[name], name
+        assert [getattr(cls, f[0]).offset for f in cls._fields_] == fields[name], name
+
+
 def test_status_strings_and_version():
     lib = _lib.load()
     for s in range(12):
