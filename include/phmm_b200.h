@@ -156,8 +156,11 @@ PHMM_API phmm_status phmm_call_region(phmm_engine* engine, uint32_t n_haps, cons
  * than that (about 100 regions of the benchmark's shape) is rejected with PHMM_ERR_LIMIT_EXCEEDED.
  * Synchronous; calls on one device are serialised and share the array.  The first call on a device
  * sets that device up (looks up the array's address, uploads the probability tables): make it
- * before any stream capture on the device.  No counterpart in the reference: an addition of this
- * library. */
+ * before any stream capture on the device.  Its copies and kernels run on the device's legacy
+ * default stream, so a call waits for, and holds back, work on the caller's blocking streams of
+ * that device (streams created with cudaStreamNonBlocking are not affected).  The calling thread's
+ * current device is the same after the call as before it.  No counterpart in the reference: an
+ * addition of this library. */
 PHMM_API phmm_status phmm_compute_regions_noalloc(const phmm_batch* batch, double* out, uint8_t* pair_flags,
                                                   int32_t device);
 

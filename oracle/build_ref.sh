@@ -12,10 +12,10 @@
 # references ReadRecord methods implemented against libhts (absent); oracle/ref_unreached.cpp binds
 # them to aborting stubs, since the vector API used here never reaches them.
 #
-# Usage: oracle/build_ref.sh [REFERENCE_ROOT]   (default /root/reference)
+# Usage: oracle/build_ref.sh REFERENCE_ROOT   (or the REFERENCE_ROOT environment variable)
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
-REF="${1:-/root/reference}"
+REF="${1:-${REFERENCE_ROOT:?pass the reference source root or set REFERENCE_ROOT}}"
 P="$REF/src/haplotypecaller/pairhmm"
 OUT="$HERE/_ref"
 if [ ! -d "$P" ]; then

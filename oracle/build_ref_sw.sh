@@ -8,10 +8,10 @@
 # avx512_sw_core.c with -mavx512f -mavx512dq -mavx512bw -mavx512vl added.  htslib's headers (the
 # vendored include tree) provide the CIGAR macros.
 #
-# Usage: oracle/build_ref_sw.sh [REFERENCE_ROOT]   (default /root/reference)
+# Usage: oracle/build_ref_sw.sh REFERENCE_ROOT   (or the REFERENCE_ROOT environment variable)
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
-REF="${1:-/root/reference}"
+REF="${1:-${REFERENCE_ROOT:?pass the reference source root or set REFERENCE_ROOT}}"
 B="$REF/src/haplotypecaller/common/base"
 OUT="$HERE/_ref"
 if [ ! -d "$B/lib/ro_sw" ]; then

@@ -43,30 +43,39 @@ def build_oracle(force: bool = False) -> Path:
     return ORACLE_LIB
 
 
-def build_ref(reference_root: str = "/root/reference") -> Path | None:
+def reference_root() -> str:
+    """The reference's source tree, read in place by the build recipes and the fixture generators:
+    the REFERENCE_ROOT environment variable, else the location this test infrastructure was set up
+    with.  Nothing on the GPU host reads it (the built oracle/_ref libraries travel instead)."""
+    return os.environ.get("REFERENCE_ROOT") or "/root/reference"
+
+
+def build_ref(root: str | None = None) -> Path | None:
     """Builds oracle/_ref from the reference sources when they are present; returns the library."""
-    if not Path(reference_root, "src/haplotypecaller/pairhmm").is_dir():
+    src = root or reference_root()
+    if not Path(src, "src/haplotypecaller/pairhmm").is_dir():
         return REF_LIB if REF_LIB.exists() else None
     srcs = [HERE / "ref_shim.cpp", HERE / "ref_kernels.cpp", HERE / "ref_region.cpp", HERE / "ref_unreached.cpp",
             HERE / "build_ref.sh"]
     if REF_LIB.exists() and all(REF_LIB.stat().st_mtime >= s.stat().st_mtime for s in srcs):
         return REF_LIB
-    subprocess.run(["bash", str(HERE / "build_ref.sh"), reference_root], check=True)
+    subprocess.run(["bash", str(HERE / "build_ref.sh"), src], check=True)
     return REF_LIB
 
 
 SW_REF_LIB = HERE / "_ref" / "libsw_ref.so"
 
 
-def build_ref_sw(reference_root: str = "/root/reference") -> Path | None:
+def build_ref_sw(root: str | None = None) -> Path | None:
     """Builds oracle/_ref/libsw_ref.so (the reference's Smith-Waterman aligner) when the reference
     sources are present; returns the library."""
-    if not Path(reference_root, "src/haplotypecaller/common/base/lib/ro_sw").is_dir():
+    src = root or reference_root()
+    if not Path(src, "src/haplotypecaller/common/base/lib/ro_sw").is_dir():
         return SW_REF_LIB if SW_REF_LIB.exists() else None
     srcs = [HERE / "ref_sw_shim.c", HERE / "build_ref_sw.sh"]
     if SW_REF_LIB.exists() and all(SW_REF_LIB.stat().st_mtime >= s.stat().st_mtime for s in srcs):
         return SW_REF_LIB
-    subprocess.run(["bash", str(HERE / "build_ref_sw.sh"), reference_root], check=True)
+    subprocess.run(["bash", str(HERE / "build_ref_sw.sh"), src], check=True)
     return SW_REF_LIB
 
 

@@ -171,6 +171,19 @@ phmm_status run(const phmm_batch& b, double* out, uint8_t* flags, int32_t device
     }
     DeviceState& d = g_devices[device];
     std::lock_guard<std::mutex> lk(d.mu);
+    // the calling thread's current device is put back on every return path
+    int prev_device = -1;
+    if (cudaGetDevice(&prev_device) != cudaSuccess) {
+        cudaGetLastError();
+        prev_device = -1;
+    }
+    struct RestoreDevice {
+        int dev;
+        ~RestoreDevice()
+        {
+            if (dev >= 0) cudaSetDevice(dev);
+        }
+    } restore{prev_device};
     NA_CK(cudaSetDevice(device));
     st = setup(d, device, err);
     if (st != PHMM_OK) return st;

@@ -114,9 +114,9 @@ def _config2_region(rng, n_reads: int = 200) -> dict:
     return _region(rng, 16, (800, 1000), n_reads, np.full(n_reads, 250), (2, 15), 0.05, (0, 3), (5, 10))
 
 
-def config2(n_regions: int = 500, seed: int = 2) -> PackedBatch:
+def config2(n_regions: int = 500, seed: int = 2, n_reads: int = 200) -> PackedBatch:
     rng = np.random.default_rng([seed, 2])
-    return _pack([_config2_region(rng) for _ in range(n_regions)])
+    return _pack([_config2_region(rng, n_reads) for _ in range(n_regions)])
 
 
 def config4(n_regions: int = 200_000, seed: int = 4, sigma: float = 0.5) -> PackedBatch:

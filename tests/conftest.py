@@ -82,6 +82,24 @@ def engine_direct():
     eng.close()
 
 
+def assert_same_values(got, want, tol: float, what: str = "") -> None:
+    """got and want agree pair for pair: NaN at the same pairs, the same infinities at the same
+    pairs, and every finite pair within tol (absolute).  A plain nanmax of the difference would
+    skip NaN-vs-value pairs and -inf - -inf pairs alike."""
+    got = np.asarray(got, dtype=np.float64)
+    want = np.asarray(want, dtype=np.float64)
+    assert got.shape == want.shape, (what, got.shape, want.shape)
+    nan_g, nan_w = np.isnan(got), np.isnan(want)
+    assert np.array_equal(nan_g, nan_w), (what, "NaN masks differ", int(np.sum(nan_g != nan_w)))
+    inf_g, inf_w = np.isinf(got), np.isinf(want)
+    assert np.array_equal(inf_g, inf_w), (what, "infinity masks differ", int(np.sum(inf_g != inf_w)))
+    assert np.array_equal(got[inf_g], want[inf_w]), (what, "infinities of different sign")
+    fin = ~(nan_g | inf_g)
+    if fin.any():
+        err = float(np.max(np.abs(got[fin] - want[fin])))
+        assert err <= tol, (what, err, tol)
+
+
 def case_tuple(c):
     return (c["hap"].encode(), c["read"].encode(), bytes(c["q"]), bytes(c["i"]), bytes(c["d"]), bytes(c["c"]))
 

@@ -32,6 +32,7 @@ ROOT = HERE.parent.parent
 sys.path.insert(0, str(ROOT))
 
 from oracle import Ref, build_ref  # noqa: E402
+from oracle.oracle import reference_root as oracle_reference_root  # noqa: E402
 from rovaca_b200 import synth  # noqa: E402
 from rovaca_b200.pairhmm import PackedBatch, Region  # noqa: E402
 
@@ -128,7 +129,8 @@ def edge_regions(rng) -> list[Region]:
     return out
 
 
-def main(reference_root: str = "/root/reference") -> None:
+def main(reference_root: str | None = None) -> None:
+    reference_root = reference_root or oracle_reference_root()
     res = Path(reference_root) / "src/haplotypecaller/pairhmm/resource"
     lib = build_ref(reference_root)
     if lib is None:

@@ -29,6 +29,7 @@ ROOT = HERE.parent.parent
 sys.path.insert(0, str(ROOT))
 
 from oracle import SwRef, build_ref_sw, cigar_string  # noqa: E402
+from oracle.oracle import reference_root as oracle_reference_root  # noqa: E402
 
 GENOTYPING = SwRef.GENOTYPING
 ASSEMBLY = SwRef.ASSEMBLY
@@ -105,7 +106,8 @@ def synthetic_pairs(rng: random.Random) -> list[tuple[bytes, bytes, tuple, int]]
     return out
 
 
-def main(ref_root: str = "/root/reference") -> None:
+def main(ref_root: str | None = None) -> None:
+    ref_root = ref_root or oracle_reference_root()
     build_ref_sw(ref_root)
     ref = SwRef()
     rng = random.Random(20240611)

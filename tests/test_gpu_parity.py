@@ -10,7 +10,7 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
-from conftest import case_tuple
+from conftest import assert_same_values, case_tuple
 from rovaca_b200 import synth
 from rovaca_b200.pairhmm import PackedBatch, PhmmError, Region
 
@@ -41,19 +41,18 @@ def test_reference_regions(engine, oracle, ref_regions, group):
     pb, ref_out = ref_regions[group]
     got, flags, stats = engine.compute(pb, want_flags=True)
     want, used = oracle.batch(pb)
-    assert np.array_equal(np.isnan(got), np.isnan(want))
-    assert np.nanmax(np.abs(got - want)) <= EXACT
+    assert_same_values(got, want, EXACT)
     assert np.array_equal(flags.astype(bool), used)
     assert stats["pairs_f64"] == int(used.sum())
     # the reference's own schedule_pairhmm output
-    assert np.nanmax(np.abs(got - ref_out)) < 1e-5
+    assert_same_values(got, ref_out, 1e-5, "reference output")
     # every FP32 -> FP64 decision equals the reference's, whichever of its kernels made it
     routes = np.concatenate([oracle.schedule_region(pb, g)[1].reshape(-1) for g in range(pb.n_regions)])
     ref_f64 = np.isin(routes, oracle.ROUTE_F64)
     assert np.array_equal(flags.astype(bool), ref_f64), int(np.sum(flags.astype(bool) != ref_f64))
     # the specification's bound against the all-FP64 oracle
     f64, _ = oracle.batch(pb, fp64_only=True)
-    assert np.nanmax(np.abs(got - f64)) < SPEC
+    assert_same_values(got, f64, SPEC, "all-FP64 oracle")
 
 
 def test_graph_and_direct_launch_agree(engine, engine_direct, ref_regions):
@@ -130,7 +129,7 @@ def test_empty_reads_and_haplotypes_give_nan(engine, oracle):
     assert np.isnan(m[1]).all() and np.isnan(m[:, 1]).all()
     assert np.isfinite(m[[0, 2]][:, [0, 2]]).all()
     want, _ = oracle.batch(pb)
-    assert np.nanmax(np.abs(got - want)) <= EXACT
+    assert_same_values(got, want, EXACT)
     assert stats["pairs"] == 4
 
 
@@ -177,8 +176,7 @@ def test_random_lengths_all_classes(engine, oracle):
     pb = PackedBatch.from_regions(regs)
     got, flags, _ = engine.compute(pb, want_flags=True)
     want, used = oracle.batch(pb)
-    assert np.array_equal(np.isnan(got), np.isnan(want))
-    assert np.nanmax(np.abs(got - want)) <= EXACT
+    assert_same_values(got, want, EXACT)
     assert np.array_equal(flags.astype(bool), used)
 
 
@@ -237,7 +235,7 @@ def test_bytes_outside_acgtn(engine, oracle):
     pb = PackedBatch.from_regions(regs)
     got, flags, _ = engine.compute(pb, want_flags=True)
     want, used = oracle.batch(pb)
-    assert np.nanmax(np.abs(got - want)) <= EXACT
+    assert_same_values(got, want, EXACT)
     assert np.array_equal(flags.astype(bool), used)
 
 
@@ -310,7 +308,7 @@ def test_every_tile_shape_gives_identical_results(oracle):
     want, used = oracle.batch(pb)
     with Engine(device=0, autotune=False, use_cuda_graph=False) as eng:
         base, fb, _ = eng.compute(pb, want_flags=True)
-        assert np.nanmax(np.abs(base - want)) <= EXACT
+        assert_same_values(base, want, EXACT, "default tiles vs oracle")
         assert np.array_equal(fb.astype(bool), used)
         for kh in range(4, 9):
             eng.set_tiles(_table(lambda m, b, kh=kh: (kh, 1) if kh < b else None))

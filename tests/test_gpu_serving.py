@@ -6,6 +6,7 @@ import threading
 import numpy as np
 import pytest
 
+from conftest import assert_same_values
 from rovaca_b200 import Engine, synth
 from rovaca_b200._lib import PhmmError
 from rovaca_b200.pairhmm import PackedBatch, call_pairhmm, schedule_pairhmm
@@ -165,8 +166,7 @@ def test_call_pairhmm_region_api(engine, oracle, pcr):
     want, wkeep = _region_api_expected(oracle, haps, reads, quals, mapq, 18, {"NONE": 0, "CONSERVATIVE": 3,
                                                                               "HOSTILE": 1}[pcr])
     assert np.array_equal(kept, np.nonzero(wkeep)[0])
-    assert np.array_equal(np.isnan(mat), np.isnan(want))
-    assert np.nanmax(np.abs(mat - want)) <= 1e-12
+    assert_same_values(mat, want, 1e-12)
     assert len(kept) < len(reads)  # the unrelated reads are dropped
 
 
