@@ -79,6 +79,53 @@ def build_ref_sw(root: str | None = None) -> Path | None:
     return SW_REF_LIB
 
 
+GENOTYPE_REF_LIB = HERE / "_ref" / "libgenotype_ref.so"
+
+
+def build_ref_genotype(root: str | None = None) -> Path | None:
+    """Builds oracle/_ref/libgenotype_ref.so (the reference's allele marginalisation and diploid
+    genotype-likelihood calculator) when the reference sources are present; returns the library."""
+    src = root or reference_root()
+    if not Path(src, "src/haplotypecaller/genotype/genotype_likelihood_calculator.cpp").is_file():
+        return GENOTYPE_REF_LIB if GENOTYPE_REF_LIB.exists() else None
+    deps = [HERE / "ref_genotype_shim.cpp", HERE / "build_ref_genotype.sh",
+            *sorted((HERE / "ref_stubs" / "boost" / "math" / "special_functions").glob("*.hpp"))]
+    if GENOTYPE_REF_LIB.exists() and all(GENOTYPE_REF_LIB.stat().st_mtime >= d.stat().st_mtime for d in deps):
+        return GENOTYPE_REF_LIB
+    subprocess.run(["bash", str(HERE / "build_ref_genotype.sh"), src], check=True)
+    return GENOTYPE_REF_LIB
+
+
+class GenotypeRef:
+    """The reference's own genotyping arithmetic (oracle/_ref/libgenotype_ref.so): for one sample
+    at ploidy 2, AlleleLikelihoods::marginalize (allele_likelihoods.hpp:189-221,702-730) and
+    GenotypeLikelihoodCalculator::genotype_likelihoods (genotype_likelihood_calculator.h:44-142)."""
+
+    def __init__(self, path: Path | str | None = None):
+        p = Path(path) if path else GENOTYPE_REF_LIB
+        if not p.exists():
+            raise FileNotFoundError(f"{p} not built (oracle/build_ref_genotype.sh needs the reference sources)")
+        self.lib = C.CDLL(str(p))
+        self.lib.ref_genotype.restype = C.c_int
+        self.lib.ref_genotype.argtypes = [C.c_int32, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p,
+                                          C.c_void_p]
+
+    def genotype(self, lk_hr: np.ndarray, hap_allele, n_alleles: int) -> tuple[np.ndarray, np.ndarray]:
+        """lk_hr: [hap][read] normalised likelihoods of the kept reads; hap_allele: allele of each
+        haplotype (-1: none).  Returns (allele likelihoods [allele][read], genotype likelihoods)."""
+        lk = np.ascontiguousarray(lk_hr, np.float64)
+        H, N = lk.shape
+        ha = np.ascontiguousarray(np.asarray(hap_allele, np.int8))
+        if ha.size != H:
+            raise ValueError("hap_allele needs one entry per haplotype")
+        alk = np.empty((n_alleles, N), np.float64)
+        gl = np.empty(n_alleles * (n_alleles + 1) // 2, np.float64)
+        rc = self.lib.ref_genotype(H, N, lk.ctypes.data, n_alleles, ha.ctypes.data, alk.ctypes.data, gl.ctypes.data)
+        if rc != 0:
+            raise ValueError(f"ref_genotype: alleles {n_alleles} outside the reference's limits")
+        return alk, gl
+
+
 class SwRef:
     """The reference's Smith-Waterman aligner (oracle/_ref/libsw_ref.so), as HaplotypeCaller calls
     it to realign a read to its best haplotype: seq1 = haplotype, seq2 = read."""

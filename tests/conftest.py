@@ -37,6 +37,15 @@ def ref():
 
 
 @pytest.fixture(scope="session")
+def genotype_ref():
+    from oracle import GenotypeRef, build_ref_genotype
+
+    if build_ref_genotype() is None:
+        pytest.skip("reference genotyping build (oracle/_ref) not available here")
+    return GenotypeRef()
+
+
+@pytest.fixture(scope="session")
 def golden_cases():
     return json.loads((GOLDEN / "golden_cases.json").read_text())["cases"]
 

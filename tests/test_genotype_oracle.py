@@ -1,7 +1,9 @@
 """The genotyping restatement of the checker (oracle/genotype.py) against the reference's own
-definition of diploid genotype likelihoods (genotype/test/genotype_likelihood_calculator_unit_test.cpp:
-86-130: GL = sum_r [log10sum_c(lk(r, a_c) + log10(count_c)) - log10(2)], accepted within 1e-4) and
-its genotype order.  No GPU."""
+compiled genotyping code (oracle/_ref/libgenotype_ref.so: AlleleLikelihoods::marginalize and
+GenotypeLikelihoodCalculator, built from the reference sources by oracle/build_ref_genotype.sh), bit
+for bit, and against the definition of the reference's unit test
+(genotype/test/genotype_likelihood_calculator_unit_test.cpp:86-130: GL = sum_r [log10sum_c(lk(r, a_c) +
+log10(count_c)) - log10(2)], accepted within 1e-4) and its genotype order.  No GPU."""
 from __future__ import annotations
 
 import math
@@ -90,3 +92,25 @@ def test_best_haplotype_priorities_break_ties():
     assert search_best_allele([-1.0, -1.5], [0, 9]) == 0               # not within 0.2: likelihood wins
     assert search_best_allele([-1.0, -1.0, -1.0], [3, 1, 3]) == 0      # equal priorities keep the first
     assert search_best_allele([-2.0], [0]) == 0
+
+
+def test_restatement_equals_the_reference_build_bit_for_bit(genotype_ref):
+    """1,000 random events: 1-6 alleles, 0-500 reads, 1-16 haplotypes (some mapped to no allele),
+    NaN likelihoods and whole NaN columns; allele likelihoods and genotype likelihoods identical."""
+    rng = np.random.default_rng(2024)
+    for k in range(1000):
+        H = int(rng.integers(1, 17))
+        N = int(rng.integers(0, 501)) if k % 10 == 0 else int(rng.integers(0, 80))
+        A = int(rng.integers(1, 7))
+        lk = -rng.exponential(rng.choice([0.5, 3.0, 20.0]), (H, N))
+        if N and k % 3 == 0:
+            lk[rng.integers(0, H, 3), rng.integers(0, N, 3)] = np.nan
+        if N and k % 7 == 0:
+            lk[:, rng.integers(0, N)] = np.nan
+        ha = rng.integers(-1, A, H).astype(np.int8)
+        alk_ref, gl_ref = genotype_ref.genotype(lk, ha, A)
+        alk = G.marginalize(lk, N, list(ha), A)
+        gl = G.genotype_likelihoods(alk)
+        assert np.array_equal(alk, alk_ref, equal_nan=True), k
+        assert np.array_equal(gl, gl_ref, equal_nan=True), k
+        assert G.best_genotype(gl) == G.best_genotype(gl_ref)
