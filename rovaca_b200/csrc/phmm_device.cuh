@@ -94,8 +94,11 @@ __device__ __forceinline__ T shfl_up1(T v)
 
 // Gap parameters: PM_ALL when a read's insertion, deletion and gap-continuation qualities are each
 // constant along it, PM_ROW otherwise.  In PM_ALL, mm, gapm, mx and my are held once per lane
-// instead of once per row (xx stays per row: pad rows need xx = 1), which frees registers.
-enum ParamMode : int { PM_ALL = 0, PM_ROW = 1 };
+// instead of once per row (xx stays per row: pad rows need xx = 1), which frees registers.  PM_EQ
+// (the FP32 kernels only) is PM_ALL with equal insertion and deletion qualities, mx == my: the
+// product M[i][j] * mx that feeds I[i+1][j] is the product M[i][j] * my that feeds D[i][j+1], so
+// it is formed once (the two reference operations have the same operands, hence the same bits).
+enum ParamMode : int { PM_ALL = 0, PM_ROW = 1, PM_EQ = 2 };
 
 // One lane's rows of the current stripe.
 template <typename T, int K, int PM>
@@ -163,7 +166,11 @@ __device__ __forceinline__ void load_rows(LaneRows<T, K, PM>& L, const BatchView
 // rows with M = I = 0) and xx = 1 keeps D, so they still reproduce the boundary row.
 // FLUSH: flush every result below 2^-1022 to zero (FP64 steps whose inputs may be that small); the
 // FP32 path flushes in hardware either way.
-template <typename T, int K, int V, int PM, bool FLUSH = true>
+// UNF: the all-FP64 check arithmetic instead of the reference's contracted one: every product
+// rounded, then summed left to right (s = (M mm + I gapm) + D gapm, I = M mx + I xx,
+// D = M my + D yy), each result flushed -- the plain-arithmetic FP64 model every likelihood's error
+// is measured against.
+template <typename T, int K, int V, int PM, bool FLUSH = true, bool UNF = false>
 __device__ __forceinline__ void cells(LaneRows<T, K, PM>& L, uint32_t hc, T sM, T sI, T dM, T dI, T dD)
 {
     auto fz = [](T x) { return FLUSH ? ftz(x) : x; };
@@ -173,14 +180,20 @@ __device__ __forceinline__ void cells(LaneRows<T, K, PM>& L, uint32_t hc, T sM, 
         const int r = PM == PM_ROW ? k : 0;
         const T oM = L.Mp[k], oI = L.Ip[k], oD = L.Dp[k];
         const T prior = codes_match(hc, L.rc[k], V) ? L.pa[k] : L.pb[k];
-        T s;
-        if (V == kInter)
-            s = fz(rfma(diD, L.gm[r], fz(rfma(diM, L.mm[r], fz(rmul(diI, L.gm[r]))))));
-        else
-            s = fz(rfma(diD, L.gm[r], fz(rfma(diI, L.gm[r], fz(rmul(diM, L.mm[r]))))));
+        T s, nI, nD;
+        if (UNF) {
+            s = fz(radd(fz(radd(fz(rmul(diM, L.mm[r])), fz(rmul(diI, L.gm[r])))), fz(rmul(diD, L.gm[r]))));
+            nI = fz(radd(fz(rmul(upM, L.mx[r])), fz(rmul(upI, L.xx[k]))));
+            nD = fz(radd(fz(rmul(oM, L.my[r])), fz(rmul(oD, L.xx[k]))));
+        } else {
+            if (V == kInter)
+                s = fz(rfma(diD, L.gm[r], fz(rfma(diM, L.mm[r], fz(rmul(diI, L.gm[r]))))));
+            else
+                s = fz(rfma(diD, L.gm[r], fz(rfma(diI, L.gm[r], fz(rmul(diM, L.mm[r]))))));
+            nI = fz(rfma(upI, L.xx[k], fz(rmul(upM, L.mx[r]))));
+            nD = fz(rfma(oD, L.xx[k], fz(rmul(oM, L.my[r]))));
+        }
         const T nM = fz(rmul(s, prior));
-        const T nI = fz(rfma(upI, L.xx[k], fz(rmul(upM, L.mx[r]))));
-        const T nD = fz(rfma(oD, L.xx[k], fz(rmul(oM, L.my[r]))));
         L.Mp[k] = nM;
         L.Ip[k] = nI;
         L.Dp[k] = nD;
@@ -246,7 +259,7 @@ struct SweepOut {
 //   FROM_SCR: the row above the stripe comes from scratch (stripe > 0), else the boundary row.
 //   TO_SCR:   the stripe's bottom row goes to scratch (not the last stripe), else it is summed.
 //   above_row0: the row above this lane's first slot is the boundary row 0 or a pad row.
-template <typename T, int K, int V, int PM, bool FROM_SCR, bool TO_SCR>
+template <typename T, int K, int V, int PM, bool FROM_SCR, bool TO_SCR, bool UNF = false>
 __device__ void sweep(LaneRows<T, K, PM>& L, const BatchView& b, const PassControl& pc, const SweepOut& so, uint32_t g_lo,
                       uint32_t g_hi, T* scr, int lane, bool above_row0)
 {
@@ -325,9 +338,9 @@ __device__ void sweep(LaneRows<T, K, PM>& L, const BatchView& b, const PassContr
         // is not checked)
         constexpr bool kVote = PHMM_F64_VOTE && sizeof(T) == 8 && !FROM_SCR;
         if (kVote && flush_free)
-            cells<T, K, V, PM, false>(L, hc, sM, sI, dM, dI, dD);
+            cells<T, K, V, PM, false, UNF>(L, hc, sM, sI, dM, dI, dD);
         else
-            cells<T, K, V, PM, true>(L, hc, sM, sI, dM, dI, dD);
+            cells<T, K, V, PM, true, UNF>(L, hc, sM, sI, dM, dI, dD);
         dM = sM;
         dI = sI;
         dD = sD;

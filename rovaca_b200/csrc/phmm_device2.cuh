@@ -14,6 +14,15 @@
 // above have M = I = 0, and xx = 1 keeps D = C/H).  Reads longer than one stripe run as stripes
 // linked through a per-warp scratch row of float2 values.
 //
+// Lane state between steps.  A lane does not keep its rows' M, I and D at its last column: it keeps,
+// per row, the values the next column starts from -- the diagonal sum s that M[i][j+1] = s * prior
+// multiplies (formed from row i-1 at column j as soon as that row is known, for the lane's first
+// row from the row above it, which arrives by shuffle) and D[i][j+1] (formed from row i at column
+// j) -- plus the bottom row's M, I and D for the next lane.  That is 2 * KH + 3 values per read
+// instead of 3 * KH + 3 (the row above's diagonal included), the same operations on the same
+// operands, and a step's M and D of every row only wait for values of the previous step; the I
+// chain down the lane's rows alone waits for this step's shuffle.
+//
 // Match prior.  A cell's prior depends only on its read row and the class of its haplotype base, and
 // a lane's rows are fixed for a stripe, so each lane tabulates its rows' priors for the five base
 // classes (kTabClasses; the class rides in the haplotype code word) in shared memory once per
@@ -22,10 +31,12 @@
 // Inter reads with bytes outside A/C/G/T can equal a haplotype byte of class 4; a warp holding such
 // a row runs every step on the checked path, which corrects the class-4 priors by comparing bytes.
 //
-// Gap parameters: PM_ALL when a read's insertion, deletion and gap-continuation qualities are each
-// constant along it (the region API without a PCR model, and the benchmark data), PM_ROW otherwise.
-// In PM_ALL, mm, gapm, mx and my are held once per lane instead of once per row (xx stays per row:
-// pad rows need xx = 1), which leaves registers for more rows per lane.
+// Gap parameters: PM_EQ when a read's insertion, deletion and gap-continuation qualities are each
+// constant along it and its insertion and deletion qualities are equal (the region API without a
+// PCR model, and the benchmark data), PM_ROW otherwise.  In PM_EQ, mm, gapm and mx (= my) are held
+// once per lane instead of once per row (xx stays per row: pad rows need xx = 1), which leaves
+// registers for more rows per lane, and a cell takes 7 operations instead of 8 (M * mx serves both
+// I of the row below and D of the next column).
 #pragma once
 
 #include <cstdint>
@@ -66,9 +77,11 @@ __host__ __device__ constexpr int tab_floats4()
 template <int KH, int PM>
 struct LaneRows2 {
     static constexpr int NR = PM == PM_ROW ? KH : 1;
-    float2 Mp[KH], Ip[KH], Dp[KH];  // (X, Y) values at the previous column
+    float2 S[KH];                   // (X, Y) diagonal sum of row a for the lane's next column
+    float2 Dn[KH];                  // (X, Y) D of row a at the lane's next column
+    float2 Mb, Ib, Db;              // bottom row at the lane's last column (shuffled to lane + 1)
     float2 xx[KH];
-    float2 mm[NR], gm[NR], mx[NR], my[NR];
+    float2 mm[NR], gm[NR], mx[NR], my[NR];  // my: unused in PM_EQ (mx == my)
     uint32_t padX, padY;            // bit a: row a of the read is a pad row
 };
 
@@ -126,7 +139,11 @@ __device__ __forceinline__ bool load_rows2(LaneRows2<KH, PM>& L, float4* tab, co
     constexpr int QJ = tab_quads<KH>();
     L.padX = 0;
     L.padY = 0;
-    if (PM == PM_ALL) {
+    // columns before the lane's first haplotype compute from these and are discarded
+#pragma unroll
+    for (int a = 0; a < KH; ++a) L.S[a] = L.Dn[a] = f2(0.f, 0.f);
+    L.Mb = L.Ib = L.Db = f2(0.f, 0.f);
+    if (PM != PM_ROW) {
         // constant along the read: any real row gives them (pad rows ignore them)
         const RowParams x0 = row_params<V>(b, tb, rp.roff[0], rp.R[0], rp.R[0] > 0 ? 0 : -1);
         const RowParams y0 = row_params<V>(b, tb, rp.roff[1], rp.R[1], rp.R[1] > 0 ? 0 : -1);
@@ -180,32 +197,49 @@ __device__ __forceinline__ float2 diag_sum(const LaneRows2<KH, PM>& L, int r, fl
     return rfma2(dgD, L.gm[r], rfma2(dgI, L.gm[r], rmul2(dgM, L.mm[r])));
 }
 
-// All KH row pairs of the lane for one step.  (upM, upI): the row above the lane's first row at this
-// column; (dgM, dgI, dgD): the same row one column to the left; pr: the rows' priors.
-// Order: row a+1's diagonal sum first (it reads row a's old values), then row a's D, M and I, so
-// every old value is dead before its row's new value is written and each row's state keeps its
-// registers from step to step.  Measured on B200 over the 2,000-region benchmark batch: 1.7% faster
-// than updating M, I and D of a row together, with the same results.
+// All KH row pairs of the lane for one step at column j.  (upM, upI, upD): the row above the lane's
+// first row at column j; pr: the rows' priors at column j.  Per row i (the reference's operations):
+//   M[i][j] = S * prior                                  S = s formed at the previous step
+//   I[i][j] = fma(I[i-1][j], xx, M[i-1][j] * mx)
+//   D[i][j] = Dn                                         Dn formed at the previous step
+//   Dn      = D[i][j+1]  = fma(D[i][j], yy, M[i][j] * my)        (yy = xx, the same ph2pr[gcp])
+//   S'      = s[i+1][j+1] from M, I, D[i][j]                     (diag_sum)
+// and the row above's values give the first row's S' for the next column.  A row's pending S is
+// read before the row above overwrites it.  In PM_EQ, M[i][j] * mx is the product that D[i][j+1]
+// needs (mx == my), formed once.
 template <int KH, int V, int PM>
 __device__ __forceinline__ void cells2(LaneRows2<KH, PM>& L, const float2 (&pr)[KH], float2 upM, float2 upI,
-                                       float2 dgM, float2 dgI, float2 dgD)
+                                       float2 upD)
 {
-    float2 s = diag_sum<V, PM>(L, 0, dgM, dgI, dgD);
+    constexpr bool EQ = PM == PM_EQ;
+    float2 Mab = upM, Iab = upI;    // the row above, this column
+    float2 Pab = f2(0.f, 0.f);      // PM_EQ: its M * mx
+    float2 nM = rmul2(L.S[0], pr[0]);
 #pragma unroll
     for (int a = 0; a < KH; ++a) {
         const int r = PM == PM_ROW ? a : 0;
-        const float2 oM = L.Mp[a], oI = L.Ip[a], oD = L.Dp[a];
-        float2 sn = s;
-        if (a + 1 < KH) sn = diag_sum<V, PM>(L, PM == PM_ROW ? a + 1 : 0, oM, oI, oD);
-        L.Dp[a] = rfma2(oD, L.xx[a], rmul2(oM, L.my[r]));
-        const float2 nM = rmul2(s, pr[a]);
-        const float2 nI = rfma2(upI, L.xx[a], rmul2(upM, L.mx[r]));
-        L.Mp[a] = nM;
-        L.Ip[a] = nI;
-        upM = nM;
-        upI = nI;
-        s = sn;
+        const float2 M = nM;
+        if (a + 1 < KH) nM = rmul2(L.S[a + 1], pr[a + 1]);  // before S[a + 1] is overwritten below
+        const float2 q = (EQ && a > 0) ? Pab : rmul2(Mab, L.mx[r]);
+        const float2 I = rfma2(Iab, L.xx[a], q);
+        const float2 D = L.Dn[a];
+        if (EQ) {
+            Pab = rmul2(M, L.mx[0]);
+            L.Dn[a] = rfma2(D, L.xx[a], Pab);
+        } else {
+            L.Dn[a] = rfma2(D, L.xx[a], rmul2(M, L.my[r]));
+        }
+        if (a + 1 < KH) {
+            L.S[a + 1] = diag_sum<V, PM>(L, PM == PM_ROW ? a + 1 : 0, M, I, D);
+        } else {
+            L.Mb = M;
+            L.Ib = I;
+            L.Db = D;
+        }
+        Mab = M;
+        Iab = I;
     }
+    L.S[0] = diag_sum<V, PM>(L, 0, upM, upI, upD);
 }
 
 // Output side of a sweep: the two reads' likelihood columns and FP64 rerun lists.
@@ -244,7 +278,6 @@ __device__ void sweep2(LaneRows2<KH, PM>& L, const float4* tab, const BatchView&
     bool started = false;
     float D0 = 0.f;
     float2 sumM = f2(0.f, 0.f), sumI = f2(0.f, 0.f);
-    float2 dM = f2(0.f, 0.f), dI = f2(0.f, 0.f), dD = f2(0.f, 0.f);
 
     const int steps = Tcols + kWarp;  // lane 31 reaches column Tcols (the end) at step Tcols + 31
 
@@ -302,19 +335,21 @@ __device__ void sweep2(LaneRows2<KH, PM>& L, const float4* tab, const BatchView&
             const int H = (int)(b.hap_off[cur + 1] - b.hap_off[cur]);
             nb += H;
             D0 = C / (float)H;
-            // Left edge of the new haplotype: column 0 is zero in every real row; pad rows stand
-            // for the boundary row 0, whose D is C/H in every column.
+            // Left edge of the new haplotype, column 0: M = I = 0 in every row, D = 0 in real rows
+            // and C/H in pad rows, which stand for the boundary row 0 (as does the row above the
+            // lane's first row when `above`).  The first column starts from the diagonal sums of
+            // column 0 and from D[i][1] = fma(D[i][0], xx, 0 * my): C/H in pad rows (xx = 1), else 0.
+            const float2 z = f2(0.f, 0.f);
+            float2 Dab = f2(aboveX ? D0 : 0.f, aboveY ? D0 : 0.f);
 #pragma unroll
             for (int a = 0; a < KH; ++a) {
-                L.Mp[a] = f2(0.f, 0.f);
-                L.Ip[a] = f2(0.f, 0.f);
-                L.Dp[a] = f2(((L.padX >> a) & 1u) ? D0 : 0.f, ((L.padY >> a) & 1u) ? D0 : 0.f);
+                const float2 Dc = f2(((L.padX >> a) & 1u) ? D0 : 0.f, ((L.padY >> a) & 1u) ? D0 : 0.f);
+                L.S[a] = diag_sum<V, PM>(L, PM == PM_ROW ? a : 0, z, z, Dab);
+                L.Dn[a] = Dc;
+                Dab = Dc;
             }
-            dM = f2(0.f, 0.f);
-            dI = f2(0.f, 0.f);
-            dD = f2(aboveX ? D0 : 0.f, aboveY ? D0 : 0.f);
-            sumM = f2(0.f, 0.f);
-            sumI = f2(0.f, 0.f);
+            sumM = z;
+            sumI = z;
         } else {
             nb = 0x7fffffff;
         }
@@ -342,9 +377,9 @@ __device__ void sweep2(LaneRows2<KH, PM>& L, const float4* tab, const BatchView&
 
     auto step = [&](int t, bool check) {
         const int p = t - lane;
-        float2 uM = shfl_up2(L.Mp[KH - 1]);
-        float2 uI = shfl_up2(L.Ip[KH - 1]);
-        float2 uD = shfl_up2(L.Dp[KH - 1]);
+        float2 uM = shfl_up2(L.Mb);
+        float2 uI = shfl_up2(L.Ib);
+        float2 uD = shfl_up2(L.Db);
         if (check && p == nb) boundary();
         if (lane == 0) {
             if (FROM_SCR) {
@@ -381,19 +416,16 @@ __device__ void sweep2(LaneRows2<KH, PM>& L, const float4* tab, const BatchView&
                     pr[a].y = tb.pmat[b.read_q[rp.roff[1] + iY] & 127];
             }
         }
-        cells2<KH, V, PM>(L, pr, uM, uI, dM, dI, dD);
-        dM = uM;
-        dI = uI;
-        dD = uD;
+        cells2<KH, V, PM>(L, pr, uM, uI, uD);
         if (TO_SCR) {
             if (writer && p >= 0 && p < Tcols) {
-                scr[3 * p + 0] = L.Mp[KH - 1];
-                scr[3 * p + 1] = L.Ip[KH - 1];
-                scr[3 * p + 2] = L.Dp[KH - 1];
+                scr[3 * p + 0] = L.Mb;
+                scr[3 * p + 1] = L.Ib;
+                scr[3 * p + 2] = L.Db;
             }
         } else {
-            sumM = radd2(sumM, L.Mp[KH - 1]);
-            sumI = radd2(sumI, L.Ip[KH - 1]);
+            sumM = radd2(sumM, L.Mb);
+            sumI = radd2(sumI, L.Ib);
         }
     };
 

@@ -82,7 +82,7 @@ __device__ __forceinline__ void run_pair2(const BatchView& b, const ProbTables<f
 template <int KH, int V, int PM>
 __host__ __device__ constexpr int min_blocks32()
 {
-    return (int)((((V == kInter && PM == PM_ALL) ? (unsigned long long)(PHMM_F32_MIN_WARPS)
+    return (int)((((V == kInter && PM != PM_ROW) ? (unsigned long long)(PHMM_F32_MIN_WARPS)
                                                  : (unsigned long long)(PHMM_F32_MIN_WARPS_OTHER)) >>
                   (8 * (KH - 1))) &
                  0xffu);

@@ -247,7 +247,9 @@ phmm_status build_plan(const phmm_batch& b, const PlanLimits& lim, Plan& plan, s
                 const uint64_t a = plan.read_off[gr], R = plan.read_off[gr + 1] - a;
                 plan.read_flags[gr] = has_n(rb + a, R);
                 if (R == 0) continue;
-                // region API: gap qualities are constant unless a PCR model caps them
+                // Mode 0 (the FP32 kernels' PM_EQ): gap qualities constant along the read, insertion
+                // and deletion qualities equal (as qualities & 127, which is what the tables read).
+                // Region API: gap-open = insertion = deletion, constant unless a PCR model caps them.
                 bool uniform;
                 if (lim.region_api) {
                     uniform = lim.region_api[g].pcr == PHMM_PCR_NONE;
@@ -255,7 +257,8 @@ phmm_status build_plan(const phmm_batch& b, const PlanLimits& lim, Plan& plan, s
                     const uint8_t* ib = b.read_ins + plan.read_base0 + a;
                     const uint8_t* db = b.read_del + plan.read_base0 + a;
                     const uint8_t* cb = b.read_gcp + plan.read_base0 + a;
-                    uniform = constant_run(ib, R) && constant_run(db, R) && constant_run(cb, R);
+                    uniform = constant_run(ib, R) && constant_run(db, R) && constant_run(cb, R) &&
+                              (ib[0] & 127) == (db[0] & 127);
                 }
                 const uint32_t n_flag = plan.read_flags[gr] & 1;
                 const int mode = n_flag ? 2 : (uniform ? 0 : 1);

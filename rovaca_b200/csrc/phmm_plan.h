@@ -16,7 +16,8 @@ constexpr int kPlanClasses = kClasses32 + kClasses64;
 
 // FP32 tile shape of every (mode, read-length bucket): kh row pairs per lane, single stripe
 // (kh >= bucket) or multi-stripe (kMinMultiKH <= kh < bucket, stripes = ceil(R / (32 * kh))).
-// Modes as in phmm_types.h: 0 inter with constant gap qualities, 1 inter per-row, 2 intra.
+// Modes as in phmm_types.h: 0 inter with constant gap qualities (insertion = deletion), 1 inter
+// per-row, 2 intra.
 struct TileTable {
     uint8_t kh[kModes32][kLenBuckets];
     uint8_t multi[kModes32][kLenBuckets];

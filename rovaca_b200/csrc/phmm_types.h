@@ -28,7 +28,8 @@ constexpr int kLenBuckets = 24;
 PHMM_HD inline int len_bucket(uint64_t R) { return (int)((R + kWarp - 1) / kWarp); }
 
 // FP32 kernel classes (packed path: two reads per warp, one per float2 component).  A class is a mode
-//   0: inter, gap qualities constant along the read;  1: inter, per-row;  2: intra (pairs with 'N')
+//   0: inter, gap qualities constant along the read with insertion = deletion;  1: inter, any other
+//   gap qualities (per-row);  2: intra (pairs with 'N')
 // and a tile shape: KH row pairs per lane in one stripe of 32*KH rows (KH = 1..8), or stripes of
 // 32*KH rows linked through per-warp scratch rows (KH = 4..8).  Which shape a read-length bucket
 // runs in is a per-engine table (default: the smallest single stripe, 256-row stripes beyond).

@@ -157,6 +157,13 @@ def test_plan_pairs_reads_and_gap_modes():
     s = plan_summary(PackedBatch.from_regions([reg]))
     assert s["class_items"][cls(0, 5, uniform=False)] == 1
     assert s["class_items"][cls(0, 5)] == 2
+    # constant along the read but insertion != deletion: mode 0 shares M * mx between I and D
+    # (mx == my), so such a read runs in the per-row class too; equal as quality & 127 is equal
+    reg.insertion_qualities[0] = bytes([40] * 150)
+    reg.insertion_qualities[1] = bytes([45 + 128] * 150)
+    s = plan_summary(PackedBatch.from_regions([reg]))
+    assert s["class_items"][cls(0, 5, uniform=False)] == 1
+    assert s["class_items"][cls(0, 5)] == 2
 
 
 def test_tile_table_shapes_route_reads():
@@ -318,3 +325,41 @@ def test_normalize_matches_reference_build(ref):
                                        out.ctypes.data_as(C.c_void_p), keep.ctypes.data_as(C.c_void_p), C.byref(nk))
         kept = keep.astype(bool)
         assert np.array_equal(out[:, : nk.value], want.T[:, kept])
+
+
+# ---- several devices: the region partitioner ----------------------------------------------
+
+def test_partition_balances_cells_and_places_every_region_once():
+    """Longest-processing-time greedy by region cells: every region in exactly one part, the part
+    cells add up, the largest part is within the ideal share plus one region (and within 4/3 of the
+    optimum's lower bound), and the split does not depend on anything but the batch."""
+    from rovaca_b200 import partition_regions, synth
+
+    pb = synth.config1(300, seed=7)
+    cells = np.array([pb.subset([g]).cells() for g in range(pb.n_regions)], np.uint64)
+    for n in (1, 2, 3, 8, 13):
+        part, load = partition_regions(pb, n)
+        assert part.shape == (pb.n_regions,) and int(part.max()) < n
+        for p in range(n):
+            assert int(load[p]) == int(cells[part == p].sum())
+        total, biggest = int(cells.sum()), int(cells.max())
+        assert int(load.max()) <= total / n + biggest
+        assert int(load.max()) <= 4 / 3 * max(total / n, biggest) + 1
+        again, _ = partition_regions(pb, n)
+        assert np.array_equal(part, again)
+
+
+def test_partition_edge_cases():
+    from rovaca_b200 import partition_regions
+
+    reg = _region([b"ACGT" * 20], [b"ACGT" * 10])
+    empty = _region([], [b"ACGT"])
+    pb = PackedBatch.from_regions([reg, empty, reg])
+    part, load = partition_regions(pb, 5)  # more parts than regions: some stay empty
+    assert part[0] != part[2]  # the two equal regions go to different parts
+    assert int(load.sum()) == 2 * 80 * 40 and (load == 0).sum() >= 3
+    with pytest.raises(_lib.PhmmError):
+        partition_regions(pb, 0)
+    with pytest.raises(_lib.PhmmError) as e:
+        partition_regions(PackedBatch.from_regions([_region([b"A" * 1537], [b"ACGT"])]), 2)
+    assert e.value.name == "PHMM_ERR_LIMIT_EXCEEDED"
