@@ -183,6 +183,16 @@ PHMM_API phmm_status phmm_resident_results(phmm_resident* resident, double* out,
  * items; 0 for FP64 classes, whose work is only known on the device).  The results equal those of
  * phmm_resident_run. */
 PHMM_API phmm_status phmm_resident_profile(phmm_resident* resident, float* class_ms, uint64_t* class_cells);
+/* Recomputes every pair of the resident batch with the all-FP64 check arithmetic -- FP64 end to
+ * end with C = 2^1020, each product rounded and then added (no fused multiply-add), every result
+ * below 2^-1022 flushed, the inter prior for pairs without 'N' and the N-aware intra model for the
+ * others -- and writes the log10 likelihoods to out (layout of phmm_compute_regions; pairs with an
+ * empty read or haplotype NaN).  This is the model every likelihood's error is measured against,
+ * computed for the whole batch on the device.  The resident's own results are overwritten: call
+ * phmm_resident_run again before phmm_resident_results.  No reference counterpart (the reference's
+ * FP64 path, computeLikelihoodsAVX512 with use_double, pairhmm_api.cpp:14-19, is the contracted
+ * form of the same model). */
+PHMM_API phmm_status phmm_resident_check_fp64(phmm_resident* resident, double* out);
 PHMM_API phmm_status phmm_resident_destroy(phmm_resident* resident);
 
 /* Measures the device's FP32 FMA throughput (independent FMA chains on every SM, about 0.1 s),
@@ -208,7 +218,8 @@ PHMM_API void phmm_host_normalize_filter(const double* lk_hap_read, uint32_t n_h
 /* ---- tile shapes and the autotuner (no reference counterpart) ---------------------------------
  *
  * The FP32 pass runs every read in a tile shape chosen by its mode and read-length bucket:
- *   mode 0: pairs without 'N' whose read has constant insertion/deletion/gap qualities,
+ *   mode 0: pairs without 'N' whose read has constant insertion/deletion/gap qualities and equal
+ *           insertion and deletion qualities,
  *   mode 1: other pairs without 'N', mode 2: pairs with 'N';
  *   bucket b = ceil(read length / 32), 1..24;
  *   shape: rows_per_lane KH (32 lanes hold 32 * KH rows of each read) in one stripe (KH >= b), or
@@ -378,6 +389,46 @@ typedef struct phmm_server_stats {
 } phmm_server_stats;
 
 PHMM_API phmm_status phmm_server_stats_get(phmm_engine* engine, phmm_server_stats* stats);
+
+/* ---- several devices --------------------------------------------------------------------
+ *
+ * The reference runs regions in parallel on a host thread pool (haplotypecaller.cpp:105,
+ * haplotypecaller_engine.cpp:119); regions are independent, so several GPUs shard whole regions with
+ * nothing exchanged between them. */
+
+/* Splits a batch's regions into n_parts parts balanced by cells (a region's cells: its total read
+ * bases times its total haplotype bases): longest-processing-time greedy, regions in decreasing cell
+ * order each to the part with the fewest cells so far (ties to the lower part), so that the largest
+ * part holds at most the ideal share plus one region.  part_of_region[n_regions] receives each
+ * region's part, cells_of_part[n_parts] each part's cells.  Host only; validates the batch like
+ * phmm_compute_regions.  No reference counterpart. */
+PHMM_API phmm_status phmm_partition_regions(const phmm_batch* batch, uint32_t n_parts, uint32_t* part_of_region,
+                                            uint64_t* cells_of_part);
+
+typedef struct phmm_device_set phmm_device_set;
+
+/* One engine per listed device (a device may be listed twice: two engines, each with its own
+ * arenas and streams).  cfg as for phmm_engine_create (NULL: defaults); its device field is
+ * replaced by each listed device.  No reference counterpart. */
+PHMM_API phmm_status phmm_device_set_create(const int32_t* devices, uint32_t n_devices, const phmm_config* cfg,
+                                            phmm_device_set** out_set);
+PHMM_API phmm_status phmm_device_set_destroy(phmm_device_set* set);
+/* The engine of member `index` (owned by the set), for per-device calls. */
+PHMM_API phmm_status phmm_device_set_engine(phmm_device_set* set, uint32_t index, phmm_engine** engine);
+/* phmm_compute_regions over the set: the regions are partitioned as by phmm_partition_regions, each
+ * part is gathered into its device's pinned staging and computed there (one host thread per
+ * device, all at once), and every region's likelihoods land in its own range of out (the layout of
+ * phmm_compute_regions; results identical to one engine's).  stats: sums over the devices, and the
+ * longest device time.  Calls on one set are serialised. */
+PHMM_API phmm_status phmm_device_set_compute_regions(phmm_device_set* set, const phmm_batch* batch, double* out,
+                                                     uint8_t* pair_flags, phmm_stats* stats);
+/* phmm_submit to the member with the fewest cells submitted and not yet waited for. */
+PHMM_API phmm_status phmm_device_set_submit(phmm_device_set* set, const phmm_batch* region, double* out,
+                                            uint8_t* pair_flags, phmm_ticket* ticket);
+/* phmm_wait for a ticket of phmm_device_set_submit; device_index (optional) receives the member
+ * that ran it. */
+PHMM_API phmm_status phmm_device_set_wait(phmm_device_set* set, phmm_ticket ticket, int64_t timeout_us,
+                                          double* queued_us, double* total_us, uint32_t* device_index);
 
 /* ---- Smith-Waterman realignment of reads to their best haplotype ------------------------------
  *

@@ -161,6 +161,7 @@ def load() -> C.CDLL:
         "phmm_resident_create": (I32, [P, C.POINTER(Batch), I32, C.POINTER(P)]),
         "phmm_resident_run": (I32, [P, I32, C.POINTER(Stats)]),
         "phmm_resident_results": (I32, [P, P, P]),
+        "phmm_resident_check_fp64": (I32, [P, P]),
         "phmm_resident_destroy": (I32, [P]),
         "phmm_fp32_fma_peak": (I32, [P, C.POINTER(D), C.POINTER(D)]),
         "phmm_compute_regions_noalloc": (I32, [C.POINTER(Batch), P, P, I32]),
@@ -182,6 +183,13 @@ def load() -> C.CDLL:
         "phmm_sw_resident_run": (I32, [P, I32, C.POINTER(C.c_float), P]),
         "phmm_sw_resident_results": (I32, [P, P, P, U64, C.POINTER(U64)]),
         "phmm_sw_resident_destroy": (I32, [P]),
+        "phmm_partition_regions": (I32, [C.POINTER(Batch), U32, P, P]),
+        "phmm_device_set_create": (I32, [P, U32, C.POINTER(Config), C.POINTER(P)]),
+        "phmm_device_set_destroy": (I32, [P]),
+        "phmm_device_set_engine": (I32, [P, U32, C.POINTER(P)]),
+        "phmm_device_set_compute_regions": (I32, [P, C.POINTER(Batch), P, P, C.POINTER(Stats)]),
+        "phmm_device_set_submit": (I32, [P, C.POINTER(Batch), P, P, C.POINTER(U64)]),
+        "phmm_device_set_wait": (I32, [P, U64, I64, C.POINTER(D), C.POINTER(D), C.POINTER(U32)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -33,7 +33,7 @@ CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-fvisibility=hidden", "-Wall", "-Wex
 CU_SOURCES = ["phmm_kernels.cu", "phmm_fwd32_m0.cu", "phmm_fwd32_m1.cu", "phmm_fwd32_m2.cu", "phmm_engine.cu",
               "phmm_noalloc.cu", "phmm_regionk.cu", "phmm_sw.cu"]
 CPP_SOURCES = ["phmm_tables.cpp", "phmm_plan.cpp", "phmm_capi.cpp", "phmm_serve.cpp", "phmm_region.cpp",
-               "phmm_tune.cpp"]
+               "phmm_tune.cpp", "phmm_multi.cpp"]
 
 
 def _headers() -> list[Path]:

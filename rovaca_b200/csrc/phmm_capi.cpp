@@ -264,6 +264,18 @@ phmm_status phmm_resident_results(phmm_resident* r, double* out, uint8_t* pair_f
     PHMM_GUARD_END
 }
 
+phmm_status phmm_resident_check_fp64(phmm_resident* r, double* out)
+{
+    PHMM_GUARD_BEGIN
+    phmm::clear_error();
+    if (!r || !r->slot) return set_error(PHMM_ERR_INVALID_ARGUMENT, "resident is null");
+    if (r->plan.out_total && !out) return set_error(PHMM_ERR_INVALID_ARGUMENT, "out is null");
+    std::string err;
+    phmm_status s = r->eng->check_fp64(*r->slot, r->plan, out, err);
+    return s == PHMM_OK ? PHMM_OK : set_error(s, err);
+    PHMM_GUARD_END
+}
+
 phmm_status phmm_fp32_fma_peak(phmm_engine* engine, double* scalar_tflops, double* packed_tflops)
 {
     PHMM_GUARD_BEGIN

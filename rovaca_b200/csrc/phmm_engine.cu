@@ -1231,6 +1231,93 @@ phmm_status Engine::time_fp32_class(Slot& s, const Plan& plan, int cls, int reps
     return PHMM_OK;
 }
 
+phmm_status Engine::check_fp64(Slot& s, const Plan& plan, double* out, std::string& err)
+{
+    PHMM_CK(cudaSetDevice(dev_));
+    cudaStream_t m = s.main;
+    // Rerun entries covering every pair: per work item and read, the item's run of haplotypes, in
+    // the FP64 class of the read's length (modes 1 and 2 only: the check kernels take any read).
+    std::vector<std::vector<RerunEntry>> per(kClasses64);
+    for (const WorkItem& it : plan.items) {
+        const RegionDesc& rg = plan.regions[it.region];
+        for (int k = 0; k < 2; ++k) {
+            const uint32_t r = it.read[k];
+            if (r == kNoRead) continue;
+            RerunEntry e;
+            e.out_idx = rg.out_off + (uint64_t)it.hap_lo * rg.n_reads + (r - rg.read_begin);
+            e.read = r;
+            e.hap = rg.hap_begin + it.hap_lo;
+            e.n_haps = (uint32_t)(it.hap_hi - it.hap_lo);
+            e.out_stride = rg.n_reads;
+            const uint64_t R = plan.read_off[r + 1] - plan.read_off[r];
+            per[class64_for_len(it.variant == kIntra ? 2 : 1, R)].push_back(e);
+        }
+    }
+    std::vector<RerunEntry> all;
+    std::vector<ClassDesc> cd(kClasses64);
+    for (int c = 0; c < kClasses64; ++c) {
+        cd[c] = ClassDesc{};
+        cd[c].rerun_off = (uint32_t)all.size();
+        cd[c].rerun_cap = cd[c].rerun_count = (uint32_t)per[c].size();
+        all.insert(all.end(), per[c].begin(), per[c].end());
+    }
+    if (all.size() > s.cap.rerun) {
+        err = "check entries exceed the slot's rerun capacity";
+        return PHMM_ERR_INTERNAL;
+    }
+    BatchView v{};
+    v.read_bases = s.d_rb;
+    v.read_q = s.d_rq;
+    v.read_i = s.d_ri;
+    v.read_d = s.d_rd;
+    v.read_c = s.d_rc;
+    v.read_off = s.d_read_off;
+    v.read_flags = s.d_read_flags;
+    v.hap_off = s.d_hap_off;
+    v.codes_inter = s.d_codes_inter;
+    v.codes_intra = s.d_codes_intra;
+    v.hap_flags = s.d_hap_flags;
+    v.regions = s.d_regions;
+    v.out = s.d_out;
+    v.pair_flags = nullptr;
+    // outputs NaN and codes rebuilt (the prep kernels of a run), then the check's own descriptors
+    PHMM_CK(cudaMemcpyAsync(s.d_desc, s.d_desc_pristine, kDescBytes, cudaMemcpyDeviceToDevice, m));
+    PHMM_CK(launch_prep(s.d_desc, s.d_hb, s.d_codes_inter, s.d_codes_intra, s.d_out, nullptr, sms_, m));
+    if (!all.empty())
+        PHMM_CK(cudaMemcpyAsync(s.d_rerun, all.data(), all.size() * sizeof(RerunEntry), cudaMemcpyHostToDevice, m));
+    PHMM_CK(cudaMemcpyAsync(s.d_classes + kClasses32, cd.data(), kClasses64 * sizeof(ClassDesc), cudaMemcpyHostToDevice,
+                            m));
+    const uint64_t warps = scratch_warps();
+    const unsigned int scr_cols = s.cap.scratch_cols ? (unsigned int)(s.cap.scratch_cols / warps) : 0u;
+    for (int c = 9; c < kClasses64; ++c) {
+        if (per[c].empty()) continue;
+        const bool multi = c % 9 == 8;
+        const int region = 1 + c / 9;
+        int occ = 0;
+        PHMM_CK(occupancy_f64_check(c, &occ));
+        uint64_t grid = std::min<uint64_t>(per[c].size(), (uint64_t)std::max(occ, 1) * sms_);
+        if (multi) grid = std::min(grid, scratch_offset_warps(region + 1) - scratch_offset_warps(region));
+        PassControl pc;
+        pc.cd = s.d_classes + kClasses32 + c;
+        pc.cd64 = s.d_classes + kClasses32;
+        pc.items = s.d_items;
+        pc.rerun = s.d_rerun;
+        pc.status = s.d_status;
+        pc.scratch = multi ? (void*)((char*)s.d_scratch + scratch_offset_warps(region) * scr_cols * 24) : nullptr;
+        pc.scratch_cols = scr_cols;
+        PHMM_CK(launch_f64_check(c, v, td_, pc, (int)std::max<uint64_t>(grid, 1), m));
+    }
+    if (plan.out_total) PHMM_CK(cudaMemcpyAsync(out, s.d_out, plan.out_total * sizeof(double), cudaMemcpyDeviceToHost, m));
+    unsigned int status = 0;
+    PHMM_CK(cudaMemcpyAsync(&status, s.d_status, sizeof(status), cudaMemcpyDeviceToHost, m));
+    PHMM_CK(cudaStreamSynchronize(m));
+    if (status != 0) {
+        err = "kernel status word " + std::to_string(status) + " in the all-FP64 check";
+        return PHMM_ERR_DEVICE_STATUS;
+    }
+    return PHMM_OK;
+}
+
 phmm_status Engine::profile_classes(Slot& s, const Plan& plan, float* class_ms, std::string& err)
 {
     PHMM_CK(cudaSetDevice(dev_));

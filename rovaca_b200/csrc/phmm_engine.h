@@ -133,6 +133,11 @@ public:
     // Runs an uploaded plan once with every class alone on the slot's main stream, timing each
     // launch with CUDA events (class_ms[kNumClasses], 0 where a class has no work).
     phmm_status profile_classes(Slot& s, const Plan& plan, float* class_ms, std::string& err);
+    // Recomputes every pair of an uploaded plan with the all-FP64 check arithmetic (plain multiply
+    // and add, FP64 end to end, every result flushed below 2^-1022) and copies the log10 values to
+    // out (the layout of compute(); pairs with an empty read or haplotype NaN).  The slot's results
+    // are overwritten; run the plan again to get the engine's own results back.
+    phmm_status check_fp64(Slot& s, const Plan& plan, double* out, std::string& err);
     // Measures the FP32 pass of one class alone on an uploaded plan: best of `reps` launches (ms).
     phmm_status time_fp32_class(Slot& s, const Plan& plan, int cls, int reps, float* best_ms, std::string& err);
     // Runs the tile-shape autotuner and installs its table (phmm_tune.cpp).

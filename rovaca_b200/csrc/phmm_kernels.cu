@@ -54,7 +54,7 @@ __global__ void reset_outputs_kernel(const BatchDesc* __restrict__ desc, double*
 // ------------------------------------------------------------------------------------------
 // One read against a run of haplotypes [g_lo, g_hi).
 // ------------------------------------------------------------------------------------------
-template <typename T, int K, int V, int PM, bool MULTI>
+template <typename T, int K, int V, int PM, bool MULTI, bool UNF = false>
 __device__ __forceinline__ void run_read(const BatchView& b, const ProbTables<T>& tb, const PassControl& pc,
                                          const SweepOut& so, uint32_t g_lo, uint32_t g_hi, int lane, T* scr)
 {
@@ -71,7 +71,7 @@ __device__ __forceinline__ void run_read(const BatchView& b, const ProbTables<T>
     if (!MULTI) {
         const int pad = kWarp * K - R;
         load_rows<T, K, V, PM>(L, b, tb, roff, R, 0, pad, lane);
-        sweep<T, K, V, PM, false, false>(L, b, pc, so, g_lo, g_hi, scr, lane, lane * K <= pad);
+        sweep<T, K, V, PM, false, false, UNF>(L, b, pc, so, g_lo, g_hi, scr, lane, lane * K <= pad);
     } else {
         constexpr int SR = kWarp * K;  // rows per stripe
         const int stripes = (R + SR - 1) / SR;
@@ -80,11 +80,11 @@ __device__ __forceinline__ void run_read(const BatchView& b, const ProbTables<T>
             load_rows<T, K, V, PM>(L, b, tb, roff, R, s * SR, pad, lane);
             const bool above_row0 = (s == 0) && (lane * K <= pad);
             if (s == 0)
-                sweep<T, K, V, PM, false, true>(L, b, pc, so, g_lo, g_hi, scr, lane, above_row0);
+                sweep<T, K, V, PM, false, true, UNF>(L, b, pc, so, g_lo, g_hi, scr, lane, above_row0);
             else if (s == stripes - 1)
-                sweep<T, K, V, PM, true, false>(L, b, pc, so, g_lo, g_hi, scr, lane, above_row0);
+                sweep<T, K, V, PM, true, false, UNF>(L, b, pc, so, g_lo, g_hi, scr, lane, above_row0);
             else
-                sweep<T, K, V, PM, true, true>(L, b, pc, so, g_lo, g_hi, scr, lane, above_row0);
+                sweep<T, K, V, PM, true, true, UNF>(L, b, pc, so, g_lo, g_hi, scr, lane, above_row0);
             __syncwarp();  // lane 31's scratch row is read by lane 0 in the next stripe
         }
     }
@@ -106,7 +106,9 @@ constexpr int min_blocks64()
     return PM == PM_ALL && K >= 7 ? PHMM_F64_MIN_WARPS : 1;
 }
 
-template <int K, int V, int PM, bool MULTI>
+// UNF: the all-FP64 check arithmetic (plain multiply and add), used to measure the error of every
+// likelihood; the recompute pass proper uses the reference's contracted arithmetic.
+template <int K, int V, int PM, bool MULTI, bool UNF = false>
 __global__ void __launch_bounds__(kFwdBlock, min_blocks64<K, PM>()) fwd_f64_kernel(BatchView b, ProbTables<double> tb, PassControl pc)
 {
     const int lane = threadIdx.x & (kWarp - 1);
@@ -124,7 +126,7 @@ __global__ void __launch_bounds__(kFwdBlock, min_blocks64<K, PM>()) fwd_f64_kern
         so.out_base = e.out_idx;
         so.out_stride = e.out_stride;
         so.read = e.read;
-        run_read<double, K, V, PM, MULTI>(b, tb, pc, so, e.hap, e.hap + e.n_haps, lane, scr);
+        run_read<double, K, V, PM, MULTI, UNF>(b, tb, pc, so, e.hap, e.hap + e.n_haps, lane, scr);
     }
 }
 
@@ -185,6 +187,16 @@ typedef void (*F64Kernel)(BatchView, ProbTables<double>, PassControl);
 static const F64Kernel kF64[kClasses64] = {PHMM_ROW64(kInter, PM_ALL), PHMM_ROW64(kInter, PM_ROW),
                                            PHMM_ROW64(kIntra, PM_ROW)};
 
+// All-FP64 check kernels: the same shapes with plain multiply/add, per-row gap parameters (any
+// read), inter and intra variants (FP64 classes of modes 1 and 2).
+#define PHMM_ROW64_CHECK(V)                                                                               \
+    fwd_f64_kernel<1, V, PM_ROW, false, true>, fwd_f64_kernel<2, V, PM_ROW, false, true>,                 \
+        fwd_f64_kernel<3, V, PM_ROW, false, true>, fwd_f64_kernel<4, V, PM_ROW, false, true>,             \
+        fwd_f64_kernel<5, V, PM_ROW, false, true>, fwd_f64_kernel<6, V, PM_ROW, false, true>,             \
+        fwd_f64_kernel<7, V, PM_ROW, false, true>, fwd_f64_kernel<8, V, PM_ROW, false, true>,             \
+        fwd_f64_kernel<8, V, PM_ROW, true, true>
+static const F64Kernel kF64Check[2 * 9] = {PHMM_ROW64_CHECK(kInter), PHMM_ROW64_CHECK(kIntra)};
+
 cudaError_t launch_prep(const BatchDesc* desc, const uint8_t* hap_bases, uint32_t* codes_inter, uint32_t* codes_intra,
                         double* out, uint8_t* flags, int num_sms, cudaStream_t st)
 {
@@ -206,6 +218,20 @@ cudaError_t launch_fwd(int precision, int cls, const BatchView& b, const ProbTab
     }
     kF64[cls]<<<grid, kFwdBlock, 0, st>>>(b, td, pc);
     return cudaGetLastError();
+}
+
+cudaError_t launch_f64_check(int cls, const BatchView& b, const ProbTables<double>& td, const PassControl& pc, int grid,
+                             cudaStream_t st)
+{
+    if (cls < 9 || cls >= kClasses64 || grid <= 0) return cudaErrorInvalidValue;
+    kF64Check[cls - 9]<<<grid, kFwdBlock, 0, st>>>(b, td, pc);
+    return cudaGetLastError();
+}
+
+cudaError_t occupancy_f64_check(int cls, int* blocks_per_sm)
+{
+    if (cls < 9 || cls >= kClasses64) return cudaErrorInvalidValue;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kF64Check[cls - 9], kFwdBlock, 0);
 }
 
 cudaError_t occupancy(int precision, int cls, int* blocks_per_sm)

@@ -24,6 +24,11 @@ cudaError_t launch_prep(const BatchDesc* desc, const uint8_t* hap_bases, uint32_
 cudaError_t launch_fwd(int precision, int cls, const BatchView& b, const ProbTables<float>& tf,
                        const ProbTables<double>& td, const PassControl& pc, int grid, cudaStream_t st);
 cudaError_t occupancy(int precision, int cls, int* blocks_per_sm);
+// All-FP64 check pass of FP64 class `cls` (9..kClasses64-1: modes 1 and 2, any read) over its rerun
+// segment, with plain multiply/add instead of the reference's contracted arithmetic.
+cudaError_t launch_f64_check(int cls, const BatchView& b, const ProbTables<double>& td, const PassControl& pc, int grid,
+                             cudaStream_t st);
+cudaError_t occupancy_f64_check(int cls, int* blocks_per_sm);
 // 256-thread blocks, each thread running 16 independent FMA chains (scalar FFMA, or packed FFMA2
 // with two FMAs per instruction) for iters steps.
 cudaError_t launch_fma_peak(float* sink, int blocks, int iters, bool packed, cudaStream_t st);

@@ -197,7 +197,8 @@ def default_tiles() -> "_lib.TileTable":
 
 
 def class32(mode: int, kh: int, multi: bool = False) -> int:
-    """FP32 kernel class of a mode (0 inter constant gaps, 1 inter per-row, 2 intra) and shape."""
+    """FP32 kernel class of a mode (0 inter with constant gaps and insertion = deletion quality, 1 other
+    inter, 2 intra) and shape."""
     return mode * 13 + (4 + kh if multi else kh - 1)
 
 
@@ -504,6 +505,14 @@ class ResidentBatch:
         check(self._lib.phmm_resident_results(self._h, _ptr(out), _ptr(fl)))
         return out, fl
 
+    def check_fp64(self) -> np.ndarray:
+        """phmm_resident_check_fp64: every pair of the batch recomputed on the device with the
+        all-FP64 check arithmetic (the oracle's fp64_only model); overwrites the resident's results
+        (run() again before results())."""
+        out = np.empty(self.batch.out_size, np.float64)
+        check(self._lib.phmm_resident_check_fp64(self._h, _ptr(out)))
+        return out
+
     def close(self) -> None:
         if getattr(self, "_h", None):
             check(self._lib.phmm_resident_destroy(self._h))
@@ -513,6 +522,70 @@ class ResidentBatch:
         return self
 
     def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def partition_regions(batch: PackedBatch, n_parts: int) -> tuple[np.ndarray, np.ndarray]:
+    """phmm_partition_regions (host only): (part of every region, cells of every part), regions
+    split by longest-processing-time greedy on their cells."""
+    part = np.empty(batch.n_regions, np.uint32)
+    cells = np.empty(n_parts, np.uint64)
+    b = batch.as_c()
+    check(_lib.load().phmm_partition_regions(C.byref(b), n_parts, _ptr(part), _ptr(cells)))
+    return part, cells
+
+
+class DeviceSet:
+    """One engine per listed device behind one handle (phmm_device_set_*): batches split across
+    the devices by region, serving requests routed to the least-loaded device."""
+
+    def __init__(self, devices: Sequence[int], use_cuda_graph: bool = True, autotune: bool = True,
+                 hbm_budget_bytes: int = 0, chunk_cells: int = 0):
+        self._lib = _lib.load()
+        devs = (C.c_int32 * len(devices))(*devices)
+        cfg = _lib.Config(0, int(use_cuda_graph), int(autotune), 0, hbm_budget_bytes, chunk_cells)
+        h = C.c_void_p()
+        check(self._lib.phmm_device_set_create(devs, len(devices), C.byref(cfg), C.byref(h)))
+        self._h = h
+        self.devices = list(devices)
+
+    def compute(self, batch: PackedBatch, want_flags: bool = False):
+        """As Engine.compute, over every device of the set."""
+        n = batch.out_size
+        out = np.empty(n, np.float64)
+        flags = np.empty(n, np.uint8) if want_flags else None
+        st = _lib.Stats()
+        b = batch.as_c()
+        check(self._lib.phmm_device_set_compute_regions(self._h, C.byref(b), _ptr(out), _ptr(flags), C.byref(st)))
+        return out, flags, st.as_dict()
+
+    def submit(self, region: PackedBatch, out: np.ndarray, flags: np.ndarray | None = None) -> int:
+        t = C.c_uint64()
+        b = region.as_c()
+        check(self._lib.phmm_device_set_submit(self._h, C.byref(b), _ptr(out), _ptr(flags), C.byref(t)))
+        return t.value
+
+    def wait(self, ticket: int, timeout_us: int = -1) -> tuple[float, float, int]:
+        """(queued µs, total µs, index of the member that ran the request)."""
+        q, tot, dev = C.c_double(), C.c_double(), C.c_uint32()
+        check(self._lib.phmm_device_set_wait(self._h, ticket, timeout_us, C.byref(q), C.byref(tot), C.byref(dev)))
+        return q.value, tot.value, dev.value
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            check(self._lib.phmm_device_set_destroy(self._h))
+            self._h = None
+
+    def __enter__(self) -> "DeviceSet":
+        return self
+
+    def __exit__(self, *exc) -> None:
         self.close()
 
     def __del__(self):
@@ -559,4 +632,4 @@ def call_pairhmm(haplotypes, reads, base_quals, mapq, min_quality_threshold: int
 
 
 __all__ = ["Engine", "Region", "PackedBatch", "PhmmError", "schedule_pairhmm", "call_pairhmm", "default_engine",
-           "plan_summary", "compute_noalloc"]
+           "plan_summary", "compute_noalloc", "partition_regions", "DeviceSet"]

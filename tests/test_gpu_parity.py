@@ -342,3 +342,20 @@ def test_autotune_installs_a_valid_table(engine_direct):
         a, _, _ = eng.compute(pb)
         b, _, _ = engine_direct.compute(pb)
         assert np.array_equal(a, b, equal_nan=True)
+
+
+@pytest.mark.parametrize("group", ["debug", "config0", "config1", "config2", "edge"])
+def test_fp64_check_equals_the_all_fp64_oracle(engine, oracle, ref_regions, group):
+    """phmm_resident_check_fp64 recomputes every pair with the all-FP64 model on the device; it
+    equals the CPU all-FP64 oracle pair for pair, and the resident gives its own results again after
+    the next run."""
+    pb, _ = ref_regions[group]
+    want, _ = oracle.batch(pb, fp64_only=True)
+    with engine.resident(pb, want_flags=True) as res:
+        own, own_flags = res.results()
+        got = res.check_fp64()
+        assert_same_values(got, want, EXACT, group)
+        res.run(1)
+        again, again_flags = res.results()
+    assert np.array_equal(again, own, equal_nan=True)
+    assert np.array_equal(again_flags, own_flags)

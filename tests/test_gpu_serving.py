@@ -295,9 +295,10 @@ def _oracle_region_lk(oracle, haps, reads, quals, mapq, thr, pcr, fp64_only):
     return lk.reshape(len(haps), len(reads))
 
 
-def test_genotyping_on_device_and_concordance(engine, oracle):
-    """Allele marginalisation and diploid genotype likelihoods on the GPU equal the checker's
-    restatement on the same normalised matrix bit for bit; the calls are identical to the calls made
+def test_genotyping_on_device_and_concordance(engine, oracle, genotype_ref):
+    """Allele marginalisation and diploid genotype likelihoods on the GPU equal the reference's own
+    genotyping code (compiled from its sources) and the checker's restatement on the same normalised
+    matrix bit for bit; the calls are identical to the calls made
     from the reference's own likelihoods (its FP32 pass with the FP64 fallback, which the engine
     reproduces pair for pair); against calls from all-FP64 likelihoods a call may differ only where
     the two genotypes' FP64 likelihoods are a near-tie (within 1e-3 log10)."""
@@ -318,6 +319,9 @@ def test_genotyping_on_device_and_concordance(engine, oracle):
             wgl = G.genotype_likelihoods(walk)
             assert np.array_equal(gl, wgl)
             assert best == G.best_genotype(wgl)
+            ralk, rgl = genotype_ref.genotype(mat[:, :K], ha, A)
+            assert np.array_equal(alk[:, :K], ralk, equal_nan=True)
+            assert np.array_equal(gl, rgl, equal_nan=True)
         lens = [len(x) for x in r["reads"]]
         lk_ref = _oracle_region_lk(oracle, r["haplotypes"], r["reads"], r["quals"], r["mapq"], 18, 3, False)
         res_ref, _, keep_ref = G.genotype_region(lk_ref, lens, r["events"])
@@ -353,3 +357,30 @@ def test_genotyping_only_results_come_back(engine):
         engine.submit_region(r["haplotypes"], r["reads"], r["quals"], r["mapq"], 18, 0,
                              events=[(50, np.zeros(len(r["haplotypes"]), np.int8))])
     assert e.value.name == "PHMM_ERR_LIMIT_EXCEEDED"
+
+
+def test_device_set_equals_one_engine():
+    """A device set of two engines (both on device 0 here: one GPU per test box) splits a batch by
+    region cells and returns exactly one engine's results, region blocks in place; serving requests
+    go to the less loaded member and return the same bits."""
+    from rovaca_b200 import DeviceSet, partition_regions
+
+    pb = synth.config1(24, seed=33)
+    with Engine(device=0, autotune=False) as eng:
+        want, want_fl, _ = eng.compute(pb, want_flags=True)
+    part, load = partition_regions(pb, 2)
+    assert set(part.tolist()) == {0, 1}
+    with DeviceSet([0, 0], autotune=False) as ds:
+        got, fl, st = ds.compute(pb, want_flags=True)
+        assert np.array_equal(got, want, equal_nan=True)
+        assert np.array_equal(fl, want_fl)
+        assert st["cells"] == pb.cells() and st["regions"] == pb.n_regions
+        got2, _, _ = ds.compute(pb)  # staging buffers reused
+        assert np.array_equal(got2, want, equal_nan=True)
+        offs = pb.out_offsets()
+        outs = [np.empty(offs[g + 1] - offs[g]) for g in range(pb.n_regions)]
+        tickets = [ds.submit(pb.subset([g]), outs[g]) for g in range(pb.n_regions)]
+        members = [ds.wait(t)[2] for t in tickets]
+        assert set(members) == {0, 1}
+        for g in range(pb.n_regions):
+            assert np.array_equal(outs[g], want[offs[g]:offs[g + 1]], equal_nan=True), g
