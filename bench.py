@@ -138,6 +138,71 @@ def reference_gcups(batch, regions, threads: int) -> tuple[float, float]:
     return cells / dt / 1e9, dt
 
 
+# The FP32 -> FP64 switch in log10 space: an FP32 sum accepted by the switch (>= 1e-28f) reports at
+# least log10(1e-28f) - log10(2^120 as the float constant); a likelihood below this value can only
+# have come from the FP64 recompute.
+LOG10_SWITCH = float(np.log10(np.float64(np.float32(1e-28))) - np.float64(np.float32(36.1236000061)))
+ERR_EDGES = [0.0, 1e-12, 1e-10, 1e-8, 1e-6, 1e-5, 1e-4, np.inf]
+
+
+def error_report(got: np.ndarray, flags: np.ndarray, f64: np.ndarray) -> dict:
+    """|log10 error| of every pair against the all-FP64 model (the pairs with an empty read or
+    haplotype, NaN on both sides, are counted apart)."""
+    fin = np.isfinite(got) & np.isfinite(f64)
+    err = np.abs(got[fin] - f64[fin])
+    fl = flags[fin].astype(bool)
+    hist = np.histogram(err, bins=ERR_EDGES)[0]
+    return {"pairs": int(err.size), "pairs_total": int(got.size),
+            "nan_pairs_agree": bool(np.array_equal(np.isnan(got), np.isnan(f64))),
+            "max": float(err.max()) if err.size else 0.0,
+            "p99": float(np.percentile(err, 99)) if err.size else 0.0,
+            "p50": float(np.percentile(err, 50)) if err.size else 0.0,
+            "over_1e-4": int(np.sum(err > 1e-4)),
+            "max_fp32_pairs": float(err[~fl].max()) if (~fl).any() else 0.0,
+            "max_fp64_pairs": float(err[fl].max()) if fl.any() else 0.0,
+            "histogram": {f"<{hi:g}" if hi != np.inf else ">=1e-4": int(c) for hi, c in zip(ERR_EDGES[1:], hist)},
+            "model": "all-FP64 check arithmetic on the device (phmm_resident_check_fp64), equal to the CPU "
+                     "all-FP64 oracle pair for pair in the GPU tests"}
+
+
+def reference_whole_batch(batch, got: np.ndarray, flags: np.ndarray, threads: int) -> dict:
+    """Every region of the batch through the reference's own schedule_pairhmm (oracle/_ref, AVX-512
+    path, `threads` host threads), compared with the engine pair by pair; and every pair whose
+    reference likelihood lies below the FP32 -> FP64 switch (a value only the FP64 recompute can
+    give) checked against the engine's FP64 flag."""
+    from oracle import Ref
+
+    ref = Ref()
+    offs = batch.out_offsets()
+    want = np.empty(batch.out_size, np.float64)
+
+    def work(g):
+        want[offs[g]:offs[g + 1]] = ref.schedule_region(batch, g, 0.02, 0.02).reshape(-1)
+
+    t = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=threads, initializer=ref.init_thread) as ex:
+        list(ex.map(work, range(batch.n_regions)))
+    dt = time.perf_counter() - t
+    fin = np.isfinite(got) & np.isfinite(want)
+    d = np.abs(got - want)
+    fl = flags.astype(bool)
+    only_f64 = fin & (want < LOG10_SWITCH)
+    near = fin & (np.abs(want - LOG10_SWITCH) < 1e-5)
+    return {"pairs": int(fin.sum()), "nan_pairs_agree": bool(np.array_equal(np.isnan(got), np.isnan(want))),
+            "max_abs_diff": float(d[fin].max()) if fin.any() else 0.0,
+            "pairs_bit_equal_le_1e-12": int(np.sum(d[fin] <= 1e-12)),
+            "pairs_diff_over_1e-12": int(np.sum(d[fin] > 1e-12)),
+            "pairs_diff_over_1e-5": int(np.sum(d[fin] > 1e-5)),
+            "reference_pairs_only_fp64": int(only_f64.sum()),
+            "fp64_flag_disagreements": int(np.sum(only_f64 & ~fl)),
+            "engine_fp64_pairs": int(fl.sum()),
+            "pairs_within_1e-5_of_switch": int(near.sum()),
+            "reference_seconds": round(dt, 2), "reference_gcups": round(batch.cells() / dt / 1e9, 2),
+            "threads": threads,
+            "note": "pairs differing by more than 1e-12 are pairs the reference leaves to its intra kernel "
+                    "(ungrouped by its SIMD packing), which rounds the prior and the log10 once more"}
+
+
 # ---- ranks --------------------------------------------------------------------------------------
 
 def shard_seed(rank: int) -> int:
@@ -163,6 +228,16 @@ def weak_scaling_value(dist, cells_per_step: float, steps: int, device_ms: float
     dev_ms = rank_reduce(dist, device_ms, "max", device)
     total = rank_reduce(dist, float(cells_per_step), "sum", device) * steps
     return total / (dev_ms / 1e3) / 1e9, dev_ms / steps
+
+
+def strong_scaling_regions(batch, rank: int, world: int) -> list[int]:
+    """The regions of one shared batch that rank `rank` of `world` computes in the strong-scaling
+    leg: the rank's part of phmm_partition_regions (longest-processing-time greedy on region cells,
+    the same split on every rank, nothing exchanged)."""
+    from rovaca_b200 import partition_regions
+
+    part, _ = partition_regions(batch, world)
+    return [int(g) for g in np.nonzero(part == rank)[0]]
 
 
 def run_reference(args, rank: int, world: int) -> None:
@@ -201,19 +276,31 @@ def run_reference(args, rank: int, world: int) -> None:
 
 # ---- our arm ----------------------------------------------------------------------------------
 
-def serving_latency(engine, batch, load: float, capacity_regions_per_s: float, seconds: float, seed: int):
-    """Poisson arrivals of the batch's regions at `load` x capacity; returns latency percentiles,
-    the sustained GCUPS of the completed requests and the serving loop's own counters."""
+class RequestPool:
+    """Every region of a batch as a request of its own (host structs built once): the serving legs
+    draw each arriving request's region uniformly at random from it, i.e. from the batch's size
+    distribution."""
+
+    def __init__(self, batch):
+        self.regions = [batch.subset([g]) for g in range(batch.n_regions)]
+        self.structs = [r.as_c() for r in self.regions]
+        self.cells = [r.cells() for r in self.regions]
+        self.sizes = [r.out_size for r in self.regions]
+
+
+def serving_latency(engine, pool: RequestPool, load: float, capacity_regions_per_s: float, seconds: float, seed: int):
+    """Poisson arrivals at `load` x capacity, each request a region drawn at random from the pool;
+    returns latency percentiles, the sustained GCUPS of the completed requests and the serving
+    loop's own counters."""
     from rovaca_b200 import _lib
 
     lib = _lib.load()
     rng = np.random.default_rng(seed)
-    regions = [batch.subset([g]) for g in range(min(batch.n_regions, 400))]
-    structs = [r.as_c() for r in regions]
-    cells = [r.cells() for r in regions]
-    sizes = [r.out_size for r in regions]
+    structs, cells, sizes = pool.structs, pool.cells, pool.sizes
     rate = load * capacity_regions_per_s
-    gaps = rng.exponential(1.0 / rate, int(rate * seconds * 1.5) + 16)
+    n_req = int(rate * seconds * 1.5) + 16
+    gaps = rng.exponential(1.0 / rate, n_req)
+    picks = rng.integers(0, len(structs), n_req)
     before = engine.server_stats()
     outs, tickets, done_cells = [], [], 0
     t0 = time.perf_counter()
@@ -226,7 +313,7 @@ def serving_latency(engine, batch, load: float, capacity_regions_per_s: float, s
             time.sleep(min(next_t - now, 0.002))
             continue
         lag = max(lag, now - next_t)
-        g = k % len(regions)
+        g = int(picks[k % n_req])
         out = np.empty(sizes[g])
         t = C.c_uint64()
         rc = lib.phmm_submit(engine._h, C.byref(structs[g]), out.ctypes.data, None, C.byref(t))
@@ -259,61 +346,139 @@ def serving_latency(engine, batch, load: float, capacity_regions_per_s: float, s
             "max_setup_ms_so_far": round(after["max_setup_ms"], 2), "max_host_ms_so_far": round(after["max_host_ms"], 2)}
 
 
-def underflow_stress(engine, n_regions: int = 100, sample: int = 2) -> dict:
-    """The underflow-stress configuration (200 reads of 250 bp, base quality U[2,15], 5% errors, 16
-    haplotypes of 800-1,000 bp with 5-10 indels): FP64 rerun fraction, GCUPS, and the FP32-vs-FP64
-    log10 error distribution on a sample of regions against the all-FP64 oracle."""
-    from oracle import Oracle
+def underflow_stress(engine, steps: int, warmup: int, cpu_threads: int | None, n_regions: int = 500) -> dict:
+    """The underflow-stress configuration at its stated size (500 regions x 200 reads of 250 bp, base
+    quality U[2,15], 5% errors, 16 haplotypes of 800-1,000 bp with 5-10 indels): FP64 rerun fraction,
+    GCUPS resident and end to end, every pair's log10 error against the all-FP64 model, and (rank 0
+    of a one-GPU run) every pair against the reference's own schedule_pairhmm on the host cores."""
     from rovaca_b200 import synth
 
     pb = synth.config2(n_regions, seed=2)
-    engine.compute(pb, want_flags=True)  # warm-up in the measured form (arena sizes, captured graphs)
-    out, flags, st = engine.compute(pb, want_flags=True)
-    orc = Oracle()
-    sub = pb.subset(list(range(sample)))
-    offs = pb.out_offsets()
-    f64, _ = orc.batch(sub, fp64_only=True)
-    _, used = orc.batch(sub)  # the reference's FP32 -> FP64 decisions, pair by pair
-    got = out[:offs[sample]]
-    fl = flags[:offs[sample]].astype(bool)
-    err = np.abs(got - f64)
-    edges = [0.0, 1e-12, 1e-10, 1e-8, 1e-6, 1e-4, np.inf]
-    hist = np.histogram(err, bins=edges)[0]
-    return {"regions": n_regions, "cells": int(st["cells"]), "gcups_device": round(st["cells"] / st["device_ms"] / 1e6, 1),
+    cells = pb.cells()
+    with engine.resident(pb, want_flags=True) as res:
+        res.run(warmup)
+        st = res.run(steps)
+        out, flags = res.results()
+        f64 = res.check_fp64()
+    pinned = pb.pinned()
+    e2e_out = np.empty(pb.out_size)
+    engine.compute(pinned, out=e2e_out)
+    t = time.perf_counter()
+    engine.compute(pinned, out=e2e_out)
+    e2e_s = time.perf_counter() - t
+    rep_ = {"regions": n_regions, "pairs": int(pb.out_size), "cells": int(cells),
+            "gcups_device": round(cells * steps / st["device_ms"] / 1e6, 1),
+            "gcups_e2e": round(cells / e2e_s / 1e9, 1),
+            "e2e_equal_resident": bool(np.array_equal(e2e_out, out, equal_nan=True)),
             "fp64_rerun_fraction": round(float(flags.mean()), 4),
-            "fp64_switch_mismatches_vs_reference": int(np.sum(fl != used)),
-            "abs_err_log10_vs_fp64": {"max": float(err.max()), "p99": float(np.percentile(err, 99)),
-                                      "max_fp32_pairs": float(err[~fl].max()) if (~fl).any() else 0.0,
-                                      "max_fp64_pairs": float(err[fl].max()) if fl.any() else 0.0,
-                                      "histogram": {f"<{hi:g}" if hi != np.inf else ">=1e-4": int(c)
-                                                    for hi, c in zip(edges[1:], hist)},
-                                      "sample_pairs": int(err.size)},
+            "abs_err_log10_vs_fp64": error_report(out, flags, f64),
             "quality_preprocessing": "vector-API semantics: raw qualities, no cap, PCR NONE"}
+    if cpu_threads:
+        # the reference runs this shape at a few GCUPS on the host (most pairs in FP64): a seeded
+        # tenth of the regions, every pair of them
+        ref_regions = min(50, n_regions)
+        end = pb.out_offsets()[ref_regions]
+        rep_["vs_reference"] = reference_whole_batch(pb.subset(list(range(ref_regions))), out[:end], flags[:end],
+                                                     cpu_threads)
+        rep_["vs_reference"]["regions"] = f"regions 0-{ref_regions - 1} of {n_regions}"
+    return rep_
 
 
-def wgs_mixture(engine, fraction: float = 0.05) -> dict:
+def wgs_mixture(engine, fraction: float, cpu_threads: int | None, sample: int = 200) -> dict:
     """A seeded share of the WGS-like mixture (depth lognormal, median 60, sigma 0.5, clipped to
     [5, 2000]; 150 bp reads (90%) or 250 bp; haplotypes geometric, mean 6, max 128, of 200-1,200 bp;
-    2% of regions from the underflow-stress regime): batched GCUPS end to end from pinned buffers."""
-    from rovaca_b200 import synth
-
-    pb = synth.make(4, scale=fraction, seed=4).pinned()
-    engine.compute(pb)
-    t = time.perf_counter()
-    _, _, st = engine.compute(pb)
-    el = time.perf_counter() - t
-    return {"regions": int(pb.n_regions), "cells": int(st["cells"]), "share_of_200k_regions": fraction,
-            "gcups_e2e": round(st["cells"] / el / 1e9, 1), "gcups_device": round(st["cells"] / st["device_ms"] / 1e6, 1),
-            "fp64_pairs": int(st["pairs_f64"]), "pairs": int(st["pairs"])}
-
-
-def genotyping_run(engine, n_regions: int = 400, check: int = 20) -> dict:
-    """Region API with genotyping events on the GPU (read preparation, likelihoods, normalise and
-    filter, allele marginalisation, diploid genotype likelihoods, calls): throughput through the
-    serving loop, and genotype concordance against calls from all-FP64 likelihoods on a sample."""
-    from oracle import Oracle
+    2% of regions from the underflow-stress regime): batched GCUPS end to end from pinned buffers,
+    the plain one-region-per-call form on a seeded sample of regions, the reference's AVX-512 host
+    path on the same sample (host threads), and genotype concordance on that sample -- calls from the
+    engine's likelihoods against calls from the reference's likelihoods (its schedule_pairhmm), both
+    normalised and filtered and genotyped by the reference's own genotyping code, for a biallelic
+    event (haplotype 0 against the rest) and a multi-allelic one (haplotype h to allele h mod 4)."""
+    from oracle import GenotypeRef, Ref, ref_available
     from oracle import genotype as G
     from rovaca_b200 import synth
+
+    pb = synth.make(4, scale=fraction, seed=4)
+    pinned = pb.pinned()
+    out = np.empty(pb.out_size)
+    engine.compute(pinned, out=out)
+    t = time.perf_counter()
+    _, _, st = engine.compute(pinned, out=out)
+    el = time.perf_counter() - t
+    rng = np.random.default_rng(44)
+    pick = sorted(int(g) for g in rng.choice(pb.n_regions, min(sample, pb.n_regions), replace=False))
+    plain_regions = [pb.subset([g]).pinned() for g in pick]
+    plain_cells = sum(r.cells() for r in plain_regions)
+    for r in plain_regions[:5]:
+        engine.compute(r)
+    t = time.perf_counter()
+    for r in plain_regions:
+        engine.compute(r)
+    plain_s = time.perf_counter() - t
+    res = {"regions": int(pb.n_regions), "cells": int(st["cells"]), "share_of_200k_regions": fraction,
+           "gcups_e2e": round(st["cells"] / el / 1e9, 1), "gcups_device": round(st["cells"] / st["device_ms"] / 1e6, 1),
+           "fp64_pairs": int(st["pairs_f64"]), "pairs": int(st["pairs"]),
+           "plain_gcups_e2e": round(plain_cells / plain_s / 1e9, 2),
+           "sample_regions": len(pick), "sample_cells": int(plain_cells)}
+    if not (cpu_threads and ref_available()):
+        return res
+    sub = pb.subset(pick)
+    ref = Ref()
+    offs = sub.out_offsets()
+    want = np.empty(sub.out_size)
+
+    def work(g):
+        want[offs[g]:offs[g + 1]] = ref.schedule_region(sub, g, 0.02, 0.02).reshape(-1)
+
+    t = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=cpu_threads, initializer=ref.init_thread) as ex:
+        list(ex.map(work, range(sub.n_regions)))
+    ref_s = time.perf_counter() - t
+    full_offs = pb.out_offsets()
+    got = np.concatenate([out[full_offs[g]:full_offs[g + 1]] for g in pick])
+    gref = GenotypeRef()
+    events = same = 0
+    max_gl = 0.0
+    read0 = np.concatenate([[0], np.cumsum(sub.n_reads.astype(np.int64))])
+    read_len = np.diff(sub.read_off.astype(np.int64))
+    for k, g in enumerate(pick):
+        M, N = int(sub.n_haps[k]), int(sub.n_reads[k])
+        lens = read_len[read0[k]:read0[k] + N].tolist()
+        mine, keep_m = G.normalize_filter(got[offs[k]:offs[k + 1]].reshape(M, N), lens)
+        theirs, keep_t = G.normalize_filter(want[offs[k]:offs[k + 1]].reshape(M, N), lens)
+        km, kt = int(keep_m.sum()), int(keep_t.sum())
+        for A, ha in ((min(2, M), [0] + [1] * (M - 1)), (min(4, M), [h % 4 for h in range(M)])):
+            _, gl_m = gref.genotype(mine[:, :km], np.array(ha, np.int8), A)
+            _, gl_t = gref.genotype(theirs[:, :kt], np.array(ha, np.int8), A)
+            events += 1
+            same += int(G.best_genotype(gl_m) == G.best_genotype(gl_t))
+            if km == kt:
+                max_gl = max(max_gl, float(np.max(np.abs(gl_m - gl_t))))
+    d = np.abs(got - want)
+    fin = np.isfinite(d)
+    res.update({"reference_host_gcups": round(sub.cells() / ref_s / 1e9, 2), "reference_threads": cpu_threads,
+                "reference_seconds": round(ref_s, 2),
+                "max_abs_diff_vs_reference_on_sample": float(d[fin].max()) if fin.any() else 0.0,
+                "genotype_events_checked": events, "genotype_calls_identical": same,
+                "max_abs_gl_diff": max_gl,
+                "concordance": "calls from the engine's and from the reference's likelihoods, normalised and filtered, "
+                               "genotyped by the reference's own code (oracle/_ref/libgenotype_ref.so)"})
+    return res
+
+
+def genotyping_run(engine, n_regions: int = 400, cpu_threads: int | None = None) -> dict:
+    """Region API with genotyping events on the GPU (read preparation, likelihoods, normalise and
+    filter, allele marginalisation, diploid genotype likelihoods, calls): throughput through the
+    serving loop; then every event checked twice -- the GPU's allele and genotype likelihoods against
+    the reference's own genotyping code (compiled from its sources) on the GPU's normalised matrix,
+    and the GPU's call against the call the reference makes from its own likelihoods (its
+    schedule_pairhmm on the prepared reads, normalised and filtered, then its genotyping code) -- and
+    the calls from all-FP64 likelihoods beside them."""
+    from oracle import GenotypeRef, Ref, ref_available
+    from oracle import genotype as G
+    import ctypes as C
+
+    from rovaca_b200 import _lib, synth
+    from rovaca_b200.pairhmm import PackedBatch, Region
 
     regions = synth.genotyping_regions(n_regions, seed=21)
     cells = sum(sum(len(h) for h in r["haplotypes"]) * sum(len(x) for x in r["reads"]) for r in regions)
@@ -326,15 +491,16 @@ def genotyping_run(engine, n_regions: int = 400, check: int = 20) -> dict:
     for tk in tickets:
         tk.wait()
     el = time.perf_counter() - t
-    orc = Oracle()
-    import ctypes as C
+    out = {"regions": n_regions, "events": int(sum(len(r["events"]) for r in regions)),
+           "regions_per_s": round(n_regions / el, 1), "gcups": round(cells / el / 1e9, 2),
+           "form": "phmm_submit_region with events, genotype likelihoods only back to the host (PCR CONSERVATIVE, Q18)"}
 
-    from rovaca_b200 import _lib
-    from rovaca_b200.pairhmm import PackedBatch, Region
-
+    # the same regions again with the normalised matrix and allele likelihoods back
+    full = [engine.submit_region(r["haplotypes"], r["reads"], r["quals"], r["mapq"], 18, 3, events=r["events"],
+                                 want_allele_lk=True) for r in regions]
     lib = _lib.load()
-    same, same64, total, truth_hits, max_gl, max_tie = 0, 0, 0, 0, 0.0, 0.0
-    for r, tk in zip(regions[:check], tickets[:check]):
+    prepared = []
+    for r in regions:
         qs, gops = [], []
         for rd, q, mq in zip(r["reads"], r["quals"], r["mapq"]):
             n = len(rd)
@@ -344,29 +510,62 @@ def genotyping_run(engine, n_regions: int = 400, check: int = 20) -> dict:
             lib.phmm_host_pcr_model(rd, n, gop, 3)
             qs.append(bytes(qq))
             gops.append(bytes(gop))
-        pb = PackedBatch.from_regions([Region(r["haplotypes"], r["reads"], qs, gops, gops,
-                                              [bytes([10]) * len(x) for x in r["reads"]])])
-        lens = [len(x) for x in r["reads"]]
+        prepared.append(Region(r["haplotypes"], r["reads"], qs, gops, gops, [bytes([10]) * len(x) for x in r["reads"]]))
+    pb = PackedBatch.from_regions(prepared)
+    offs = pb.out_offsets()
+    with engine.resident(pb) as res:
+        lk64_all = res.check_fp64()
+    if not ref_available():
+        out["reference"] = "unavailable (oracle/_ref not built)"
+        return out
+    gref = GenotypeRef()
+    ref = Ref()
+    lk_ref_all = np.empty(pb.out_size)
+
+    def work(g):
+        lk_ref_all[offs[g]:offs[g + 1]] = ref.schedule_region(pb, g, 0.02, 0.02).reshape(-1)
+
+    with ThreadPoolExecutor(max_workers=cpu_threads or (os.cpu_count() or 1), initializer=ref.init_thread) as ex:
+        list(ex.map(work, range(pb.n_regions)))
+    total = gl_equal = alk_equal = calls_ref = calls_64 = truth_hits = keep_equal = 0
+    max_gl_vs_ref_lk, max_tie = 0.0, 0.0
+    for g, (r, tk) in enumerate(zip(regions, full)):
+        mat, keep = tk.wait()
+        got = tk.genotypes()
         M, N = len(r["haplotypes"]), len(r["reads"])
-        lk_ref, _ = orc.batch(pb)
-        res_ref, _, _ = G.genotype_region(lk_ref.reshape(M, N), lens, r["events"])
-        lk64, _ = orc.batch(pb, fp64_only=True)
-        res64, _, _ = G.genotype_region(lk64.reshape(M, N), lens, r["events"])
-        for (gl, best, _), (glr, bestr, _), (gl64, best64, _), truth in zip(tk.genotypes(), res_ref, res64, r["truth"]):
+        K = int(keep.sum())
+        lens = [len(x) for x in r["reads"]]
+        norm_ref, keep_ref = G.normalize_filter(lk_ref_all[offs[g]:offs[g + 1]].reshape(M, N), lens)
+        norm64, keep64 = G.normalize_filter(lk64_all[offs[g]:offs[g + 1]].reshape(M, N), lens)
+        K64 = int(keep64.sum())
+        keep_equal += int(np.array_equal(keep_ref, keep.astype(bool)))
+        K_ref = int(keep_ref.sum())
+        for (A, ha), (gl, best, alk), truth in zip(r["events"], got, r["truth"]):
             total += 1
-            same += int(best == bestr)
-            same64 += int(best == best64)
-            if best != best64:
-                max_tie = max(max_tie, abs(float(gl64[best] - gl64[best64])))
+            ralk, rgl = gref.genotype(mat[:, :K], ha, A)
+            alk_equal += int(np.array_equal(alk[:, :K], ralk, equal_nan=True))
+            gl_equal += int(np.array_equal(gl, rgl, equal_nan=True))
+            _, gl_r = gref.genotype(norm_ref[:, :K_ref], ha, A)
+            calls_ref += int(best == G.best_genotype(gl_r))
+            max_gl_vs_ref_lk = max(max_gl_vs_ref_lk, float(np.max(np.abs(gl - gl_r))))
+            _, gl64 = gref.genotype(norm64[:, :K64], ha, A)
+            b64 = G.best_genotype(gl64)
+            calls_64 += int(best == b64)
+            if best != b64:
+                max_tie = max(max_tie, abs(float(gl64[best] - gl64[b64])))
             truth_hits += int(best == truth)
-            max_gl = max(max_gl, float(np.max(np.abs(gl - gl64))))
-    return {"regions": n_regions, "events": int(sum(len(r["events"]) for r in regions)),
-            "regions_per_s": round(n_regions / el, 1), "gcups": round(cells / el / 1e9, 2),
-            "checked_events": total, "calls_identical_to_reference_likelihoods": same,
-            "calls_identical_to_fp64_likelihoods": same64,
-            "max_fp64_gl_gap_where_calls_differ": max_tie, "calls_equal_truth": truth_hits,
-            "max_abs_gl_diff_vs_fp64": max_gl,
-            "form": "phmm_submit_region with events, genotype likelihoods only back to the host (PCR CONSERVATIVE, Q18)"}
+    out.update({"checked_events": total,
+                "gl_bit_equal_to_reference_genotyping_on_gpu_matrix": gl_equal,
+                "allele_lk_bit_equal_to_reference_marginalisation": alk_equal,
+                "regions_with_kept_reads_equal_to_reference_likelihoods": keep_equal,
+                "calls_identical_to_reference_likelihoods_and_genotyping": calls_ref,
+                "max_abs_gl_diff_vs_reference_likelihoods": max_gl_vs_ref_lk,
+                "calls_identical_to_fp64_likelihoods": calls_64,
+                "max_fp64_gl_gap_where_calls_differ": max_tie, "calls_equal_truth": truth_hits,
+                "reference": "schedule_pairhmm (oracle/_ref/libphmm_ref.so) on the prepared reads, normalise/filter "
+                             "restated (pinned to pairhmm_internal.cpp by the host tests), AlleleLikelihoods::marginalize "
+                             "and GenotypeLikelihoodCalculator (oracle/_ref/libgenotype_ref.so)"})
+    return out
 
 
 def smith_waterman_run(engine, batch, steps: int, warmup: int, cpu: bool) -> dict:
@@ -492,10 +691,27 @@ def run_ours(args, rank: int, world: int, dist) -> None:
     value, ms_per_step = weak_scaling_value(dist, float(cells), args.steps, st["device_ms"], dev)
     total_cells = value * ms_per_step * args.steps * 1e6
     fp32_pass_ms = max_over_ranks(st["fp32_ms"])
+    strong = None
+    if world > 1:
+        # strong scaling: one 2,000-region batch (the same seed on every rank) split across the ranks
+        shared = batch if rank == 0 else synth.config1(seed=shard_seed(0))
+        mine = shared.subset(strong_scaling_regions(shared, rank, world))
+        with engine.resident(mine) as rs:
+            rs.run(args.warmup)
+            barrier()
+            sst = rs.run(args.steps)
+            barrier()
+        s_ms = max_over_ranks(sst["device_ms"])
+        strong = {"value": round(shared.cells() * args.steps / (s_ms / 1e3) / 1e9, 2), "unit": "GCUPS",
+                  "ms_per_step": round(s_ms / args.steps, 3), "cells_per_step": int(shared.cells()),
+                  "split": "regions of one 2,000-region batch by phmm_partition_regions (cells per rank balanced)"}
     out, flags = res.results()
     # every kernel class alone, after the timed region (CUDA events around each launch)
     prof = res.profile()
+    # every pair again with the all-FP64 model, for the error of every likelihood
+    f64_all = res.check_fp64()
     res.close()
+    accuracy = error_report(out, flags, f64_all)
     f64_frac = float(flags.mean())
     launches = int(st["kernel_launches"])
 
@@ -534,27 +750,23 @@ def run_ours(args, rank: int, world: int, dist) -> None:
         plain = plain_cells / plain_s / 1e9
         plain_dev = plain_cells / (plain_dev_ms / 1e3) / 1e9
 
-        # accuracy on a seeded sample of regions against the all-FP64 oracle
-        from oracle import Oracle
+        # every pair against the reference's own schedule_pairhmm on the host cores (one GPU only:
+        # the host is shared by all ranks otherwise)
+        from oracle import Oracle, ref_available
 
         orc = Oracle()
-        offs = batch.out_offsets()
-        sample = [3, 1000, 1997]
-        f64, _ = orc.batch(batch.subset(sample), fp64_only=True)
-        _, used = orc.batch(batch.subset(sample))
-        got = np.concatenate([out[offs[g]:offs[g + 1]] for g in sample])
-        got_flags = np.concatenate([flags[offs[g]:offs[g + 1]] for g in sample]).astype(bool)
-        max_err = float(np.max(np.abs(got - f64)))
-        switch_mismatches = int(np.sum(got_flags != used))
+        cores = os.cpu_count() or 1
+        vs_ref = reference_whole_batch(batch, out, flags, cores) if world == 1 and ref_available() else None
 
         # serving loop latency (after a warm-up burst: slots sized, graphs captured, kernels loaded)
         cap = batch.n_regions / (e2e_s / args.steps)
-        serving_latency(engine, batch, 2.0, cap, 1.0, seed=99)
-        lat = [serving_latency(engine, batch, load, cap, args.serve_seconds, seed=rank)
-               for load in (0.25, 0.5, 0.8, 0.95)]
-        stress = underflow_stress(engine)
-        wgs = wgs_mixture(engine)
-        geno = genotyping_run(engine)
+        pool = RequestPool(batch)
+        serving_latency(engine, pool, 2.0, cap, 1.0, seed=99)
+        lat = [serving_latency(engine, pool, load, cap, args.serve_seconds, seed=100 + k)
+               for k, load in enumerate((0.25, 0.5, 0.8, 0.95))]
+        stress = underflow_stress(engine, args.steps, args.warmup, cores if world == 1 and ref_available() else None)
+        wgs = wgs_mixture(engine, args.wgs_fraction, cores if world == 1 and ref_available() else None)
+        geno = genotyping_run(engine, cpu_threads=cores)
         swr = smith_waterman_run(engine, batch, args.steps, args.warmup, world == 1)
 
         # roofline of the FP32 wavefront pass against the measured FP32 FMA peak
@@ -577,9 +789,6 @@ def run_ours(args, rank: int, world: int, dist) -> None:
         # CPU baseline: the reference's own PairHMM on all host cores, bounded sample
         cpu = None
         if world == 1:
-            from oracle import ref_available
-
-            cores = os.cpu_count() or 1
             if ref_available():
                 sample_regions = list(range(64))
                 reference_gcups(batch, sample_regions[:4], cores)
@@ -609,7 +818,14 @@ def run_ours(args, rank: int, world: int, dist) -> None:
                                                 "PCR NONE; the genotyping leg uses the region API (Q18, PCR CONSERVATIVE)",
                        "parallelism": f"regions sharded per rank x{world}, no collective"},
             "e2e": {"value": round(e2e, 2), "unit": "GCUPS", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "ms_per_step": round(1e3 * e2e_s / args.steps, 3), "results_identical_to_resident": same},
+                    "ms_per_step": round(1e3 * e2e_s / args.steps, 3), "results_identical_to_resident": same,
+                    "batched_vs_plain": round(e2e / plain, 2), "plain_gcups": round(plain, 2),
+                    "p50_p99_region_latency_ms_at_80pct_load": [next(x for x in lat if x["load"] == 0.8)["p50_ms"],
+                                                                next(x for x in lat if x["load"] == 0.8)["p99_ms"]],
+                    "max_abs_log10_err_vs_fp64_every_pair": accuracy["max"],
+                    "pairs_checked_vs_fp64": accuracy["pairs"],
+                    "max_abs_diff_vs_reference_every_pair": vs_ref["max_abs_diff"] if vs_ref else None,
+                    "fp64_flag_disagreements_vs_reference": vs_ref["fp64_flag_disagreements"] if vs_ref else None},
             "gpu_launches": launches,
             "roofline": {"bound": "fp32", "achieved": round(achieved, 2), "peak": round(peak, 2), "unit": "TFLOP/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,
@@ -630,11 +846,10 @@ def run_ours(args, rank: int, world: int, dist) -> None:
                       "form": "one region per phmm_compute_regions call"},
             "batched_vs_plain": {"e2e": round(e2e / plain, 2), "device": round(value / world / plain_dev, 2)},
             "fp32_pass_ms": round(fp32_pass_ms, 3),
+            "strong_scaling": strong,
             "fp64_rerun_fraction": round(f64_frac, 5),
-            "max_abs_err_log10_vs_fp64": max_err,
-            "fp64_switch_mismatches_vs_reference": {"pairs": int(got_flags.size), "mismatches": switch_mismatches,
-                                                    "sample": "regions 3, 1000, 1997 against the oracle's "
-                                                              "restatement of the reference's scheduler"},
+            "accuracy_vs_fp64": accuracy,
+            "vs_reference_every_pair": vs_ref,
             "latency": next(x for x in lat if x["load"] == 0.8),
             "latency_by_load": lat,
             "underflow_stress": stress,
@@ -654,6 +869,8 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--serve-seconds", type=float, default=6.0)
+    ap.add_argument("--wgs-fraction", type=float, default=0.1,
+                    help="share of the 200,000-region WGS-like mixture run in its leg (1.0: all of it)")
     ap.add_argument("--no-autotune", action="store_true",
                     help="default tile shapes (profiling runs: no calibration launches before the batch)")
     ap.add_argument("--only", choices=["all", "resident", "sw"], default="all",
