@@ -633,12 +633,12 @@ def run_resident_only(args) -> None:
     from rovaca_b200 import Engine, synth
 
     torch.cuda.set_device(0)
-    batch = synth.config1(seed=1)
+    batch = synth.config1(n_regions=args.regions, seed=1)
     with Engine(device=0, use_cuda_graph=not args.no_graph, autotune=not args.no_autotune) as engine:
         with engine.resident(batch) as res:
             res.run(args.warmup)
             st = res.run(args.steps)
-    print(json.dumps({"mode": "resident", "graph": not args.no_graph, "steps": args.steps,
+    print(json.dumps({"mode": "resident", "regions": args.regions, "graph": not args.no_graph, "steps": args.steps,
                       "ms_per_step": st["device_ms"] / args.steps, "fp32_pass_ms": st["fp32_ms"],
                       "fp64_pass_ms": st["fp64_ms"], "gcups": batch.cells() * args.steps / st["device_ms"] / 1e6,
                       "kernel_launches": st["kernel_launches"]}), flush=True)
@@ -877,6 +877,8 @@ def main() -> None:
                     help="resident: only the device-resident replay (for profiling); sw: only the resident "
                          "Smith-Waterman realignment of a 500-region batch's reads (for profiling)")
     ap.add_argument("--no-graph", action="store_true", help="direct launches instead of CUDA-graph replay")
+    ap.add_argument("--regions", type=int, default=2000,
+                    help="--only resident: regions of the batch (a smaller batch of the same shape for profiling)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be at least 3")

@@ -36,7 +36,11 @@ namespace {
 using Clock = std::chrono::steady_clock;
 
 constexpr int kSlots = 3;                            // batches in flight at once
-constexpr uint64_t kMaxBatchCells = 200000000000ull;  // bound on one batch's work (~0.1 s on B200)
+// Bound on one batch's work (~35 ms on B200): a burst of requests becomes several batches that
+// pipeline through the slots instead of one long batch that every later arrival waits behind.
+constexpr uint64_t kMaxBatchCells = 80000000000ull;
+// Queued requests a forming batch looks through for requests of its kind.
+constexpr size_t kAdmitScan = 4096;
 constexpr size_t kMaxQueued = 1u << 20;
 
 enum class ReqState { Queued, Running, Done };
@@ -216,10 +220,15 @@ void Server::worker(int idx)
             // submit).
             const uint64_t batch_cap = budget / kSlots;
             const auto now = Clock::now();
-            while (!queue.empty()) {
-                auto& r = queue.front();
-                // a batch holds requests of one kind (region API or plain likelihoods)
-                if (!batch.empty() && r->region_api != batch.front()->region_api) break;
+            size_t scanned = 0;
+            for (auto it = queue.begin(); it != queue.end() && scanned < kAdmitScan; ++scanned) {
+                auto& r = *it;
+                // A batch holds requests of one kind (region API or plain likelihoods).  A request
+                // of the other kind stays queued, in order, and heads the next slot's batch.
+                if (!batch.empty() && r->region_api != batch.front()->region_api) {
+                    ++it;
+                    continue;
+                }
                 const bool fits = in_use + batch_bytes + r->bytes <= budget &&
                                   (batch.empty() || batch_bytes + r->bytes <= batch_cap);
                 if (!fits || (!batch.empty() && cells + r->cells > kMaxBatchCells)) break;
@@ -231,7 +240,7 @@ void Server::worker(int idx)
                 r->state = ReqState::Running;
                 r->t_admit = now;
                 batch.push_back(r);
-                queue.pop_front();
+                it = queue.erase(it);
             }
             in_use += batch_bytes;
         }
