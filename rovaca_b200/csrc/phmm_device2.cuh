@@ -182,6 +182,29 @@ __device__ __forceinline__ bool load_rows2(LaneRows2<KH, PM>& L, float4* tab, co
     return exotic;
 }
 
+// Haplotype code words staged in shared memory (build-time setting): each warp keeps a ring of
+// kCodeRing words, the columns its lanes read in the current chunk of steps, and copies the next
+// chunk's words from global memory with cp.async while the current chunk computes, so a step reads
+// its code word from shared memory instead of through L1.  A chunk reads columns [t0-31, t0+kChunk)
+// and the copies in flight write [t0+kChunk, t0+2 kChunk): 31 + 2 kChunk < kCodeRing slots, so no
+// copy overwrites a word a lane still reads.  Columns stay within the stream's guard words
+// (t0 + 2 kChunk <= Tcols + 32 + 2 kChunk < Tcols + kCodePad).
+#ifndef PHMM_CODES_STAGED
+#define PHMM_CODES_STAGED 0
+#endif
+constexpr int kCodeRing = 64;
+static_assert(31 + 2 * kChunk < kCodeRing && 32 + 2 * kChunk <= kCodePad, "code ring too small for the chunk");
+// float4 slots the ring adds to a warp's shared prior table
+constexpr int kRingFloat4 = PHMM_CODES_STAGED ? kCodeRing / 4 : 0;
+
+__device__ __forceinline__ void copy_word_async(uint32_t* dst_shared, const uint32_t* src)
+{
+    const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst_shared);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void copies_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void copies_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 // Load the next step's priors during the current step (build-time setting): shortens the step of
 // a warp that runs alone on its scheduler, at the cost of KH register pairs.  Measured on B200 with
 // 12 warps per SM for KH >= 4: one region per call 140 instead of 124 GCUPS on the device, the
@@ -189,6 +212,7 @@ __device__ __forceinline__ bool load_rows2(LaneRows2<KH, PM>& L, float4* tab, co
 #ifndef PHMM_PRIOR_PREFETCH
 #define PHMM_PRIOR_PREFETCH 0
 #endif
+static_assert(!(PHMM_PRIOR_PREFETCH && PHMM_CODES_STAGED), "the prefetch reads a code word before the ring is filled");
 
 template <int V, int PM, int KH>
 __device__ __forceinline__ float2 diag_sum(const LaneRows2<KH, PM>& L, int r, float2 dgM, float2 dgI, float2 dgD)
@@ -259,7 +283,7 @@ struct SweepOut2 {
 // row 0 or a pad row, per read.  exotic: the warp holds an inter row with a byte outside A/C/G/T
 // (every step runs the checked path).
 template <int KH, int V, int PM, bool FROM_SCR, bool TO_SCR>
-__device__ void sweep2(LaneRows2<KH, PM>& L, const float4* tab, const BatchView& b, const ProbTables<float>& tb,
+__device__ void sweep2(LaneRows2<KH, PM>& L, float4* tab, const BatchView& b, const ProbTables<float>& tb,
                        const PassControl& pc, const SweepOut2& so, const ReadPair& rp, int first, uint32_t g_lo,
                        uint32_t g_hi, float2* scr, int lane, bool aboveX, bool aboveY, bool exotic)
 {
@@ -268,6 +292,8 @@ __device__ void sweep2(LaneRows2<KH, PM>& L, const float4* tab, const BatchView&
     const int Tcols = (int)(b.hap_off[g_hi] - s0);
     const uint32_t* codes = (V == kInter ? b.codes_inter : b.codes_intra) + kCodePad + s0;
     const char* tab_lane = reinterpret_cast<const char*>(tab) + lane * (int)sizeof(float4);
+    // the warp's code ring follows its prior table (PHMM_CODES_STAGED)
+    uint32_t* ring = reinterpret_cast<uint32_t*>(tab + tab_floats4<KH>());
     const float C = Scale<float>::initial();
     const bool writer = lane == kWarp - 1;
 
@@ -358,7 +384,11 @@ __device__ void sweep2(LaneRows2<KH, PM>& L, const float4* tab, const BatchView&
     // The priors of a column: its code word's class selects the plane of the lane's table.
     auto load_priors = [&](int p, float2(&dst)[KH]) -> uint32_t {
         // p lies in [-31, Tcols + 32]: the guard words around the stream cover it
+#if PHMM_CODES_STAGED
+        const uint32_t w = ring[p & (kCodeRing - 1)];
+#else
         const uint32_t w = codes[p];
+#endif
         const char* tp = tab_lane + ((w & kTabMask) >> tab_shift<KH>());
 #pragma unroll
         for (int j = 0; j < QJ; ++j) {
@@ -429,7 +459,19 @@ __device__ void sweep2(LaneRows2<KH, PM>& L, const float4* tab, const BatchView&
         }
     };
 
+#if PHMM_CODES_STAGED
+    // columns [-32, kChunk) before the first chunk
+    for (int q = lane - kWarp; q < kChunk; q += kWarp) ring[q & (kCodeRing - 1)] = codes[q];
+    __syncwarp();
+#endif
     for (int t0 = 0; t0 < steps; t0 += kChunk) {
+#if PHMM_CODES_STAGED
+        // this chunk's columns are in the ring; start copying the next chunk's
+        copies_wait_all();
+        __syncwarp();
+        if (lane < kChunk) copy_word_async(&ring[(t0 + kChunk + lane) & (kCodeRing - 1)], codes + t0 + kChunk + lane);
+        copies_commit();
+#endif
         // Lanes cover stream columns [t0-31, t0+kChunk-1] in this chunk.  Lane 31 trails, so its
         // next boundary is the first boundary at or after t0-31: past the chunk means no lane meets
         // a boundary and the chunk needs no per-step check.
@@ -442,6 +484,10 @@ __device__ void sweep2(LaneRows2<KH, PM>& L, const float4* tab, const BatchView&
                 if (t0 + u < steps) step(t0 + u, true);
         }
     }
+#if PHMM_CODES_STAGED
+    copies_wait_all();
+    __syncwarp();
+#endif
 }
 
 }  // namespace phmm

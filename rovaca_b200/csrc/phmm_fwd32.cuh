@@ -92,7 +92,7 @@ template <int KH, int V, int PM, bool MULTI>
 __global__ void __launch_bounds__(kFwdBlock, min_blocks32<KH, V, PM>()) fwd_f32_kernel(BatchView b, ProbTables<float> tb,
                                                                                  PassControl pc)
 {
-    __shared__ float4 tab[tab_floats4<KH>()];
+    __shared__ float4 tab[tab_floats4<KH>() + kRingFloat4];
     const int lane = threadIdx.x & (kWarp - 1);
     const unsigned int warp_id = (blockIdx.x * blockDim.x + threadIdx.x) / kWarp;
     float2* scr = MULTI ? (float2*)pc.scratch + (size_t)warp_id * pc.scratch_cols * 3 : nullptr;
