@@ -98,7 +98,9 @@ __global__ void __launch_bounds__(kFwdBlock, min_blocks32<KH, V, PM>()) fwd_f32_
     float2* scr = MULTI ? (float2*)pc.scratch + (size_t)warp_id * pc.scratch_cols * 3 : nullptr;
     const unsigned int n = pc.cd->n_items;
     const WorkItem* items = pc.items + pc.cd->item_off;
-    const int mode = mode32(V, PM);
+    // the kernel's class mode (0 constant gaps with insertion = deletion, 1 per-row, 2 intra); its
+    // underflowed pairs go to the FP64 classes of that mode
+    const int mode = mode32(V, PM == PM_ROW ? 1 : 0);
     for (;;) {
         const unsigned int idx = claim(&pc.cd->claim32, lane);
         if (idx >= n) break;
