@@ -197,6 +197,7 @@ static_assert(31 + 2 * kChunk < kCodeRing && 32 + 2 * kChunk <= kCodePad, "code 
 // float4 slots the ring adds to a warp's shared prior table
 constexpr int kRingFloat4 = PHMM_CODES_STAGED ? kCodeRing / 4 : 0;
 
+#if PHMM_CODES_STAGED
 __device__ __forceinline__ void copy_word_async(uint32_t* dst_shared, const uint32_t* src)
 {
     const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst_shared);
@@ -204,6 +205,7 @@ __device__ __forceinline__ void copy_word_async(uint32_t* dst_shared, const uint
 }
 __device__ __forceinline__ void copies_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void copies_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+#endif
 
 // Load the next step's priors during the current step (build-time setting): shortens the step of
 // a warp that runs alone on its scheduler, at the cost of KH register pairs.  Measured on B200 with

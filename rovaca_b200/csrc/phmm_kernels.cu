@@ -8,8 +8,8 @@
 // union of all paths.  Work items are grouped by class on the host.
 #include <cuda_runtime.h>
 
-#include "phmm_device.cuh"
 #include "phmm_fwd32.cuh"
+#include "phmm_warp64.cuh"
 #include "phmm_kernels.h"
 
 namespace phmm {
@@ -52,45 +52,6 @@ __global__ void reset_outputs_kernel(const BatchDesc* __restrict__ desc, double*
 }
 
 // ------------------------------------------------------------------------------------------
-// One read against a run of haplotypes [g_lo, g_hi).
-// ------------------------------------------------------------------------------------------
-template <typename T, int K, int V, int PM, bool MULTI, bool UNF = false>
-__device__ __forceinline__ void run_read(const BatchView& b, const ProbTables<T>& tb, const PassControl& pc,
-                                         const SweepOut& so, uint32_t g_lo, uint32_t g_hi, int lane, T* scr)
-{
-    LaneRows<T, K, PM> L;
-    const uint64_t roff = b.read_off[so.read];
-    const int R = (int)(b.read_off[so.read + 1] - roff);
-    const int Tcols = (int)(b.hap_off[g_hi] - b.hap_off[g_lo]);
-    // A read that does not fit the class's stripe, or a multi-stripe stream longer than the
-    // scratch row, means a planning bug: report it and leave the pairs as NaN.
-    if (R <= 0 || (!MULTI && R > kWarp * K) || (MULTI && (R <= kWarp * K || Tcols > (int)pc.scratch_cols))) {
-        if (lane == 0) atomicOr(pc.status, kStatusBadItem);
-        return;
-    }
-    if (!MULTI) {
-        const int pad = kWarp * K - R;
-        load_rows<T, K, V, PM>(L, b, tb, roff, R, 0, pad, lane);
-        sweep<T, K, V, PM, false, false, UNF>(L, b, pc, so, g_lo, g_hi, scr, lane, lane * K <= pad);
-    } else {
-        constexpr int SR = kWarp * K;  // rows per stripe
-        const int stripes = (R + SR - 1) / SR;
-        const int pad = SR * stripes - R;
-        for (int s = 0; s < stripes; ++s) {
-            load_rows<T, K, V, PM>(L, b, tb, roff, R, s * SR, pad, lane);
-            const bool above_row0 = (s == 0) && (lane * K <= pad);
-            if (s == 0)
-                sweep<T, K, V, PM, false, true, UNF>(L, b, pc, so, g_lo, g_hi, scr, lane, above_row0);
-            else if (s == stripes - 1)
-                sweep<T, K, V, PM, true, false, UNF>(L, b, pc, so, g_lo, g_hi, scr, lane, above_row0);
-            else
-                sweep<T, K, V, PM, true, true, UNF>(L, b, pc, so, g_lo, g_hi, scr, lane, above_row0);
-            __syncwarp();  // lane 31's scratch row is read by lane 0 in the next stripe
-        }
-    }
-}
-
-// ------------------------------------------------------------------------------------------
 // FP64 pass for one class over the runs of underflowed pairs the FP32 pass appended, one run per
 // claim, streamed through the read like an FP32 work item.
 // ------------------------------------------------------------------------------------------
@@ -113,21 +74,7 @@ __global__ void __launch_bounds__(kFwdBlock, min_blocks64<K, PM>()) fwd_f64_kern
 {
     const int lane = threadIdx.x & (kWarp - 1);
     const unsigned int warp_id = (blockIdx.x * blockDim.x + threadIdx.x) / kWarp;
-    double* scr = MULTI ? (double*)pc.scratch + (size_t)warp_id * pc.scratch_cols * 3 : nullptr;
-    const unsigned int n = min(pc.cd->rerun_count, pc.cd->rerun_cap);
-    const RerunEntry* rerun = pc.rerun + pc.cd->rerun_off;
-    for (;;) {
-        const unsigned int idx = claim(&pc.cd->claim64, lane);
-        if (idx >= n) break;
-        const RerunEntry e = rerun[idx];
-        SweepOut so;
-        so.out = b.out;
-        so.pair_flags = nullptr;
-        so.out_base = e.out_idx;
-        so.out_stride = e.out_stride;
-        so.read = e.read;
-        run_read<double, K, V, PM, MULTI, UNF>(b, tb, pc, so, e.hap, e.hap + e.n_haps, lane, scr);
-    }
+    warp_reruns64<K, V, PM, MULTI, UNF>(b, tb, pc, lane, warp_id);
 }
 
 // ------------------------------------------------------------------------------------------

@@ -1,0 +1,114 @@
+"""The engine's wavefront kernels run on the CPU: tests/native/warp_emu.cpp compiles their device
+code (rovaca_b200/csrc/phmm_warp32.cuh, phmm_warp64.cuh and what they include) with g++ and runs each
+class on one emulated warp, 32 host threads standing for the lanes (tests/native/warp_emu_shim.h),
+over a batch the engine's own planner cuts.  Results must equal the oracle's pair for pair, as the GPU
+tests require: equal raw sums (|log10 diff| <= 1e-12) and the same FP32 -> FP64 decisions.
+
+The emulator's cost grows with the haplotype columns a warp streams, not with read length, so the
+batches pair long reads (every rows-per-lane shape, multi-stripe reads up to 768) with short
+haplotypes.  One region per kernel mode: equal constant gap qualities (mode 0), per-row and unequal
+constant gap qualities (mode 1), N in reads and haplotypes (intra), and bytes outside A/C/G/T/N
+(the inter kernel's checked path)."""
+from __future__ import annotations
+
+import shutil
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from conftest import assert_same_values
+from rovaca_b200.pairhmm import PackedBatch, Region
+
+ROOT = Path(__file__).resolve().parent.parent
+NATIVE = ROOT / "tests" / "native"
+BIN = NATIVE / "_build" / "warp_emu"
+CSRC = ROOT / "rovaca_b200" / "csrc"
+EXACT = 1e-12
+LENS = (17, 40, 70, 100, 150, 180, 200, 240, 256, 300, 500, 768)
+
+
+@pytest.fixture(scope="module")
+def emulator():
+    gxx = shutil.which("g++")
+    if gxx is None:
+        pytest.skip("g++ not available")
+    srcs = [NATIVE / "warp_emu.cpp", NATIVE / "warp_emu_shim.h", CSRC / "phmm_plan.cpp", CSRC / "phmm_tables.cpp",
+            *CSRC.glob("*.cuh"), *CSRC.glob("*.h"), ROOT / "include" / "phmm_b200.h"]
+    if not BIN.exists() or any(s.stat().st_mtime > BIN.stat().st_mtime for s in srcs):
+        BIN.parent.mkdir(exist_ok=True)
+        subprocess.run([gxx, "-std=c++20", "-O2", "-mfma", "-ffp-contract=off", "-pthread", "-w",
+                        str(NATIVE / "warp_emu.cpp"), str(CSRC / "phmm_plan.cpp"), str(CSRC / "phmm_tables.cpp"),
+                        "-o", str(BIN)], check=True)
+    return BIN
+
+
+def _write(pb: PackedBatch, path: Path) -> None:
+    with open(path, "wb") as f:
+        f.write(b"PHMMEMU1")
+        f.write(np.array([pb.n_regions], np.uint32).tobytes())
+        f.write(np.array([pb.n_haps.sum(), pb.n_reads.sum(), pb.hap_bases.size, pb.read_bases.size], np.uint64).tobytes())
+        for a, t in ((pb.n_haps, np.uint32), (pb.n_reads, np.uint32), (pb.hap_off, np.uint64),
+                     (pb.read_off, np.uint64)):
+            f.write(np.ascontiguousarray(a, t).tobytes())
+        for a in (pb.hap_bases, pb.read_bases, pb.read_qual, pb.read_ins, pb.read_del, pb.read_gcp):
+            f.write(np.ascontiguousarray(a, np.uint8).tobytes())
+
+
+def _run(binary, pb: PackedBatch, tmp_path: Path, mode: str = "engine", tiles: str = "default"):
+    src, dst = tmp_path / "batch.bin", tmp_path / "out.bin"
+    _write(pb, src)
+    subprocess.run([str(binary), str(src), str(dst), mode, tiles], check=True, timeout=900)
+    raw = dst.read_bytes()
+    n = pb.out_size
+    return (np.frombuffer(raw[:8 * n], np.float64), np.frombuffer(raw[8 * n:9 * n], np.uint8),
+            int(np.frombuffer(raw[9 * n:], np.uint32)[0]))
+
+
+def _batch(seed: int) -> PackedBatch:
+    rng = np.random.default_rng(seed)
+    acgt = np.frombuffer(b"ACGT", np.uint8)
+    regs = []
+    for kind in ("equal", "per-row", "unequal", "N", "exotic"):
+        haps = [bytearray(acgt[rng.integers(0, 4, int(rng.integers(8, 40)))]) for _ in range(int(rng.integers(2, 4)))]
+        reads, q, ins, dels = [], [], [], []
+        for L in LENS:
+            r = bytearray(acgt[rng.integers(0, 4, L)])
+            if kind == "N" and rng.random() < 0.5:
+                r[L // 2] = ord("N")
+            if kind == "exotic" and rng.random() < 0.5:
+                r[L // 3] = ord("R")
+            reads.append(bytes(r))
+            q.append(rng.integers(2, 41, L).astype(np.uint8).tobytes())
+            if kind == "per-row":
+                ins.append(rng.integers(20, 46, L).astype(np.uint8).tobytes())
+                dels.append(rng.integers(20, 46, L).astype(np.uint8).tobytes())
+            else:
+                ins.append(bytes([45] * L))
+                dels.append(bytes([40 if kind == "unequal" else 45] * L))
+        if kind == "N":
+            haps[0][len(haps[0]) // 2] = ord("N")
+        if kind == "exotic":
+            haps[-1][1] = ord("R")
+        regs.append(Region([bytes(h) for h in haps], reads, q, ins, dels, [bytes([10] * len(r)) for r in reads]))
+    return PackedBatch.from_regions(regs)
+
+
+@pytest.mark.parametrize("tiles", ["default", "multi4"])
+def test_emulated_kernels_equal_the_oracle(emulator, oracle, tmp_path, tiles):
+    pb = _batch(11)
+    got, flags, status = _run(emulator, pb, tmp_path, tiles=tiles)
+    want, used = oracle.batch(pb)
+    assert status == 0
+    assert_same_values(got, want, EXACT, tiles)
+    assert np.array_equal(flags.astype(bool), used)
+    assert used.any() and not used.all()  # both passes ran
+
+
+def test_emulated_all_fp64_check_equals_the_oracle(emulator, oracle, tmp_path):
+    pb = _batch(12)
+    got, _, status = _run(emulator, pb, tmp_path, mode="check64")
+    want, _ = oracle.batch(pb, fp64_only=True)
+    assert status == 0
+    assert_same_values(got, want, EXACT)
