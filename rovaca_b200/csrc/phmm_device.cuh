@@ -100,21 +100,38 @@ __device__ __forceinline__ T shfl_up1(T v)
 // it is formed once (the two reference operations have the same operands, hence the same bits).
 enum ParamMode : int { PM_ALL = 0, PM_ROW = 1, PM_EQ = 2 };
 
-// One lane's rows of the current stripe.
+// One lane's rows of the current stripe.  The match priors are not held here: each lane tabulates
+// its rows' priors for the five haplotype base classes in shared memory (prior_slot), so a cell
+// takes its prior with a load at its column's class instead of a compare and a select.
 template <typename T, int K, int PM>
 struct LaneRows {
     static constexpr int NR = PM == PM_ROW ? K : 1;
     T Mp[K], Ip[K], Dp[K];        // values at the previous column
-    T pa[K], pb[K], xx[K];
+    T xx[K];
     T mm[NR], gm[NR], mx[NR], my[NR];
-    uint32_t rc[K];
     uint32_t padmask;             // bit k: slot k is a pad row
 };
 
+// A warp's prior table: [class][row slot][lane], kTabClasses * K * kWarp values.
+template <int K>
+__host__ __device__ constexpr int prior_table_size()
+{
+    return kTabClasses * K * kWarp;
+}
+template <int K>
+__device__ __forceinline__ int prior_slot(uint32_t cls, int k, int lane)
+{
+    return ((int)cls * K + k) * kWarp + lane;
+}
+
+// Loads this lane's rows of the stripe and writes their priors to the warp's table.  Returns true
+// when one of the lane's rows is an inter row with a byte outside A/C/G/T: such a byte can equal a
+// haplotype byte of class 4, whose table entry holds the mismatch prior (sweep corrects it).
 template <typename T, int K, int V, int PM>
-__device__ __forceinline__ void load_rows(LaneRows<T, K, PM>& L, const BatchView& b, const ProbTables<T>& tb,
+__device__ __forceinline__ bool load_rows(LaneRows<T, K, PM>& L, T* tab, const BatchView& b, const ProbTables<T>& tb,
                                           uint64_t roff, int R, int first_padded_row, int pad, int lane)
 {
+    bool exotic = false;
     L.padmask = 0;
     if (PM == PM_ALL) {
         // constant along the read: its first row gives them (pad rows ignore them)
@@ -130,11 +147,13 @@ __device__ __forceinline__ void load_rows(LaneRows<T, K, PM>& L, const BatchView
     for (int k = 0; k < K; ++k) {
         const int i = first_padded_row + lane * K + k - pad;  // 0-based read position
         const int r = PM == PM_ROW ? k : 0;
+        T pa = T(0), pb = T(0);  // pad rows: prior 0 for every class
+        uint32_t rc = 0u;
         if (i >= 0 && i < R) {
             const uint64_t o = roff + (uint64_t)i;
             const int q = b.read_q[o] & 127, c = b.read_c[o] & 127;
-            L.pa[k] = tb.pmat[q];
-            L.pb[k] = (V == kInter) ? tb.pmis_inter[q] : tb.pmis_intra[q];
+            pa = tb.pmat[q];
+            pb = (V == kInter) ? tb.pmis_inter[q] : tb.pmis_intra[q];
             L.xx[k] = tb.ph2pr[c];
             if (PM == PM_ROW) {
                 const int iq = b.read_i[o] & 127, dq = b.read_d[o] & 127;
@@ -143,10 +162,10 @@ __device__ __forceinline__ void load_rows(LaneRows<T, K, PM>& L, const BatchView
                 L.mx[r] = tb.ph2pr[iq];
                 L.my[r] = tb.ph2pr[dq];
             }
-            L.rc[k] = match_code(b.read_bases[o], V);
+            const uint8_t base = b.read_bases[o];
+            rc = match_code(base, V);
+            if (V == kInter) exotic |= base_class(base) == 4u;
         } else {
-            L.pa[k] = T(0);
-            L.pb[k] = T(0);
             L.xx[k] = T(1);
             if (PM == PM_ROW) {
                 L.mm[r] = T(0);
@@ -154,10 +173,12 @@ __device__ __forceinline__ void load_rows(LaneRows<T, K, PM>& L, const BatchView
                 L.mx[r] = T(0);
                 L.my[r] = T(0);
             }
-            L.rc[k] = 0u;
             L.padmask |= 1u << k;
         }
+#pragma unroll
+        for (int c = 0; c < kTabClasses; ++c) tab[prior_slot<K>((uint32_t)c, k, lane)] = class_matches((uint32_t)c, rc, V) ? pa : pb;
     }
+    return exotic;
 }
 
 // Compute column p for all K rows of this lane.  (sM, sI, sD): the row above this lane's first
@@ -171,7 +192,7 @@ __device__ __forceinline__ void load_rows(LaneRows<T, K, PM>& L, const BatchView
 // D = M my + D yy), each result flushed -- the plain-arithmetic FP64 model every likelihood's error
 // is measured against.
 template <typename T, int K, int V, int PM, bool FLUSH = true, bool UNF = false>
-__device__ __forceinline__ void cells(LaneRows<T, K, PM>& L, uint32_t hc, T sM, T sI, T dM, T dI, T dD)
+__device__ __forceinline__ void cells(LaneRows<T, K, PM>& L, const T (&pr)[K], T sM, T sI, T dM, T dI, T dD)
 {
     auto fz = [](T x) { return FLUSH ? ftz(x) : x; };
     T diM = dM, diI = dI, diD = dD, upM = sM, upI = sI;
@@ -179,7 +200,7 @@ __device__ __forceinline__ void cells(LaneRows<T, K, PM>& L, uint32_t hc, T sM, 
     for (int k = 0; k < K; ++k) {
         const int r = PM == PM_ROW ? k : 0;
         const T oM = L.Mp[k], oI = L.Ip[k], oD = L.Dp[k];
-        const T prior = codes_match(hc, L.rc[k], V) ? L.pa[k] : L.pb[k];
+        const T prior = pr[k];
         T s, nI, nD;
         if (UNF) {
             s = fz(radd(fz(radd(fz(rmul(diM, L.mm[r])), fz(rmul(diI, L.gm[r])))), fz(rmul(diD, L.gm[r]))));
@@ -259,9 +280,12 @@ struct SweepOut {
 //   FROM_SCR: the row above the stripe comes from scratch (stripe > 0), else the boundary row.
 //   TO_SCR:   the stripe's bottom row goes to scratch (not the last stripe), else it is summed.
 //   above_row0: the row above this lane's first slot is the boundary row 0 or a pad row.
+//   tab: the warp's prior table (load_rows); exotic: this lane holds an inter row with a byte
+//   outside A/C/G/T, read position row0 + lane * K + k in slot k (roff, R: the read).
 template <typename T, int K, int V, int PM, bool FROM_SCR, bool TO_SCR, bool UNF = false>
-__device__ void sweep(LaneRows<T, K, PM>& L, const BatchView& b, const PassControl& pc, const SweepOut& so, uint32_t g_lo,
-                      uint32_t g_hi, T* scr, int lane, bool above_row0)
+__device__ void sweep(LaneRows<T, K, PM>& L, const T* tab, const BatchView& b, const ProbTables<T>& tb,
+                      const PassControl& pc, const SweepOut& so, uint32_t g_lo, uint32_t g_hi, T* scr, int lane,
+                      bool above_row0, bool exotic, uint64_t roff, int R, int row0)
 {
     const uint64_t s0 = b.hap_off[g_lo];
     const int Tcols = (int)(b.hap_off[g_hi] - s0);
@@ -332,15 +356,30 @@ __device__ void sweep(LaneRows<T, K, PM>& L, const BatchView& b, const PassContr
                 sD = D0;
             }
         }
-        const uint32_t hc = codes[p] & kCodeMatchMask;
+        // the column's priors: its code word's class selects the row slots of the lane's table
+        const uint32_t w = codes[p];
+        const uint32_t cls = (w & kTabMask) >> kTabShift;
+        T pr[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) pr[k] = tab[prior_slot<K>(cls, k, lane)];
+        if (V == kInter && exotic && cls == 4u) {
+            // class 4 holds the mismatch prior for every row; a row whose byte equals this
+            // haplotype byte takes the match prior (the raw byte compare of the inter variant)
+            const uint32_t hb = w & kCodeMatchMask;
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                const int i = row0 + lane * K + k;
+                if (i >= 0 && i < R && b.read_bases[roff + i] == hb) pr[k] = tb.pmat[b.read_q[roff + i] & 127];
+            }
+        }
         // FP64: the flushes can only change a step whose inputs hold a value below the bound; the
         // warp votes every PHMM_F64_VOTE_EVERY steps (the scratch row read by stripes after the first
         // is not checked)
         constexpr bool kVote = PHMM_F64_VOTE && sizeof(T) == 8 && !FROM_SCR;
         if (kVote && flush_free)
-            cells<T, K, V, PM, false, UNF>(L, hc, sM, sI, dM, dI, dD);
+            cells<T, K, V, PM, false, UNF>(L, pr, sM, sI, dM, dI, dD);
         else
-            cells<T, K, V, PM, true, UNF>(L, hc, sM, sI, dM, dI, dD);
+            cells<T, K, V, PM, true, UNF>(L, pr, sM, sI, dM, dI, dD);
         dM = sM;
         dI = sI;
         dD = sD;

@@ -72,9 +72,10 @@ constexpr int min_blocks64()
 template <int K, int V, int PM, bool MULTI, bool UNF = false>
 __global__ void __launch_bounds__(kFwdBlock, min_blocks64<K, PM>()) fwd_f64_kernel(BatchView b, ProbTables<double> tb, PassControl pc)
 {
+    __shared__ double tab[prior_table_size<K>()];
     const int lane = threadIdx.x & (kWarp - 1);
     const unsigned int warp_id = (blockIdx.x * blockDim.x + threadIdx.x) / kWarp;
-    warp_reruns64<K, V, PM, MULTI, UNF>(b, tb, pc, lane, warp_id);
+    warp_reruns64<K, V, PM, MULTI, UNF>(b, tb, pc, tab, lane, warp_id);
 }
 
 // ------------------------------------------------------------------------------------------

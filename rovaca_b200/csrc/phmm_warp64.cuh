@@ -13,7 +13,7 @@ namespace phmm {
 // ------------------------------------------------------------------------------------------
 template <typename T, int K, int V, int PM, bool MULTI, bool UNF = false>
 __device__ __forceinline__ void run_read(const BatchView& b, const ProbTables<T>& tb, const PassControl& pc,
-                                         const SweepOut& so, uint32_t g_lo, uint32_t g_hi, int lane, T* scr)
+                                         const SweepOut& so, uint32_t g_lo, uint32_t g_hi, int lane, T* scr, T* tab)
 {
     LaneRows<T, K, PM> L;
     const uint64_t roff = b.read_off[so.read];
@@ -27,21 +27,26 @@ __device__ __forceinline__ void run_read(const BatchView& b, const ProbTables<T>
     }
     if (!MULTI) {
         const int pad = kWarp * K - R;
-        load_rows<T, K, V, PM>(L, b, tb, roff, R, 0, pad, lane);
-        sweep<T, K, V, PM, false, false, UNF>(L, b, pc, so, g_lo, g_hi, scr, lane, lane * K <= pad);
+        const bool exotic = load_rows<T, K, V, PM>(L, tab, b, tb, roff, R, 0, pad, lane);
+        sweep<T, K, V, PM, false, false, UNF>(L, tab, b, tb, pc, so, g_lo, g_hi, scr, lane, lane * K <= pad, exotic,
+                                              roff, R, -pad);
     } else {
         constexpr int SR = kWarp * K;  // rows per stripe
         const int stripes = (R + SR - 1) / SR;
         const int pad = SR * stripes - R;
         for (int s = 0; s < stripes; ++s) {
-            load_rows<T, K, V, PM>(L, b, tb, roff, R, s * SR, pad, lane);
+            const bool exotic = load_rows<T, K, V, PM>(L, tab, b, tb, roff, R, s * SR, pad, lane);
             const bool above_row0 = (s == 0) && (lane * K <= pad);
+            const int row0 = s * SR - pad;  // read position of slot 0 of lane 0
             if (s == 0)
-                sweep<T, K, V, PM, false, true, UNF>(L, b, pc, so, g_lo, g_hi, scr, lane, above_row0);
+                sweep<T, K, V, PM, false, true, UNF>(L, tab, b, tb, pc, so, g_lo, g_hi, scr, lane, above_row0, exotic,
+                                                     roff, R, row0);
             else if (s == stripes - 1)
-                sweep<T, K, V, PM, true, false, UNF>(L, b, pc, so, g_lo, g_hi, scr, lane, above_row0);
+                sweep<T, K, V, PM, true, false, UNF>(L, tab, b, tb, pc, so, g_lo, g_hi, scr, lane, above_row0, exotic,
+                                                     roff, R, row0);
             else
-                sweep<T, K, V, PM, true, true, UNF>(L, b, pc, so, g_lo, g_hi, scr, lane, above_row0);
+                sweep<T, K, V, PM, true, true, UNF>(L, tab, b, tb, pc, so, g_lo, g_hi, scr, lane, above_row0, exotic,
+                                                    roff, R, row0);
             __syncwarp();  // lane 31's scratch row is read by lane 0 in the next stripe
         }
     }
@@ -49,10 +54,11 @@ __device__ __forceinline__ void run_read(const BatchView& b, const ProbTables<T>
 
 // The claim loop of one warp over the class's rerun segment (pc.cd).  UNF: the all-FP64 check
 // arithmetic (plain multiply and add); the recompute pass proper uses the reference's contracted
-// arithmetic.  warp_id: the warp's index in the grid (its scratch row).
+// arithmetic.  tab: the warp's shared prior table (prior_table_size<K>() values); warp_id: the
+// warp's index in the grid (its scratch row).
 template <int K, int V, int PM, bool MULTI, bool UNF = false>
 __device__ __forceinline__ void warp_reruns64(const BatchView& b, const ProbTables<double>& tb, const PassControl& pc,
-                                              int lane, unsigned int warp_id)
+                                              double* tab, int lane, unsigned int warp_id)
 {
     double* scr = MULTI ? (double*)pc.scratch + (size_t)warp_id * pc.scratch_cols * 3 : nullptr;
     const unsigned int n = min(pc.cd->rerun_count, pc.cd->rerun_cap);
@@ -67,7 +73,7 @@ __device__ __forceinline__ void warp_reruns64(const BatchView& b, const ProbTabl
         so.out_base = e.out_idx;
         so.out_stride = e.out_stride;
         so.read = e.read;
-        run_read<double, K, V, PM, MULTI, UNF>(b, tb, pc, so, e.hap, e.hap + e.n_haps, lane, scr);
+        run_read<double, K, V, PM, MULTI, UNF>(b, tb, pc, so, e.hap, e.hap + e.n_haps, lane, scr, tab);
     }
 }
 

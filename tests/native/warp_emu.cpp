@@ -84,7 +84,8 @@ void f32_mode(int shape, const BatchView& b, const ProbTables<float>& t, const P
 template <int K, int V, int PM, bool MULTI, bool UNF>
 void f64_class(const BatchView& b, const ProbTables<double>& t, const PassControl& pc)
 {
-    run_warp([&](int lane) { warp_reruns64<K, V, PM, MULTI, UNF>(b, t, pc, lane, 0); });
+    std::vector<double> tab(prior_table_size<K>());
+    run_warp([&](int lane) { warp_reruns64<K, V, PM, MULTI, UNF>(b, t, pc, tab.data(), lane, 0); });
 }
 
 template <int V, int PM, bool UNF>
