@@ -343,7 +343,9 @@ def serving_latency(engine, pool: RequestPool, load: float, capacity_regions_per
             "max_submit_lag_ms": round(lag * 1e3, 2),
             "arena_grows": after["arena_grows"] - before["arena_grows"],
             "graph_captures": after["graph_captures"] - before["graph_captures"],
-            "max_setup_ms_so_far": round(after["max_setup_ms"], 2), "max_host_ms_so_far": round(after["max_host_ms"], 2)}
+            "max_setup_ms_so_far": round(after["max_setup_ms"], 2), "max_host_ms_so_far": round(after["max_host_ms"], 2),
+            "mean_phase_ms": {k: round((after[k + "_ms"] - before[k + "_ms"]) / max(batches, 1), 3)
+                              for k in ("gather", "plan", "enqueue", "wait", "scatter")}}
 
 
 def underflow_stress(engine, steps: int, warmup: int, cpu_threads: int | None, n_regions: int = 500) -> dict:

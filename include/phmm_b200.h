@@ -386,6 +386,10 @@ typedef struct phmm_server_stats {
     uint64_t graph_captures;      /* CUDA graph captures of the serving slots */
     double max_setup_ms;          /* longest arena growth + graph capture inside one batch */
     double max_host_ms;           /* longest host part of one batch (gather, plan, scatter) */
+    /* summed over the batches, in ms: gathering the requests into pinned staging, planning,
+     * uploading and launching, waiting for the device (and the results' copy back), and
+     * copying the results to the requests */
+    double gather_ms, plan_ms, enqueue_ms, wait_ms, scatter_ms;
 } phmm_server_stats;
 
 PHMM_API phmm_status phmm_server_stats_get(phmm_engine* engine, phmm_server_stats* stats);

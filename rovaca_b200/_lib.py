@@ -110,7 +110,8 @@ class ServerStats(C.Structure):
                 ("max_batch_regions", C.c_uint64), ("queue_peak", C.c_uint64), ("cells_done", C.c_uint64),
                 ("batch_ms", C.c_double), ("device_ms", C.c_double), ("max_batch_ms", C.c_double),
                 ("max_queue_ms", C.c_double), ("arena_grows", C.c_uint64), ("graph_captures", C.c_uint64),
-                ("max_setup_ms", C.c_double), ("max_host_ms", C.c_double)]
+                ("max_setup_ms", C.c_double), ("max_host_ms", C.c_double), ("gather_ms", C.c_double),
+                ("plan_ms", C.c_double), ("enqueue_ms", C.c_double), ("wait_ms", C.c_double), ("scatter_ms", C.c_double)]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}

@@ -249,6 +249,9 @@ void Server::worker(int idx)
         const uint64_t grows0 = slot ? slot->arena_grows : 0, caps0 = slot ? slot->graph_captures : 0;
         const double setup0 = slot ? slot->setup_ms : 0.0;
         double wait_ms = 0.0;  // time blocked on the device in finish()
+        // host phases of the batch (ms): gather into pinned staging, planning, upload and launch,
+        // results back to the requests
+        double gather_ms = 0.0, plan_ms = 0.0, enqueue_ms = 0.0, scatter_ms = 0.0;
         phmm_status st = mk;
         std::string berr = err;
         double device_ms = 0.0;
@@ -317,6 +320,8 @@ void Server::worker(int idx)
             b.read_del = rd[3];
             b.read_gcp = rd[4];
             b.read_off = roff.data();
+            const auto t_gathered = Clock::now();
+            gather_ms = ms_between(t_start, t_gathered);
             Plan plan;
             const TileTable tiles = eng->tiles();
             PlanLimits lim = Engine::limits_with(tiles);
@@ -344,6 +349,8 @@ void Server::worker(int idx)
                 plan.gl_total = gl_o;
                 plan.allele_lk_total = alk_o;
             }
+            const auto t_planned = Clock::now();
+            plan_ms = ms_between(t_gathered, t_planned);
             if (st == PHMM_OK) st = eng->enqueue(*slot, plan, b, want_flags, berr, api ? mq : nullptr);
             // realignment of the kept reads of the requests that asked for it, after the pipeline
             RealignBatch rb;
@@ -379,12 +386,14 @@ void Server::worker(int idx)
             if (want_flags) flags = (uint8_t*)(best + n_events);  // plain batches have no events
             phmm_stats ps{};
             const auto t_fin = Clock::now();
+            enqueue_ms = ms_between(t_planned, t_fin);
             if (st == PHMM_OK)
                 st = eng->finish(*slot, plan, (!api || want_out) ? out : nullptr, flags, &ps, berr, keep, kept_n,
                                  n_events ? gl : nullptr, n_events ? best : nullptr, want_alk ? alk : nullptr);
             if (st == PHMM_OK && rb.plan.n) st = eng->realign_finish(*slot, rb, berr);
             device_ms = ps.device_ms;
-            wait_ms = ms_between(t_fin, Clock::now());
+            const auto t_back = Clock::now();
+            wait_ms = ms_between(t_fin, t_back);
             if (st == PHMM_OK) {
                 uint64_t o = 0, ko = 0, go = 0, ao = 0, eo = 0;
                 for (size_t i = 0; i < batch.size(); ++i) {
@@ -408,6 +417,7 @@ void Server::worker(int idx)
                     eo += r->n_alleles.size();
                 }
             }
+            scatter_ms = ms_between(t_back, Clock::now());
         }
         {
             std::lock_guard<std::mutex> lk(mu);
@@ -428,6 +438,11 @@ void Server::worker(int idx)
             stats.batch_ms += ms_between(t_start, now);
             stats.device_ms += device_ms;
             stats.max_batch_ms = std::max(stats.max_batch_ms, ms_between(t_start, now));
+            stats.gather_ms += gather_ms;
+            stats.plan_ms += plan_ms;
+            stats.enqueue_ms += enqueue_ms;
+            stats.wait_ms += wait_ms;
+            stats.scatter_ms += scatter_ms;
             if (slot) {
                 stats.arena_grows += slot->arena_grows - grows0;
                 stats.graph_captures += slot->graph_captures - caps0;

@@ -47,7 +47,9 @@ int main(void)
     F(phmm_server_stats, max_batch_regions); F(phmm_server_stats, queue_peak); F(phmm_server_stats, cells_done);
     F(phmm_server_stats, batch_ms); F(phmm_server_stats, device_ms); F(phmm_server_stats, max_batch_ms);
     F(phmm_server_stats, max_queue_ms); F(phmm_server_stats, arena_grows); F(phmm_server_stats, graph_captures);
-    F(phmm_server_stats, max_setup_ms); F(phmm_server_stats, max_host_ms);
+    F(phmm_server_stats, max_setup_ms); F(phmm_server_stats, max_host_ms); F(phmm_server_stats, gather_ms);
+    F(phmm_server_stats, plan_ms); F(phmm_server_stats, enqueue_ms); F(phmm_server_stats, wait_ms);
+    F(phmm_server_stats, scatter_ms);
     S(phmm_sw_item);
     F(phmm_sw_item, hap_offset); F(phmm_sw_item, read_offset); F(phmm_sw_item, hap_len); F(phmm_sw_item, read_len);
     S(phmm_sw_result);
