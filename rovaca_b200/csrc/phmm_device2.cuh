@@ -8,11 +8,11 @@
 // components, through the same run of haplotype columns.  Lane l holds rows l*KH .. l*KH+KH-1 of
 // both reads' stripes and works on stream column p = t - l at step t, so the two components of every
 // float2 meet the same haplotype base: one packed instruction updates row a of X and row a of Y.
-// The three values of a lane's bottom rows go to lane l+1 by shuffle; lane 31 holds both reads'
-// last rows and sums them per haplotype.  Rows are padded at the top, each read by its own count,
-// and pad rows reproduce the boundary row exactly (prior 0 keeps M = 0, I stays 0 because the rows
-// above have M = I = 0, and xx = 1 keeps D = C/H).  Reads longer than one stripe run as stripes
-// linked through a per-warp scratch row of float2 values.
+// The three values of a lane's bottom rows go to lane l+1 by shuffle (two values formed from them in
+// PM_EQ); lane 31 holds both reads' last rows and sums them per haplotype.  Rows are padded at the
+// top, each read by its own count, and pad rows reproduce the boundary row exactly (prior 0 keeps
+// M = 0, I stays 0 because the rows above have M = I = 0, and xx = 1 keeps D = C/H).  Reads longer
+// than one stripe run as stripes linked through a per-warp scratch row of float2 values.
 //
 // Lane state between steps.  A lane does not keep its rows' M, I and D at its last column: it keeps,
 // per row, the values the next column starts from -- the diagonal sum s that M[i][j+1] = s * prior
@@ -36,7 +36,8 @@
 // PCR model, and the benchmark data), PM_ROW otherwise.  In PM_EQ, mm, gapm and mx (= my) are held
 // once per lane instead of once per row (xx stays per row: pad rows need xx = 1), which leaves
 // registers for more rows per lane, and a cell takes 7 operations instead of 8 (M * mx serves both
-// I of the row below and D of the next column).
+// I of the row below and D of the next column); the lane above forms the first row's I and diagonal
+// sum (cells2_eq), so a step shuffles two values instead of three.
 #pragma once
 
 #include <cstdint>
@@ -79,7 +80,12 @@ struct LaneRows2 {
     static constexpr int NR = PM == PM_ROW ? KH : 1;
     float2 S[KH];                   // (X, Y) diagonal sum of row a for the lane's next column
     float2 Dn[KH];                  // (X, Y) D of row a at the lane's next column
-    float2 Mb, Ib, Db;              // bottom row at the lane's last column (shuffled to lane + 1)
+    float2 Mb, Ib, Db;              // bottom row at the lane's last column (shuffled to lane + 1;
+                                    // PM_EQ: Mb and Ib only feed lane 31's sums)
+    float2 In, Sn;                  // PM_EQ: I of the row below the lane and that row's diagonal sum
+                                    // for its next column, formed from the bottom row (shuffled to
+                                    // lane + 1 in place of Mb, Ib and Db)
+    float2 xxn;                     // PM_EQ: xx of the row below the lane (1 for a pad row)
     float2 xx[KH];
     float2 mm[NR], gm[NR], mx[NR], my[NR];  // my: unused in PM_EQ (mx == my)
     uint32_t padX, padY;            // bit a: row a of the read is a pad row
@@ -142,7 +148,13 @@ __device__ __forceinline__ bool load_rows2(LaneRows2<KH, PM>& L, float4* tab, co
     // columns before the lane's first haplotype compute from these and are discarded
 #pragma unroll
     for (int a = 0; a < KH; ++a) L.S[a] = L.Dn[a] = f2(0.f, 0.f);
-    L.Mb = L.Ib = L.Db = f2(0.f, 0.f);
+    L.Mb = L.Ib = L.Db = L.In = L.Sn = f2(0.f, 0.f);
+    if (PM == PM_EQ) {
+        // for lane 31 the row below is the next stripe's first row
+        const int below = first + lane * KH + KH;
+        L.xxn = f2(row_params<V>(b, tb, rp.roff[0], rp.R[0], below - rp.pad[0]).xx,
+                   row_params<V>(b, tb, rp.roff[1], rp.R[1], below - rp.pad[1]).xx);
+    }
     if (PM != PM_ROW) {
         // constant along the read: any real row gives them (pad rows ignore them)
         const RowParams x0 = row_params<V>(b, tb, rp.roff[0], rp.R[0], rp.R[0] > 0 ? 0 : -1);
@@ -188,23 +200,39 @@ __device__ __forceinline__ bool load_rows2(LaneRows2<KH, PM>& L, float4* tab, co
 // its code word from shared memory instead of through L1.  A chunk reads columns [t0-31, t0+kChunk)
 // and the copies in flight write [t0+kChunk, t0+2 kChunk): 31 + 2 kChunk < kCodeRing slots, so no
 // copy overwrites a word a lane still reads.  Columns stay within the stream's guard words
-// (t0 + 2 kChunk <= Tcols + 32 + 2 kChunk < Tcols + kCodePad).
+// (t0 + 2 kChunk <= Tcols + 32 + 2 kChunk < Tcols + kCodePad).  Measured on B200 over the
+// 2,000-region benchmark batch: 1.3% faster than loading the words through L1.
 #ifndef PHMM_CODES_STAGED
-#define PHMM_CODES_STAGED 0
+#define PHMM_CODES_STAGED 1
 #endif
 constexpr int kCodeRing = 64;
 static_assert(31 + 2 * kChunk < kCodeRing && 32 + 2 * kChunk <= kCodePad, "code ring too small for the chunk");
 // float4 slots the ring adds to a warp's shared prior table
 constexpr int kRingFloat4 = PHMM_CODES_STAGED ? kCodeRing / 4 : 0;
 
+// (compiled for the host, as the CPU warp emulator does, a copy completes at once)
 #if PHMM_CODES_STAGED
 __device__ __forceinline__ void copy_word_async(uint32_t* dst_shared, const uint32_t* src)
 {
+#ifdef __CUDA_ARCH__
     const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst_shared);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+#else
+    *dst_shared = *src;
+#endif
 }
-__device__ __forceinline__ void copies_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void copies_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+__device__ __forceinline__ void copies_commit()
+{
+#ifdef __CUDA_ARCH__
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+#endif
+}
+__device__ __forceinline__ void copies_wait_all()
+{
+#ifdef __CUDA_ARCH__
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+#endif
+}
 #endif
 
 // Load the next step's priors during the current step (build-time setting): shortens the step of
@@ -223,38 +251,31 @@ __device__ __forceinline__ float2 diag_sum(const LaneRows2<KH, PM>& L, int r, fl
     return rfma2(dgD, L.gm[r], rfma2(dgI, L.gm[r], rmul2(dgM, L.mm[r])));
 }
 
-// All KH row pairs of the lane for one step at column j.  (upM, upI, upD): the row above the lane's
-// first row at column j; pr: the rows' priors at column j.  Per row i (the reference's operations):
+// All KH row pairs of the lane for one step at column j (PM_ALL and PM_ROW).  (upM, upI, upD): the
+// row above the lane's first row at column j; pr: the rows' priors at column j.  Per row i (the
+// reference's operations):
 //   M[i][j] = S * prior                                  S = s formed at the previous step
 //   I[i][j] = fma(I[i-1][j], xx, M[i-1][j] * mx)
 //   D[i][j] = Dn                                         Dn formed at the previous step
 //   Dn      = D[i][j+1]  = fma(D[i][j], yy, M[i][j] * my)        (yy = xx, the same ph2pr[gcp])
 //   S'      = s[i+1][j+1] from M, I, D[i][j]                     (diag_sum)
 // and the row above's values give the first row's S' for the next column.  A row's pending S is
-// read before the row above overwrites it.  In PM_EQ, M[i][j] * mx is the product that D[i][j+1]
-// needs (mx == my), formed once.
+// read before the row above overwrites it.
 template <int KH, int V, int PM>
 __device__ __forceinline__ void cells2(LaneRows2<KH, PM>& L, const float2 (&pr)[KH], float2 upM, float2 upI,
                                        float2 upD)
 {
-    constexpr bool EQ = PM == PM_EQ;
+    static_assert(PM != PM_EQ, "PM_EQ steps through cells2_eq");
     float2 Mab = upM, Iab = upI;    // the row above, this column
-    float2 Pab = f2(0.f, 0.f);      // PM_EQ: its M * mx
     float2 nM = rmul2(L.S[0], pr[0]);
 #pragma unroll
     for (int a = 0; a < KH; ++a) {
         const int r = PM == PM_ROW ? a : 0;
         const float2 M = nM;
         if (a + 1 < KH) nM = rmul2(L.S[a + 1], pr[a + 1]);  // before S[a + 1] is overwritten below
-        const float2 q = (EQ && a > 0) ? Pab : rmul2(Mab, L.mx[r]);
-        const float2 I = rfma2(Iab, L.xx[a], q);
+        const float2 I = rfma2(Iab, L.xx[a], rmul2(Mab, L.mx[r]));
         const float2 D = L.Dn[a];
-        if (EQ) {
-            Pab = rmul2(M, L.mx[0]);
-            L.Dn[a] = rfma2(D, L.xx[a], Pab);
-        } else {
-            L.Dn[a] = rfma2(D, L.xx[a], rmul2(M, L.my[r]));
-        }
+        L.Dn[a] = rfma2(D, L.xx[a], rmul2(M, L.my[r]));
         if (a + 1 < KH) {
             L.S[a + 1] = diag_sum<V, PM>(L, PM == PM_ROW ? a + 1 : 0, M, I, D);
         } else {
@@ -266,6 +287,40 @@ __device__ __forceinline__ void cells2(LaneRows2<KH, PM>& L, const float2 (&pr)[
         Iab = I;
     }
     L.S[0] = diag_sum<V, PM>(L, 0, upM, upI, upD);
+}
+
+// The same step in PM_EQ, where mm, gapm and mx (= my) are one value per read, so the lane above
+// can form the first row's inputs itself: upI = I[i0][j] of the lane's first row i0 and upS =
+// s[i0][j+1], both formed by the lane above from its bottom row at column j with the same operations
+// and operands (I from its M * mx and its copy of this lane's first xx, the sum from M, I, D).  That
+// shuffles two values instead of three and leaves 7 operations per cell: M * mx serves I of the row
+// below and D of the next column, and the bottom row's goes to the lane below as part of its I.
+template <int KH, int V, int PM>
+__device__ __forceinline__ void cells2_eq(LaneRows2<KH, PM>& L, const float2 (&pr)[KH], float2 upI, float2 upS)
+{
+    static_assert(PM == PM_EQ, "cells2_eq is the PM_EQ step");
+    float2 Iab = upI, Pab = f2(0.f, 0.f);  // I and M * mx of the row above, this column
+    float2 nM = rmul2(L.S[0], pr[0]);
+#pragma unroll
+    for (int a = 0; a < KH; ++a) {
+        const float2 M = nM;
+        if (a + 1 < KH) nM = rmul2(L.S[a + 1], pr[a + 1]);  // before S[a + 1] is overwritten below
+        const float2 I = a == 0 ? upI : rfma2(Iab, L.xx[a], Pab);
+        const float2 D = L.Dn[a];
+        Pab = rmul2(M, L.mx[0]);
+        L.Dn[a] = rfma2(D, L.xx[a], Pab);
+        const float2 s = diag_sum<V, PM>(L, 0, M, I, D);
+        if (a + 1 < KH) {
+            L.S[a + 1] = s;
+        } else {
+            L.Mb = M;
+            L.Ib = I;
+            L.Sn = s;
+            L.In = rfma2(I, L.xxn, Pab);
+        }
+        Iab = I;
+    }
+    L.S[0] = upS;
 }
 
 // Output side of a sweep: the two reads' likelihood columns and FP64 rerun lists.
@@ -305,6 +360,9 @@ __device__ void sweep2(LaneRows2<KH, PM>& L, float4* tab, const BatchView& b, co
     int nb = 0;
     bool started = false;
     float D0 = 0.f;
+    // PM_EQ: lane 0's first-row sum below the boundary row (M = I = 0, D = C/H) for the next column
+    constexpr bool EQ = PM == PM_EQ;
+    float2 Stop = f2(0.f, 0.f);
     float2 sumM = f2(0.f, 0.f), sumI = f2(0.f, 0.f);
 
     const int steps = Tcols + kWarp;  // lane 31 reaches column Tcols (the end) at step Tcols + 31
@@ -368,6 +426,7 @@ __device__ void sweep2(LaneRows2<KH, PM>& L, float4* tab, const BatchView& b, co
             // lane's first row when `above`).  The first column starts from the diagonal sums of
             // column 0 and from D[i][1] = fma(D[i][0], xx, 0 * my): C/H in pad rows (xx = 1), else 0.
             const float2 z = f2(0.f, 0.f);
+            if (EQ) Stop = diag_sum<V, PM>(L, 0, z, z, f2(D0, D0));
             float2 Dab = f2(aboveX ? D0 : 0.f, aboveY ? D0 : 0.f);
 #pragma unroll
             for (int a = 0; a < KH; ++a) {
@@ -409,16 +468,32 @@ __device__ void sweep2(LaneRows2<KH, PM>& L, float4* tab, const BatchView& b, co
 
     auto step = [&](int t, bool check) {
         const int p = t - lane;
-        float2 uM = shfl_up2(L.Mb);
-        float2 uI = shfl_up2(L.Ib);
-        float2 uD = shfl_up2(L.Db);
+        // the row above the lane's first row: its M, I and D, or (PM_EQ) the first row's I and sum
+        float2 uM, uI, uD;
+        if (EQ) {
+            uI = shfl_up2(L.In);
+            uD = shfl_up2(L.Sn);
+        } else {
+            uM = shfl_up2(L.Mb);
+            uI = shfl_up2(L.Ib);
+            uD = shfl_up2(L.Db);
+        }
         if (check && p == nb) boundary();
         if (lane == 0) {
             if (FROM_SCR) {
                 const bool ok = p >= 0 && p < Tcols;
-                uM = ok ? scr[3 * p + 0] : f2(0.f, 0.f);
-                uI = ok ? scr[3 * p + 1] : f2(0.f, 0.f);
-                uD = ok ? scr[3 * p + 2] : f2(0.f, 0.f);
+                if (EQ) {
+                    uI = ok ? scr[2 * p + 0] : f2(0.f, 0.f);
+                    uD = ok ? scr[2 * p + 1] : f2(0.f, 0.f);
+                } else {
+                    uM = ok ? scr[3 * p + 0] : f2(0.f, 0.f);
+                    uI = ok ? scr[3 * p + 1] : f2(0.f, 0.f);
+                    uD = ok ? scr[3 * p + 2] : f2(0.f, 0.f);
+                }
+            } else if (EQ) {
+                // below the boundary row (M = I = 0, D = C/H): I = fma(0, xx, 0 * mx) = 0
+                uI = f2(0.f, 0.f);
+                uD = Stop;
             } else {
                 uM = f2(0.f, 0.f);
                 uI = f2(0.f, 0.f);
@@ -448,12 +523,20 @@ __device__ void sweep2(LaneRows2<KH, PM>& L, float4* tab, const BatchView& b, co
                     pr[a].y = tb.pmat[b.read_q[rp.roff[1] + iY] & 127];
             }
         }
-        cells2<KH, V, PM>(L, pr, uM, uI, uD);
+        if constexpr (EQ)
+            cells2_eq<KH, V, PM>(L, pr, uI, uD);
+        else
+            cells2<KH, V, PM>(L, pr, uM, uI, uD);
         if (TO_SCR) {
             if (writer && p >= 0 && p < Tcols) {
-                scr[3 * p + 0] = L.Mb;
-                scr[3 * p + 1] = L.Ib;
-                scr[3 * p + 2] = L.Db;
+                if (EQ) {
+                    scr[2 * p + 0] = L.In;
+                    scr[2 * p + 1] = L.Sn;
+                } else {
+                    scr[3 * p + 0] = L.Mb;
+                    scr[3 * p + 1] = L.Ib;
+                    scr[3 * p + 2] = L.Db;
+                }
             }
         } else {
             sumM = radd2(sumM, L.Mb);

@@ -21,6 +21,18 @@
 #include "phmm_regionk.h"
 #include "phmm_tables.h"
 
+// FP32 single-stripe grids are PHMM_F32_WAVES times the resident warps, each warp taking an equal
+// share of its class's items and exiting, so that SMs free up during the pass (build-time setting;
+// 1 = persistent warps).  PHMM_CLASS_PRIORITY (build-time, 0 or 1) launches each mode's FP32 classes
+// longest reads first on low-priority streams and the FP64 classes on high-priority streams, so an
+// FP64 class whose sources have finished takes the SMs that FP32 blocks free.
+#ifndef PHMM_F32_WAVES
+#define PHMM_F32_WAVES 1
+#endif
+#ifndef PHMM_CLASS_PRIORITY
+#define PHMM_CLASS_PRIORITY 0
+#endif
+
 namespace phmm {
 
 #define PHMM_CK(call)                                                                    \
@@ -434,7 +446,10 @@ phmm_status Engine::make_slot(int id, Slot** out, std::string& err)
     s->id = id;
     auto cleanup = [&]() { free_slot(s); };
     cudaError_t e = cudaStreamCreateWithFlags(&s->main, cudaStreamNonBlocking);
-    for (int c = 0; c < kNumClasses && e == cudaSuccess; ++c) e = cudaStreamCreateWithFlags(&s->side[c], cudaStreamNonBlocking);
+    int least = 0, greatest = 0;
+    if (PHMM_CLASS_PRIORITY && e == cudaSuccess) e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    for (int c = 0; c < kNumClasses && e == cudaSuccess; ++c)
+        e = cudaStreamCreateWithPriority(&s->side[c], cudaStreamNonBlocking, c < kClasses32 ? least : greatest);
     for (int c = 0; c < kNumClasses && e == cudaSuccess; ++c) e = cudaEventCreateWithFlags(&s->ev_side[c], cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreate(&s->ev_t0);
@@ -557,9 +572,19 @@ phmm_status Engine::reserve(Slot& s, const Capacity& want, std::string& err)
     return PHMM_OK;
 }
 
+static unsigned int waves32(int cls)
+{
+    return class32_multi(cls) ? 1u : (unsigned int)PHMM_F32_WAVES;
+}
+
+int Engine::full_grid(int precision, int cls) const
+{
+    return occ_[precision == 32 ? 0 : 1][cls] * sms_ * (precision == 32 ? (int)waves32(cls) : 1);
+}
+
 int Engine::grid_for(int precision, int cls, uint32_t work) const
 {
-    const int full = occ_[precision == 32 ? 0 : 1][cls] * sms_;
+    const int full = full_grid(precision, cls);
     const int warps_per_block = kFwdBlock / kWarp;
     const int need = (int)std::min<uint64_t>(((uint64_t)work + warps_per_block - 1) / warps_per_block, (uint64_t)full);
     return std::max(need, 1);
@@ -654,15 +679,18 @@ phmm_status Engine::launch_pipeline(Slot& s, bool want_flags, const Plan* plan, 
         const int precision = pass == 0 ? 32 : 64;
         const int n_cls = pass == 0 ? kClasses32 : kClasses64;
         const int slot0 = pass == 0 ? 0 : kClasses32;  // descriptor slot of the pass's first class
-        for (int c = 0; c < n_cls; ++c) {
+        for (int k = 0; k < n_cls; ++k) {
+            // FP32 classes of a mode longest reads first (multi-stripe shapes, then KH = 8 .. 1)
+            const int c = pass == 0 && PHMM_CLASS_PRIORITY ? (k / kShapes32) * kShapes32 + kShapes32 - 1 - k % kShapes32
+                                                           : k;
             uint32_t work = 0;
             if (plan) {
                 work = pass == 0 ? plan->classes[c].n_items : plan->classes[slot0 + c].rerun_cap;
                 if (work == 0) continue;
             }
             // FP32 items hold two reads (warps = items); FP64 claims are single pairs
-            const int grid = plan ? grid_for(precision, c, work) : occ_[pass][c] * sms_;
-            PassControl pc;
+            const int grid = plan ? grid_for(precision, c, work) : full_grid(precision, c);
+            PassControl pc{};
             pc.cd = s.d_classes + slot0 + c;
             pc.cd64 = s.d_classes + kClasses32;
             pc.items = s.d_items;
@@ -672,6 +700,7 @@ phmm_status Engine::launch_pipeline(Slot& s, bool want_flags, const Plan* plan, 
             const int region = pass == 0 ? 0 : 1 + c / 9;
             pc.scratch = multi ? (void*)((char*)s.d_scratch + scratch_offset_warps(region) * scr_cols * 24) : nullptr;
             pc.scratch_cols = scr_cols;
+            pc.waves = pass == 0 ? waves32(c) : 1u;
             cudaStream_t st = s.side[slot0 + c];
             PHMM_CK(cudaStreamWaitEvent(st, s.ev_fork, 0));
             // FP32 multi-stripe classes share one scratch region: each waits for the previous one
@@ -730,7 +759,7 @@ phmm_status Engine::capture_graph(Slot& s, bool want_flags, const TileTable& til
         err = std::string("graph capture failed: ") + cudaGetErrorString(e);
         return PHMM_ERR_CUDA;
     }
-    e = cudaGraphInstantiate(&s.graph, g, 0);
+    e = cudaGraphInstantiate(&s.graph, g, PHMM_CLASS_PRIORITY ? cudaGraphInstantiateFlagUseNodePriority : 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) {
         s.graph = nullptr;
@@ -1198,7 +1227,7 @@ phmm_status Engine::time_fp32_class(Slot& s, const Plan& plan, int cls, int reps
     v.out = s.d_out;
     v.pair_flags = nullptr;
     const uint64_t warps = scratch_warps();
-    PassControl pc;
+    PassControl pc{};
     pc.cd = s.d_classes + cls;
     pc.cd64 = s.d_classes + kClasses32;
     pc.items = s.d_items;
@@ -1206,6 +1235,7 @@ phmm_status Engine::time_fp32_class(Slot& s, const Plan& plan, int cls, int reps
     pc.status = s.d_status;
     pc.scratch = s.d_scratch;  // the FP32 multi-stripe region
     pc.scratch_cols = s.cap.scratch_cols ? (unsigned int)(s.cap.scratch_cols / warps) : 0u;
+    pc.waves = waves32(cls);
     const int grid = grid_for(32, cls, plan.classes[cls].n_items);
     cudaStream_t m = s.main;
     float best = 0.f;
@@ -1297,7 +1327,7 @@ phmm_status Engine::check_fp64(Slot& s, const Plan& plan, double* out, std::stri
         PHMM_CK(occupancy_f64_check(c, &occ));
         uint64_t grid = std::min<uint64_t>(per[c].size(), (uint64_t)std::max(occ, 1) * sms_);
         if (multi) grid = std::min(grid, scratch_offset_warps(region + 1) - scratch_offset_warps(region));
-        PassControl pc;
+        PassControl pc{};
         pc.cd = s.d_classes + kClasses32 + c;
         pc.cd64 = s.d_classes + kClasses32;
         pc.items = s.d_items;
@@ -1363,7 +1393,7 @@ phmm_status Engine::profile_classes(Slot& s, const Plan& plan, float* class_ms, 
             if (work == 0) continue;
             const bool multi = pass == 0 ? class32_multi(c) : c % 9 == 8;
             const int region = pass == 0 ? 0 : 1 + c / 9;
-            PassControl pc;
+            PassControl pc{};
             pc.cd = s.d_classes + slot0 + c;
             pc.cd64 = s.d_classes + kClasses32;
             pc.items = s.d_items;
@@ -1371,6 +1401,7 @@ phmm_status Engine::profile_classes(Slot& s, const Plan& plan, float* class_ms, 
             pc.status = s.d_status;
             pc.scratch = multi ? (void*)((char*)s.d_scratch + scratch_offset_warps(region) * scr_cols * 24) : nullptr;
             pc.scratch_cols = scr_cols;
+            pc.waves = pass == 0 ? waves32(c) : 1u;
             PHMM_CK(cudaEventRecord(ev[2 * (slot0 + c)], m));
             PHMM_CK(launch_fwd(precision, c, v, tf_, td_, pc, grid_for(precision, c, work), m));
             PHMM_CK(cudaEventRecord(ev[2 * (slot0 + c) + 1], m));

@@ -177,6 +177,7 @@ private:
     int dev_ = 0;
     int sms_ = 0;
     int occ_[2][kNumClasses] = {};
+    int full_grid(int precision, int cls) const;  // resident blocks of a class (times its waves)
     // device probability tables
     void* d_tables_ = nullptr;
     ProbTables<float> tf_{};

@@ -42,7 +42,12 @@ __global__ void __launch_bounds__(kFwdBlock, min_blocks32<KH, V, PM>()) fwd_f32_
     __shared__ float4 tab[tab_floats4<KH>() + kRingFloat4];
     const int lane = threadIdx.x & (kWarp - 1);
     const unsigned int warp_id = (blockIdx.x * blockDim.x + threadIdx.x) / kWarp;
-    warp_items32<KH, V, PM, MULTI>(b, tb, pc, tab, lane, warp_id);
+    // Over-subscribed grid (waves > 1): warps that exit after their share leave room on the SMs for
+    // blocks of higher-priority kernels.  Multi-stripe warps index scratch rows by warp and stay
+    // persistent.
+    const unsigned int n_warps = gridDim.x * (blockDim.x / kWarp);
+    const unsigned int cap = (!MULTI && pc.waves > 1) ? (pc.cd->n_items + n_warps - 1) / n_warps : 0xffffffffu;
+    warp_items32<KH, V, PM, MULTI>(b, tb, pc, tab, lane, warp_id, cap);
 }
 
 typedef void (*F32Kernel)(BatchView, ProbTables<float>, PassControl);

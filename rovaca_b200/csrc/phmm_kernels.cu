@@ -55,11 +55,12 @@ __global__ void reset_outputs_kernel(const BatchDesc* __restrict__ desc, double*
 // FP64 pass for one class over the runs of underflowed pairs the FP32 pass appended, one run per
 // claim, streamed through the read like an FP32 work item.
 // ------------------------------------------------------------------------------------------
-// FP64 kernels with constant gap parameters and 7-8 rows per lane fit three warps per scheduler when
-// held to 168 registers (no spills at 8 rows, 16 bytes for the multi-stripe one); the others keep
-// what they need.
+// FP64 kernels with constant gap parameters and 7-8 rows per lane run four warps per scheduler at 128
+// registers (spilling a few hundred bytes, which stay in L1): measured on B200 with the per-lane
+// prior tables, 3% faster than three warps at 168 registers without spills on the benchmark batch's
+// FP64 pass and 2.4% on the underflow-stress shape.  The others keep what they need.
 #ifndef PHMM_F64_MIN_WARPS
-#define PHMM_F64_MIN_WARPS 12
+#define PHMM_F64_MIN_WARPS 16
 #endif
 template <int K, int PM>
 constexpr int min_blocks64()

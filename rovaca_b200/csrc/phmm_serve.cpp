@@ -5,9 +5,10 @@
 // requests: phmm_submit validates and copies the region and queues it; kSlots worker threads each
 // own a device slot (arena, streams, captured graph) and pinned staging buffers.  A worker that is
 // free takes every queued request that fits the HBM budget and the per-batch cell cap, gathers them
-// into its pinned buffer, runs them as one batch, scatters the results and signals the requests.  While one slot's batch is on the GPU the next worker is already forming
-// and launching the next one, so requests that arrive meanwhile are admitted as soon as a slot and
-// budget are free, and their kernels overlap with the running ones on the device.  Each pair's
+// into its pinned buffer, runs them as one batch, scatters the results and signals the requests.
+// While one slot's batch is on the GPU the next worker is already forming and launching the next
+// one, so requests that arrive meanwhile are admitted as soon as a slot and budget are free, and
+// their kernels overlap with the running ones on the device.  Each pair's
 // arithmetic does not depend on what it was batched with, so a region's likelihoods are the same
 // alone and in any mix.
 #include <algorithm>
@@ -35,7 +36,16 @@ namespace {
 
 using Clock = std::chrono::steady_clock;
 
-constexpr int kSlots = 3;                            // batches in flight at once
+// Batches in flight at once (build-time setting).
+#ifndef PHMM_SERVE_SLOTS
+#define PHMM_SERVE_SLOTS 3
+#endif
+constexpr int kSlots = PHMM_SERVE_SLOTS;
+// Gathering a batch's requests into pinned staging runs on up to kGatherThreads threads (the
+// worker and helpers) once the batch holds more than kGatherSplit bytes: one thread copies about
+// 5 GB/s into page-locked memory, which made the gather a third of a large batch's host time.
+constexpr int kGatherThreads = 4;
+constexpr size_t kGatherSplit = 4u << 20;
 // Bound on one batch's work (~35 ms on B200): a burst of requests becomes several batches that
 // pipeline through the slots instead of one long batch that every later arrival waits behind.
 constexpr uint64_t kMaxBatchCells = 80000000000ull;
@@ -133,6 +143,37 @@ struct Server {
 std::mutex g_reg_mu;
 std::map<phmm_engine*, std::unique_ptr<Server>> g_servers;
 
+struct HostCopy {
+    uint8_t* dst;
+    const uint8_t* src;
+    size_t n;
+};
+
+// Runs the copies on up to kGatherThreads threads, split into runs of about equal bytes.
+void run_copies(const std::vector<HostCopy>& copies, size_t total)
+{
+    auto run = [&](size_t lo, size_t hi) {
+        for (size_t i = lo; i < hi; ++i) std::memcpy(copies[i].dst, copies[i].src, copies[i].n);
+    };
+    const int T = total < kGatherSplit ? 1 : (int)std::min<size_t>(kGatherThreads, copies.size());
+    if (T <= 1) {
+        run(0, copies.size());
+        return;
+    }
+    std::vector<size_t> cut(T + 1, copies.size());
+    cut[0] = 0;
+    size_t acc = 0;
+    int k = 1;
+    for (size_t i = 0; i < copies.size() && k < T; ++i) {
+        acc += copies[i].n;
+        if (acc * T >= total * k) cut[k++] = i + 1;
+    }
+    std::vector<std::thread> helpers;
+    for (int t = 1; t < T; ++t) helpers.emplace_back(run, cut[t], cut[t + 1]);
+    run(cut[0], cut[1]);
+    for (auto& h : helpers) h.join();
+}
+
 uint64_t footprint(uint64_t read_bases, uint64_t hap_bases, uint64_t pairs, uint64_t n_reads, uint64_t n_haps)
 {
     return read_bases * 5 + hap_bases * 9 + pairs * (8 + 1 + 16) + n_reads * 17 + n_haps * 9 + 4096;
@@ -203,6 +244,7 @@ void Server::worker(int idx)
     std::vector<uint32_t> nh, nr;
     std::vector<uint64_t> hoff, roff;
     std::vector<RegionApiParams> params;
+    std::vector<HostCopy> copies;
     PinnedBuf in_buf, out_buf;
     if (slot && slot->floor.read_bases) {
         in_buf.reserve(in_floor);
@@ -292,22 +334,29 @@ void Server::worker(int idx)
             hoff.assign(1, 0);
             roff.assign(1, 0);
             uint64_t ho = 0, ro = 0;
+            copies.clear();
+            size_t copy_bytes = 0;
+            auto add = [&](uint8_t* dst, const uint8_t* src, size_t n) {
+                if (n) copies.push_back({dst, src, n});
+                copy_bytes += n;
+            };
             for (auto& r : batch) {
                 nh.push_back(r->n_haps);
                 nr.push_back(r->n_reads);
                 for (uint32_t h = 0; h < r->n_haps; ++h) hoff.push_back(ho + r->hap_off[h + 1]);
                 for (uint32_t k = 0; k < r->n_reads; ++k) roff.push_back(ro + r->read_off[k + 1]);
-                if (r->hap_bases) std::memcpy(hb + ho, r->data.data(), r->hap_bases);
+                add(hb + ho, r->data.data(), r->hap_bases);
                 for (int k = 0; k < read_arrays && r->read_bases; ++k)
-                    std::memcpy(rd[k] + ro, r->data.data() + r->hap_bases + (uint64_t)k * r->read_bases, r->read_bases);
+                    add(rd[k] + ro, r->data.data() + r->hap_bases + (uint64_t)k * r->read_bases, r->read_bases);
                 if (api) {
-                    if (r->n_reads) std::memcpy(mq + mo, r->mapq.data(), r->n_reads);
+                    add(mq + mo, r->mapq.data(), r->n_reads);
                     mo += r->n_reads;
                     params.push_back(r->params);
                 }
                 ho += r->hap_bases;
                 ro += r->read_bases;
             }
+            run_copies(copies, copy_bytes);
             phmm_batch b{};
             b.n_regions = (uint32_t)batch.size();
             b.n_haps = nh.data();

@@ -197,6 +197,9 @@ struct PassControl {
     unsigned int* status;         // StatusBits, OR-ed
     void* scratch;                // per-warp stripe rows (multi-stripe reads)
     unsigned int scratch_cols;    // columns per warp scratch row
+    unsigned int waves;           // FP32 single-stripe classes: the grid is this many times the
+                                  // resident warps and each warp takes an equal share of the items
+                                  // (0 or 1: persistent warps that take items until none are left)
 };
 
 // Per-byte match codes.

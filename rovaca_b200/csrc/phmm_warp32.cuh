@@ -61,11 +61,12 @@ __device__ __forceinline__ void run_pair2(const BatchView& b, const ProbTables<f
     }
 }
 
-// The claim loop of one warp: work items of the class (pc.cd) until its counter runs out.  tab: the
-// warp's shared prior table (and code ring); warp_id: the warp's index in the grid (its scratch row).
+// The claim loop of one warp: work items of the class (pc.cd) until its counter runs out or the warp
+// has taken `cap` of them.  tab: the warp's shared prior table (and code ring); warp_id: the warp's
+// index in the grid (its scratch row).
 template <int KH, int V, int PM, bool MULTI>
 __device__ __forceinline__ void warp_items32(const BatchView& b, const ProbTables<float>& tb, const PassControl& pc,
-                                             float4* tab, int lane, unsigned int warp_id)
+                                             float4* tab, int lane, unsigned int warp_id, unsigned int cap)
 {
     float2* scr = MULTI ? (float2*)pc.scratch + (size_t)warp_id * pc.scratch_cols * 3 : nullptr;
     const unsigned int n = pc.cd->n_items;
@@ -73,7 +74,7 @@ __device__ __forceinline__ void warp_items32(const BatchView& b, const ProbTable
     // the kernel's class mode (0 constant gaps with insertion = deletion, 1 per-row, 2 intra); its
     // underflowed pairs go to the FP64 classes of that mode
     const int mode = mode32(V, PM == PM_ROW ? 1 : 0);
-    for (;;) {
+    for (unsigned int taken = 0; taken < cap; ++taken) {
         const unsigned int idx = claim(&pc.cd->claim32, lane);
         if (idx >= n) break;
         const WorkItem it = items[idx];

@@ -58,7 +58,7 @@ template <int KH, int V, int PM, bool MULTI>
 void f32_class(const BatchView& b, const ProbTables<float>& t, const PassControl& pc)
 {
     std::vector<float4> tab(tab_floats4<KH>() + kRingFloat4);
-    run_warp([&](int lane) { warp_items32<KH, V, PM, MULTI>(b, t, pc, tab.data(), lane, 0); });
+    run_warp([&](int lane) { warp_items32<KH, V, PM, MULTI>(b, t, pc, tab.data(), lane, 0, 0xffffffffu); });
 }
 
 template <int V, int PM>
