@@ -195,18 +195,18 @@ __device__ __forceinline__ bool load_rows2(LaneRows2<KH, PM>& L, float4* tab, co
 }
 
 // Haplotype code words staged in shared memory (build-time setting): each warp keeps a ring of
-// kCodeRing words, the columns its lanes read in the current chunk of steps, and copies the next
-// chunk's words from global memory with cp.async while the current chunk computes, so a step reads
-// its code word from shared memory instead of through L1.  A chunk reads columns [t0-31, t0+kChunk)
-// and the copies in flight write [t0+kChunk, t0+2 kChunk): 31 + 2 kChunk < kCodeRing slots, so no
-// copy overwrites a word a lane still reads.  Columns stay within the stream's guard words
-// (t0 + 2 kChunk <= Tcols + 32 + 2 kChunk < Tcols + kCodePad).  Measured on B200 over the
+// kCodeRing words, the columns its lanes read in the current chunk of steps and the next
+// kRingAhead chunks', copying the words of the chunk after those from global memory with cp.async
+// while the current chunk computes, so a step reads its code word from shared memory instead of
+// through L1.  A chunk reads columns [t0-31, t0+kChunk] and the copies in flight write
+// [t0+(A)kChunk, t0+(A+1)kChunk) (A = kRingAhead): 31 + (A+1) kChunk <= kCodeRing slots, so no copy
+// overwrites a word a lane still reads.  Columns stay within the stream's guard words
+// (t0 + (A+1) kChunk <= Tcols + 32 + (A+1) kChunk <= Tcols + kCodePad).  Measured on B200 over the
 // 2,000-region benchmark batch: 1.3% faster than loading the words through L1.
 #ifndef PHMM_CODES_STAGED
 #define PHMM_CODES_STAGED 1
 #endif
 constexpr int kCodeRing = 64;
-static_assert(31 + 2 * kChunk < kCodeRing && 32 + 2 * kChunk <= kCodePad, "code ring too small for the chunk");
 // float4 slots the ring adds to a warp's shared prior table
 constexpr int kRingFloat4 = PHMM_CODES_STAGED ? kCodeRing / 4 : 0;
 
@@ -235,14 +235,19 @@ __device__ __forceinline__ void copies_wait_all()
 }
 #endif
 
-// Load the next step's priors during the current step (build-time setting): shortens the step of
-// a warp that runs alone on its scheduler, at the cost of KH register pairs.  Measured on B200 with
-// 12 warps per SM for KH >= 4: one region per call 140 instead of 124 GCUPS on the device, the
-// 2,000-region batch 2279 instead of 2361 GCUPS; off by default, the batch being the target.
+// Load the next step's priors during the current step (build-time setting): shortens the step of a
+// warp that runs alone on its scheduler at the cost of KH register pairs.  Measured on B200 with 12
+// warps per SM for KH >= 4: one region per call 140 instead of 124 GCUPS on the device, the
+// 2,000-region batch 2279 instead of 2361 GCUPS.  Loading only the first two row pairs' priors ahead
+// (the first rows of a step need them first) ran the batch 1.4% slower than none.  0 by default.
 #ifndef PHMM_PRIOR_PREFETCH
 #define PHMM_PRIOR_PREFETCH 0
 #endif
-static_assert(!(PHMM_PRIOR_PREFETCH && PHMM_CODES_STAGED), "the prefetch reads a code word before the ring is filled");
+// Chunks of code words the ring holds ahead of the chunk being computed: a prefetching step reads
+// the word of the column after its own, which at a chunk's last step is the next chunk's first.
+constexpr int kRingAhead = PHMM_PRIOR_PREFETCH ? 2 : 1;
+static_assert(31 + (kRingAhead + 1) * kChunk <= kCodeRing && 32 + (kRingAhead + 1) * kChunk <= kCodePad,
+              "code ring too small for the chunks it holds ahead");
 
 template <int V, int PM, int KH>
 __device__ __forceinline__ float2 diag_sum(const LaneRows2<KH, PM>& L, int r, float2 dgM, float2 dgI, float2 dgD)
@@ -461,6 +466,11 @@ __device__ void sweep2(LaneRows2<KH, PM>& L, float4* tab, const BatchView& b, co
         }
         return w;
     };
+#if PHMM_CODES_STAGED
+    // columns [-32, kRingAhead * kChunk) before the first chunk
+    for (int q = lane - kWarp; q < kRingAhead * kChunk; q += kWarp) ring[q & (kCodeRing - 1)] = codes[q];
+    __syncwarp();
+#endif
 #if PHMM_PRIOR_PREFETCH
     float2 prn[KH];
     uint32_t wn = load_priors(-lane, prn);
@@ -544,17 +554,15 @@ __device__ void sweep2(LaneRows2<KH, PM>& L, float4* tab, const BatchView& b, co
         }
     };
 
-#if PHMM_CODES_STAGED
-    // columns [-32, kChunk) before the first chunk
-    for (int q = lane - kWarp; q < kChunk; q += kWarp) ring[q & (kCodeRing - 1)] = codes[q];
-    __syncwarp();
-#endif
     for (int t0 = 0; t0 < steps; t0 += kChunk) {
 #if PHMM_CODES_STAGED
-        // this chunk's columns are in the ring; start copying the next chunk's
+        // the columns up to kRingAhead chunks ahead are in the ring; start copying the chunk after
         copies_wait_all();
         __syncwarp();
-        if (lane < kChunk) copy_word_async(&ring[(t0 + kChunk + lane) & (kCodeRing - 1)], codes + t0 + kChunk + lane);
+        if (lane < kChunk) {
+            const int q = t0 + kRingAhead * kChunk + lane;
+            copy_word_async(&ring[q & (kCodeRing - 1)], codes + q);
+        }
         copies_commit();
 #endif
         // Lanes cover stream columns [t0-31, t0+kChunk-1] in this chunk.  Lane 31 trails, so its
