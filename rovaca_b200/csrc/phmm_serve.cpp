@@ -41,14 +41,19 @@ using Clock = std::chrono::steady_clock;
 #define PHMM_SERVE_SLOTS 3
 #endif
 constexpr int kSlots = PHMM_SERVE_SLOTS;
-// Gathering a batch's requests into pinned staging runs on up to kGatherThreads threads (the
-// worker and helpers) once the batch holds more than kGatherSplit bytes: one thread copies about
-// 5 GB/s into page-locked memory, which made the gather a third of a large batch's host time.
+// Gathering a batch's requests into pinned staging, and copying the results out to the requests, run
+// on up to kGatherThreads threads (the worker and helpers) once a batch moves more than kGatherSplit
+// bytes: one thread copies about 5 GB/s to or from page-locked memory, which made the gather a third
+// of a large batch's host time.
 constexpr int kGatherThreads = 4;
 constexpr size_t kGatherSplit = 4u << 20;
-// Bound on one batch's work (~35 ms on B200): a burst of requests becomes several batches that
-// pipeline through the slots instead of one long batch that every later arrival waits behind.
-constexpr uint64_t kMaxBatchCells = 80000000000ull;
+// Bound on one batch's work (~30 ms on B200; build-time setting): a burst of requests becomes several
+// batches that pipeline through the slots instead of one long batch that every later arrival waits
+// behind.
+#ifndef PHMM_SERVE_MAX_CELLS
+#define PHMM_SERVE_MAX_CELLS 80000000000ull
+#endif
+constexpr uint64_t kMaxBatchCells = PHMM_SERVE_MAX_CELLS;
 // Queued requests a forming batch looks through for requests of its kind.
 constexpr size_t kAdmitScan = 4096;
 constexpr size_t kMaxQueued = 1u << 20;
@@ -445,19 +450,25 @@ void Server::worker(int idx)
             wait_ms = ms_between(t_fin, t_back);
             if (st == PHMM_OK) {
                 uint64_t o = 0, ko = 0, go = 0, ao = 0, eo = 0;
+                copies.clear();
+                size_t copy_bytes = 0;
+                auto add = [&](void* dst, const void* src, size_t n) {
+                    if (n) copies.push_back({(uint8_t*)dst, (const uint8_t*)src, n});
+                    copy_bytes += n;
+                };
                 for (size_t i = 0; i < batch.size(); ++i) {
                     auto& r = batch[i];
-                    if (r->out && r->out_n) std::memcpy(r->out, out + o, r->out_n * sizeof(double));
-                    if (r->flags && r->out_n) std::memcpy(r->flags, flags + o, r->out_n);
+                    if (r->out) add(r->out, out + o, r->out_n * sizeof(double));
+                    if (r->flags) add(r->flags, flags + o, r->out_n);
                     if (api) {
-                        if (r->n_reads) std::memcpy(r->keep, keep + ko, r->n_reads);
+                        add(r->keep, keep + ko, r->n_reads);
                         *r->n_kept = kept_n[i];
                     }
                     if (r->realign) scatter_realign(*r, rb, i);
                     if (!r->n_alleles.empty()) {
-                        std::memcpy(r->gl, gl + go, r->gl_n * sizeof(double));
-                        std::memcpy(r->best, best + eo, r->n_alleles.size() * sizeof(int32_t));
-                        if (r->allele_lk) std::memcpy(r->allele_lk, alk + ao, r->allele_lk_n * sizeof(double));
+                        add(r->gl, gl + go, r->gl_n * sizeof(double));
+                        add(r->best, best + eo, r->n_alleles.size() * sizeof(int32_t));
+                        if (r->allele_lk) add(r->allele_lk, alk + ao, r->allele_lk_n * sizeof(double));
                     }
                     o += r->out_n;
                     ko += r->n_reads;
@@ -465,6 +476,7 @@ void Server::worker(int idx)
                     ao += r->allele_lk_n;
                     eo += r->n_alleles.size();
                 }
+                run_copies(copies, copy_bytes);
             }
             scatter_ms = ms_between(t_back, Clock::now());
         }
