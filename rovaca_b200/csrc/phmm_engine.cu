@@ -21,17 +21,16 @@
 #include "phmm_regionk.h"
 #include "phmm_tables.h"
 
-// FP32 single-stripe grids are PHMM_F32_WAVES times the resident warps, each warp taking an equal
-// share of its class's items and exiting, so that SMs free up during the pass (build-time setting;
-// 1 = persistent warps).  PHMM_CLASS_PRIORITY (build-time, 0 or 1) launches each mode's FP32 classes
-// longest reads first on low-priority streams and the FP64 classes on high-priority streams, so an
-// FP64 class whose sources have finished takes the SMs that FP32 blocks free.
-#ifndef PHMM_F32_WAVES
-#define PHMM_F32_WAVES 1
-#endif
-#ifndef PHMM_CLASS_PRIORITY
-#define PHMM_CLASS_PRIORITY 0
-#endif
+// Serving slots share the GPU with the other slots' batches.  Their FP32 single-stripe grids are
+// kOverlapWaves times the resident warps, each warp taking an equal share of its class's items and
+// exiting, so SMs free up during the pass; their FP32 classes run longest reads first on
+// low-priority streams and their FP64 classes on high-priority streams, so an FP64 class whose
+// sources have finished takes the SMs that FP32 blocks free, and a batch finishes before the next
+// slot's FP32 work has drained.  Measured on B200 (serving loop, 2,000-region pool, 95% of the
+// end-to-end batched rate): with 3 slots p50/p99 293/464 ms without, 142/208 ms with; with 5 slots
+// 102/183 ms without, 37/57 ms with.  A lone batch (the resident and chunked paths) gains nothing
+// from either (1% slower): its FP64 pass is work at full occupancy, not idle SMs.
+constexpr unsigned int kOverlapWaves = 4;
 
 namespace phmm {
 
@@ -438,7 +437,7 @@ phmm_status Engine::sw_aligner(SwAligner** out, std::string& err)
     return PHMM_OK;
 }
 
-phmm_status Engine::make_slot(int id, Slot** out, std::string& err)
+phmm_status Engine::make_slot(int id, Slot** out, std::string& err, bool overlap)
 {
     *out = nullptr;
     PHMM_CK(cudaSetDevice(dev_));
@@ -446,8 +445,9 @@ phmm_status Engine::make_slot(int id, Slot** out, std::string& err)
     s->id = id;
     auto cleanup = [&]() { free_slot(s); };
     cudaError_t e = cudaStreamCreateWithFlags(&s->main, cudaStreamNonBlocking);
+    s->overlap = overlap;
     int least = 0, greatest = 0;
-    if (PHMM_CLASS_PRIORITY && e == cudaSuccess) e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    if (overlap && e == cudaSuccess) e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
     for (int c = 0; c < kNumClasses && e == cudaSuccess; ++c)
         e = cudaStreamCreateWithPriority(&s->side[c], cudaStreamNonBlocking, c < kClasses32 ? least : greatest);
     for (int c = 0; c < kNumClasses && e == cudaSuccess; ++c) e = cudaEventCreateWithFlags(&s->ev_side[c], cudaEventDisableTiming);
@@ -572,19 +572,20 @@ phmm_status Engine::reserve(Slot& s, const Capacity& want, std::string& err)
     return PHMM_OK;
 }
 
-static unsigned int waves32(int cls)
+// Multi-stripe warps index scratch rows by warp and stay persistent.
+static unsigned int waves32(int cls, bool overlap)
 {
-    return class32_multi(cls) ? 1u : (unsigned int)PHMM_F32_WAVES;
+    return overlap && !class32_multi(cls) ? kOverlapWaves : 1u;
 }
 
-int Engine::full_grid(int precision, int cls) const
+int Engine::full_grid(int precision, int cls, unsigned int waves) const
 {
-    return occ_[precision == 32 ? 0 : 1][cls] * sms_ * (precision == 32 ? (int)waves32(cls) : 1);
+    return occ_[precision == 32 ? 0 : 1][cls] * sms_ * (precision == 32 ? (int)waves : 1);
 }
 
-int Engine::grid_for(int precision, int cls, uint32_t work) const
+int Engine::grid_for(int precision, int cls, uint32_t work, unsigned int waves) const
 {
-    const int full = full_grid(precision, cls);
+    const int full = full_grid(precision, cls, waves);
     const int warps_per_block = kFwdBlock / kWarp;
     const int need = (int)std::min<uint64_t>(((uint64_t)work + warps_per_block - 1) / warps_per_block, (uint64_t)full);
     return std::max(need, 1);
@@ -681,15 +682,15 @@ phmm_status Engine::launch_pipeline(Slot& s, bool want_flags, const Plan* plan, 
         const int slot0 = pass == 0 ? 0 : kClasses32;  // descriptor slot of the pass's first class
         for (int k = 0; k < n_cls; ++k) {
             // FP32 classes of a mode longest reads first (multi-stripe shapes, then KH = 8 .. 1)
-            const int c = pass == 0 && PHMM_CLASS_PRIORITY ? (k / kShapes32) * kShapes32 + kShapes32 - 1 - k % kShapes32
-                                                           : k;
+            const int c = pass == 0 && s.overlap ? (k / kShapes32) * kShapes32 + kShapes32 - 1 - k % kShapes32 : k;
             uint32_t work = 0;
             if (plan) {
                 work = pass == 0 ? plan->classes[c].n_items : plan->classes[slot0 + c].rerun_cap;
                 if (work == 0) continue;
             }
             // FP32 items hold two reads (warps = items); FP64 claims are single pairs
-            const int grid = plan ? grid_for(precision, c, work) : full_grid(precision, c);
+            const unsigned int waves = pass == 0 ? waves32(c, s.overlap) : 1u;
+            const int grid = plan ? grid_for(precision, c, work, waves) : full_grid(precision, c, waves);
             PassControl pc{};
             pc.cd = s.d_classes + slot0 + c;
             pc.cd64 = s.d_classes + kClasses32;
@@ -700,7 +701,7 @@ phmm_status Engine::launch_pipeline(Slot& s, bool want_flags, const Plan* plan, 
             const int region = pass == 0 ? 0 : 1 + c / 9;
             pc.scratch = multi ? (void*)((char*)s.d_scratch + scratch_offset_warps(region) * scr_cols * 24) : nullptr;
             pc.scratch_cols = scr_cols;
-            pc.waves = pass == 0 ? waves32(c) : 1u;
+            pc.waves = waves;
             cudaStream_t st = s.side[slot0 + c];
             PHMM_CK(cudaStreamWaitEvent(st, s.ev_fork, 0));
             // FP32 multi-stripe classes share one scratch region: each waits for the previous one
@@ -759,7 +760,7 @@ phmm_status Engine::capture_graph(Slot& s, bool want_flags, const TileTable& til
         err = std::string("graph capture failed: ") + cudaGetErrorString(e);
         return PHMM_ERR_CUDA;
     }
-    e = cudaGraphInstantiate(&s.graph, g, PHMM_CLASS_PRIORITY ? cudaGraphInstantiateFlagUseNodePriority : 0);
+    e = cudaGraphInstantiate(&s.graph, g, s.overlap ? cudaGraphInstantiateFlagUseNodePriority : 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) {
         s.graph = nullptr;
@@ -1235,7 +1236,6 @@ phmm_status Engine::time_fp32_class(Slot& s, const Plan& plan, int cls, int reps
     pc.status = s.d_status;
     pc.scratch = s.d_scratch;  // the FP32 multi-stripe region
     pc.scratch_cols = s.cap.scratch_cols ? (unsigned int)(s.cap.scratch_cols / warps) : 0u;
-    pc.waves = waves32(cls);
     const int grid = grid_for(32, cls, plan.classes[cls].n_items);
     cudaStream_t m = s.main;
     float best = 0.f;
@@ -1401,7 +1401,6 @@ phmm_status Engine::profile_classes(Slot& s, const Plan& plan, float* class_ms, 
             pc.status = s.d_status;
             pc.scratch = multi ? (void*)((char*)s.d_scratch + scratch_offset_warps(region) * scr_cols * 24) : nullptr;
             pc.scratch_cols = scr_cols;
-            pc.waves = pass == 0 ? waves32(c) : 1u;
             PHMM_CK(cudaEventRecord(ev[2 * (slot0 + c)], m));
             PHMM_CK(launch_fwd(precision, c, v, tf_, td_, pc, grid_for(precision, c, work), m));
             PHMM_CK(cudaEventRecord(ev[2 * (slot0 + c) + 1], m));

@@ -38,6 +38,7 @@ struct Slot {
     size_t pinned_bytes = 0;
     Capacity cap;
     Capacity floor;                  // the arena is never sized below this (serving slots pre-size)
+    bool overlap = false;            // serving slot: over-subscribed FP32 grids, prioritised streams
     // carved device pointers
     BatchDesc* d_desc = nullptr;
     char* d_desc_pristine = nullptr;  // the batch's descriptor block as uploaded, for replays
@@ -91,7 +92,9 @@ public:
     phmm_status compute(const phmm_batch& b, double* out, uint8_t* pair_flags, phmm_stats* stats, std::string& err);
 
     // Pieces used by the serving loop (phmm_serve.cpp), each on a caller-owned slot.
-    phmm_status make_slot(int id, Slot** out, std::string& err);
+    // overlap: the slot's batches share the GPU with other slots' (serving): over-subscribed FP32
+    // grids and prioritised class streams
+    phmm_status make_slot(int id, Slot** out, std::string& err, bool overlap = false);
     void free_slot(Slot* s);
     // mapq: MAPQ per read, region-API plans only (their raw qualities are prepared on the device).
     // raw_sent: the batch's bases and qualities were already copied to this arena (upload_raw) and it
@@ -162,7 +165,7 @@ private:
     phmm_status ensure_capacity(Slot& s, const Plan& plan, std::string& err);
     phmm_status launch_pipeline(Slot& s, bool want_flags, const Plan* plan, const TileTable& tiles, std::string& err);
     phmm_status capture_graph(Slot& s, bool want_flags, const TileTable& tiles, std::string& err);
-    int grid_for(int precision, int cls, uint32_t work) const;
+    int grid_for(int precision, int cls, uint32_t work, unsigned int waves = 1) const;
     uint64_t scratch_warps() const;
     // First warp row of scratch region r (0: FP32 multi-stripe classes, 1 + m: the FP64 multi-stripe
     // class of mode m; 1 + kModes32: the total).
@@ -177,7 +180,7 @@ private:
     int dev_ = 0;
     int sms_ = 0;
     int occ_[2][kNumClasses] = {};
-    int full_grid(int precision, int cls) const;  // resident blocks of a class (times its waves)
+    int full_grid(int precision, int cls, unsigned int waves) const;  // resident blocks (times waves)
     // device probability tables
     void* d_tables_ = nullptr;
     ProbTables<float> tf_{};

@@ -65,7 +65,7 @@ __global__ void reset_outputs_kernel(const BatchDesc* __restrict__ desc, double*
 template <int K, int PM>
 constexpr int min_blocks64()
 {
-    return PM == PM_ALL && K >= 7 ? PHMM_F64_MIN_WARPS : 1;
+    return PM == PM_EQ && K >= 7 ? PHMM_F64_MIN_WARPS : 1;
 }
 
 // UNF: the all-FP64 check arithmetic (plain multiply and add), used to measure the error of every
@@ -133,7 +133,7 @@ typedef void (*F64Kernel)(BatchView, ProbTables<double>, PassControl);
         fwd_f64_kernel<4, V, PM, false>, fwd_f64_kernel<5, V, PM, false>, fwd_f64_kernel<6, V, PM, false>, \
         fwd_f64_kernel<7, V, PM, false>, fwd_f64_kernel<8, V, PM, false>, fwd_f64_kernel<8, V, PM, true>
 
-static const F64Kernel kF64[kClasses64] = {PHMM_ROW64(kInter, PM_ALL), PHMM_ROW64(kInter, PM_ROW),
+static const F64Kernel kF64[kClasses64] = {PHMM_ROW64(kInter, PM_EQ), PHMM_ROW64(kInter, PM_ROW),
                                            PHMM_ROW64(kIntra, PM_ROW)};
 
 // All-FP64 check kernels: the same shapes with plain multiply/add, per-row gap parameters (any

@@ -5,6 +5,7 @@
 #pragma once
 
 #include "phmm_device.cuh"
+#include "phmm_device64.cuh"
 
 namespace phmm {
 
@@ -15,7 +16,6 @@ template <typename T, int K, int V, int PM, bool MULTI, bool UNF = false>
 __device__ __forceinline__ void run_read(const BatchView& b, const ProbTables<T>& tb, const PassControl& pc,
                                          const SweepOut& so, uint32_t g_lo, uint32_t g_hi, int lane, T* scr, T* tab)
 {
-    LaneRows<T, K, PM> L;
     const uint64_t roff = b.read_off[so.read];
     const int R = (int)(b.read_off[so.read + 1] - roff);
     const int Tcols = (int)(b.hap_off[g_hi] - b.hap_off[g_lo]);
@@ -25,29 +25,53 @@ __device__ __forceinline__ void run_read(const BatchView& b, const ProbTables<T>
         if (lane == 0) atomicOr(pc.status, kStatusBadItem);
         return;
     }
-    if (!MULTI) {
-        const int pad = kWarp * K - R;
-        const bool exotic = load_rows<T, K, V, PM>(L, tab, b, tb, roff, R, 0, pad, lane);
-        sweep<T, K, V, PM, false, false, UNF>(L, tab, b, tb, pc, so, g_lo, g_hi, scr, lane, lane * K <= pad, exotic,
-                                              roff, R, -pad);
-    } else {
+    if constexpr (PM == PM_EQ) {
+        // constant gaps with insertion = deletion: the two-value lane state (phmm_device64.cuh)
+        static_assert(sizeof(T) == 8 && !UNF, "PM_EQ is the FP64 recompute of mode 0");
+        LaneRowsEq<K> L;
         constexpr int SR = kWarp * K;  // rows per stripe
-        const int stripes = (R + SR - 1) / SR;
+        const int stripes = MULTI ? (R + SR - 1) / SR : 1;
         const int pad = SR * stripes - R;
         for (int s = 0; s < stripes; ++s) {
-            const bool exotic = load_rows<T, K, V, PM>(L, tab, b, tb, roff, R, s * SR, pad, lane);
+            const bool exotic = load_rows_eq<K, V>(L, tab, b, tb, roff, R, s * SR, pad, lane);
             const bool above_row0 = (s == 0) && (lane * K <= pad);
             const int row0 = s * SR - pad;  // read position of slot 0 of lane 0
-            if (s == 0)
-                sweep<T, K, V, PM, false, true, UNF>(L, tab, b, tb, pc, so, g_lo, g_hi, scr, lane, above_row0, exotic,
-                                                     roff, R, row0);
+            if (!MULTI)
+                sweep_eq<K, V, false, false>(L, tab, b, tb, so, g_lo, g_hi, scr, lane, above_row0, exotic, roff, R, row0);
+            else if (s == 0)
+                sweep_eq<K, V, false, true>(L, tab, b, tb, so, g_lo, g_hi, scr, lane, above_row0, exotic, roff, R, row0);
             else if (s == stripes - 1)
-                sweep<T, K, V, PM, true, false, UNF>(L, tab, b, tb, pc, so, g_lo, g_hi, scr, lane, above_row0, exotic,
-                                                     roff, R, row0);
+                sweep_eq<K, V, true, false>(L, tab, b, tb, so, g_lo, g_hi, scr, lane, above_row0, exotic, roff, R, row0);
             else
-                sweep<T, K, V, PM, true, true, UNF>(L, tab, b, tb, pc, so, g_lo, g_hi, scr, lane, above_row0, exotic,
-                                                    roff, R, row0);
-            __syncwarp();  // lane 31's scratch row is read by lane 0 in the next stripe
+                sweep_eq<K, V, true, true>(L, tab, b, tb, so, g_lo, g_hi, scr, lane, above_row0, exotic, roff, R, row0);
+            if (MULTI) __syncwarp();  // lane 31's scratch row is read by lane 0 in the next stripe
+        }
+    } else {
+        LaneRows<T, K, PM> L;
+        if (!MULTI) {
+            const int pad = kWarp * K - R;
+            const bool exotic = load_rows<T, K, V, PM>(L, tab, b, tb, roff, R, 0, pad, lane);
+            sweep<T, K, V, PM, false, false, UNF>(L, tab, b, tb, pc, so, g_lo, g_hi, scr, lane, lane * K <= pad, exotic,
+                                                  roff, R, -pad);
+        } else {
+            constexpr int SR = kWarp * K;  // rows per stripe
+            const int stripes = (R + SR - 1) / SR;
+            const int pad = SR * stripes - R;
+            for (int s = 0; s < stripes; ++s) {
+                const bool exotic = load_rows<T, K, V, PM>(L, tab, b, tb, roff, R, s * SR, pad, lane);
+                const bool above_row0 = (s == 0) && (lane * K <= pad);
+                const int row0 = s * SR - pad;  // read position of slot 0 of lane 0
+                if (s == 0)
+                    sweep<T, K, V, PM, false, true, UNF>(L, tab, b, tb, pc, so, g_lo, g_hi, scr, lane, above_row0, exotic,
+                                                         roff, R, row0);
+                else if (s == stripes - 1)
+                    sweep<T, K, V, PM, true, false, UNF>(L, tab, b, tb, pc, so, g_lo, g_hi, scr, lane, above_row0, exotic,
+                                                         roff, R, row0);
+                else
+                    sweep<T, K, V, PM, true, true, UNF>(L, tab, b, tb, pc, so, g_lo, g_hi, scr, lane, above_row0, exotic,
+                                                        roff, R, row0);
+                __syncwarp();  // lane 31's scratch row is read by lane 0 in the next stripe
+            }
         }
     }
 }

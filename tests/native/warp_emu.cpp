@@ -109,7 +109,7 @@ void f64_mode(int shape, const BatchView& b, const ProbTables<double>& t, const 
 int main(int argc, char** argv)
 {
     if (argc < 5) {
-        std::fprintf(stderr, "usage: warp_emu IN OUT engine|check64 default|multi<KH>\n");
+        std::fprintf(stderr, "usage: warp_emu IN OUT engine|check64|eq64 default|multi<KH>\n");
         return 2;
     }
     const std::string mode = argv[3], tiles_arg = argv[4];
@@ -214,15 +214,19 @@ int main(int argc, char** argv)
             if (!classes[kClasses32 + c].rerun_count) continue;
             pc.cd = classes.data() + kClasses32 + c;
             const int m = c / 9, s = c % 9;
-            if (m == 0) f64_mode<kInter, PM_ALL, false>(s, v, td, pc);
+            if (m == 0) f64_mode<kInter, PM_EQ, false>(s, v, td, pc);
             else if (m == 1) f64_mode<kInter, PM_ROW, false>(s, v, td, pc);
             else f64_mode<kIntra, PM_ROW, false>(s, v, td, pc);
         }
-    } else if (mode == "check64") {
+    } else if (mode == "check64" || mode == "eq64") {
         // every pair: per work item and read, the item's haplotype run, in the FP64 class of the
-        // read's length (modes 1 and 2), as Engine::check_fp64 lays them out
+        // read's length (modes 1 and 2), as Engine::check_fp64 lays them out.  eq64: every pair of the
+        // FP32 classes of mode 0 through the FP64 recompute classes of mode 0 instead (the
+        // reference's FP64 kernel for each of them, not only for the underflowed ones)
+        const bool eq = mode == "eq64";
         std::vector<std::vector<RerunEntry>> per(kClasses64);
         for (const WorkItem& it : plan.items) {
+            if (eq && mode32(it.variant, it.pmode) != 0) continue;
             const RegionDesc& rg = plan.regions[it.region];
             for (int k = 0; k < 2; ++k) {
                 const uint32_t r = it.read[k];
@@ -233,7 +237,8 @@ int main(int argc, char** argv)
                 e.hap = rg.hap_begin + it.hap_lo;
                 e.n_haps = (uint32_t)(it.hap_hi - it.hap_lo);
                 e.out_stride = rg.n_reads;
-                per[class64_for_len(it.variant == kIntra ? 2 : 1, plan.read_off[r + 1] - plan.read_off[r])].push_back(e);
+                const int m64 = eq ? 0 : it.variant == kIntra ? 2 : 1;
+                per[class64_for_len(m64, plan.read_off[r + 1] - plan.read_off[r])].push_back(e);
             }
         }
         rerun.clear();
@@ -246,11 +251,12 @@ int main(int argc, char** argv)
         }
         rerun.resize(std::max<size_t>(rerun.size(), 1));
         pc.rerun = rerun.data();
-        for (int c = 9; c < kClasses64; ++c) {
+        for (int c = eq ? 0 : 9; c < (eq ? 9 : kClasses64); ++c) {
             if (!classes[kClasses32 + c].rerun_count) continue;
             pc.cd = classes.data() + kClasses32 + c;
             const int s = c % 9;
-            if (c / 9 == 1) f64_mode<kInter, PM_ROW, true>(s, v, td, pc);
+            if (eq) f64_mode<kInter, PM_EQ, false>(s, v, td, pc);
+            else if (c / 9 == 1) f64_mode<kInter, PM_ROW, true>(s, v, td, pc);
             else f64_mode<kIntra, PM_ROW, true>(s, v, td, pc);
         }
     } else {

@@ -27,6 +27,7 @@ BIN = NATIVE / "_build" / "warp_emu"
 CSRC = ROOT / "rovaca_b200" / "csrc"
 EXACT = 1e-12
 LENS = (17, 40, 70, 100, 150, 180, 200, 240, 256, 300, 500, 768)
+LOG10_C_F64 = 307.050595577260822  # log10 of the FP64 initial scale 2^1020
 
 
 @pytest.fixture(scope="module")
@@ -112,3 +113,27 @@ def test_emulated_all_fp64_check_equals_the_oracle(emulator, oracle, tmp_path):
     want, _ = oracle.batch(pb, fp64_only=True)
     assert status == 0
     assert_same_values(got, want, EXACT)
+
+
+def test_emulated_fp64_recompute_of_mode0_equals_the_oracle(emulator, oracle, tmp_path):
+    """Every pair of the constant-gap, insertion = deletion region through the FP64 recompute classes
+    of mode 0 (the two-value lane state with the reference's flush-to-zero and the warp's vote), not
+    only the pairs that underflow in FP32: each equals the reference's FP64 kernel on that pair."""
+    pb = _batch(13)
+    got, _, status = _run(emulator, pb, tmp_path, mode="eq64")
+    assert status == 0
+    n_h, n_r = int(pb.n_haps[0]), int(pb.n_reads[0])
+    got0 = got[:n_h * n_r].reshape(n_h, n_r)
+    want = np.empty((n_h, n_r))
+    for h in range(n_h):
+        hap = bytes(pb.hap_bases[pb.hap_off[h]:pb.hap_off[h + 1]])
+        for r in range(n_r):
+            s = slice(int(pb.read_off[r]), int(pb.read_off[r + 1]))
+            raw = oracle.raw_f64(hap, bytes(pb.read_bases[s]), bytes(pb.read_qual[s]), bytes(pb.read_ins[s]),
+                                 bytes(pb.read_del[s]), bytes(pb.read_gcp[s]))
+            with np.errstate(divide="ignore"):
+                want[h, r] = np.log10(raw) - LOG10_C_F64
+    assert_same_values(got0, want, EXACT, "mode-0 FP64")
+    # reads up to 500 bases end far below the FP32 range (-500 log10) but within FP64's; the 768-base
+    # read underflows FP64 as well (-inf on both sides), through the flushes
+    assert np.isfinite(want[:, :-1]).all() and (want[:, :-1] < -300).any() and np.isinf(want[:, -1]).all()
