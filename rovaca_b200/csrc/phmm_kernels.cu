@@ -55,17 +55,22 @@ __global__ void reset_outputs_kernel(const BatchDesc* __restrict__ desc, double*
 // FP64 pass for one class over the runs of underflowed pairs the FP32 pass appended, one run per
 // claim, streamed through the read like an FP32 work item.
 // ------------------------------------------------------------------------------------------
-// FP64 kernels with constant gap parameters and 7-8 rows per lane run four warps per scheduler at 128
-// registers (spilling a few hundred bytes, which stay in L1): measured on B200 with the per-lane
-// prior tables, 3% faster than three warps at 168 registers without spills on the benchmark batch's
-// FP64 pass and 2.4% on the underflow-stress shape.  The others keep what they need.
-#ifndef PHMM_F64_MIN_WARPS
-#define PHMM_F64_MIN_WARPS 16
+// Resident warps per SM of the FP64 classes of mode 0 (constant gaps, insertion = deletion), the
+// compiler's register bound: 8 rows per lane at 12 warps (168 registers, no spills), 7 rows at 16
+// (128 registers, 48 bytes of spill loads).  Measured on B200 with the two-value lane state: 8 rows
+// at 12 warps ran the underflow-stress shape's FP64 pass in 43.7 ms against 44.9 at 16, and the
+// benchmark batch's 8-row class in 8.8 against 9.1 ms; 7 rows ran 5.1 ms at 16 against 5.3 at 12.
+// The other classes keep what they need.  Build-time settings.
+#ifndef PHMM_F64_MIN_WARPS_K8
+#define PHMM_F64_MIN_WARPS_K8 12
+#endif
+#ifndef PHMM_F64_MIN_WARPS_K7
+#define PHMM_F64_MIN_WARPS_K7 16
 #endif
 template <int K, int PM>
 constexpr int min_blocks64()
 {
-    return PM == PM_EQ && K >= 7 ? PHMM_F64_MIN_WARPS : 1;
+    return PM != PM_EQ ? 1 : K == 8 ? PHMM_F64_MIN_WARPS_K8 : K == 7 ? PHMM_F64_MIN_WARPS_K7 : 1;
 }
 
 // UNF: the all-FP64 check arithmetic (plain multiply and add), used to measure the error of every
