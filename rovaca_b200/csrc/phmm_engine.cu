@@ -1007,7 +1007,9 @@ struct ChunkRange {
 // first chunk gets the device going after little planning and uploading, and the rest is planned
 // and uploaded while it runs.  Measured on B200 over the 2,000-region benchmark batch end to end:
 // one cut at 15% 2278 GCUPS, one pipeline 2213; cuts at 10% and 55% 2238 and at 12.5%, 42% and 71%
-// 2237, their extra chunk tails adding 7-8 ms of device time.
+// 2237, their extra chunk tails adding 7-8 ms of device time.  With the current kernels: one cut
+// 2713 GCUPS, cuts at 15% and 85% 2682, and either with the serving slots' overlap scheduling on the
+// two chunk slots 2712 and 2717 (within noise).
 std::vector<ChunkRange> split_chunks(const phmm_batch& b, uint64_t total_cells)
 {
     static const double kEnds[] = {0.15};
