@@ -206,7 +206,10 @@ __device__ __forceinline__ bool load_rows2(LaneRows2<KH, PM>& L, float4* tab, co
 #ifndef PHMM_CODES_STAGED
 #define PHMM_CODES_STAGED 1
 #endif
-constexpr int kCodeRing = 64;
+#ifndef PHMM_CODE_RING
+#define PHMM_CODE_RING 64
+#endif
+constexpr int kCodeRing = PHMM_CODE_RING;  // a power of two
 // float4 slots the ring adds to a warp's shared prior table
 constexpr int kRingFloat4 = PHMM_CODES_STAGED ? kCodeRing / 4 : 0;
 

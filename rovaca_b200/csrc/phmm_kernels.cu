@@ -28,11 +28,13 @@ __global__ void prep_codes_kernel(const BatchDesc* __restrict__ desc, const uint
         codes_intra[kCodePad + i] = hap_code(b, kIntra);
     }
     // guard codes on both sides of the stream: match nothing
-    if (blockIdx.x == 0 && threadIdx.x < kCodePad) {
-        codes_inter[threadIdx.x] = 0u;
-        codes_intra[threadIdx.x] = 0u;
-        codes_inter[kCodePad + total + threadIdx.x] = 0u;
-        codes_intra[kCodePad + total + threadIdx.x] = 0u;
+    if (blockIdx.x == 0) {
+        for (int k = threadIdx.x; k < kCodePad; k += blockDim.x) {
+            codes_inter[k] = 0u;
+            codes_intra[k] = 0u;
+            codes_inter[kCodePad + total + k] = 0u;
+            codes_intra[kCodePad + total + k] = 0u;
+        }
     }
 }
 

@@ -13,7 +13,10 @@ namespace phmm {
 
 constexpr int kWarp = 32;
 constexpr int kMaxK = 8;          // rows per lane in one stripe (stripe = 256 rows)
-constexpr int kCodePad = 64;      // guard codes before/after the haplotype code stream
+#ifndef PHMM_CODE_PAD
+#define PHMM_CODE_PAD 64
+#endif
+constexpr int kCodePad = PHMM_CODE_PAD;  // guard codes before/after the haplotype code stream
 // Steps per boundary-free chunk of the packed FP32 sweep (build-time setting; 8 measured best on
 // B200 against 4 and 16).
 #ifndef PHMM_CHUNK_PACKED
