@@ -17,10 +17,14 @@ constexpr int kMaxK = 8;          // rows per lane in one stripe (stripe = 256 r
 #define PHMM_CODE_PAD 64
 #endif
 constexpr int kCodePad = PHMM_CODE_PAD;  // guard codes before/after the haplotype code stream
-// Steps per boundary-free chunk of the packed FP32 sweep (build-time setting; 8 measured best on
-// B200 against 4 and 16).
+// Steps per boundary-free chunk of the packed FP32 sweep (build-time setting).  Measured on B200 with
+// the two-value lane state over the 2,000-region benchmark batch: 8 steps 196.8 ms, 10 194.5, 12
+// 192.7, 14 191.7, 16 191.3, 20 190.3 (with a 128-word code ring; the per-row gap mode 1.1% slower
+// than at 16, the dominant class 0.3%), 24 195.3.  The code ring holds 31 + 2 chunks of words
+// (phmm_device2.cuh): beyond 16 steps, or with the prior prefetch, build with PHMM_CODE_RING=128 and
+// PHMM_CODE_PAD=128.
 #ifndef PHMM_CHUNK_PACKED
-#define PHMM_CHUNK_PACKED 8
+#define PHMM_CHUNK_PACKED 16
 #endif
 constexpr int kChunk = PHMM_CHUNK_PACKED;  // steps per boundary-free fast chunk of the FP32 sweep
 
