@@ -8,8 +8,8 @@
 // components, through the same run of haplotype columns.  Lane l holds rows l*KH .. l*KH+KH-1 of
 // both reads' stripes and works on stream column p = t - l at step t, so the two components of every
 // float2 meet the same haplotype base: one packed instruction updates row a of X and row a of Y.
-// The three values of a lane's bottom rows go to lane l+1 by shuffle (two values formed from them in
-// PM_EQ); lane 31 holds both reads' last rows and sums them per haplotype.  Rows are padded at the
+// Two values formed from a lane's bottom rows go to lane l+1 by shuffle (three, M, I and D, in
+// PM_ALL); lane 31 holds both reads' last rows and sums them per haplotype.  Rows are padded at the
 // top, each read by its own count, and pad rows reproduce the boundary row exactly (prior 0 keeps
 // M = 0, I stays 0 because the rows above have M = I = 0, and xx = 1 keeps D = C/H).  Reads longer
 // than one stripe run as stripes linked through a per-warp scratch row of float2 values.
@@ -36,8 +36,8 @@
 // PCR model, and the benchmark data), PM_ROW otherwise.  In PM_EQ, mm, gapm and mx (= my) are held
 // once per lane instead of once per row (xx stays per row: pad rows need xx = 1), which leaves
 // registers for more rows per lane, and a cell takes 7 operations instead of 8 (M * mx serves both
-// I of the row below and D of the next column); the lane above forms the first row's I and diagonal
-// sum (cells2_eq), so a step shuffles two values instead of three.
+// I of the row below and D of the next column).  In both modes the lane above forms the first row's
+// I and diagonal sum (cells2_eq, cells2_row), so a step shuffles two values instead of three.
 #pragma once
 
 #include <cstdint>
@@ -81,11 +81,12 @@ struct LaneRows2 {
     float2 S[KH];                   // (X, Y) diagonal sum of row a for the lane's next column
     float2 Dn[KH];                  // (X, Y) D of row a at the lane's next column
     float2 Mb, Ib, Db;              // bottom row at the lane's last column (shuffled to lane + 1;
-                                    // PM_EQ: Mb and Ib only feed lane 31's sums)
-    float2 In, Sn;                  // PM_EQ: I of the row below the lane and that row's diagonal sum
+                                    // hand-off: Mb and Ib only feed lane 31's sums)
+    float2 In, Sn;                  // hand-off: I of the row below the lane and that row's diagonal sum
                                     // for its next column, formed from the bottom row (shuffled to
                                     // lane + 1 in place of Mb, Ib and Db)
-    float2 xxn;                     // PM_EQ: xx of the row below the lane (1 for a pad row)
+    float2 xxn;                     // PM_EQ, PM_ROW: xx of the row below the lane (1 for a pad row)
+    float2 mmn, gmn, mxn;           // PM_ROW: that row's mm, gapm and mx
     float2 xx[KH];
     float2 mm[NR], gm[NR], mx[NR], my[NR];  // my: unused in PM_EQ (mx == my)
     uint32_t padX, padY;            // bit a: row a of the read is a pad row
@@ -149,11 +150,18 @@ __device__ __forceinline__ bool load_rows2(LaneRows2<KH, PM>& L, float4* tab, co
 #pragma unroll
     for (int a = 0; a < KH; ++a) L.S[a] = L.Dn[a] = f2(0.f, 0.f);
     L.Mb = L.Ib = L.Db = L.In = L.Sn = f2(0.f, 0.f);
-    if (PM == PM_EQ) {
-        // for lane 31 the row below is the next stripe's first row
+    if (PM != PM_ALL) {
+        // the row below the lane (for lane 31 the next stripe's first row), whose first-row inputs
+        // this lane forms
         const int below = first + lane * KH + KH;
-        L.xxn = f2(row_params<V>(b, tb, rp.roff[0], rp.R[0], below - rp.pad[0]).xx,
-                   row_params<V>(b, tb, rp.roff[1], rp.R[1], below - rp.pad[1]).xx);
+        const RowParams xn = row_params<V>(b, tb, rp.roff[0], rp.R[0], below - rp.pad[0]);
+        const RowParams yn = row_params<V>(b, tb, rp.roff[1], rp.R[1], below - rp.pad[1]);
+        L.xxn = f2(xn.xx, yn.xx);
+        if (PM == PM_ROW) {
+            L.mmn = f2(xn.mm, yn.mm);
+            L.gmn = f2(xn.gm, yn.gm);
+            L.mxn = f2(xn.mx, yn.mx);
+        }
     }
     if (PM != PM_ROW) {
         // constant along the read: any real row gives them (pad rows ignore them)
@@ -252,11 +260,17 @@ constexpr int kRingAhead = PHMM_PRIOR_PREFETCH ? 2 : 1;
 static_assert(31 + (kRingAhead + 1) * kChunk <= kCodeRing && 32 + (kRingAhead + 1) * kChunk <= kCodePad,
               "code ring too small for the chunks it holds ahead");
 
+template <int V>
+__device__ __forceinline__ float2 diag_sum_p(float2 mm, float2 gm, float2 dgM, float2 dgI, float2 dgD)
+{
+    if (V == kInter) return rfma2(dgD, gm, rfma2(dgM, mm, rmul2(dgI, gm)));
+    return rfma2(dgD, gm, rfma2(dgI, gm, rmul2(dgM, mm)));
+}
+
 template <int V, int PM, int KH>
 __device__ __forceinline__ float2 diag_sum(const LaneRows2<KH, PM>& L, int r, float2 dgM, float2 dgI, float2 dgD)
 {
-    if (V == kInter) return rfma2(dgD, L.gm[r], rfma2(dgM, L.mm[r], rmul2(dgI, L.gm[r])));
-    return rfma2(dgD, L.gm[r], rfma2(dgI, L.gm[r], rmul2(dgM, L.mm[r])));
+    return diag_sum_p<V>(L.mm[r], L.gm[r], dgM, dgI, dgD);
 }
 
 // All KH row pairs of the lane for one step at column j (PM_ALL and PM_ROW).  (upM, upI, upD): the
@@ -331,6 +345,37 @@ __device__ __forceinline__ void cells2_eq(LaneRows2<KH, PM>& L, const float2 (&p
     L.S[0] = upS;
 }
 
+// The same hand-off with per-row gap parameters (PM_ROW): the lane above forms the first row's I
+// with that row's mx and xx and its diagonal sum with that row's mm and gapm (mxn, xxn, mmn, gmn),
+// the operations and operands the lane itself would use.  Two shuffled values instead of three; the
+// 8 operations per cell stay (M * mx of the row below and M * my of the row differ).
+template <int KH, int V, int PM>
+__device__ __forceinline__ void cells2_row(LaneRows2<KH, PM>& L, const float2 (&pr)[KH], float2 upI, float2 upS)
+{
+    static_assert(PM == PM_ROW, "cells2_row is the PM_ROW step");
+    float2 Mab = f2(0.f, 0.f), Iab = upI;  // the row above, this column
+    float2 nM = rmul2(L.S[0], pr[0]);
+#pragma unroll
+    for (int a = 0; a < KH; ++a) {
+        const float2 M = nM;
+        if (a + 1 < KH) nM = rmul2(L.S[a + 1], pr[a + 1]);  // before S[a + 1] is overwritten below
+        const float2 I = a == 0 ? upI : rfma2(Iab, L.xx[a], rmul2(Mab, L.mx[a]));
+        const float2 D = L.Dn[a];
+        L.Dn[a] = rfma2(D, L.xx[a], rmul2(M, L.my[a]));
+        if (a + 1 < KH) {
+            L.S[a + 1] = diag_sum<V, PM>(L, a + 1, M, I, D);
+        } else {
+            L.Mb = M;
+            L.Ib = I;
+            L.Sn = diag_sum_p<V>(L.mmn, L.gmn, M, I, D);
+            L.In = rfma2(I, L.xxn, rmul2(M, L.mxn));
+        }
+        Mab = M;
+        Iab = I;
+    }
+    L.S[0] = upS;
+}
+
 // Output side of a sweep: the two reads' likelihood columns and FP64 rerun lists.
 struct SweepOut2 {
     double* out;
@@ -369,7 +414,8 @@ __device__ void sweep2(LaneRows2<KH, PM>& L, float4* tab, const BatchView& b, co
     bool started = false;
     float D0 = 0.f;
     // PM_EQ: lane 0's first-row sum below the boundary row (M = I = 0, D = C/H) for the next column
-    constexpr bool EQ = PM == PM_EQ;
+    // the lane above forms the first row's inputs (PM_EQ, PM_ROW)
+    constexpr bool HANDOFF = PM != PM_ALL;
     float2 Stop = f2(0.f, 0.f);
     float2 sumM = f2(0.f, 0.f), sumI = f2(0.f, 0.f);
 
@@ -434,7 +480,7 @@ __device__ void sweep2(LaneRows2<KH, PM>& L, float4* tab, const BatchView& b, co
             // lane's first row when `above`).  The first column starts from the diagonal sums of
             // column 0 and from D[i][1] = fma(D[i][0], xx, 0 * my): C/H in pad rows (xx = 1), else 0.
             const float2 z = f2(0.f, 0.f);
-            if (EQ) Stop = diag_sum<V, PM>(L, 0, z, z, f2(D0, D0));
+            if (HANDOFF) Stop = diag_sum<V, PM>(L, 0, z, z, f2(D0, D0));
             float2 Dab = f2(aboveX ? D0 : 0.f, aboveY ? D0 : 0.f);
 #pragma unroll
             for (int a = 0; a < KH; ++a) {
@@ -481,9 +527,9 @@ __device__ void sweep2(LaneRows2<KH, PM>& L, float4* tab, const BatchView& b, co
 
     auto step = [&](int t, bool check) {
         const int p = t - lane;
-        // the row above the lane's first row: its M, I and D, or (PM_EQ) the first row's I and sum
+        // the row above the lane's first row: its M, I and D, or (hand-off) the first row's I and sum
         float2 uM, uI, uD;
-        if (EQ) {
+        if (HANDOFF) {
             uI = shfl_up2(L.In);
             uD = shfl_up2(L.Sn);
         } else {
@@ -495,7 +541,7 @@ __device__ void sweep2(LaneRows2<KH, PM>& L, float4* tab, const BatchView& b, co
         if (lane == 0) {
             if (FROM_SCR) {
                 const bool ok = p >= 0 && p < Tcols;
-                if (EQ) {
+                if (HANDOFF) {
                     uI = ok ? scr[2 * p + 0] : f2(0.f, 0.f);
                     uD = ok ? scr[2 * p + 1] : f2(0.f, 0.f);
                 } else {
@@ -503,7 +549,7 @@ __device__ void sweep2(LaneRows2<KH, PM>& L, float4* tab, const BatchView& b, co
                     uI = ok ? scr[3 * p + 1] : f2(0.f, 0.f);
                     uD = ok ? scr[3 * p + 2] : f2(0.f, 0.f);
                 }
-            } else if (EQ) {
+            } else if (HANDOFF) {
                 // below the boundary row (M = I = 0, D = C/H): I = fma(0, xx, 0 * mx) = 0
                 uI = f2(0.f, 0.f);
                 uD = Stop;
@@ -536,13 +582,15 @@ __device__ void sweep2(LaneRows2<KH, PM>& L, float4* tab, const BatchView& b, co
                     pr[a].y = tb.pmat[b.read_q[rp.roff[1] + iY] & 127];
             }
         }
-        if constexpr (EQ)
+        if constexpr (PM == PM_EQ)
             cells2_eq<KH, V, PM>(L, pr, uI, uD);
+        else if constexpr (PM == PM_ROW)
+            cells2_row<KH, V, PM>(L, pr, uI, uD);
         else
             cells2<KH, V, PM>(L, pr, uM, uI, uD);
         if (TO_SCR) {
             if (writer && p >= 0 && p < Tcols) {
-                if (EQ) {
+                if (HANDOFF) {
                     scr[2 * p + 0] = L.In;
                     scr[2 * p + 1] = L.Sn;
                 } else {
