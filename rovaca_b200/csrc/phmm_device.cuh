@@ -95,9 +95,10 @@ __device__ __forceinline__ T shfl_up1(T v)
 // Gap parameters: PM_ALL when a read's insertion, deletion and gap-continuation qualities are each
 // constant along it, PM_ROW otherwise.  In PM_ALL, mm, gapm, mx and my are held once per lane
 // instead of once per row (xx stays per row: pad rows need xx = 1), which frees registers.  PM_EQ
-// (the FP32 kernels only) is PM_ALL with equal insertion and deletion qualities, mx == my: the
-// product M[i][j] * mx that feeds I[i+1][j] is the product M[i][j] * my that feeds D[i][j+1], so
-// it is formed once (the two reference operations have the same operands, hence the same bits).
+// (the FP32 kernels of mode 0 and the FP64 classes of mode 0, phmm_device64.cuh) is PM_ALL with
+// equal insertion and deletion qualities, mx == my: the product M[i][j] * mx that feeds I[i+1][j] is
+// the product M[i][j] * my that feeds D[i][j+1], so it is formed once (the two reference operations
+// have the same operands, hence the same bits).  The sweep below serves PM_ALL and PM_ROW.
 enum ParamMode : int { PM_ALL = 0, PM_ROW = 1, PM_EQ = 2 };
 
 // One lane's rows of the current stripe.  The match priors are not held here: each lane tabulates
