@@ -43,17 +43,18 @@ def build_oracle(force: bool = False) -> Path:
     return ORACLE_LIB
 
 
-def reference_root() -> str:
+def reference_root() -> str | None:
     """The reference's source tree, read in place by the build recipes and the fixture generators:
-    the REFERENCE_ROOT environment variable, else the location this test infrastructure was set up
-    with.  Nothing on the GPU host reads it (the built oracle/_ref libraries travel instead)."""
-    return os.environ.get("REFERENCE_ROOT") or "/root/reference"
+    the REFERENCE_ROOT environment variable (None when unset; the build functions then keep the
+    libraries already built).  Nothing on the GPU host reads it (the built oracle/_ref libraries
+    travel instead)."""
+    return os.environ.get("REFERENCE_ROOT") or None
 
 
 def build_ref(root: str | None = None) -> Path | None:
     """Builds oracle/_ref from the reference sources when they are present; returns the library."""
     src = root or reference_root()
-    if not Path(src, "src/haplotypecaller/pairhmm").is_dir():
+    if src is None or not Path(src, "src/haplotypecaller/pairhmm").is_dir():
         return REF_LIB if REF_LIB.exists() else None
     srcs = [HERE / "ref_shim.cpp", HERE / "ref_kernels.cpp", HERE / "ref_region.cpp", HERE / "ref_unreached.cpp",
             HERE / "build_ref.sh"]
@@ -70,7 +71,7 @@ def build_ref_sw(root: str | None = None) -> Path | None:
     """Builds oracle/_ref/libsw_ref.so (the reference's Smith-Waterman aligner) when the reference
     sources are present; returns the library."""
     src = root or reference_root()
-    if not Path(src, "src/haplotypecaller/common/base/lib/ro_sw").is_dir():
+    if src is None or not Path(src, "src/haplotypecaller/common/base/lib/ro_sw").is_dir():
         return SW_REF_LIB if SW_REF_LIB.exists() else None
     srcs = [HERE / "ref_sw_shim.c", HERE / "build_ref_sw.sh"]
     if SW_REF_LIB.exists() and all(SW_REF_LIB.stat().st_mtime >= s.stat().st_mtime for s in srcs):
@@ -86,7 +87,7 @@ def build_ref_genotype(root: str | None = None) -> Path | None:
     """Builds oracle/_ref/libgenotype_ref.so (the reference's allele marginalisation and diploid
     genotype-likelihood calculator) when the reference sources are present; returns the library."""
     src = root or reference_root()
-    if not Path(src, "src/haplotypecaller/genotype/genotype_likelihood_calculator.cpp").is_file():
+    if src is None or not Path(src, "src/haplotypecaller/genotype/genotype_likelihood_calculator.cpp").is_file():
         return GENOTYPE_REF_LIB if GENOTYPE_REF_LIB.exists() else None
     deps = [HERE / "ref_genotype_shim.cpp", HERE / "build_ref_genotype.sh",
             *sorted((HERE / "ref_stubs" / "boost" / "math" / "special_functions").glob("*.hpp"))]

@@ -131,6 +131,8 @@ def edge_regions(rng) -> list[Region]:
 
 def main(reference_root: str | None = None) -> None:
     reference_root = reference_root or oracle_reference_root()
+    if reference_root is None:
+        raise SystemExit("pass the reference's source root or set REFERENCE_ROOT")
     res = Path(reference_root) / "src/haplotypecaller/pairhmm/resource"
     lib = build_ref(reference_root)
     if lib is None:

@@ -108,6 +108,8 @@ def synthetic_pairs(rng: random.Random) -> list[tuple[bytes, bytes, tuple, int]]
 
 def main(ref_root: str | None = None) -> None:
     ref_root = ref_root or oracle_reference_root()
+    if ref_root is None:
+        raise SystemExit("pass the reference's source root or set REFERENCE_ROOT")
     build_ref_sw(ref_root)
     ref = SwRef()
     rng = random.Random(20240611)
