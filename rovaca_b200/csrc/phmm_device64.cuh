@@ -118,16 +118,26 @@ __device__ __forceinline__ void cells_eq(LaneRowsEq<K>& L, const double (&pr)[K]
 // below (that lane's first-row inputs).  The longest product chain of a step is still K + 1 factors
 // (the insertion chain from the first row's M down to the value handed on), so the bound of
 // rows_flush_free holds.
+// The minimum is taken as a tree (depth log2(2 K + 2) instead of a chain of 2 K + 2 dependent
+// operations): the next step's arithmetic waits on this vote.
 template <int K>
 __device__ __forceinline__ bool rows_flush_free_eq(const LaneRowsEq<K>& L)
 {
-    uint32_t m = min((uint32_t)__double2hiint(L.In) - 1u, (uint32_t)__double2hiint(L.Sn) - 1u);
+    constexpr int N = 2 * K + 2;
+    uint32_t v[N];
 #pragma unroll
     for (int k = 0; k < K; ++k) {
-        m = min(m, (uint32_t)__double2hiint(L.S[k]) - 1u);
-        m = min(m, (uint32_t)__double2hiint(L.Dn[k]) - 1u);
+        v[2 * k] = (uint32_t)__double2hiint(L.S[k]) - 1u;
+        v[2 * k + 1] = (uint32_t)__double2hiint(L.Dn[k]) - 1u;
     }
-    return m >= flush_free_hi<K>() - 1u;
+    v[2 * K] = (uint32_t)__double2hiint(L.In) - 1u;
+    v[2 * K + 1] = (uint32_t)__double2hiint(L.Sn) - 1u;
+#pragma unroll
+    for (int w = 1; w < N; w *= 2) {
+#pragma unroll
+        for (int i = 0; i + w < N; i += 2 * w) v[i] = min(v[i], v[i + w]);
+    }
+    return v[0] >= flush_free_hi<K>() - 1u;
 }
 
 // Sweep one stripe over the column stream of haplotypes [g_lo, g_hi): as `sweep` (phmm_device.cuh),
