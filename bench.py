@@ -281,11 +281,16 @@ class RequestPool:
     draw each arriving request's region uniformly at random from it, i.e. from the batch's size
     distribution."""
 
-    def __init__(self, batch):
+    def __init__(self, batch, expected=None):
         self.regions = [batch.subset([g]) for g in range(batch.n_regions)]
         self.structs = [r.as_c() for r in self.regions]
         self.cells = [r.cells() for r in self.regions]
         self.sizes = [r.out_size for r in self.regions]
+        # each region's likelihoods from the batched run, for checking every served request
+        self.expected = None
+        if expected is not None:
+            offs = np.concatenate([[0], np.cumsum(self.sizes)])
+            self.expected = [expected[offs[g]:offs[g + 1]] for g in range(batch.n_regions)]
 
 
 def serving_latency(engine, pool: RequestPool, load: float, capacity_regions_per_s: float, seconds: float, seed: int):
@@ -332,6 +337,12 @@ def serving_latency(engine, pool: RequestPool, load: float, capacity_regions_per
     after = engine.server_stats()
     lat = np.array(lat)
     batches = after["batches"] - before["batches"]
+    # every served request's likelihoods against the same region's in the batched run (bit for bit:
+    # a pair's arithmetic does not depend on what it was batched with)
+    mismatched = None
+    if pool.expected is not None:
+        mismatched = sum(not np.array_equal(o, pool.expected[g], equal_nan=True)
+                         for o, (_, g) in zip(outs, tickets))
     return {"load": load, "offered_regions_per_s": round(rate, 1), "requests": len(lat),
             "p50_ms": round(float(np.percentile(lat, 50)), 3), "p99_ms": round(float(np.percentile(lat, 99)), 3),
             "sustained_gcups": round(done_cells / elapsed / 1e9, 2),
@@ -345,7 +356,8 @@ def serving_latency(engine, pool: RequestPool, load: float, capacity_regions_per
             "graph_captures": after["graph_captures"] - before["graph_captures"],
             "max_setup_ms_so_far": round(after["max_setup_ms"], 2), "max_host_ms_so_far": round(after["max_host_ms"], 2),
             "mean_phase_ms": {k: round((after[k + "_ms"] - before[k + "_ms"]) / max(batches, 1), 3)
-                              for k in ("gather", "plan", "enqueue", "wait", "scatter")}}
+                              for k in ("gather", "plan", "enqueue", "wait", "scatter")},
+            "requests_differing_from_batched": mismatched}
 
 
 def underflow_stress(engine, steps: int, warmup: int, cpu_threads: int | None, n_regions: int = 500) -> dict:
@@ -762,7 +774,7 @@ def run_ours(args, rank: int, world: int, dist) -> None:
 
         # serving loop latency (after a warm-up burst: slots sized, graphs captured, kernels loaded)
         cap = batch.n_regions / (e2e_s / args.steps)
-        pool = RequestPool(batch)
+        pool = RequestPool(batch, out)
         serving_latency(engine, pool, 2.0, cap, 1.0, seed=99)
         lat = [serving_latency(engine, pool, load, cap, args.serve_seconds, seed=100 + k)
                for k, load in enumerate((0.25, 0.5, 0.8, 0.95))]

@@ -41,6 +41,36 @@ def test_each_result_same_alone_and_in_the_mix(engine):
     assert 1 <= st["batches"] <= st["requests_done"] and st["cells_done"] >= pb.cells()
 
 
+def test_burst_from_many_threads_matches_the_batched_run():
+    """A burst of 240 regions from 8 threads, which piles up while the slots are busy and is served
+    in batches of many regions (large enough for the multi-threaded gather into pinned staging and
+    copy back out): every request's likelihoods equal the same region's in one batched call."""
+    pb = synth.config1(240, seed=43)
+    with Engine(device=0, autotune=False) as eng:
+        want, _, _ = eng.compute(pb)
+        sizes = [int(pb.n_haps[g]) * int(pb.n_reads[g]) for g in range(pb.n_regions)]
+        offs = np.concatenate([[0], np.cumsum(sizes)])
+        regions = [pb.subset([g]) for g in range(pb.n_regions)]
+        outs = [np.empty(n) for n in sizes]
+        tickets = [None] * pb.n_regions
+
+        def producer(k0):
+            for g in range(k0, pb.n_regions, 8):
+                tickets[g] = eng.submit(regions[g], outs[g])
+
+        threads = [threading.Thread(target=producer, args=(k,)) for k in range(8)]
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join()
+        for t in tickets:
+            eng.wait(t)
+        st = eng.server_stats()
+    for g in range(pb.n_regions):
+        assert np.array_equal(outs[g], want[offs[g]:offs[g + 1]], equal_nan=True), g
+    assert st["requests_done"] == pb.n_regions and st["max_batch_regions"] >= 2
+
+
 def test_flags_and_poll(engine, oracle):
     pb = synth.config2(1, seed=41)
     out = np.empty(pb.out_size)
