@@ -1,6 +1,8 @@
-// FP64 recompute of reads with constant gap qualities and equal insertion and deletion quality (the
-// FP64 classes of mode 0, PM_EQ): the lane state and step of the FP32 kernels (phmm_device2.cuh)
-// in scalar double, one read per warp, with the reference's flush-to-zero.
+// FP64 recompute (the pass that reruns the pairs whose FP32 sum underflowed): the lane state and step
+// of the FP32 kernels (phmm_device2.cuh) in scalar double, one read per warp, with the reference's
+// flush-to-zero.  LaneRowsEq for constant gap qualities with equal insertion and deletion quality
+// (the FP64 classes of mode 0, PM_EQ), LaneRowsRow for per-row gap parameters (modes 1 and 2); the
+// all-FP64 check kernels keep phmm_device.cuh's sweep.
 //
 // Lane state between steps: per row the pending diagonal sum s (M[i][j+1] = s * prior) and
 // D[i][j+1]; the lane above forms the lane's first-row I and diagonal sum from its bottom row (mm,
@@ -8,7 +10,7 @@
 // operations on the same operands as phmm_device.cuh `cells` (M * mx, formed once, is also M * my
 // since mx == my), each result flushed below 2^-1022 unless the warp's vote has shown that no result
 // of the step can fall there: the same results bit for bit, with 2 K + 3 doubles of lane state
-// instead of 4 K + 3, two shuffles instead of three, and 7 operations per cell instead of 8.
+// instead of 4 K + 3, two shuffles instead of three, and (PM_EQ) 7 operations per cell instead of 8.
 #pragma once
 
 #include "phmm_device.cuh"
@@ -75,6 +77,70 @@ __device__ __forceinline__ bool load_rows_eq(LaneRowsEq<K>& L, double* tab, cons
     return exotic;
 }
 
+// The same lane state with per-row gap parameters (PM_ROW: the FP64 classes of modes 1 and 2): each
+// row's mm, gapm, mx and my, and those of the row below the lane (whose first-row I and diagonal sum
+// this lane forms).
+template <int K>
+struct LaneRowsRow {
+    double S[K];
+    double Dn[K];
+    double In, Sn;
+    double Mb, Ib;
+    double xx[K], mm[K], gm[K], mx[K], my[K];
+    double xxn, mmn, gmn, mxn;      // the row below the lane (xx 1 and the rest 0 for a pad row)
+    uint32_t padmask;
+};
+
+template <int K, int V>
+__device__ __forceinline__ bool load_rows_row(LaneRowsRow<K>& L, double* tab, const BatchView& b,
+                                              const ProbTables<double>& tb, uint64_t roff, int R, int first_padded_row,
+                                              int pad, int lane)
+{
+    bool exotic = false;
+    L.padmask = 0;
+    L.In = L.Sn = L.Mb = L.Ib = 0.0;
+    // gap parameters of read row i (a pad row: xx 1, the others 0)
+    auto params = [&](int i, double& xx, double& mm, double& gm, double& mx, double& my) {
+        if (i >= 0 && i < R) {
+            const uint64_t o = roff + (uint64_t)i;
+            const int iq = b.read_i[o] & 127, dq = b.read_d[o] & 127, c = b.read_c[o] & 127;
+            xx = tb.ph2pr[c];
+            mm = tb.mm[iq * 128 + dq];
+            gm = tb.gapm[c];
+            mx = tb.ph2pr[iq];
+            my = tb.ph2pr[dq];
+        } else {
+            xx = 1.0;
+            mm = gm = mx = my = 0.0;
+        }
+    };
+    double myn;
+    params(first_padded_row + lane * K + K - pad, L.xxn, L.mmn, L.gmn, L.mxn, myn);
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        L.S[k] = L.Dn[k] = 0.0;
+        const int i = first_padded_row + lane * K + k - pad;  // 0-based read position
+        params(i, L.xx[k], L.mm[k], L.gm[k], L.mx[k], L.my[k]);
+        double pa = 0.0, pb = 0.0;  // pad rows: prior 0 for every class
+        uint32_t rc = 0u;
+        if (i >= 0 && i < R) {
+            const uint64_t o = roff + (uint64_t)i;
+            const int q = b.read_q[o] & 127;
+            pa = tb.pmat[q];
+            pb = (V == kInter) ? tb.pmis_inter[q] : tb.pmis_intra[q];
+            const uint8_t base = b.read_bases[o];
+            rc = match_code(base, V);
+            if (V == kInter) exotic |= base_class(base) == 4u;
+        } else {
+            L.padmask |= 1u << k;
+        }
+#pragma unroll
+        for (int c = 0; c < kTabClasses; ++c)
+            tab[prior_slot<K>((uint32_t)c, k, lane)] = class_matches((uint32_t)c, rc, V) ? pa : pb;
+    }
+    return exotic;
+}
+
 template <int V, bool FLUSH>
 __device__ __forceinline__ double diag_eq(double gm, double mm, double dgM, double dgI, double dgD)
 {
@@ -113,6 +179,47 @@ __device__ __forceinline__ void cells_eq(LaneRowsEq<K>& L, const double (&pr)[K]
     L.S[0] = upS;
 }
 
+// The same step with per-row gap parameters (8 operations per cell: M * mx of the row below and
+// M * my of the row differ).
+template <int K, int V, bool FLUSH>
+__device__ __forceinline__ void cells_eq(LaneRowsRow<K>& L, const double (&pr)[K], double upI, double upS)
+{
+    auto fz = [](double x) { return FLUSH ? ftz(x) : x; };
+    double Mab = 0.0, Iab = upI;  // the row above, this column
+    double nM = fz(rmul(L.S[0], pr[0]));
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        const double M = nM;
+        if (k + 1 < K) nM = fz(rmul(L.S[k + 1], pr[k + 1]));
+        const double I = k == 0 ? upI : fz(rfma(Iab, L.xx[k], fz(rmul(Mab, L.mx[k]))));
+        const double D = L.Dn[k];
+        L.Dn[k] = fz(rfma(D, L.xx[k], fz(rmul(M, L.my[k]))));
+        if (k + 1 < K) {
+            L.S[k + 1] = diag_eq<V, FLUSH>(L.gm[k + 1], L.mm[k + 1], M, I, D);
+        } else {
+            L.Mb = M;
+            L.Ib = I;
+            L.Sn = diag_eq<V, FLUSH>(L.gmn, L.mmn, M, I, D);
+            L.In = fz(rfma(I, L.xxn, fz(rmul(M, L.mxn))));
+        }
+        Mab = M;
+        Iab = I;
+    }
+    L.S[0] = upS;
+}
+
+// A row's diagonal sum from (M, I, D) of the row above (flushed), with that row's gap parameters.
+template <int V, int K>
+__device__ __forceinline__ double row_diag(const LaneRowsEq<K>& L, int, double dgM, double dgI, double dgD)
+{
+    return diag_eq<V, true>(L.gm, L.mm, dgM, dgI, dgD);
+}
+template <int V, int K>
+__device__ __forceinline__ double row_diag(const LaneRowsRow<K>& L, int k, double dgM, double dgI, double dgD)
+{
+    return diag_eq<V, true>(L.gm[k], L.mm[k], dgM, dgI, dgD);
+}
+
 // Whether every nonzero input of the lane's next PHMM_F64_VOTE_EVERY steps reaches
 // flush_free_hi<K>(): its rows' pending sums and next-column D, and the two values it hands the lane
 // below (that lane's first-row inputs).  The longest product chain of a step is still K + 1 factors
@@ -120,8 +227,8 @@ __device__ __forceinline__ void cells_eq(LaneRowsEq<K>& L, const double (&pr)[K]
 // rows_flush_free holds.
 // The minimum is taken as a tree (depth log2(2 K + 2) instead of a chain of 2 K + 2 dependent
 // operations): the next step's arithmetic waits on this vote.
-template <int K>
-__device__ __forceinline__ bool rows_flush_free_eq(const LaneRowsEq<K>& L)
+template <int K, typename LR>
+__device__ __forceinline__ bool rows_flush_free_eq(const LR& L)
 {
     constexpr int N = 2 * K + 2;
     uint32_t v[N];
@@ -141,9 +248,9 @@ __device__ __forceinline__ bool rows_flush_free_eq(const LaneRowsEq<K>& L)
 }
 
 // Sweep one stripe over the column stream of haplotypes [g_lo, g_hi): as `sweep` (phmm_device.cuh),
-// the scratch row holding the handed-on (I, sum) pair per column.
-template <int K, int V, bool FROM_SCR, bool TO_SCR>
-__device__ void sweep_eq(LaneRowsEq<K>& L, const double* tab, const BatchView& b, const ProbTables<double>& tb,
+// the scratch row holding the handed-on (I, sum) pair per column.  LR: LaneRowsEq or LaneRowsRow.
+template <int K, int V, bool FROM_SCR, bool TO_SCR, typename LR>
+__device__ void sweep_eq(LR& L, const double* tab, const BatchView& b, const ProbTables<double>& tb,
                          const SweepOut& so, uint32_t g_lo, uint32_t g_hi, double* scr, int lane, bool above_row0,
                          bool exotic, uint64_t roff, int R, int row0)
 {
@@ -181,12 +288,12 @@ __device__ void sweep_eq(LaneRowsEq<K>& L, const double* tab, const BatchView& b
             // and C/H in pad rows (which stand for the boundary row, as does the row above the lane's
             // first row when above_row0).  The first column starts from the diagonal sums of column 0
             // and from D[i][1] = fma(D[i][0], xx, 0 * my): C/H in pad rows (xx = 1), else 0.
-            Stop = diag_eq<V, true>(L.gm, L.mm, 0.0, 0.0, D0);
+            Stop = row_diag<V, K>(L, 0, 0.0, 0.0, D0);
             double Dab = above_row0 ? D0 : 0.0;
 #pragma unroll
             for (int k = 0; k < K; ++k) {
                 const double Dc = ((L.padmask >> k) & 1u) ? D0 : 0.0;
-                L.S[k] = diag_eq<V, true>(L.gm, L.mm, 0.0, 0.0, Dab);
+                L.S[k] = row_diag<V, K>(L, k, 0.0, 0.0, Dab);
                 L.Dn[k] = Dc;
                 Dab = Dc;
             }
@@ -242,7 +349,7 @@ __device__ void sweep_eq(LaneRowsEq<K>& L, const double* tab, const BatchView& b
         }
         if constexpr (kVote)
             if (PHMM_F64_VOTE_EVERY == 1 || t % PHMM_F64_VOTE_EVERY == PHMM_F64_VOTE_EVERY - 1)
-                flush_free = __all_sync(0xffffffffu, rows_flush_free_eq(L));
+                flush_free = __all_sync(0xffffffffu, rows_flush_free_eq<K>(L));
     };
 
     for (int t0 = 0; t0 < steps; t0 += kChunkScalar) {

@@ -4,6 +4,8 @@
 // tests/native/warp_emu.cpp runs it on 32 threads standing for the lanes.
 #pragma once
 
+#include <type_traits>
+
 #include "phmm_device.cuh"
 #include "phmm_device64.cuh"
 
@@ -25,15 +27,21 @@ __device__ __forceinline__ void run_read(const BatchView& b, const ProbTables<T>
         if (lane == 0) atomicOr(pc.status, kStatusBadItem);
         return;
     }
-    if constexpr (PM == PM_EQ) {
-        // constant gaps with insertion = deletion: the two-value lane state (phmm_device64.cuh)
-        static_assert(sizeof(T) == 8 && !UNF, "PM_EQ is the FP64 recompute of mode 0");
-        LaneRowsEq<K> L;
+    if constexpr (PM == PM_EQ || (PM == PM_ROW && !UNF)) {
+        // the recompute pass: the two-value lane state (phmm_device64.cuh), one value per read for
+        // constant gaps with insertion = deletion, per row otherwise
+        static_assert(sizeof(T) == 8 && !UNF, "the two-value lane state is the FP64 recompute");
+        using LR = typename std::conditional<PM == PM_EQ, LaneRowsEq<K>, LaneRowsRow<K>>::type;
+        LR L;
         constexpr int SR = kWarp * K;  // rows per stripe
         const int stripes = MULTI ? (R + SR - 1) / SR : 1;
         const int pad = SR * stripes - R;
         for (int s = 0; s < stripes; ++s) {
-            const bool exotic = load_rows_eq<K, V>(L, tab, b, tb, roff, R, s * SR, pad, lane);
+            bool exotic;
+            if constexpr (PM == PM_EQ)
+                exotic = load_rows_eq<K, V>(L, tab, b, tb, roff, R, s * SR, pad, lane);
+            else
+                exotic = load_rows_row<K, V>(L, tab, b, tb, roff, R, s * SR, pad, lane);
             const bool above_row0 = (s == 0) && (lane * K <= pad);
             const int row0 = s * SR - pad;  // read position of slot 0 of lane 0
             if (!MULTI)

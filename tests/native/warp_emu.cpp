@@ -109,7 +109,7 @@ void f64_mode(int shape, const BatchView& b, const ProbTables<double>& t, const 
 int main(int argc, char** argv)
 {
     if (argc < 5) {
-        std::fprintf(stderr, "usage: warp_emu IN OUT engine|check64|eq64 default|multi<KH>\n");
+        std::fprintf(stderr, "usage: warp_emu IN OUT engine|check64|eq64|row64 default|multi<KH>\n");
         return 2;
     }
     const std::string mode = argv[3], tiles_arg = argv[4];
@@ -218,15 +218,16 @@ int main(int argc, char** argv)
             else if (m == 1) f64_mode<kInter, PM_ROW, false>(s, v, td, pc);
             else f64_mode<kIntra, PM_ROW, false>(s, v, td, pc);
         }
-    } else if (mode == "check64" || mode == "eq64") {
+    } else if (mode == "check64" || mode == "eq64" || mode == "row64") {
         // every pair: per work item and read, the item's haplotype run, in the FP64 class of the
         // read's length (modes 1 and 2), as Engine::check_fp64 lays them out.  eq64: every pair of the
         // FP32 classes of mode 0 through the FP64 recompute classes of mode 0 instead (the
         // reference's FP64 kernel for each of them, not only for the underflowed ones)
-        const bool eq = mode == "eq64";
+        const bool eq = mode == "eq64", row = mode == "row64";
         std::vector<std::vector<RerunEntry>> per(kClasses64);
         for (const WorkItem& it : plan.items) {
             if (eq && mode32(it.variant, it.pmode) != 0) continue;
+            if (row && mode32(it.variant, it.pmode) == 0) continue;
             const RegionDesc& rg = plan.regions[it.region];
             for (int k = 0; k < 2; ++k) {
                 const uint32_t r = it.read[k];
@@ -255,9 +256,12 @@ int main(int argc, char** argv)
             if (!classes[kClasses32 + c].rerun_count) continue;
             pc.cd = classes.data() + kClasses32 + c;
             const int s = c % 9;
+            const bool unf = !row;  // check64: the all-FP64 check arithmetic
             if (eq) f64_mode<kInter, PM_EQ, false>(s, v, td, pc);
-            else if (c / 9 == 1) f64_mode<kInter, PM_ROW, true>(s, v, td, pc);
-            else f64_mode<kIntra, PM_ROW, true>(s, v, td, pc);
+            else if (c / 9 == 1 && unf) f64_mode<kInter, PM_ROW, true>(s, v, td, pc);
+            else if (c / 9 == 1) f64_mode<kInter, PM_ROW, false>(s, v, td, pc);
+            else if (unf) f64_mode<kIntra, PM_ROW, true>(s, v, td, pc);
+            else f64_mode<kIntra, PM_ROW, false>(s, v, td, pc);
         }
     } else {
         return 2;

@@ -137,3 +137,38 @@ def test_emulated_fp64_recompute_of_mode0_equals_the_oracle(emulator, oracle, tm
     # reads up to 500 bases end far below the FP32 range (-500 log10) but within FP64's; the 768-base
     # read underflows FP64 as well (-inf on both sides), through the flushes
     assert np.isfinite(want[:, :-1]).all() and (want[:, :-1] < -300).any() and np.isinf(want[:, -1]).all()
+
+
+def test_emulated_fp64_recompute_of_per_row_modes_equals_the_oracle(emulator, oracle, tmp_path):
+    """Every pair of the FP32 classes of modes 1 (per-row or unequal gap qualities) and 2 (intra)
+    through the FP64 recompute classes of those modes (the two-value lane state with per-row gap
+    parameters), not only the underflowed ones: each equals the reference's FP64 kernel of its
+    variant on that pair."""
+    pb = _batch(14)
+    got, _, status = _run(emulator, pb, tmp_path, mode="row64")
+    assert status == 0
+    sizes = pb.n_haps.astype(np.int64) * pb.n_reads.astype(np.int64)
+    offs = np.concatenate([[0], np.cumsum(sizes)])
+    h0 = np.concatenate([[0], np.cumsum(pb.n_haps)])
+    r0 = np.concatenate([[0], np.cumsum(pb.n_reads)])
+    checked = 0
+    for g in (1, 2, 3):  # per-row, unequal, N (its intra pairs)
+        n_h, n_r = int(pb.n_haps[g]), int(pb.n_reads[g])
+        blk = got[offs[g]:offs[g + 1]].reshape(n_h, n_r)
+        for h in range(n_h):
+            hh = int(h0[g]) + h
+            hap = bytes(pb.hap_bases[pb.hap_off[hh]:pb.hap_off[hh + 1]])
+            for r in range(n_r):
+                rr = int(r0[g]) + r
+                s = slice(int(pb.read_off[rr]), int(pb.read_off[rr + 1]))
+                read = bytes(pb.read_bases[s])
+                intra = b"N" in hap or b"N" in read
+                if g == 3 and not intra:
+                    continue  # constant equal gaps: mode 0, not run here
+                raw = oracle.raw_f64(hap, read, bytes(pb.read_qual[s]), bytes(pb.read_ins[s]), bytes(pb.read_del[s]),
+                                     bytes(pb.read_gcp[s]), kernel=1 if intra else 0)
+                with np.errstate(divide="ignore"):
+                    want = np.log10(raw) - LOG10_C_F64
+                assert_same_values(np.array([blk[h, r]]), np.array([want]), EXACT, f"region {g} hap {h} read {r}")
+                checked += 1
+    assert checked > 60
