@@ -19,9 +19,10 @@ namespace phmm {
 // time settings (1 leaves the compiler free).  Measured on B200: mode 0 runs the 2,000-region batch
 // 1.5% faster with 16 warps per SM than with 12 for KH >= 4; modes 1 and 2 spill at 128 registers
 // and run a batch of per-row gap qualities and N reads (300 regions) at 2090 GCUPS with 12 warps per
-// SM against 1614 with 16.
+// SM against 1614 with 16.  KH 4 and 5 in mode 0 run 24 warps per SM (80 registers, spills in the
+// boundary code): their classes 1.4% and 0.8% faster than at 16 on the 2,000-region batch.
 #ifndef PHMM_F32_MIN_WARPS
-#define PHMM_F32_MIN_WARPS 0x10101010100c0101ull
+#define PHMM_F32_MIN_WARPS 0x10101018180c0101ull
 #endif
 #ifndef PHMM_F32_MIN_WARPS_OTHER
 #define PHMM_F32_MIN_WARPS_OTHER 0x0c0c0c0c0c0c0101ull
