@@ -1009,10 +1009,15 @@ struct ChunkRange {
 // one cut at 15% 2278 GCUPS, one pipeline 2213; cuts at 10% and 55% 2238 and at 12.5%, 42% and 71%
 // 2237, their extra chunk tails adding 7-8 ms of device time.  With the current kernels: one cut
 // 2713 GCUPS, cuts at 15% and 85% 2682, and either with the serving slots' overlap scheduling on the
-// two chunk slots 2712 and 2717 (within noise).
+// two chunk slots 2712 and 2717 (within noise); later, one cut at 15% 199.3-199.5 ms per batch, at 8%
+// 198.2-199.0, at 5% 197.9-198.4, at 3% 201.6-202.1 (the first chunk then ends before the second is
+// planned and uploaded) and at 22% 199.8.  The default (build-time setting) is 8%.
 std::vector<ChunkRange> split_chunks(const phmm_batch& b, uint64_t total_cells)
 {
-    static const double kEnds[] = {0.15};
+#ifndef PHMM_CHUNK_FIRST
+#define PHMM_CHUNK_FIRST 0.08
+#endif
+    static const double kEnds[] = {PHMM_CHUNK_FIRST};
     constexpr int kCuts = (int)(sizeof(kEnds) / sizeof(kEnds[0]));
     std::vector<ChunkRange> ch;
     ChunkRange cur{0, 0, 0, 0, 0};
